@@ -1,0 +1,195 @@
+"""Test infrastructure: ctypes wrappers over the CPU oracle (``oracle/_build/liboracle.so``).
+
+The oracle is the checker for the CUDA path, never the product: only ``tests/``,
+``__graft_entry__.smoke()`` and the ``cpu_baseline`` leg of ``bench.py`` import this
+module. Each wrapped function names the reference source it restates in the C++ file.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_f32p = ctypes.POINTER(ctypes.c_float)
+
+
+def build():
+    """Compile the oracle (make in oracle/)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _lib.oracle_morton32.restype = ctypes.c_uint32
+        _lib.oracle_morton32.argtypes = [ctypes.c_float] * 3
+        _lib.oracle_morton64.restype = ctypes.c_uint64
+        _lib.oracle_morton64.argtypes = [ctypes.c_float] * 3 + [ctypes.c_uint32]
+        _lib.oracle_lbvh_build.restype = ctypes.c_int
+        _lib.oracle_lbvh_query.restype = ctypes.c_uint64
+        _lib.oracle_ef_narrow.restype = ctypes.c_uint32
+        _lib.oracle_find_split.restype = ctypes.c_int
+        _lib.oracle_threads_used.restype = ctypes.c_int
+    return _lib
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+def _pn(a, t):
+    return None if a is None else _p(a, t)
+
+
+TREE_VERT, TREE_FACE, TREE_EDGE = 0, 1, 2
+
+
+def threads():
+    return lib().oracle_threads_used()
+
+
+def morton32(p):
+    return lib().oracle_morton32(*[ctypes.c_float(v) for v in p])
+
+
+def morton64(p, idx):
+    return lib().oracle_morton64(*[ctypes.c_float(v) for v in p], ctypes.c_uint32(idx))
+
+
+def determine_range(keys, i):
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    out = np.zeros(2, np.int32)
+    lib().oracle_determine_range(_p(keys, _u64p), ctypes.c_uint32(len(keys)), ctypes.c_uint32(i), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return int(out[0]), int(out[1])
+
+
+def find_split(keys, i, j):
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    return lib().oracle_find_split(_p(keys, _u64p), ctypes.c_int(i), ctypes.c_int(j))
+
+
+def karras(keys_sorted):
+    keys_sorted = np.ascontiguousarray(keys_sorted, dtype=np.uint64)
+    n = len(keys_sorted)
+    parent = np.full(2 * n - 1, 0xFFFFFFFF, np.uint32)
+    children = np.zeros((2 * n - 1, 2), np.uint32)
+    lib().oracle_lbvh_karras(_p(keys_sorted, _u64p), ctypes.c_uint32(n), _p(parent, _u32p), _p(children, _u32p))
+    return parent, children
+
+
+class OracleTree:
+    """Arrays of one built tree (lbvh.h:77-150 layout, node AABBs as float[8])."""
+
+    def __init__(self, tree_type, n):
+        self.tree_type = tree_type
+        self.n = n
+        nn = max(2 * n - 1, 1)
+        self.gaabb = np.zeros(6, np.float32)
+        self.keys_sorted = np.zeros(max(n, 1), np.uint64)
+        self.sorted_get_original = np.zeros(max(n, 1), np.uint32)
+        self.parent = np.full(nn, 0xFFFFFFFF, np.uint32)
+        self.children = np.zeros((nn, 2), np.uint32)
+        self.object_idx = np.full(nn, 0xFFFFFFFF, np.uint32)
+        self.node_aabb = np.zeros((nn, 8), np.float32)
+        self.unhealthy = 0
+
+
+def lbvh_build(tree_type, x, prims, num_verts=None):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    nv = x.shape[0] if num_verts is None else num_verts
+    if tree_type == TREE_VERT:
+        n = nv
+        prims_p = None
+    else:
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        n = prims.shape[0]
+        prims_p = _p(prims, _u32p)
+    t = OracleTree(tree_type, n)
+    t.unhealthy = lib().oracle_lbvh_build(
+        ctypes.c_int(tree_type), _p(x, _f32p), ctypes.c_uint32(nv), prims_p, ctypes.c_uint32(n),
+        _p(t.gaabb, _f32p), _p(t.keys_sorted, _u64p), _p(t.sorted_get_original, _u32p),
+        _p(t.parent, _u32p), _p(t.children, _u32p), _p(t.object_idx, _u32p))
+    return t
+
+
+def lbvh_refit(tree, x0, x1, thickness, prims):
+    x0 = np.ascontiguousarray(x0, dtype=np.float32)
+    x1 = np.ascontiguousarray(x1, dtype=np.float32)
+    thickness = np.ascontiguousarray(thickness, dtype=np.float32)
+    prims_p = None if prims is None else _p(np.ascontiguousarray(prims, dtype=np.uint32), _u32p)
+    if prims is not None:
+        prims = np.ascontiguousarray(prims, dtype=np.uint32)
+        prims_p = _p(prims, _u32p)
+    lib().oracle_lbvh_refit(
+        ctypes.c_int(tree.tree_type), ctypes.c_uint32(tree.n), _p(x0, _f32p), _p(x1, _f32p), _p(thickness, _f32p),
+        prims_p, _p(tree.sorted_get_original, _u32p), _p(tree.children, _u32p), _p(tree.node_aabb, _f32p))
+    return tree.node_aabb
+
+
+QUERY_VERTS, QUERY_EDGES, QUERY_EDGES_UNCULLED = 0, 1, 2
+
+
+def lbvh_query(tree, mode, x0, x1, edges, d_hat, thickness, max_pairs=None):
+    """Broad phase (lbvh.cpp:295-363, 780-894). Returns (pairs[k,2], total, overflow)."""
+    x0 = np.ascontiguousarray(x0, dtype=np.float32)
+    x1 = np.ascontiguousarray(x1, dtype=np.float32)
+    d_hat = np.ascontiguousarray(d_hat, dtype=np.float32)
+    thickness = np.ascontiguousarray(thickness, dtype=np.float32)
+    if mode == QUERY_VERTS:
+        nq = x0.shape[0]
+        edges_p = None
+    else:
+        edges = np.ascontiguousarray(edges, dtype=np.uint32)
+        nq = edges.shape[0]
+        edges_p = _p(edges, _u32p)
+    if max_pairs is None:
+        max_pairs = 1 << 20
+    while True:
+        pairs = np.zeros((max(max_pairs, 1), 2), np.uint32)
+        overflow = np.zeros(1, np.uint32)
+        total = lib().oracle_lbvh_query(
+            ctypes.c_int(mode), ctypes.c_uint32(nq), _p(x0, _f32p), _p(x1, _f32p), edges_p,
+            _p(d_hat, _f32p), _p(thickness, _f32p), ctypes.c_uint32(tree.n), _p(tree.children, _u32p),
+            _p(tree.object_idx, _u32p), _p(tree.node_aabb, _f32p), _p(pairs, _u32p), ctypes.c_uint64(max_pairs),
+            _p(overflow, _u32p))
+        if total <= max_pairs:
+            return pairs[:total], int(total), int(overflow[0])
+        max_pairs = int(total)
+
+
+EF_PAIR_DTYPE = np.dtype([("idx", np.uint32, 5), ("bary", np.float32, 3), ("grad", np.float32, 3), ("stiff", np.float32)])
+assert EF_PAIR_DTYPE.itemsize == 48
+
+
+def ef_narrow(broad_pairs, x, edges, faces, d_hat, vprop=None):
+    """EF narrow phase (intersection_resolver.cpp:86-197), canonical order."""
+    broad_pairs = np.ascontiguousarray(broad_pairs, dtype=np.uint32).reshape(-1, 2)
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    edges = np.ascontiguousarray(edges, dtype=np.uint32)
+    faces = np.ascontiguousarray(faces, dtype=np.uint32)
+    d_hat = np.ascontiguousarray(d_hat, dtype=np.float32)
+    vp = None if vprop is None else np.ascontiguousarray(vprop, dtype=np.uint32)
+    nb = broad_pairs.shape[0]
+    out = np.zeros(max(nb, 1), EF_PAIR_DTYPE)
+    idx = np.zeros((max(nb, 1), 2), np.uint32)
+    cnt = lib().oracle_ef_narrow(
+        _p(broad_pairs, _u32p), ctypes.c_uint32(nb), _p(x, _f32p), _p(edges, _u32p), _p(faces, _u32p),
+        _pn(vp, _u32p), _p(d_hat, _f32p), out.ctypes.data_as(ctypes.c_void_p), _p(idx, _u32p), ctypes.c_uint32(nb))
+    return out[:cnt], idx[:cnt]
+
+
+def line_intersection(p0, p1, a, b, c):
+    arrs = [np.ascontiguousarray(v, dtype=np.float32) for v in (p0, p1, a, b, c)]
+    bary = np.zeros(3, np.float32)
+    t = ctypes.c_float(0)
+    hit = lib().oracle_line_intersection(*[_p(v, _f32p) for v in arrs], _p(bary, _f32p), ctypes.byref(t))
+    return bool(hit), bary, t.value

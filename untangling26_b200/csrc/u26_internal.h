@@ -1,0 +1,104 @@
+// Host-side internals of libu26: the context object, grow-only device buffers and
+// error plumbing shared by the .cu translation units.
+#pragma once
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "u26_common.cuh"
+
+struct u26_ctx
+{
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	std::string last_error;
+	uint64_t launches = 0;
+	// device word the kernels OR error flags into (U26_DEVERR_*)
+	uint32_t* dev_err = nullptr;
+	// pinned host staging word for small readbacks
+	uint32_t* host_word = nullptr;
+};
+
+namespace u26
+{
+	// Grow-only device allocation owned by a context-side object.
+	struct DevBuf
+	{
+		void* ptr = nullptr;
+		size_t bytes = 0;
+		cudaError_t reserve(size_t want)
+		{
+			if (want <= bytes)
+				return cudaSuccess;
+			if (ptr)
+				cudaFree(ptr);
+			ptr = nullptr;
+			bytes = 0;
+			cudaError_t e = cudaMalloc(&ptr, want);
+			if (e == cudaSuccess)
+				bytes = want;
+			return e;
+		}
+		void release()
+		{
+			if (ptr)
+				cudaFree(ptr);
+			ptr = nullptr;
+			bytes = 0;
+		}
+		template <typename T>
+		T* as() const { return static_cast<T*>(ptr); }
+	};
+
+	inline u26_status set_error(u26_ctx* ctx, u26_status st, const char* fmt, ...)
+	{
+		char buf[512];
+		va_list ap;
+		va_start(ap, fmt);
+		vsnprintf(buf, sizeof(buf), fmt, ap);
+		va_end(ap);
+		if (ctx)
+			ctx->last_error = buf;
+		return st;
+	}
+
+	inline u26_status cuda_status(u26_ctx* ctx, cudaError_t e, const char* what)
+	{
+		if (e == cudaSuccess)
+			return U26_OK;
+		return set_error(ctx, U26_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+	}
+
+	// Check the last launch; counts it.
+	inline u26_status after_launch(u26_ctx* ctx, const char* what)
+	{
+		ctx->launches++;
+		return cuda_status(ctx, cudaGetLastError(), what);
+	}
+
+	// Radix sort of (key64, value32) pairs over bits [bit_lo, bit_hi), stable.
+	// keys/vals are sorted in place (ping-pong through internal scratch).
+	struct RadixSorter
+	{
+		DevBuf keys_alt, vals_alt, counts;
+		u26_status sort(u26_ctx* ctx, uint64_t* keys, uint32_t* vals, uint32_t n, int bit_lo, int bit_hi);
+		void release()
+		{
+			keys_alt.release();
+			vals_alt.release();
+			counts.release();
+		}
+	};
+} // namespace u26
+
+#define U26_TRY(expr)                   \
+	do                                  \
+	{                                   \
+		u26_status _st = (expr);        \
+		if (_st != U26_OK)              \
+			return _st;                 \
+	}                                   \
+	while (0)
+
+#define U26_CUDA(ctx, call) U26_TRY(::u26::cuda_status((ctx), (call), #call))

@@ -1,0 +1,129 @@
+"""Collision detection stages of the untangling hot path behind the reference's interfaces.
+
+* ``IntersectionResolver.ef_dcd_intersection_query`` mirrors
+  IntersectionResolver::ef_dcd_intersection_query (intersection_resolver.h:41-52,
+  intersection_resolver.cpp:365-423): EF narrow phase over a broad-phase list.
+* ``CollisionScene`` owns the face/edge LBVHs and the per-vertex buffers of one mesh and
+  exposes the solver's call sites (NewtonSolver::device_construct_lbvh,
+  device_broadphase_dcd, device_narrowphase_dcd; newton_solver.cpp:1218-1380) for the
+  EF path, plus the fused detection form.
+
+EF pairs come back as a structured numpy array with the reference's 48-byte EfPair
+layout (collision_data.h:150-220) and (eid, fid) indices, in canonical (eid, fid) order.
+"""
+import numpy as np
+import torch
+
+from . import _native as nat
+from ._native import ptr
+from .lbvh import LBVH, TREE_EDGE, TREE_FACE
+
+EF_PAIR_DTYPE = np.dtype([("idx", np.uint32, 5), ("bary", np.float32, 3), ("grad", np.float32, 3), ("stiff", np.float32)])
+
+
+def _u32(t):
+    return t.view(torch.int32) if t.dtype != torch.int32 else t
+
+
+class IntersectionResolver:
+    def __init__(self, ctx, max_ef_pairs):
+        self.ctx = ctx
+        self.max_ef = int(max_ef_pairs)
+        dev = torch.device("cuda", ctx.device)
+        self.ef_count = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.ef_list = torch.zeros((self.max_ef, 12), dtype=torch.int32, device=dev)  # 48 B rows
+        self.ef_indices = torch.zeros((self.max_ef, 2), dtype=torch.int32, device=dev)
+
+    def reset(self):
+        self.ef_count.zero_()
+
+    def ef_dcd_intersection_query(self, broad_pairs, broad_count, x, edges, faces, vert_property, d_hat):
+        """Narrow phase over the broad-phase (eid, fid) list (count read on the device)."""
+        max_broad = broad_pairs.numel() // 2
+        self.ctx.check(self.ctx.lib.u26_ef_narrow_phase(
+            self.ctx.handle, ptr(broad_pairs), ptr(broad_count), max_broad, ptr(x), ptr(edges), ptr(faces),
+            ptr(vert_property), ptr(d_hat), ptr(self.ef_count), ptr(self.ef_list), ptr(self.ef_indices), self.max_ef),
+            "ef_narrow_phase")
+
+    def canonicalize(self, num_edges, num_faces):
+        """Sort the EF list by (eid, fid) on the device (synchronises for the count)."""
+        n = int(self.ef_count.item())
+        if n > self.max_ef:
+            raise nat.U26Error(1, f"EF list overflow: {n} pairs > capacity {self.max_ef}")
+        self.ctx.check(self.ctx.lib.u26_ef_canonicalize(self.ctx.handle, n, ptr(self.ef_list), ptr(self.ef_indices),
+                                                        num_edges, num_faces), "ef_canonicalize")
+        return n
+
+    def download(self, n):
+        pairs = self.ef_list[:n].cpu().numpy().view(EF_PAIR_DTYPE).reshape(-1)
+        idx = self.ef_indices[:n].cpu().numpy().view(np.uint32)
+        return pairs.copy(), idx.copy()
+
+
+class CollisionScene:
+    """Device-resident mesh + face/edge trees for the EF detection path of one scene."""
+
+    def __init__(self, ctx, mesh, d_hat=1e-3, thickness=0.0, max_broad_pairs=None, max_ef_pairs=None):
+        self.ctx = ctx
+        self.mesh = mesh
+        dev = torch.device("cuda", ctx.device)
+        self.dev = dev
+        self.x = torch.from_numpy(mesh.x).to(dev)
+        self.edges = torch.from_numpy(mesh.edges.view(np.int32)).to(dev)
+        self.faces = torch.from_numpy(mesh.faces.view(np.int32)).to(dev)
+        self.vert_property = torch.from_numpy(mesh.vert_property.view(np.int32)).to(dev)
+        nv = mesh.num_verts
+        self.d_hat = torch.full((nv,), float(d_hat), dtype=torch.float32, device=dev)
+        self.thickness = torch.full((nv,), float(thickness), dtype=torch.float32, device=dev)
+        self.face_tree = LBVH(ctx, TREE_FACE, mesh.num_faces)
+        self.edge_tree = LBVH(ctx, TREE_EDGE, mesh.num_edges)
+        self.max_broad = int(max_broad_pairs or max(1 << 16, 8 * mesh.num_edges))
+        self.broad_count = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.broad_pairs = torch.zeros((self.max_broad, 2), dtype=torch.int32, device=dev)
+        self.resolver = IntersectionResolver(ctx, max_ef_pairs or max(1 << 14, mesh.num_edges))
+        self.stats = torch.zeros(4, dtype=torch.int64, device=dev)
+
+    def set_positions(self, x):
+        self.x.copy_(torch.as_tensor(x, dtype=torch.float32).reshape(-1, 3))
+
+    # NewtonSolver::device_construct_lbvh (newton_solver.cpp:1218-1224)
+    def construct_lbvh(self, x_step_start=None):
+        xs = self.x if x_step_start is None else x_step_start
+        self.face_tree.reduce_face_tree_aabb(xs, self.faces)
+        self.edge_tree.reduce_edge_tree_aabb(xs, self.edges)
+        self.face_tree.construct_tree()
+        self.edge_tree.construct_tree()
+
+    # NewtonSolver::device_broadphase_dcd, EF part (newton_solver.cpp:1260-1299)
+    def broadphase_dcd_ef(self, fused_refit=True):
+        if fused_refit:
+            self.face_tree.update_and_refit(self.thickness, self.x, self.x, self.faces)
+        else:
+            self.face_tree.update_face_tree_leave_aabb(self.thickness, self.x, self.x, self.faces)
+            self.face_tree.refit()
+        self.broad_count.zero_()
+        self.face_tree.broad_phase_query_from_edges_unculled(self.x, self.x, self.edges, self.broad_count, self.broad_pairs,
+                                                             self.d_hat, self.thickness)
+
+    # NewtonSolver::device_narrowphase_dcd, EF part (newton_solver.cpp:1340-1380)
+    def narrowphase_dcd_ef(self):
+        self.resolver.reset()
+        self.resolver.ef_dcd_intersection_query(self.broad_pairs, self.broad_count, self.x, self.edges, self.faces,
+                                                self.vert_property, self.d_hat)
+
+    def detect_ef_fused(self, with_stats=False):
+        """Refit + fused broad/narrow EF detection (no broad-phase list)."""
+        self.face_tree.update_and_refit(self.thickness, self.x, self.x, self.faces)
+        self.resolver.reset()
+        if with_stats:
+            self.stats.zero_()
+        self.ctx.check(self.ctx.lib.u26_ef_detect(
+            self.face_tree.handle, ptr(self.x), ptr(self.edges), self.mesh.num_edges, ptr(self.faces),
+            ptr(self.vert_property), ptr(self.d_hat), ptr(self.thickness), ptr(self.resolver.ef_count),
+            ptr(self.resolver.ef_list), ptr(self.resolver.ef_indices), self.resolver.max_ef,
+            ptr(self.stats) if with_stats else None), "ef_detect")
+
+    def ef_pairs(self):
+        """Canonical EF pairs (numpy) of the last detection."""
+        n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
+        return self.resolver.download(n)
