@@ -113,10 +113,17 @@ class CollisionScene:
 
     def detect_ef_fused(self, with_stats=False):
         """Refit + fused broad/narrow EF detection (no broad-phase list)."""
-        self.face_tree.update_and_refit(self.thickness, self.x, self.x, self.faces)
+        self.refit_face_tree()
         self.resolver.reset()
         if with_stats:
             self.stats.zero_()
+        self.ef_detect(with_stats)
+
+    def refit_face_tree(self):
+        self.face_tree.update_and_refit(self.thickness, self.x, self.x, self.faces)
+
+    def ef_detect(self, with_stats=False):
+        """The fused EF kernel alone (face tree already refit, counter already reset)."""
         self.ctx.check(self.ctx.lib.u26_ef_detect(
             self.face_tree.handle, ptr(self.x), ptr(self.edges), self.mesh.num_edges, ptr(self.faces),
             ptr(self.vert_property), ptr(self.d_hat), ptr(self.thickness), ptr(self.resolver.ef_count),
