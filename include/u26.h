@@ -104,6 +104,13 @@ U26_API u26_status u26_lbvh_query(u26_lbvh* tree, int mode, const float* x_begin
 	const uint32_t* edges, uint32_t num_queries, const float* d_hat, const float* thickness, uint32_t* count,
 	uint32_t* pairs, uint32_t max_pairs);
 /* LBVH::check_health (lbvh.cpp:1081-1085). Synchronises. *healthy = 1 or 0. */
+/* Tree options (no reference counterpart; defaults reproduce the reference):
+ *   U26_LBVH_OPT_FULL_GLOBAL_AABB = 1: normalise Morton codes by the AABB of ALL leaves
+ *   instead of the reference's first ceil(num_verts/256) blocks (lbvh.cpp:999-1021).
+ *   Query and EF results are unchanged (they do not depend on the topology unless a
+ *   traversal stack overflows); the tree is better balanced in space. */
+#define U26_LBVH_OPT_FULL_GLOBAL_AABB 1
+U26_API u26_status u26_lbvh_set_option(u26_lbvh* tree, int option, int value);
 U26_API u26_status u26_lbvh_check_health(u26_lbvh* tree, int* healthy);
 
 typedef struct u26_lbvh_arrays
@@ -135,10 +142,14 @@ U26_API u26_status u26_ef_narrow_phase(u26_ctx* ctx, const uint32_t* broad_pairs
 /* Fused EF detection: edges of the mesh against a refit face tree, segment-triangle
  * test at each overlapping leaf, no broad-phase list in between. Same EF pair set as
  * u26_lbvh_query(U26_QUERY_EDGES_UNCULLED) + u26_ef_narrow_phase whenever the broad
- * list would not have overflowed. */
+ * list would not have overflowed. edge_order (optional, uint32[num_edges]) is the order
+ * in which threads take the edges, e.g. an edge tree's sorted_get_original so that a
+ * warp walks spatially close edges; NULL means edge id order. stats (optional,
+ * uint64[2]) accumulates node boxes tested and leaf triangles tested. */
 U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint32_t* edges, uint32_t num_edges,
 	const uint32_t* faces, const uint32_t* vert_property, const float* d_hat, const float* thickness,
-	uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices, uint32_t max_ef, uint64_t* stats);
+	const uint32_t* edge_order, uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices, uint32_t max_ef,
+	uint64_t* stats);
 
 /* Canonical EF order on the device: sort by (eid, fid) — the order
  * host_preprocess_ef_pairs establishes (intersection_resolver.cpp:693-726). count is a

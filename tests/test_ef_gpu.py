@@ -22,7 +22,8 @@ def _oracle_ef(oracle, m, d_hat, th):
 
 @pytest.mark.parametrize("scene", ["two_sheets64", "folded128", "folded256"])
 @pytest.mark.parametrize("fused", [False, True])
-def test_ef_pairs_bit_exact(oracle, u26ctx, scene, fused):
+@pytest.mark.parametrize("parity_tree", [True, False])
+def test_ef_pairs_bit_exact(oracle, u26ctx, scene, fused, parity_tree):
     if scene == "two_sheets64":
         m = synthetic.two_sheets(64, seed=0)
     elif scene == "folded128":
@@ -33,7 +34,8 @@ def test_ef_pairs_bit_exact(oracle, u26ctx, scene, fused):
     th = np.zeros(m.num_verts, np.float32)
     ef_ref, idx_ref, total = _oracle_ef(oracle, m, d_hat, th)
     assert len(ef_ref) > 0
-    sc = CollisionScene(u26ctx, m, d_hat=1e-3, thickness=0.0, max_broad_pairs=total + 64, max_ef_pairs=len(ef_ref) + 64)
+    sc = CollisionScene(u26ctx, m, d_hat=1e-3, thickness=0.0, max_broad_pairs=total + 64, max_ef_pairs=len(ef_ref) + 64,
+                        parity_tree=parity_tree)
     sc.construct_lbvh()
     if fused:
         sc.detect_ef_fused()

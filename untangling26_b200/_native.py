@@ -62,7 +62,8 @@ _SIGS = {
     "u26_lbvh_check_health": (c_int, [c_vp, ctypes.POINTER(c_int)]),
     "u26_lbvh_arrays_get": (c_int, [c_vp, ctypes.POINTER(U26LbvhArrays)]),
     "u26_ef_narrow_phase": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32]),
-    "u26_ef_detect": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
+    "u26_ef_detect": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
+    "u26_lbvh_set_option": (c_int, [c_vp, c_int, c_int]),
     "u26_ef_canonicalize": (c_int, [c_vp, c_u32, c_vp, c_vp, c_u32, c_u32]),
 }
 

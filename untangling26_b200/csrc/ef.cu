@@ -157,11 +157,12 @@ namespace u26
 			uint32_t num_edges, const uint32_t* __restrict__ faces, const uint32_t* __restrict__ vprop,
 			const float* __restrict__ d_hat, const float* __restrict__ thickness, uint32_t* __restrict__ ef_count,
 			EfPairDev* __restrict__ out, uint32_t* __restrict__ out_idx, uint32_t max_ef, unsigned long long* __restrict__ stats,
-			uint32_t* __restrict__ dev_err)
+			const uint32_t* __restrict__ edge_order, uint32_t* __restrict__ dev_err)
 		{
-			const uint32_t eid = blockIdx.x * blockDim.x + threadIdx.x;
-			if (eid >= num_edges)
+			const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+			if (tid >= num_edges)
 				return;
+			const uint32_t eid = edge_order ? __ldg(edge_order + tid) : tid;
 			if (*tv.health == 0u)
 				return;
 			const uint2 e = __ldg(edges + eid);
@@ -322,8 +323,8 @@ U26_API u26_status u26_ef_narrow_phase(u26_ctx* ctx, const uint32_t* broad_pairs
 }
 
 U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint32_t* edges, uint32_t num_edges,
-	const uint32_t* faces, const uint32_t* vert_property, const float* d_hat, const float* thickness, uint32_t* ef_count,
-	void* ef_pairs, uint32_t* ef_indices, uint32_t max_ef, uint64_t* stats)
+	const uint32_t* faces, const uint32_t* vert_property, const float* d_hat, const float* thickness, const uint32_t* edge_order,
+	uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices, uint32_t max_ef, uint64_t* stats)
 {
 	if (!face_tree)
 		return U26_ERR_INVALID_INPUT;
@@ -336,7 +337,7 @@ U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint
 		return U26_OK;
 	ef_detect_kernel<<<div_up(num_edges, 128), 128, 0, ctx->stream>>>(tree_view(face_tree), x, reinterpret_cast<const uint2*>(edges),
 		num_edges, faces, vert_property, d_hat, thickness, ef_count, static_cast<EfPairDev*>(ef_pairs), ef_indices, max_ef,
-		reinterpret_cast<unsigned long long*>(stats), ctx->dev_err);
+		reinterpret_cast<unsigned long long*>(stats), edge_order, ctx->dev_err);
 	return after_launch(ctx, "ef_detect_kernel");
 }
 

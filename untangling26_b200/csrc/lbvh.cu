@@ -572,7 +572,7 @@ U26_API u26_status u26_lbvh_reduce_aabb(u26_lbvh* t, const float* x, uint32_t nu
 	u26_ctx* ctx = t->ctx;
 	const uint32_t nb_leaf = div_up(t->n, 256);
 	// lbvh.cpp:999-1021: the edge/face trees reduce ceil(num_verts/256) blocks in the second pass.
-	uint32_t nb = t->type == U26_TREE_VERT ? nb_leaf : std::min(nb_leaf, div_up(num_verts, 256));
+	uint32_t nb = (t->type == U26_TREE_VERT || t->full_global_aabb) ? nb_leaf : std::min(nb_leaf, div_up(num_verts, 256));
 	if (nb == 0)
 		nb = 1;
 	U26_DISPATCH_TYPE(t->type, reduce_blocks_kernel, nb_leaf, 256, ctx->stream, x, prims, t->n, t->block_aabb.as<float>());
@@ -715,4 +715,16 @@ U26_API u26_status u26_lbvh_arrays_get(const u26_lbvh* t, u26_lbvh_arrays* out)
 	out->node_aabb = t->node_aabb.as<float>();
 	out->global_aabb = t->global_aabb.as<float>();
 	return U26_OK;
+}
+
+U26_API u26_status u26_lbvh_set_option(u26_lbvh* t, int option, int value)
+{
+	if (!t)
+		return U26_ERR_INVALID_INPUT;
+	if (option == U26_LBVH_OPT_FULL_GLOBAL_AABB)
+	{
+		t->full_global_aabb = value != 0;
+		return U26_OK;
+	}
+	return set_error(t->ctx, U26_ERR_INVALID_INPUT, "u26_lbvh_set_option: unknown option %d", option);
 }

@@ -23,6 +23,9 @@ struct u26_lbvh
 	// keeps sa_leaf_center from the reduce pass)
 	const float* last_x = nullptr;
 	const uint32_t* last_prims = nullptr;
+	// 0: the reference's second-pass block count ceil(num_verts/256) (parity mode);
+	// 1: all leaf blocks (the true global AABB, better Morton spread)
+	int full_global_aabb = 0;
 	uint32_t last_num_verts = 0;
 
 	uint32_t num_inner() const { return n > 0 ? n - 1 : 0; }

@@ -11,12 +11,14 @@
 EF pairs come back as a structured numpy array with the reference's 48-byte EfPair
 layout (collision_data.h:150-220) and (eid, fid) indices, in canonical (eid, fid) order.
 """
+import ctypes
+
 import numpy as np
 import torch
 
 from . import _native as nat
 from ._native import ptr
-from .lbvh import LBVH, TREE_EDGE, TREE_FACE
+from .lbvh import LBVH, TREE_EDGE, TREE_FACE, device_view
 
 EF_PAIR_DTYPE = np.dtype([("idx", np.uint32, 5), ("bary", np.float32, 3), ("grad", np.float32, 3), ("stiff", np.float32)])
 
@@ -63,7 +65,7 @@ class IntersectionResolver:
 class CollisionScene:
     """Device-resident mesh + face/edge trees for the EF detection path of one scene."""
 
-    def __init__(self, ctx, mesh, d_hat=1e-3, thickness=0.0, max_broad_pairs=None, max_ef_pairs=None):
+    def __init__(self, ctx, mesh, d_hat=1e-3, thickness=0.0, max_broad_pairs=None, max_ef_pairs=None, parity_tree=False):
         self.ctx = ctx
         self.mesh = mesh
         dev = torch.device("cuda", ctx.device)
@@ -77,6 +79,13 @@ class CollisionScene:
         self.thickness = torch.full((nv,), float(thickness), dtype=torch.float32, device=dev)
         self.face_tree = LBVH(ctx, TREE_FACE, mesh.num_faces)
         self.edge_tree = LBVH(ctx, TREE_EDGE, mesh.num_edges)
+        # chosen form: Morton codes over the full scene AABB and Morton-ordered queries
+        # (parity_tree=True keeps the reference's tree topology bit for bit)
+        self.parity_tree = parity_tree
+        if not parity_tree:
+            self.face_tree.set_full_global_aabb(True)
+            self.edge_tree.set_full_global_aabb(True)
+        self.edge_order = None
         self.max_broad = int(max_broad_pairs or max(1 << 16, 8 * mesh.num_edges))
         self.broad_count = torch.zeros(1, dtype=torch.int32, device=dev)
         self.broad_pairs = torch.zeros((self.max_broad, 2), dtype=torch.int32, device=dev)
@@ -93,6 +102,11 @@ class CollisionScene:
         self.edge_tree.reduce_edge_tree_aabb(xs, self.edges)
         self.face_tree.construct_tree()
         self.edge_tree.construct_tree()
+        if not self.parity_tree:
+            # edge queries in the edge tree's Morton order: a warp walks nearby edges
+            a = nat.U26LbvhArrays()
+            self.ctx.check(self.ctx.lib.u26_lbvh_arrays_get(self.edge_tree.handle, ctypes.byref(a)), "arrays")
+            self.edge_order = device_view(a.sorted_get_original, self.mesh.num_edges, np.uint32)
 
     # NewtonSolver::device_broadphase_dcd, EF part (newton_solver.cpp:1260-1299)
     def broadphase_dcd_ef(self, fused_refit=True):
@@ -126,7 +140,7 @@ class CollisionScene:
         """The fused EF kernel alone (face tree already refit, counter already reset)."""
         self.ctx.check(self.ctx.lib.u26_ef_detect(
             self.face_tree.handle, ptr(self.x), ptr(self.edges), self.mesh.num_edges, ptr(self.faces),
-            ptr(self.vert_property), ptr(self.d_hat), ptr(self.thickness), ptr(self.resolver.ef_count),
+            ptr(self.vert_property), ptr(self.d_hat), ptr(self.thickness), ptr(self.edge_order), ptr(self.resolver.ef_count),
             ptr(self.resolver.ef_list), ptr(self.resolver.ef_indices), self.resolver.max_ef,
             ptr(self.stats) if with_stats else None), "ef_detect")
 

@@ -71,6 +71,11 @@ class LBVH:
         """Leaf update and bottom-up refit in one launch."""
         self.ctx.check(self.ctx.lib.u26_lbvh_update_and_refit(self.handle, ptr(thickness), ptr(x_start), ptr(x_end), ptr(prims)), "update_and_refit")
 
+    def set_full_global_aabb(self, on=True):
+        """Morton codes over the AABB of all leaves instead of the reference's partial
+        second-pass reduction (lbvh.cpp:999-1021). Query results are unchanged."""
+        self.ctx.check(self.ctx.lib.u26_lbvh_set_option(self.handle, 1, int(bool(on))), "set_option")
+
     def check_health(self):
         h = ctypes.c_int(0)
         self.ctx.check(self.ctx.lib.u26_lbvh_check_health(self.handle, ctypes.byref(h)), "check_health")
