@@ -193,3 +193,115 @@ def line_intersection(p0, p1, a, b, c):
     t = ctypes.c_float(0)
     hit = lib().oracle_line_intersection(*[_p(v, _f32p) for v in arrs], _p(bary, _f32p), ctypes.byref(t))
     return bool(hit), bary, t.value
+
+
+# ---- PRP contour evaluation (oracle_prp.cpp) -------------------------------------
+class PrpParams(ctypes.Structure):
+    """Parameters of one PRP pass (SceneParams fields, scene_params.h:65-81)."""
+    _fields_ = [
+        ("max_contours", ctypes.c_uint32),      # untangling_process_contours_count
+        ("direction_mode", ctypes.c_uint32),    # 0 reference seeds, 1 the 26 lattice directions
+        ("use_ccr", ctypes.c_uint32),           # PRP_use_intrinsic_contour_side_candidates
+        ("ccr_tau", ctypes.c_float),            # PRP_intrinsic_tau
+        ("ccr_use_rest", ctypes.c_uint32),      # PRP_use_rest_geodesic_distance_for_intrinsic_candidates
+        ("ccr_use_current", ctypes.c_uint32),   # PRP_use_deformed_boundary_distance_for_intrinsic_candidates
+        ("batch_size", ctypes.c_uint32),        # PRP_cpu_contour_batch_size
+        ("brute_force_raycast", ctypes.c_uint32),
+    ]
+
+
+def prp_params(**kw):
+    p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
+                  batch_size=32, brute_force_raycast=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+RESULT_DTYPE = np.dtype([
+    ("contour_idx", np.uint32), ("contour_type", np.uint32), ("num_pairs", np.uint32), ("combo_idx", np.uint32),
+    ("num_dirs", np.uint32), ("hit_count", np.uint32), ("unculled_hit_count", np.uint32), ("covered_anchor_count", np.uint32),
+    ("boundary_anchor_count", np.uint32), ("eval_k_src", np.uint32), ("eval_k_dst", np.uint32),
+    ("max_frontier_hop_src", np.uint32), ("max_frontier_hop_dst", np.uint32), ("expansion_level_count", np.uint32),
+    ("flags", np.uint32), ("object_id0", np.uint32), ("object_id1", np.uint32), ("init_k_src", np.uint32),
+    ("init_k_dst", np.uint32), ("diam_src", np.uint32), ("diam_dst", np.uint32), ("num_boundary_src", np.uint32),
+    ("num_boundary_dst", np.uint32), ("reserved", np.uint32),
+    ("dir", np.float32, 3), ("depth", np.float32), ("volume", np.float32), ("objective", np.float32),
+    ("area", np.float32), ("displacement_cost", np.float32), ("coverage", np.float32),
+    ("normalized_objective", np.float32), ("pre_finalize_area", np.float32), ("reserved_f", np.float32)])
+HIT_DTYPE = np.dtype([("type", np.uint32), ("src_id", np.uint32), ("dst_id", np.uint32), ("sv", np.uint32, 3),
+                      ("dv", np.uint32, 3), ("bary", np.float32, 2), ("dist", np.float32)])
+assert RESULT_DTYPE.itemsize == 144 and HIT_DTYPE.itemsize == 48
+
+
+class PrpRun:
+    """All outputs of one oracle PRP pass."""
+
+    def __init__(self, mesh, ef_pairs, ef_indices, params=None, x=None):
+        L = lib()
+        L.oracle_prp_run.restype = ctypes.c_void_p
+        for n in ("oracle_prp_num_pairs", "oracle_prp_num_orig_pairs", "oracle_prp_num_contours", "oracle_prp_contour",
+                  "oracle_prp_hits", "oracle_prp_directions"):
+            getattr(L, n).restype = ctypes.c_uint32
+        params = params or prp_params()
+        desc = mesh.desc(x)
+        ef_pairs = np.ascontiguousarray(ef_pairs)
+        ef_indices = np.ascontiguousarray(ef_indices, dtype=np.uint32)
+        h = ctypes.c_void_p(L.oracle_prp_run(ctypes.byref(desc), ef_pairs.ctypes.data_as(ctypes.c_void_p),
+                                             _p(ef_indices, _u32p), ctypes.c_uint32(len(ef_pairs)), ctypes.byref(params)))
+        try:
+            n = L.oracle_prp_num_pairs(h)
+            self.num_orig_pairs = L.oracle_prp_num_orig_pairs(h)
+            self.pairs = np.zeros(max(n, 1), EF_PAIR_DTYPE)
+            self.pair_indices = np.zeros((max(n, 1), 2), np.uint32)
+            self.mesh_index = np.zeros(max(n, 1), np.uint32)
+            self.contour_index = np.zeros(max(n, 1), np.uint32)
+            self.pair_length = np.zeros(max(n, 1), np.float32)
+            L.oracle_prp_pairs(h, self.pairs.ctypes.data_as(ctypes.c_void_p), _p(self.pair_indices, _u32p),
+                               _p(self.mesh_index, _u32p), _p(self.contour_index, _u32p), _p(self.pair_length, _f32p))
+            self.pairs, self.pair_indices = self.pairs[:n], self.pair_indices[:n]
+            self.mesh_index, self.contour_index, self.pair_length = self.mesh_index[:n], self.contour_index[:n], self.pair_length[:n]
+            nc = L.oracle_prp_num_contours(h)
+            self.contours = []
+            self.results = np.zeros(nc, RESULT_DTYPE)
+            self.hits = []
+            self.directions = []
+            for c in range(nc):
+                k = L.oracle_prp_contour(h, ctypes.c_uint32(c), None)
+                buf = np.zeros(max(k, 1), np.uint32)
+                L.oracle_prp_contour(h, ctypes.c_uint32(c), _p(buf, _u32p))
+                self.contours.append(buf[:k])
+                L.oracle_prp_result(h, ctypes.c_uint32(c), self.results[c:c + 1].ctypes.data_as(ctypes.c_void_p))
+                nh = L.oracle_prp_hits(h, ctypes.c_uint32(c), None)
+                hb = np.zeros(max(nh, 1), HIT_DTYPE)
+                L.oracle_prp_hits(h, ctypes.c_uint32(c), hb.ctypes.data_as(ctypes.c_void_p))
+                self.hits.append(hb[:nh])
+                if self.results[c]["flags"] & 16:
+                    nd = L.oracle_prp_directions(h, ctypes.c_uint32(c), None)
+                    db = np.zeros((max(nd, 1), 3), np.float32)
+                    L.oracle_prp_directions(h, ctypes.c_uint32(c), _p(db, _f32p))
+                    self.directions.append(db[:nd])
+                else:
+                    self.directions.append(np.zeros((0, 3), np.float32))
+            st = np.zeros(2, np.uint64)
+            L.oracle_prp_stats(h, _p(st, _u64p))
+            self.tested, self.requests = int(st[0]), int(st[1])
+        finally:
+            L.oracle_prp_free(h)
+
+
+def eigen3(S):
+    S = np.ascontiguousarray(np.asarray(S, np.float32).T)  # columns
+    out = np.zeros(9, np.float32)
+    lib().oracle_eigen3(_p(S.reshape(-1), _f32p), _p(out, _f32p))
+    return out.reshape(3, 3)
+
+
+def detect_ef(mesh, d_hat=1e-3, thickness=0.0):
+    """EF pairs of a mesh at its current positions (LBVH broad phase + narrow phase)."""
+    dh = np.full(mesh.num_verts, d_hat, np.float32)
+    th = np.full(mesh.num_verts, thickness, np.float32)
+    tree = lbvh_build(TREE_FACE, mesh.x, mesh.faces)
+    lbvh_refit(tree, mesh.x, mesh.x, th, mesh.faces)
+    broad, _, _ = lbvh_query(tree, QUERY_EDGES_UNCULLED, mesh.x, mesh.x, mesh.edges, dh, th)
+    return ef_narrow(broad, mesh.x, mesh.edges, mesh.faces, dh, mesh.vert_property)

@@ -1,0 +1,2070 @@
+// Test infrastructure (oracle): CPU restatement of the reference's PRP contour evaluation
+// (host_resolve_intersections_PRP, the CPU batched path), from the canonical EF list to
+// the selected per-contour responses. Loaded only by tests/ and bench.py's CPU legs.
+//
+// Followed, stage by stage (all in Solver/CollisionDetector/):
+//   EF preprocessing      intersection_resolver.cpp:431-558, 683-1096 (ignore_near_zero_dist_pairs = true)
+//   contours              intersection_resolver2.cpp:254-309, intersection_resolver_helper.cpp:518-575
+//   classification        intersection_resolver2.cpp:311-375, 2811-2845
+//   boundary flags        intersection_resolver2.cpp:2646-2680, hit attachment 378-412
+//   normals               intersection_resolver2.cpp:2605-2644
+//   runtime               intersection_resolver2.cpp:2428-2585, hop/geodesic 618-722, directions 1488-1569
+//   candidates + CCR      intersection_resolver2.cpp:1571-1804, intersection_resolver2.h:405-506
+//   ray casting           cached_bvh.cpp:131-555, cached_bvh.hpp:6-46 (median split, leaf 8)
+//   hit adjacency         intersection_resolver_helper.cpp:771-902
+//   cluster culling       intersection_resolver2.cpp:3003-3771
+//   metrics / J           intersection_resolver2.cpp:1806-1954, helper.cpp:611-645
+//   adaptive k-ring       intersection_resolver2.cpp:1058-1230, intersection_resolver2.h:1177-1187
+//   selection             intersection_resolver2.h:807-912, intersection_resolver2.cpp:996-1057
+//   merge / suppression   intersection_resolver2.cpp:413-592, finalize 1956-2103
+//
+// Deviations, all shared with the CUDA path and stated once here:
+//  * The 3x3 symmetric eigen solver (the reference calls Eigen::SelfAdjointEigenSolver::
+//    computeDirect, not in this checkout) is cyclic Jacobi in double with eigenvalues
+//    ascending and each eigenvector's largest-magnitude component made positive.
+//  * Sums over a hit list (J, volume, area, displacement cost) run over the hits in
+//    canonical order (type, source id, target id) with a fixed 32-lane strided partial
+//    sum and xor-butterfly combine, the reduction order of the CUDA metrics kernel.
+//    The reference reduces in its own (BVH-dependent) hit order; its sets are what
+//    parity pins, its float sums agree to rounding.
+//  * Solid-interior hit links (intersection_resolver2.cpp:3298-3464) apply only to rigid
+//    or tetrahedral meshes; the scenes here are cloth, so they never fire and are not
+//    restated.
+#include <map>
+#include <memory>
+#include <mutex>
+#include <queue>
+#include <set>
+#include <string>
+
+#include "oracle_common.h"
+
+namespace u26o
+{
+	bool line_intersection(V3 p0, V3 p1, V3 A, V3 B, V3 C, V3& out_bary, float& out_time);
+}
+
+using namespace u26o;
+
+namespace
+{
+	constexpr uint kInf = 0xFFFFFFFFu;
+	constexpr float kGeoInf = std::numeric_limits<float>::max();
+
+	struct MeshIn
+	{
+		uint num_verts, num_edges, num_faces, num_objects;
+		const float* x;
+		const float* rest_x;
+		const uint* edges;
+		const uint* faces;
+		const uint* face_adj_edges;
+		const uint *vav_off, *vav;
+		const uint *vae_off, *vae;
+		const uint *vaf_off, *vaf;
+		const uint *eaf_off, *eaf;
+		const uint *eae_off, *eae;
+		const uint *prefix_verts, *prefix_edges, *prefix_faces;
+		const uint* vert_object;
+		const uint* vert_component;
+		const float *rest_vert_area, *rest_edge_area, *rest_face_area, *vert_mass;
+		const uint* mesh_orientation;
+	};
+
+	struct Params
+	{
+		uint max_contours;
+		uint direction_mode; // 0: reference seeds, 1: 26 lattice directions
+		uint use_ccr;
+		float ccr_tau;
+		uint ccr_use_rest;
+		uint ccr_use_current;
+		uint batch_size;
+		uint brute_force_raycast;
+	};
+
+	struct EfPair
+	{
+		uint idx[5];
+		float bary[3];
+		float grad[3];
+		float stiff;
+		bool is_loop() const { return idx[0] == idx[1]; }
+	};
+	static_assert(sizeof(EfPair) == 48, "EfPair");
+
+	struct Span
+	{
+		const uint* p;
+		uint n;
+		const uint* begin() const { return p; }
+		const uint* end() const { return p + n; }
+		uint size() const { return n; }
+	};
+	inline Span row(const uint* off, const uint* data, uint i) { return Span{ data + off[i], off[i + 1] - off[i] }; }
+
+	enum HitType : uint
+	{
+		VF = 0,
+		EE = 1,
+		FV = 2
+	};
+
+	struct Hit
+	{
+		uint type, src_id, dst_id;
+		uint sv[3], dv[3];
+		float bary[2];
+		float dist;
+		uint64_t key() const
+		{
+			return (uint64_t(type) << 62) | (uint64_t(src_id & 0x3fffffffu) << 31) | uint64_t(dst_id & 0x7fffffffu);
+		}
+		uint vid() const { return type == VF ? src_id : dst_id; }
+		uint fid() const { return type == VF ? dst_id : src_id; }
+	};
+
+	struct ComboInfo
+	{
+		bool present = false;
+		uint combo_idx = 0;
+		V3 dir = v3(0.0f);
+		float depth = 0, volume = 0, objective = 0, area = 0, cost = 0;
+		uint hit_count = 0, unculled = 0;
+		uint covered = 0, anchors = 0;
+		float coverage = 0;
+		uint max_front_src = 0, max_front_dst = 0;
+		uint eval_k_src = kInf, eval_k_dst = kInf;
+		uint levels = 0;
+		bool eligible = false, full_mesh = false;
+		std::vector<Hit> hits;
+	};
+
+	inline bool finitef(float v) { return std::isfinite(v); }
+
+	// intersection_resolver2.h:807-850
+	inline bool has_usable(const ComboInfo& c)
+	{
+		return !c.hits.empty() && c.covered > 0 && finitef(c.objective) && finitef(c.coverage) && c.coverage > 0.0f;
+	}
+	inline bool has_valid(const ComboInfo& c) { return c.eligible && has_usable(c); }
+	inline float objective_div_cov2(float obj, float cov)
+	{
+		if (!finitef(obj) || !finitef(cov) || cov <= 0.0f)
+			return std::numeric_limits<float>::infinity();
+		const double o = double(obj) / (double(cov) * double(cov));
+		return (std::isfinite(o) && o <= double(std::numeric_limits<float>::max())) ? float(o) : std::numeric_limits<float>::infinity();
+	}
+	inline float response_objective(const ComboInfo& c) { return objective_div_cov2(c.objective, c.coverage); }
+
+	// prp_response_is_better (intersection_resolver2.h:852-884)
+	inline int scalar_cmp(float lhs, float rhs)
+	{
+		const bool lf = finitef(lhs), rf = finitef(rhs);
+		if (lf != rf)
+			return lf ? -1 : 1;
+		if (!lf)
+			return 0;
+		const float tol = 1e-7f + 1e-5f * std::fmax(std::fabs(lhs), std::fabs(rhs));
+		if (lhs + tol < rhs)
+			return -1;
+		if (rhs + tol < lhs)
+			return 1;
+		return 0;
+	}
+	inline bool response_is_better(const ComboInfo& a, const ComboInfo& b)
+	{
+		int c = scalar_cmp(response_objective(a), response_objective(b));
+		if (c != 0)
+			return c < 0;
+		c = scalar_cmp(a.depth, b.depth);
+		if (c != 0)
+			return c < 0;
+		c = scalar_cmp(a.cost, b.cost);
+		if (c != 0)
+			return c < 0;
+		if (a.hit_count != b.hit_count)
+			return a.hit_count < b.hit_count;
+		return a.combo_idx < b.combo_idx;
+	}
+
+	// ---- 3x3 symmetric eigen decomposition (cyclic Jacobi, double)
+	void jacobi3(const double A_in[3][3], double evals[3], double evecs[3][3])
+	{
+		double A[3][3], V[3][3] = { { 1, 0, 0 }, { 0, 1, 0 }, { 0, 0, 1 } };
+		for (int i = 0; i < 3; i++)
+			for (int j = 0; j < 3; j++)
+				A[i][j] = A_in[i][j];
+		for (int sweep = 0; sweep < 64; sweep++)
+		{
+			const double off = A[0][1] * A[0][1] + A[0][2] * A[0][2] + A[1][2] * A[1][2];
+			const double diag = A[0][0] * A[0][0] + A[1][1] * A[1][1] + A[2][2] * A[2][2];
+			if (off <= 1e-30 * diag || off == 0.0)
+				break;
+			const int P[3] = { 0, 0, 1 }, Q[3] = { 1, 2, 2 };
+			for (int k = 0; k < 3; k++)
+			{
+				const int p = P[k], q = Q[k];
+				if (A[p][q] == 0.0)
+					continue;
+				const double theta = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
+				const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+				const double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+				for (int r = 0; r < 3; r++)
+				{
+					const double arp = A[r][p], arq = A[r][q];
+					A[r][p] = c * arp - s * arq;
+					A[r][q] = s * arp + c * arq;
+				}
+				for (int r = 0; r < 3; r++)
+				{
+					const double apr = A[p][r], aqr = A[q][r];
+					A[p][r] = c * apr - s * aqr;
+					A[q][r] = s * apr + c * aqr;
+				}
+				for (int r = 0; r < 3; r++)
+				{
+					const double vrp = V[r][p], vrq = V[r][q];
+					V[r][p] = c * vrp - s * vrq;
+					V[r][q] = s * vrp + c * vrq;
+				}
+			}
+		}
+		int order[3] = { 0, 1, 2 };
+		std::stable_sort(order, order + 3, [&](int a, int b)
+			{ return A[a][a] < A[b][b]; });
+		for (int k = 0; k < 3; k++)
+		{
+			const int c = order[k];
+			evals[k] = A[c][c];
+			int big = 0;
+			for (int r = 1; r < 3; r++)
+				if (std::fabs(V[r][c]) > std::fabs(V[big][c]))
+					big = r;
+			const double sgn = V[big][c] < 0 ? -1.0 : 1.0;
+			for (int r = 0; r < 3; r++)
+				evecs[r][k] = sgn * V[r][c];
+		}
+	}
+
+	struct Mat3
+	{
+		V3 c[3]; // columns
+	};
+	inline Mat3 mat_zero() { return Mat3{ { v3(0.0f), v3(0.0f), v3(0.0f) } }; }
+	inline Mat3 outer(V3 a, V3 b) { return Mat3{ { a * b.x, a * b.y, a * b.z } }; }
+	inline Mat3 mscale(float s, const Mat3& m) { return Mat3{ { m.c[0] * s, m.c[1] * s, m.c[2] * s } }; }
+	inline Mat3 madd(const Mat3& a, const Mat3& b) { return Mat3{ { a.c[0] + b.c[0], a.c[1] + b.c[1], a.c[2] + b.c[2] } }; }
+
+	inline bool valid_dir(V3 v) { return finitef(v.x) && finitef(v.y) && finitef(v.z) && length_sq(v) > 1e-12f; }
+
+	// compute_all_eigenvectors (intersection_resolver_helper.cpp:679-714)
+	void all_eigenvectors(const Mat3& S, V3 out[3])
+	{
+		const V3 def[3] = { v3(0, 1, 0), v3(1, 0, 0), v3(0, 0, 1) };
+		for (int i = 0; i < 3; i++)
+			out[i] = def[i];
+		for (int c = 0; c < 3; c++)
+			if (!finitef(S.c[c].x) || !finitef(S.c[c].y) || !finitef(S.c[c].z))
+				return;
+		const float trace = S.c[0].x + S.c[1].y + S.c[2].z;
+		if (trace < 1e-10f)
+			return;
+		float frob = 0.0f;
+		for (int c = 0; c < 3; c++)
+			frob += dot(S.c[c], S.c[c]);
+		if (frob < 1e-20f)
+			return;
+		double A[3][3], ev[3], V[3][3];
+		for (int r = 0; r < 3; r++)
+		{
+			A[r][0] = S.c[0].x * (r == 0) + S.c[0].y * (r == 1) + S.c[0].z * (r == 2);
+			A[r][1] = S.c[1].x * (r == 0) + S.c[1].y * (r == 1) + S.c[1].z * (r == 2);
+			A[r][2] = S.c[2].x * (r == 0) + S.c[2].y * (r == 1) + S.c[2].z * (r == 2);
+		}
+		jacobi3(A, ev, V);
+		for (int k = 0; k < 3; k++)
+		{
+			const V3 v = v3(float(V[0][k]), float(V[1][k]), float(V[2][k]));
+			out[k] = length_sq(v) > 1e-12f ? normalize(v) : def[k];
+		}
+	}
+
+	// ---- CachedBVH restatement (cached_bvh.hpp / cached_bvh.cpp)
+	struct BvhNode
+	{
+		V3 bmin, bmax;
+		int left = -1, right = -1, start = -1, count = 0;
+	};
+	struct CachedBVH
+	{
+		std::vector<BvhNode> nodes;
+		std::vector<uint> order;
+		bool faces = true;
+
+		template <typename Bounds>
+		int build_node(int start, int end, std::vector<V3>& centroids, Bounds& bounds)
+		{
+			BvhNode node;
+			bounds(start, end, node.bmin, node.bmax);
+			const int idx = int(nodes.size());
+			nodes.push_back(node);
+			const int count = end - start;
+			if (count <= 8)
+			{
+				nodes[idx].start = start;
+				nodes[idx].count = count;
+				return idx;
+			}
+			const V3 ext = node.bmax - node.bmin;
+			int axis = 0;
+			if (ext.y > ext.x && ext.y >= ext.z)
+				axis = 1;
+			else if (ext.z > ext.x && ext.z > ext.y)
+				axis = 2;
+			const int mid = (start + end) / 2;
+			std::nth_element(order.begin() + start, order.begin() + mid, order.begin() + end, [&](uint a, uint b)
+				{
+					if (axis == 0) return centroids[a].x < centroids[b].x;
+					if (axis == 1) return centroids[a].y < centroids[b].y;
+					return centroids[a].z < centroids[b].z; });
+			const int l = build_node(start, mid, centroids, bounds);
+			const int r = build_node(mid, end, centroids, bounds);
+			nodes[idx].left = l;
+			nodes[idx].right = r;
+			return idx;
+		}
+
+		void build(const std::vector<uint>& ids, const MeshIn& m, bool is_faces)
+		{
+			faces = is_faces;
+			order = ids;
+			nodes.clear();
+			if (order.empty())
+				return;
+			uint mx = 0;
+			for (uint id : order)
+				mx = std::max(mx, id);
+			std::vector<V3> centroids(mx + 1);
+			for (uint id : order)
+			{
+				if (faces)
+				{
+					const V3 a = load3(m.x, m.faces[3 * id]), b = load3(m.x, m.faces[3 * id + 1]), c = load3(m.x, m.faces[3 * id + 2]);
+					centroids[id] = ((a + b) + c) / 3.0f;
+				}
+				else
+				{
+					const V3 a = load3(m.x, m.edges[2 * id]), b = load3(m.x, m.edges[2 * id + 1]);
+					centroids[id] = (a + b) * 0.5f;
+				}
+			}
+			auto bounds = [&](int s, int e, V3& mn, V3& mxv)
+			{
+				bool first = true;
+				for (int i = s; i < e; i++)
+				{
+					const uint id = order[i];
+					V3 lo, hi;
+					if (faces)
+					{
+						const V3 a = load3(m.x, m.faces[3 * id]), b = load3(m.x, m.faces[3 * id + 1]), c = load3(m.x, m.faces[3 * id + 2]);
+						lo = vmin(a, vmin(b, c));
+						hi = vmax(a, vmax(b, c));
+					}
+					else
+					{
+						const V3 a = load3(m.x, m.edges[2 * id]), b = load3(m.x, m.edges[2 * id + 1]);
+						lo = vmin(a, b);
+						hi = vmax(a, b);
+					}
+					if (first)
+					{
+						mn = lo;
+						mxv = hi;
+						first = false;
+					}
+					else
+					{
+						mn = vmin(mn, lo);
+						mxv = vmax(mxv, hi);
+					}
+				}
+			};
+			build_node(0, int(order.size()), centroids, bounds);
+		}
+	};
+
+	struct VertRequest
+	{
+		uint vid;
+		V3 dir;
+		bool fv;
+		uint target_lo, target_cnt; // dense span
+		const std::vector<uint>* targets;
+		const std::vector<uint>* hop;
+		uint max_hop;
+	};
+	struct EdgeRequest
+	{
+		uint eid;
+		V3 dir;
+		float max_dist;
+		float target_proj_min;
+		uint target_lo, target_cnt;
+		const std::vector<uint>* targets;
+		const std::vector<uint>* hop;
+		uint max_hop;
+	};
+
+	inline bool in_span(uint id, uint lo, uint cnt)
+	{
+		if (cnt == 0)
+			return false;
+		if (cnt != kInf && (id < lo || id >= lo + cnt))
+			return false;
+		return true;
+	}
+
+	// VF (ray from vertex along dir) / FV (ray from vertex along -dir) primitive test
+	// (cached_bvh.cpp:258-289).
+	inline bool vert_face_test(const MeshIn& m, uint vid, V3 orig, V3 end, uint fid, Hit& h, bool fv, float ray_max)
+	{
+		const uint f0 = m.faces[3 * fid], f1 = m.faces[3 * fid + 1], f2 = m.faces[3 * fid + 2];
+		if (vid == f0 || vid == f1 || vid == f2)
+			return false;
+		V3 bary;
+		float t;
+		if (!line_intersection(orig, end, load3(m.x, f0), load3(m.x, f1), load3(m.x, f2), bary, t) || !(t >= 0.0f && t <= 1.0f))
+			return false;
+		h.type = fv ? FV : VF;
+		h.src_id = fv ? fid : vid;
+		h.dst_id = fv ? vid : fid;
+		if (fv)
+		{
+			h.sv[0] = f0; h.sv[1] = f1; h.sv[2] = f2;
+			h.dv[0] = vid; h.dv[1] = kInf; h.dv[2] = kInf;
+		}
+		else
+		{
+			h.sv[0] = vid; h.sv[1] = kInf; h.sv[2] = kInf;
+			h.dv[0] = f0; h.dv[1] = f1; h.dv[2] = f2;
+		}
+		h.bary[0] = bary.x;
+		h.bary[1] = bary.y;
+		h.dist = t * ray_max;
+		return true;
+	}
+
+	// EE swept-edge test (cached_bvh.cpp:377-473, primitive part).
+	struct EdgeRay
+	{
+		V3 p0, p1, e1, dir;
+		bool plane;
+		V3 pn;
+		float pd;
+		float max_dist;
+	};
+	inline EdgeRay make_edge_ray(const MeshIn& m, uint eid, V3 dir, float max_dist)
+	{
+		EdgeRay r;
+		r.p0 = load3(m.x, m.edges[2 * eid]);
+		r.p1 = load3(m.x, m.edges[2 * eid + 1]);
+		r.e1 = r.p1 - r.p0;
+		r.dir = dir;
+		r.max_dist = max_dist;
+		r.pn = cross(r.e1, dir);
+		const float nl = length(r.pn);
+		r.plane = nl >= 1e-10f;
+		r.pd = 0.0f;
+		if (r.plane)
+		{
+			r.pn = r.pn / nl;
+			r.pd = dot(r.pn, r.p0);
+		}
+		return r;
+	}
+	inline bool edge_edge_test(const MeshIn& m, const EdgeRay& r, uint eid1, uint eid2, Hit& h)
+	{
+		const uint a0 = m.edges[2 * eid1], a1 = m.edges[2 * eid1 + 1];
+		const uint b0 = m.edges[2 * eid2], b1 = m.edges[2 * eid2 + 1];
+		if (a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1)
+			return false;
+		const V3 q0 = load3(m.x, b0), q1 = load3(m.x, b1);
+		if (r.plane)
+		{
+			const float d0 = dot(r.pn, q0) - r.pd;
+			const float d1 = dot(r.pn, q1) - r.pd;
+			if ((d0 > 1e-6f && d1 > 1e-6f) || (d0 < -1e-6f && d1 < -1e-6f))
+				return false;
+		}
+		const V3 e2 = q1 - q0;
+		const V3 rr = q0 - r.p0;
+		const V3 n = cross(r.e1, e2);
+		const float det = -dot(r.dir, n);
+		if (std::fabs(det) < 1e-10f)
+			return false;
+		const float inv = 1.0f / det;
+		const float d_r_e1_e2 = dot(rr, cross(r.e1, e2));
+		const float d_dir_r_e2 = dot(r.dir, cross(rr, e2));
+		const float d_dir_e1_r = dot(r.dir, cross(r.e1, rr));
+		const float s = -d_r_e1_e2 * inv;
+		const float t1 = -d_dir_r_e2 * inv;
+		const float t2 = d_dir_e1_r * inv;
+		if (!(s >= 0.0f && s <= r.max_dist && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f))
+			return false;
+		h.type = EE;
+		h.src_id = eid1;
+		h.dst_id = eid2;
+		h.sv[0] = a0; h.sv[1] = a1; h.sv[2] = kInf;
+		h.dv[0] = b0; h.dv[1] = b1; h.dv[2] = kInf;
+		h.bary[0] = 1.0f - t1;
+		h.bary[1] = 1.0f - t2;
+		h.dist = s;
+		return true;
+	}
+
+	inline bool hop_ok(const std::vector<uint>* hop, uint max_hop, std::initializer_list<uint> vs)
+	{
+		if (hop == nullptr || max_hop == kInf)
+			return true;
+		for (uint v : vs)
+			if ((*hop)[v] > max_hop)
+				return false;
+		return true;
+	}
+
+	// ray_cast_from_verts_batched for one request (BVH or brute force over the targets)
+	void cast_vert(const MeshIn& m, const CachedBVH* bvh, const VertRequest& q, std::vector<Hit>& out, uint64_t& tested)
+	{
+		const float ray_max = 1.0f;
+		if (q.target_cnt == 0)
+			return;
+		const V3 cast = q.fv ? -q.dir : q.dir;
+		const V3 orig = load3(m.x, q.vid);
+		const V3 end = orig + cast * ray_max;
+		auto leaf = [&](uint fid)
+		{
+			tested++;
+			if (!in_span(fid, q.target_lo, q.target_cnt))
+				return;
+			if (q.targets && !std::binary_search(q.targets->begin(), q.targets->end(), fid))
+				return;
+			if (!hop_ok(q.hop, q.max_hop, { m.faces[3 * fid], m.faces[3 * fid + 1], m.faces[3 * fid + 2] }))
+				return;
+			Hit h;
+			if (vert_face_test(m, q.vid, orig, end, fid, h, q.fv, ray_max))
+				out.push_back(h);
+		};
+		if (bvh == nullptr)
+		{
+			for (uint fid : *q.targets)
+				leaf(fid);
+			return;
+		}
+		if (bvh->nodes.empty())
+			return;
+		const V3 inv = v3(1.0f / cast.x, 1.0f / cast.y, 1.0f / cast.z);
+		auto slab = [&](const BvhNode& n)
+		{
+			float t1 = (n.bmin.x - orig.x) * inv.x, t2 = (n.bmax.x - orig.x) * inv.x;
+			float tmin = std::fmin(t1, t2), tmax = std::fmax(t1, t2);
+			t1 = (n.bmin.y - orig.y) * inv.y;
+			t2 = (n.bmax.y - orig.y) * inv.y;
+			tmin = std::fmax(tmin, std::fmin(t1, t2));
+			tmax = std::fmin(tmax, std::fmax(t1, t2));
+			t1 = (n.bmin.z - orig.z) * inv.z;
+			t2 = (n.bmax.z - orig.z) * inv.z;
+			tmin = std::fmax(tmin, std::fmin(t1, t2));
+			tmax = std::fmin(tmax, std::fmax(t1, t2));
+			return tmax >= std::fmax(tmin, 0.0f) && tmin <= ray_max;
+		};
+		std::vector<int> stack{ 0 };
+		while (!stack.empty())
+		{
+			const int nid = stack.back();
+			stack.pop_back();
+			const BvhNode& n = bvh->nodes[nid];
+			if (!slab(n))
+				continue;
+			if (n.left == -1 && n.right == -1)
+			{
+				for (int i = n.start; i < n.start + n.count; i++)
+					leaf(bvh->order[i]);
+			}
+			else
+			{
+				if (n.left != -1)
+					stack.push_back(n.left);
+				if (n.right != -1)
+					stack.push_back(n.right);
+			}
+		}
+	}
+
+	void cast_edge(const MeshIn& m, const CachedBVH* bvh, const EdgeRequest& q, std::vector<Hit>& out, uint64_t& tested)
+	{
+		const float ray_max = std::fmin(std::fmax(q.max_dist, 0.0f), 1.0f);
+		if (ray_max <= 0.0f || q.target_cnt == 0)
+			return;
+		const EdgeRay r = make_edge_ray(m, q.eid, q.dir, ray_max);
+		auto leaf = [&](uint eid2)
+		{
+			tested++;
+			if (!in_span(eid2, q.target_lo, q.target_cnt))
+				return;
+			if (q.targets && !std::binary_search(q.targets->begin(), q.targets->end(), eid2))
+				return;
+			if (!hop_ok(q.hop, q.max_hop, { m.edges[2 * eid2], m.edges[2 * eid2 + 1] }))
+				return;
+			Hit h;
+			if (edge_edge_test(m, r, q.eid, eid2, h))
+				out.push_back(h);
+		};
+		if (bvh == nullptr)
+		{
+			for (uint e : *q.targets)
+				leaf(e);
+			return;
+		}
+		if (bvh->nodes.empty())
+			return;
+		const V3 a_end = r.p0 + q.dir * ray_max, b_end = r.p1 + q.dir * ray_max;
+		const V3 smin = vmin(vmin(r.p0, r.p1), vmin(a_end, b_end));
+		const V3 smax = vmax(vmax(r.p0, r.p1), vmax(a_end, b_end));
+		const float ep0 = dot(r.p0, q.dir), ep1 = dot(r.p1, q.dir);
+		const float dl2 = dot(q.dir, q.dir);
+		const float proj_min = std::fmax(std::fmin(ep0, ep1), q.target_proj_min - 1e-5f);
+		const float proj_max = std::fmax(ep0, ep1) + ray_max * dl2;
+		auto node_ok = [&](const BvhNode& n)
+		{
+			if (!((smin.x <= n.bmax.x && smax.x >= n.bmin.x) && (smin.y <= n.bmax.y && smax.y >= n.bmin.y) && (smin.z <= n.bmax.z && smax.z >= n.bmin.z)))
+				return false;
+			const V3 c = (n.bmin + n.bmax) * 0.5f;
+			const V3 e = (n.bmax - n.bmin) * 0.5f;
+			const float cp = dot(c, q.dir);
+			const float pr = (e.x * std::fabs(q.dir.x) + e.y * std::fabs(q.dir.y)) + e.z * std::fabs(q.dir.z);
+			if (cp + pr < proj_min - 1e-6f || cp - pr > proj_max + 1e-6f)
+				return false;
+			if (!r.plane)
+				return true;
+			const float cd = dot(r.pn, c) - r.pd;
+			const float rad = (e.x * std::fabs(r.pn.x) + e.y * std::fabs(r.pn.y)) + e.z * std::fabs(r.pn.z);
+			return std::fabs(cd) <= rad + 1e-6f;
+		};
+		std::vector<int> stack{ 0 };
+		while (!stack.empty())
+		{
+			const int nid = stack.back();
+			stack.pop_back();
+			const BvhNode& n = bvh->nodes[nid];
+			if (!node_ok(n))
+				continue;
+			if (n.left == -1 && n.right == -1)
+			{
+				for (int i = n.start; i < n.start + n.count; i++)
+					leaf(bvh->order[i]);
+			}
+			else
+			{
+				if (n.left != -1)
+					stack.push_back(n.left);
+				if (n.right != -1)
+					stack.push_back(n.right);
+			}
+		}
+	}
+
+	// ---- the evaluation state of one contour (PrpStandardContourRuntime)
+	struct Runtime
+	{
+		uint contour_idx = 0;
+		std::vector<uint> contour;
+		uint object_ids[2] = { 0, 0 };
+		uint comp_ids[2] = { kInf, kInf };
+		std::vector<uint> boundary[2];
+		std::vector<uint> hop[2];
+		std::vector<float> geo[2];
+		uint diam[2] = { 0, 0 };
+		std::vector<V3> dirs;
+		std::vector<ComboInfo> results;
+		std::vector<uint8_t> converged, pruned, present;
+		uint init_k[2] = { 0, 0 }, k[2] = { 0, 0 };
+		bool finished = false, no_response = false;
+		std::vector<uint> cand_v[2], cand_e[2], cand_f[2];
+		std::map<uint, float> cur_dist[2];
+	};
+
+	struct Scene
+	{
+		MeshIn m;
+		Params p;
+		// EF data (augmented with loop-vertex pairs)
+		std::vector<EfPair> ef;
+		std::vector<uint> ef_e, ef_f;
+		uint num_orig_pairs = 0;
+		std::vector<std::vector<uint>> adj;
+		std::vector<V3> pos3;
+		std::vector<float> length;
+		std::vector<std::vector<uint>> contours;
+		std::vector<uint> mesh_index, contour_index;
+		std::vector<uint> contour_type;
+		std::vector<std::vector<uint>> vflags;
+		std::vector<V3> fn, en, vn;
+		std::vector<Runtime> rt;
+		std::vector<ComboInfo> selected;
+		std::vector<uint8_t> processed, suppressed;
+		std::vector<float> pre_area;
+		std::vector<std::vector<uint>> merge_adj;
+		uint64_t tested = 0, requests = 0;
+		// per-object BVHs (faces, edges)
+		std::vector<std::unique_ptr<CachedBVH>> face_bvh, edge_bvh;
+		std::mutex mtx;
+	};
+
+	inline uint edge_of(const MeshIn& m, uint eid, int k) { return m.edges[2 * eid + k]; }
+	inline uint face_of(const MeshIn& m, uint fid, int k) { return m.faces[3 * fid + k]; }
+	inline bool contains(Span s, uint v) { return std::find(s.begin(), s.end(), v) != s.end(); }
+
+	// ---- EF preprocessing (intersection_resolver.cpp:431-558, 683-1096)
+	void preprocess(Scene& S)
+	{
+		const MeshIn& m = S.m;
+		const uint n = uint(S.ef.size());
+		S.num_orig_pairs = n;
+		auto build_adj = [&](uint count)
+		{
+			std::vector<std::vector<uint>> edge_pairs(m.num_edges), face_pairs(m.num_faces), adj(count);
+			for (uint p = 0; p < count; p++)
+				edge_pairs[S.ef_e[p]].push_back(p);
+			for (uint f = 0; f < m.num_faces; f++)
+				for (int j = 0; j < 3; j++)
+				{
+					const auto& ep = edge_pairs[m.face_adj_edges[3 * f + j]];
+					face_pairs[f].insert(face_pairs[f].end(), ep.begin(), ep.end());
+				}
+			for (uint p = 0; p < count; p++)
+			{
+				const uint eid = S.ef_e[p], fid = S.ef_f[p];
+				auto& out = adj[p];
+				for (uint ae : row(m.eae_off, m.eae, eid))
+					for (uint q : edge_pairs[ae])
+						if (S.ef_f[q] == fid && q != p)
+							out.push_back(q);
+				const Span af = row(m.eaf_off, m.eaf, eid);
+				for (uint q : face_pairs[fid])
+					if (q != p)
+						for (uint a : af)
+							if (S.ef_f[q] == a && S.ef_e[q] != eid && q != p)
+								out.push_back(q);
+			}
+			return adj;
+		};
+		S.adj = build_adj(n);
+		// loop vertices (find_loop_vertex, non-GIA path)
+		std::vector<uint> loop_vid, loop_pair, loop_e, loop_f;
+		for (uint p = 0; p < n; p++)
+		{
+			const uint eid = S.ef_e[p], fid = S.ef_f[p];
+			const uint ex = edge_of(m, eid, 0), ey = edge_of(m, eid, 1);
+			for (uint af : row(m.eaf_off, m.eaf, eid))
+			{
+				const uint av = face_of(m, af, 0) + face_of(m, af, 1) + face_of(m, af, 2) - ex - ey;
+				if (av == face_of(m, fid, 0) || av == face_of(m, fid, 1) || av == face_of(m, fid, 2))
+				{
+					const uint* fa = m.face_adj_edges + 3 * af;
+					auto has = [&](uint e, uint v)
+					{ return edge_of(m, e, 0) == v || edge_of(m, e, 1) == v; };
+					uint le;
+					if (eid == fa[0])
+						le = has(fa[1], av) ? fa[1] : fa[2];
+					else if (eid == fa[1])
+						le = has(fa[0], av) ? fa[0] : fa[2];
+					else
+						le = has(fa[0], av) ? fa[0] : fa[1];
+					loop_vid.push_back(av);
+					loop_pair.push_back(p);
+					loop_e.push_back(le);
+					loop_f.push_back(fid);
+				}
+			}
+		}
+		for (size_t l = 0; l < loop_vid.size(); l++)
+		{
+			const uint v = loop_vid[l];
+			EfPair lp{};
+			lp.idx[0] = lp.idx[1] = lp.idx[2] = lp.idx[3] = lp.idx[4] = v;
+			lp.bary[0] = 1.0f;
+			lp.bary[1] = 1.0f;
+			lp.bary[2] = 0.0f;
+			const uint np = uint(S.ef.size());
+			S.ef.push_back(lp);
+			S.ef_e.push_back(loop_e[l]);
+			S.ef_f.push_back(loop_f[l]);
+			S.adj.push_back({ loop_pair[l] });
+			S.adj[loop_pair[l]].push_back(np);
+		}
+		const uint na = uint(S.ef.size());
+		S.pos3.resize(na);
+		S.length.resize(na);
+		for (uint p = 0; p < na; p++)
+		{
+			const EfPair& e = S.ef[p];
+			const float b0 = e.bary[0], b1 = 1.0f - e.bary[0];
+			S.pos3[p] = load3(m.x, e.idx[0]) * b0 + load3(m.x, e.idx[1]) * b1;
+		}
+		for (uint p = 0; p < na; p++)
+		{
+			float sum = 0.0f;
+			for (uint q : S.adj[p])
+				sum += length(S.pos3[q] - S.pos3[p]);
+			S.length[p] = 0.5f * sum;
+		}
+	}
+
+	// ---- contours + classification
+	void contours(Scene& S)
+	{
+		const uint n = uint(S.ef.size());
+		std::vector<std::vector<uint>> w(n);
+		for (uint p = 0; p < n; p++)
+		{
+			for (uint q : S.adj[p])
+			{
+				const bool same = S.ef[p].idx[2] == S.ef[q].idx[2] && S.ef[p].idx[3] == S.ef[q].idx[3] && S.ef[p].idx[4] == S.ef[q].idx[4];
+				w[p].push_back(same ? 0u : 1u);
+			}
+		}
+		std::vector<uint8_t> visited(n, 0);
+		S.mesh_index.assign(n, kInf);
+		for (uint seed = 0; seed < n; seed++)
+		{
+			if (visited[seed])
+				continue;
+			std::vector<std::pair<uint, uint>> group{ { seed, 0 } }, todo{ { seed, 0 } };
+			visited[seed] = 1;
+			while (!todo.empty())
+			{
+				const auto [pi, ps] = todo.back();
+				todo.pop_back();
+				for (size_t j = 0; j < S.adj[pi].size(); j++)
+				{
+					const uint q = S.adj[pi][j];
+					if (!visited[q])
+					{
+						visited[q] = 1;
+						todo.push_back({ q, ps + w[pi][j] });
+						group.push_back({ q, ps + w[pi][j] });
+					}
+				}
+			}
+			std::vector<uint> c;
+			for (auto& [pi, ps] : group)
+			{
+				c.push_back(pi);
+				S.mesh_index[pi] = ps % 2;
+			}
+			S.contours.push_back(c);
+		}
+		S.contour_index.assign(n, kInf);
+		for (uint c = 0; c < S.contours.size(); c++)
+			for (uint p : S.contours[c])
+				S.contour_index[p] = c;
+		// classify_contour_type
+		const MeshIn& m = S.m;
+		S.contour_type.resize(S.contours.size());
+		for (uint c = 0; c < S.contours.size(); c++)
+		{
+			std::vector<uint> bnd, loops;
+			bool closed = true;
+			for (uint p : S.contours[c])
+			{
+				const bool is_bnd = (m.eaf_off[S.ef_e[p] + 1] - m.eaf_off[S.ef_e[p]]) <= 1;
+				if (S.ef[p].is_loop())
+					loops.push_back(p);
+				if (is_bnd)
+				{
+					bnd.push_back(p);
+					closed = false;
+				}
+				if (!S.ef[p].is_loop() && S.adj[p].size() == 1)
+					closed = false;
+			}
+			uint t = 0;
+			if (bnd.empty())
+			{
+				if (loops.empty() && closed)
+					t = 1;
+				else if (loops.size() == 1 && closed)
+					t = 2;
+				else if (loops.size() == 2 && closed)
+					t = 3;
+			}
+			else if (loops.empty())
+			{
+				if (bnd.size() == 2)
+					t = S.mesh_index[bnd.front()] == S.mesh_index[bnd.back()] ? 7 : 6;
+			}
+			else if (loops.size() == 1)
+			{
+				if (bnd.size() == 1)
+					t = 4;
+				else if (bnd.size() == 2)
+					t = 5;
+			}
+			S.contour_type[c] = t;
+		}
+		// vertex boundary flags
+		S.vflags.assign(m.num_verts, {});
+		for (uint p = 0; p < n; p++)
+		{
+			if (S.ef[p].is_loop())
+				continue;
+			const uint ef_flag = 2 * S.contour_index[p] + S.mesh_index[p];
+			const uint ff = ef_flag ^ 1u;
+			S.vflags[S.ef[p].idx[0]].push_back(ef_flag);
+			S.vflags[S.ef[p].idx[1]].push_back(ef_flag);
+			S.vflags[S.ef[p].idx[2]].push_back(ff);
+			S.vflags[S.ef[p].idx[3]].push_back(ff);
+			S.vflags[S.ef[p].idx[4]].push_back(ff);
+		}
+		for (auto& r : S.vflags)
+		{
+			std::sort(r.begin(), r.end());
+			r.erase(std::unique(r.begin(), r.end()), r.end());
+		}
+	}
+
+	void normals(Scene& S)
+	{
+		const MeshIn& m = S.m;
+		auto safe_n = [](V3 n)
+		{
+			const float l2 = dot(n, n);
+			return l2 > 1e-20f ? n / std::sqrt(l2) : v3(0.0f);
+		};
+		S.fn.resize(m.num_faces);
+		S.en.resize(m.num_edges);
+		S.vn.resize(m.num_verts);
+		for (uint f = 0; f < m.num_faces; f++)
+		{
+			const V3 a = load3(m.x, face_of(m, f, 0)), b = load3(m.x, face_of(m, f, 1)), c = load3(m.x, face_of(m, f, 2));
+			const V3 n = safe_n(cross(b - a, c - a));
+			const uint obj = m.vert_object[face_of(m, f, 0)];
+			S.fn[f] = (m.mesh_orientation == nullptr || m.mesh_orientation[obj] == 0 ? 1.0f : -1.0f) * n;
+		}
+		for (uint e = 0; e < m.num_edges; e++)
+		{
+			V3 s = v3(0.0f);
+			for (uint f : row(m.eaf_off, m.eaf, e))
+				s = s + m.rest_face_area[f] * S.fn[f];
+			S.en[e] = safe_n(s);
+		}
+		for (uint v = 0; v < m.num_verts; v++)
+		{
+			V3 s = v3(0.0f);
+			for (uint f : row(m.vaf_off, m.vaf, v))
+				s = s + m.rest_face_area[f] * S.fn[f];
+			S.vn[v] = safe_n(s);
+		}
+	}
+
+	// ---- runtime initialisation
+	void hop_geo(const Scene& S, Runtime& r)
+	{
+		const MeshIn& m = S.m;
+		for (int side = 0; side < 2; side++)
+		{
+			const uint lo = m.prefix_verts[r.object_ids[side]], hi = m.prefix_verts[r.object_ids[side] + 1];
+			auto& hop = r.hop[side];
+			auto& geo = r.geo[side];
+			hop.assign(m.num_verts, kInf);
+			geo.assign(m.num_verts, kGeoInf);
+			std::priority_queue<std::pair<uint, uint>, std::vector<std::pair<uint, uint>>, std::greater<>> hq;
+			std::priority_queue<std::pair<float, uint>, std::vector<std::pair<float, uint>>, std::greater<>> gq;
+			for (uint v : r.boundary[side])
+			{
+				hop[v] = 0;
+				geo[v] = 0.0f;
+				hq.emplace(0u, v);
+				gq.emplace(0.0f, v);
+			}
+			while (!hq.empty())
+			{
+				auto [d, v] = hq.top();
+				hq.pop();
+				if (d > hop[v])
+					continue;
+				for (uint a : row(m.vav_off, m.vav, v))
+				{
+					if (a < lo || a >= hi)
+						continue;
+					if (d + 1 < hop[a])
+					{
+						hop[a] = d + 1;
+						hq.emplace(d + 1, a);
+					}
+				}
+			}
+			while (!gq.empty())
+			{
+				auto [d, v] = gq.top();
+				gq.pop();
+				if (d > geo[v])
+					continue;
+				for (uint a : row(m.vav_off, m.vav, v))
+				{
+					if (a < lo || a >= hi)
+						continue;
+					const float nd = d + length(load3(m.rest_x, v) - load3(m.rest_x, a));
+					if (nd < geo[a])
+					{
+						geo[a] = nd;
+						gq.emplace(nd, a);
+					}
+				}
+			}
+			uint mx = 0;
+			for (uint v = lo; v < hi; v++)
+				if (hop[v] != kInf)
+					mx = std::max(mx, hop[v]);
+			r.diam[side] = mx;
+		}
+	}
+
+	std::vector<V3> ray_directions(const Scene& S, const Runtime& r)
+	{
+		const MeshIn& m = S.m;
+		std::vector<V3> dirs;
+		if (S.p.direction_mode == 1)
+		{
+			for (int dx = -1; dx <= 1; dx++)
+				for (int dy = -1; dy <= 1; dy++)
+					for (int dz = -1; dz <= 1; dz++)
+						if (dx || dy || dz)
+							dirs.push_back(normalize(v3(float(dx), float(dy), float(dz))));
+			return dirs;
+		}
+		auto add_seed = [&](V3 d)
+		{
+			if (!valid_dir(d))
+				return;
+			dirs.push_back(normalize(d));
+		};
+		auto add_signed = [&](V3 d)
+		{
+			add_seed(d);
+			add_seed(-d);
+		};
+		// weighted mean of the contour points (helper.h:199-228)
+		V3 ws = v3(0.0f), us = v3(0.0f);
+		float sw = 0.0f;
+		for (uint p : r.contour)
+		{
+			const float w = S.length[p];
+			us = us + S.pos3[p];
+			ws = ws + S.pos3[p] * w;
+			sw += w;
+		}
+		const V3 center = sw == 0.0f ? us / float(r.contour.size()) : ws / sw;
+		V3 mc[2] = { v3(0.0f), v3(0.0f) };
+		Mat3 Sw = mat_zero();
+		for (int side = 0; side < 2; side++)
+		{
+			float wsum = 0.0f;
+			std::vector<float> wts;
+			for (uint v : r.boundary[side])
+			{
+				const V3 x = load3(m.x, v);
+				const float w = std::fmax(m.rest_vert_area[v], 1e-8f);
+				wts.push_back(w);
+				mc[side] = mc[side] + x * w;
+				const V3 c = x - center;
+				Sw = madd(Sw, mscale(w, outer(c, c)));
+			}
+			for (float w : wts)
+				wsum += w;
+			mc[side] = wsum > 1e-8f ? mc[side] / wsum : center;
+		}
+		V3 ev[3];
+		all_eigenvectors(Sw, ev);
+		for (int k = 0; k < 3; k++)
+			add_signed(ev[k]);
+		for (int side = 0; side < 2; side++)
+		{
+			V3 d = center - mc[side];
+			if (!valid_dir(d))
+				d = ev[side + 1];
+			add_seed(d);
+		}
+		V3 gc = v3(0.0f);
+		float tm = 0.0f;
+		for (uint v = 0; v < m.num_verts; v++)
+		{
+			const float w = std::fmax(m.rest_vert_area[v], 1e-8f);
+			gc = gc + load3(m.x, v) * w;
+			tm += w;
+		}
+		if (tm > 1e-8f)
+		{
+			gc = gc / tm;
+			const V3 rad = center - gc;
+			if (valid_dir(rad))
+				add_signed(rad);
+		}
+		if (dirs.empty())
+			add_signed(v3(0, 1, 0));
+		return dirs;
+	}
+
+	inline uint kring_init(uint boundary_count, uint diam)
+	{
+		const uint k0 = 3;
+		if (diam == 0)
+			return k0;
+		const uint ka = uint(std::ceil(std::sqrt(float(boundary_count))));
+		return std::max(k0, std::min(ka, diam));
+	}
+
+	void init_runtime(const Scene& S, Runtime& r, uint c)
+	{
+		const MeshIn& m = S.m;
+		r.contour_idx = c;
+		r.contour = S.contours[c];
+		const uint first = r.contour.front();
+		const EfPair& fp = S.ef[first];
+		const uint es = S.mesh_index[first];
+		r.object_ids[es] = m.vert_object[fp.idx[0]];
+		r.comp_ids[es] = m.vert_component ? m.vert_component[fp.idx[0]] : 0;
+		r.object_ids[es ^ 1] = m.vert_object[fp.idx[2]];
+		r.comp_ids[es ^ 1] = m.vert_component ? m.vert_component[fp.idx[2]] : 0;
+		std::set<uint> bs[2];
+		for (uint p : r.contour)
+		{
+			const uint mi = S.mesh_index[p];
+			bs[mi].insert(S.ef[p].idx[0]);
+			bs[mi].insert(S.ef[p].idx[1]);
+			bs[mi ^ 1].insert(S.ef[p].idx[2]);
+			bs[mi ^ 1].insert(S.ef[p].idx[3]);
+			bs[mi ^ 1].insert(S.ef[p].idx[4]);
+		}
+		for (int s = 0; s < 2; s++)
+			r.boundary[s].assign(bs[s].begin(), bs[s].end());
+		hop_geo(S, r);
+		r.dirs = ray_directions(S, r);
+		const size_t nd = r.dirs.size();
+		r.results.assign(nd, ComboInfo{});
+		r.converged.assign(nd, 0);
+		r.pruned.assign(nd, 0);
+		r.present.assign(nd, 0);
+		for (int s = 0; s < 2; s++)
+		{
+			r.init_k[s] = kring_init(uint(r.boundary[s].size()), r.diam[s]);
+			r.k[s] = r.init_k[s];
+		}
+	}
+
+	// ---- candidates at level k with contour-side restriction (CCR)
+	inline bool owns_1(float own, float opp, float tau)
+	{
+		const float unreach = std::numeric_limits<float>::max() * 0.5f;
+		if (!finitef(own) || own >= unreach)
+			return false;
+		if (!finitef(opp) || opp >= unreach)
+			return true;
+		// compute_normalized_phi with both reachable
+		const float phi = (own - opp) / (own + opp + 1e-6f);
+		return phi <= tau;
+	}
+
+	void build_candidates(const Scene& S, Runtime& r)
+	{
+		const MeshIn& m = S.m;
+		for (int s = 0; s < 2; s++)
+		{
+			const uint obj = r.object_ids[s];
+			const uint k = r.k[s];
+			const auto& d = r.hop[s];
+			auto& cv = r.cand_v[s];
+			auto& ce = r.cand_e[s];
+			auto& cf = r.cand_f[s];
+			cv.clear();
+			ce.clear();
+			cf.clear();
+			for (uint v = m.prefix_verts[obj]; v < m.prefix_verts[obj + 1]; v++)
+				if (d[v] <= k)
+					cv.push_back(v);
+			for (uint e = m.prefix_edges[obj]; e < m.prefix_edges[obj + 1]; e++)
+				if (d[edge_of(m, e, 0)] <= k && d[edge_of(m, e, 1)] <= k)
+					ce.push_back(e);
+			for (uint f = m.prefix_faces[obj]; f < m.prefix_faces[obj + 1]; f++)
+				if (d[face_of(m, f, 0)] <= k && d[face_of(m, f, 1)] <= k && d[face_of(m, f, 2)] <= k)
+					cf.push_back(f);
+		}
+		if (!S.p.use_ccr || !(S.p.ccr_use_rest || S.p.ccr_use_current))
+			return;
+		// restriction applies: deformed distance on -> both object ids valid; else shared topology
+		bool applies;
+		if (S.p.ccr_use_current)
+			applies = true;
+		else
+			applies = r.object_ids[0] == r.object_ids[1] && r.comp_ids[0] != kInf && r.comp_ids[0] == r.comp_ids[1];
+		if (!applies)
+			return;
+		auto cur = [&](int role, uint v)
+		{
+			auto it = r.cur_dist[role].find(v);
+			if (it != r.cur_dist[role].end())
+				return it->second;
+			const V3 x = load3(m.x, v);
+			float md = std::numeric_limits<float>::max();
+			for (uint b : r.boundary[role])
+				md = std::fmin(md, length(x - load3(m.x, b)));
+			r.cur_dist[role].emplace(v, md);
+			return md;
+		};
+		for (int role = 0; role < 2; role++)
+		{
+			auto owns = [&](uint v)
+			{
+				const float ro = r.geo[role][v], rp = r.geo[role ^ 1][v];
+				const float tau = S.p.ccr_tau;
+				if (S.p.ccr_use_rest && !owns_1(ro, rp, tau))
+					return false;
+				if (!S.p.ccr_use_current)
+					return true;
+				return (!S.p.ccr_use_rest || owns_1(ro, rp, tau)) && owns_1(cur(role, v), cur(role ^ 1, v), tau);
+			};
+			auto& cv = r.cand_v[role];
+			cv.erase(std::remove_if(cv.begin(), cv.end(), [&](uint v)
+						 { return !owns(v); }),
+				cv.end());
+			auto& ce = r.cand_e[role];
+			ce.erase(std::remove_if(ce.begin(), ce.end(), [&](uint e)
+						 { return !owns(edge_of(m, e, 0)) && !owns(edge_of(m, e, 1)); }),
+				ce.end());
+			auto& cf = r.cand_f[role];
+			cf.erase(std::remove_if(cf.begin(), cf.end(), [&](uint f)
+						 { return !owns(face_of(m, f, 0)) && !owns(face_of(m, f, 1)) && !owns(face_of(m, f, 2)); }),
+				cf.end());
+		}
+	}
+
+	// ---- hit adjacency (find_adjacent_hits), as exact-key lookups in the sorted hit list
+	struct HitIndex
+	{
+		std::vector<uint64_t> keys;
+		std::vector<uint> idx;
+		void build(const std::vector<Hit>& hits)
+		{
+			std::vector<std::pair<uint64_t, uint>> kv;
+			for (uint i = 0; i < hits.size(); i++)
+				kv.push_back({ hits[i].key(), i });
+			std::sort(kv.begin(), kv.end());
+			keys.clear();
+			idx.clear();
+			for (auto& [k, i] : kv)
+			{
+				keys.push_back(k);
+				idx.push_back(i);
+			}
+		}
+		template <typename F>
+		void find(uint type, uint src, uint dst, F&& f) const
+		{
+			const uint64_t k = (uint64_t(type) << 62) | (uint64_t(src & 0x3fffffffu) << 31) | uint64_t(dst & 0x7fffffffu);
+			auto it = std::lower_bound(keys.begin(), keys.end(), k);
+			for (; it != keys.end() && *it == k; ++it)
+				f(idx[it - keys.begin()]);
+		}
+	};
+
+	// neighbours of hit i (intersection_resolver_helper.cpp:771-902), each rule restated as the
+	// exact (type, source, target) keys its bucket scan would accept.
+	void hit_neighbours(const MeshIn& m, const std::vector<Hit>& H, const HitIndex& ix, uint i, std::vector<uint>& out)
+	{
+		const Hit& h = H[i];
+		auto add = [&](uint j)
+		{
+			if (j != i)
+				out.push_back(j);
+		};
+		if (h.type == VF)
+		{
+			const uint v = h.src_id, f = h.dst_id;
+			for (uint av : row(m.vav_off, m.vav, v))
+				ix.find(VF, av, f, add);
+			for (uint af : row(m.vaf_off, m.vaf, v))
+				for (int k = 0; k < 3; k++)
+					ix.find(FV, af, face_of(m, f, k), add);
+			for (uint ae : row(m.vae_off, m.vae, v))
+				for (int k = 0; k < 3; k++)
+					ix.find(EE, ae, m.face_adj_edges[3 * f + k], add);
+		}
+		else if (h.type == FV)
+		{
+			const uint f = h.src_id, w = h.dst_id;
+			for (int k = 0; k < 3; k++)
+				for (uint af : row(m.vaf_off, m.vaf, w))
+					ix.find(VF, face_of(m, f, k), af, add);
+			for (uint aw : row(m.vav_off, m.vav, w))
+				ix.find(FV, f, aw, add);
+			for (int k = 0; k < 3; k++)
+				for (uint ae : row(m.vae_off, m.vae, w))
+					ix.find(EE, m.face_adj_edges[3 * f + k], ae, add);
+		}
+		else
+		{
+			const uint e1 = h.src_id, e2 = h.dst_id;
+			for (int k = 0; k < 2; k++)
+				for (uint af : row(m.eaf_off, m.eaf, e2))
+					ix.find(VF, edge_of(m, e1, k), af, add);
+			for (uint af : row(m.eaf_off, m.eaf, e1))
+				for (int k = 0; k < 2; k++)
+					ix.find(FV, af, edge_of(m, e2, k), add);
+			for (uint ae2 : row(m.eae_off, m.eae, e2))
+				ix.find(EE, e1, ae2, add);
+			for (uint ae1 : row(m.eae_off, m.eae, e1))
+				ix.find(EE, ae1, e2, add);
+		}
+	}
+
+	// Canonical 32-lane strided sum + xor butterfly (the CUDA metrics kernel's order).
+	template <typename F>
+	float lane_sum(uint n, F&& val)
+	{
+		float s[32];
+		for (int l = 0; l < 32; l++)
+			s[l] = 0.0f;
+		for (uint i = 0; i < n; i++)
+			s[i & 31] = s[i & 31] + val(i);
+		for (int off = 16; off >= 1; off >>= 1)
+		{
+			float t[32];
+			for (int l = 0; l < 32; l++)
+				t[l] = s[l] + s[l ^ off];
+			for (int l = 0; l < 32; l++)
+				s[l] = t[l];
+		}
+		return s[0];
+	}
+
+	// prp_eval_penetration_v2 + prp_fill_combo_eval_info over hits in canonical order
+	void fill_metrics(const Scene& S, const Runtime& r, ComboInfo& c)
+	{
+		const MeshIn& m = S.m;
+		std::sort(c.hits.begin(), c.hits.end(), [](const Hit& a, const Hit& b)
+			{ return a.key() < b.key(); });
+		const uint n = uint(c.hits.size());
+		auto inv_mass = [&](uint v)
+		{ return 1.0f / std::fmax(m.vert_mass[v], 1e-8f); };
+		auto area_alpha = [&](const Hit& h, float& area, float& alpha)
+		{
+			const V3 d = c.dir;
+			if (h.type == VF)
+			{
+				area = m.rest_vert_area[h.src_id];
+				alpha = std::fabs(dot(S.vn[h.src_id], d));
+			}
+			else if (h.type == EE)
+			{
+				area = m.rest_edge_area[h.src_id];
+				alpha = std::fabs(dot(S.en[h.src_id], d));
+			}
+			else
+			{
+				area = m.rest_face_area[h.src_id];
+				alpha = std::fabs(dot(S.fn[h.src_id], d));
+			}
+		};
+		auto eff_inv = [&](const Hit& h)
+		{
+			if (h.type == VF)
+			{
+				const float bx = h.bary[0], by = h.bary[1], bz = 1.0f - h.bary[0] - h.bary[1];
+				return ((inv_mass(h.sv[0]) + bx * bx * inv_mass(h.dv[0])) + by * by * inv_mass(h.dv[1])) + bz * bz * inv_mass(h.dv[2]);
+			}
+			if (h.type == FV)
+			{
+				const float bx = h.bary[0], by = h.bary[1], bz = 1.0f - h.bary[0] - h.bary[1];
+				return ((bx * bx * inv_mass(h.sv[0]) + by * by * inv_mass(h.sv[1])) + bz * bz * inv_mass(h.sv[2])) + inv_mass(h.dv[0]);
+			}
+			const float a0 = h.bary[0], a1 = 1.0f - h.bary[0], b0 = h.bary[1], b1 = 1.0f - h.bary[1];
+			return ((a0 * a0 * inv_mass(h.sv[0]) + a1 * a1 * inv_mass(h.sv[1])) + b0 * b0 * inv_mass(h.dv[0])) + b1 * b1 * inv_mass(h.dv[1]);
+		};
+		float depth = 0.0f;
+		for (const Hit& h : c.hits)
+			depth = std::fmax(depth, h.dist);
+		const float area = lane_sum(n, [&](uint i)
+			{ float a, al; area_alpha(c.hits[i], a, al); return a; });
+		const float volume = lane_sum(n, [&](uint i)
+			{ float a, al; area_alpha(c.hits[i], a, al); return (a * al) * c.hits[i].dist; });
+		const float kappa = lane_sum(n, [&](uint i)
+			{
+				const float sd = c.hits[i].dist + 3e-3f;
+				const float e = eff_inv(c.hits[i]);
+				return e > 1e-8f ? (sd * sd) / e : 0.0f; });
+		c.depth = depth;
+		c.volume = volume;
+		c.area = area;
+		c.objective = (area * depth) * depth;
+		c.cost = kappa;
+		c.hit_count = n;
+		// EF-anchor coverage
+		std::set<uint> sup[2];
+		for (const Hit& h : c.hits)
+		{
+			for (int k = 0; k < 3; k++)
+				if (h.sv[k] != kInf)
+					sup[0].insert(h.sv[k]);
+			for (int k = 0; k < 3; k++)
+				if (h.dv[k] != kInf)
+					sup[1].insert(h.dv[k]);
+		}
+		uint cov = 0;
+		for (uint p : r.contour)
+		{
+			const uint mi = S.mesh_index[p];
+			const EfPair& e = S.ef[p];
+			const bool eo = sup[mi].count(e.idx[0]) || sup[mi].count(e.idx[1]);
+			const bool fo = sup[mi ^ 1].count(e.idx[2]) || sup[mi ^ 1].count(e.idx[3]) || sup[mi ^ 1].count(e.idx[4]);
+			cov += (eo && fo) ? 1 : 0;
+		}
+		c.anchors = uint(r.contour.size());
+		c.covered = cov;
+		c.coverage = c.anchors > 0 ? float(cov) / float(c.anchors) : 0.0f;
+		// frontier hops
+		uint mfs = 0, mfd = 0;
+		for (const Hit& h : c.hits)
+		{
+			for (int k = 0; k < 3; k++)
+				if (h.sv[k] != kInf && r.hop[0][h.sv[k]] != kInf)
+					mfs = std::max(mfs, r.hop[0][h.sv[k]]);
+			for (int k = 0; k < 3; k++)
+				if (h.dv[k] != kInf && r.hop[1][h.dv[k]] != kInf)
+					mfd = std::max(mfd, r.hop[1][h.dv[k]]);
+		}
+		c.max_front_src = mfs;
+		c.max_front_dst = mfd;
+	}
+
+	// One (contour, combo) evaluation at the current k-ring (evaluate_batched_contours_of_single_combo).
+	ComboInfo eval_combo(Scene& S, Runtime& r, uint combo)
+	{
+		const MeshIn& m = S.m;
+		ComboInfo info;
+		info.present = true;
+		info.combo_idx = combo;
+		info.dir = r.dirs[combo];
+		info.eval_k_src = r.k[0];
+		info.eval_k_dst = r.k[1];
+		const V3 dir = r.dirs[combo];
+		const float dl2 = dot(dir, dir);
+		auto span = [](const std::vector<uint>& ids, uint& lo, uint& cnt)
+		{
+			if (ids.empty())
+			{
+				lo = 0;
+				cnt = 0;
+				return;
+			}
+			uint mn = kInf, mx = 0;
+			for (uint id : ids)
+			{
+				mn = std::min(mn, id);
+				mx = std::max(mx, id);
+			}
+			lo = mn;
+			cnt = mx - mn + 1;
+		};
+		std::vector<Hit> hits;
+		uint64_t tested = 0, requests = 0;
+		const bool brute = S.p.brute_force_raycast != 0;
+		const CachedBVH* fb_dst = brute ? nullptr : S.face_bvh[r.object_ids[1]].get();
+		const CachedBVH* eb_dst = brute ? nullptr : S.edge_bvh[r.object_ids[1]].get();
+		const CachedBVH* fb_src = brute ? nullptr : S.face_bvh[r.object_ids[0]].get();
+		// VF
+		if (!r.cand_f[1].empty())
+		{
+			VertRequest q{};
+			span(r.cand_f[1], q.target_lo, q.target_cnt);
+			q.dir = dir;
+			q.fv = false;
+			q.targets = &r.cand_f[1];
+			q.hop = &r.hop[1];
+			q.max_hop = r.k[1];
+			for (uint v : r.cand_v[0])
+			{
+				q.vid = v;
+				cast_vert(m, fb_dst, q, hits, tested);
+				requests++;
+			}
+		}
+		// EE
+		if (!r.cand_e[1].empty())
+		{
+			float pmin = std::numeric_limits<float>::max(), pmax = -std::numeric_limits<float>::max();
+			for (uint e : r.cand_e[1])
+			{
+				const float a = dot(load3(m.x, edge_of(m, e, 0)), dir), b = dot(load3(m.x, edge_of(m, e, 1)), dir);
+				pmin = std::fmin(pmin, std::fmin(a, b));
+				pmax = std::fmax(pmax, std::fmax(a, b));
+			}
+			EdgeRequest q{};
+			span(r.cand_e[1], q.target_lo, q.target_cnt);
+			q.dir = dir;
+			q.targets = &r.cand_e[1];
+			q.hop = &r.hop[1];
+			q.max_hop = r.k[1];
+			q.target_proj_min = pmin;
+			for (uint e : r.cand_e[0])
+			{
+				q.eid = e;
+				if (dl2 <= 1e-12f)
+					q.max_dist = 1.0f;
+				else
+				{
+					const float smin = std::fmin(dot(load3(m.x, edge_of(m, e, 0)), dir), dot(load3(m.x, edge_of(m, e, 1)), dir));
+					q.max_dist = std::fmin(std::fmax((pmax - smin) / dl2 + 1e-5f, 0.0f), 1.0f);
+				}
+				cast_edge(m, eb_dst, q, hits, tested);
+				requests++;
+			}
+		}
+		// FV
+		if (!r.cand_f[0].empty())
+		{
+			VertRequest q{};
+			span(r.cand_f[0], q.target_lo, q.target_cnt);
+			q.dir = dir;
+			q.fv = true;
+			q.targets = &r.cand_f[0];
+			q.hop = &r.hop[0];
+			q.max_hop = r.k[0];
+			for (uint v : r.cand_v[1])
+			{
+				q.vid = v;
+				cast_vert(m, fb_src, q, hits, tested);
+				requests++;
+			}
+		}
+		{
+			std::lock_guard<std::mutex> lock(S.mtx);
+			S.tested += tested;
+			S.requests += requests;
+		}
+		info.unculled = uint(hits.size());
+		if (hits.empty())
+			return info;
+		// boundary attachment (is_hit_adj_contour), src mesh role 0
+		const uint c = r.contour_idx;
+		auto flag = [&](uint v, uint mi)
+		{
+			const auto& f = S.vflags[v];
+			return std::binary_search(f.begin(), f.end(), 2 * c + mi);
+		};
+		std::vector<uint8_t> attached(hits.size());
+		for (size_t i = 0; i < hits.size(); i++)
+		{
+			const Hit& h = hits[i];
+			bool ok = true;
+			for (int k = 0; k < 3; k++)
+				if (h.sv[k] != kInf)
+					ok = ok && flag(h.sv[k], 0);
+			for (int k = 0; k < 3; k++)
+				if (h.dv[k] != kInf)
+					ok = ok && flag(h.dv[k], 1);
+			attached[i] = ok;
+		}
+		// components
+		HitIndex ix;
+		ix.build(hits);
+		std::vector<uint8_t> vis(hits.size(), 0);
+		std::vector<uint> nb;
+		uint best_cov = 0, best_n = 0;
+		uint64_t best_key = ~0ull;
+		bool found = false;
+		std::vector<uint> best_comp;
+		for (uint seed = 0; seed < hits.size(); seed++)
+		{
+			if (vis[seed])
+				continue;
+			std::vector<uint> comp, todo{ seed };
+			vis[seed] = 1;
+			bool att = false;
+			while (!todo.empty())
+			{
+				const uint i = todo.back();
+				todo.pop_back();
+				comp.push_back(i);
+				att = att || attached[i];
+				nb.clear();
+				hit_neighbours(m, hits, ix, i, nb);
+				for (uint j : nb)
+					if (!vis[j])
+					{
+						vis[j] = 1;
+						todo.push_back(j);
+					}
+			}
+			if (!att)
+				continue;
+			// coverage of this component
+			std::set<uint> sup[2];
+			uint64_t key = ~0ull;
+			for (uint i : comp)
+			{
+				const Hit& h = hits[i];
+				key = std::min(key, h.key());
+				for (int k = 0; k < 3; k++)
+					if (h.sv[k] != kInf)
+						sup[0].insert(h.sv[k]);
+				for (int k = 0; k < 3; k++)
+					if (h.dv[k] != kInf)
+						sup[1].insert(h.dv[k]);
+			}
+			uint cov = 0;
+			for (uint p : r.contour)
+			{
+				const uint mi = S.mesh_index[p];
+				const EfPair& e = S.ef[p];
+				const bool eo = sup[mi].count(e.idx[0]) || sup[mi].count(e.idx[1]);
+				const bool fo = sup[mi ^ 1].count(e.idx[2]) || sup[mi ^ 1].count(e.idx[3]) || sup[mi ^ 1].count(e.idx[4]);
+				cov += (eo && fo) ? 1 : 0;
+			}
+			const uint nh = uint(comp.size());
+			const bool better = !found || cov > best_cov || (cov == best_cov && nh > best_n) || (cov == best_cov && nh == best_n && key < best_key);
+			if (better)
+			{
+				found = true;
+				best_cov = cov;
+				best_n = nh;
+				best_key = key;
+				best_comp = comp;
+			}
+		}
+		if (!found)
+			return info;
+		for (uint i : best_comp)
+			info.hits.push_back(hits[i]);
+		fill_metrics(S, r, info);
+		return info;
+	}
+
+	// evaluate_current_runtime_directions_template (intersection_resolver2.cpp:1058-1230)
+	void evaluate_directions(Scene& S, std::vector<uint>& batch)
+	{
+		uint max_combo = 0;
+		for (uint c : batch)
+		{
+			Runtime& r = S.rt[c];
+			r.k[0] = r.init_k[0];
+			r.k[1] = r.init_k[1];
+			r.finished = false;
+			r.no_response = false;
+			max_combo = std::max(max_combo, uint(r.dirs.size()));
+			std::fill(r.converged.begin(), r.converged.end(), 0);
+			std::fill(r.pruned.begin(), r.pruned.end(), 0);
+			std::fill(r.present.begin(), r.present.end(), 0);
+			std::fill(r.results.begin(), r.results.end(), ComboInfo{});
+		}
+		auto grow = [](uint cur, uint diam) -> uint
+		{
+			if (cur >= diam)
+				return cur;
+			return uint(std::min<uint64_t>(diam, std::max<uint64_t>(1u, uint64_t(cur) * 2u)));
+		};
+		std::vector<uint> remaining = batch;
+		for (uint level = 0; !remaining.empty() && level < 65; level++)
+		{
+			parallel_for(uint(remaining.size()), [&](uint i)
+				{ build_candidates(S, S.rt[remaining[i]]); }, 1);
+			for (uint combo = 0; combo < max_combo; combo++)
+			{
+				std::vector<uint> active;
+				for (uint c : remaining)
+				{
+					const Runtime& r = S.rt[c];
+					if (combo < r.dirs.size() && !r.converged[combo] && !r.pruned[combo])
+						active.push_back(c);
+				}
+				parallel_for(uint(active.size()), [&](uint i)
+					{
+						Runtime& r = S.rt[active[i]];
+						ComboInfo info = eval_combo(S, r, combo);
+						info.levels = level + 1;
+						info.full_mesh = r.k[0] >= r.diam[0] && r.k[1] >= r.diam[1];
+						const bool usable = has_usable(info);
+						const bool src_ok = info.max_front_src < r.k[0] || r.k[0] >= r.diam[0];
+						const bool dst_ok = info.max_front_dst < r.k[1] || r.k[1] >= r.diam[1];
+						info.eligible = usable && src_ok && dst_ok;
+						r.converged[combo] = (info.eligible || info.full_mesh) ? 1 : 0;
+						r.present[combo] = 1;
+						r.results[combo] = std::move(info); }, 1);
+			}
+			std::vector<uint> next;
+			for (uint c : remaining)
+			{
+				Runtime& r = S.rt[c];
+				bool has = false;
+				float best = std::numeric_limits<float>::infinity();
+				for (size_t ci = 0; ci < r.dirs.size(); ci++)
+					if (has_valid(r.results[ci]))
+					{
+						has = true;
+						best = std::fmin(best, response_objective(r.results[ci]));
+					}
+				if (has)
+					for (size_t ci = 0; ci < r.dirs.size(); ci++)
+						if (!r.converged[ci] && r.present[ci] && response_objective(r.results[ci]) >= best)
+							r.pruned[ci] = 1;
+				bool pending = false, gs = false, gd = false;
+				for (size_t ci = 0; ci < r.dirs.size(); ci++)
+				{
+					if (r.converged[ci] || r.pruned[ci])
+						continue;
+					pending = true;
+					const ComboInfo& info = r.results[ci];
+					gs = gs || (r.k[0] < r.diam[0] && (!has_usable(info) || info.max_front_src >= r.k[0]));
+					gd = gd || (r.k[1] < r.diam[1] && (!has_usable(info) || info.max_front_dst >= r.k[1]));
+				}
+				if (!pending)
+				{
+					r.finished = true;
+					r.no_response = !has;
+					continue;
+				}
+				const uint ns = gs ? grow(r.k[0], r.diam[0]) : r.k[0];
+				const uint nd = gd ? grow(r.k[1], r.diam[1]) : r.k[1];
+				if (ns <= r.k[0] && nd <= r.k[1])
+				{
+					r.finished = true; // stalled: cannot happen when a role still grows
+					continue;
+				}
+				r.k[0] = ns;
+				r.k[1] = nd;
+				next.push_back(c);
+			}
+			remaining.swap(next);
+		}
+	}
+
+	// get_adj_contours (intersection_resolver2.cpp:413-451) for one hit
+	void adj_contours(const Scene& S, const Hit& h, uint c, std::set<uint>& out)
+	{
+		std::vector<uint> sv, dv;
+		for (int k = 0; k < 3; k++)
+			if (h.sv[k] != kInf)
+				sv.push_back(h.sv[k]);
+		for (int k = 0; k < 3; k++)
+			if (h.dv[k] != kInf)
+				dv.push_back(h.dv[k]);
+		auto inter = [&](const std::vector<uint>& vs)
+		{
+			std::vector<uint> acc = S.vflags[vs.front()];
+			for (uint v : vs)
+			{
+				std::vector<uint> t;
+				std::set_intersection(S.vflags[v].begin(), S.vflags[v].end(), acc.begin(), acc.end(), std::back_inserter(t));
+				acc.swap(t);
+			}
+			std::vector<uint> t;
+			const uint rm[2] = { 2 * c, 2 * c + 1 };
+			std::set_difference(acc.begin(), acc.end(), rm, rm + 2, std::back_inserter(t));
+			return t;
+		};
+		const auto sf = inter(sv), df = inter(dv);
+		for (uint a : sf)
+			for (uint b : df)
+				if (a == (b ^ 1u))
+					out.insert(a / 2);
+	}
+
+	void run(Scene& S)
+	{
+		const MeshIn& m = S.m;
+		preprocess(S);
+		contours(S);
+		normals(S);
+		const uint nc = uint(S.contours.size());
+		S.rt.resize(nc);
+		S.selected.assign(nc, ComboInfo{});
+		S.processed.assign(nc, 0);
+		S.suppressed.assign(nc, 0);
+		S.pre_area.assign(nc, 0.0f);
+		S.merge_adj.assign(nc, {});
+		if (!S.p.brute_force_raycast)
+		{
+			S.face_bvh.resize(m.num_objects);
+			S.edge_bvh.resize(m.num_objects);
+			parallel_for(m.num_objects * 2, [&](uint i)
+				{
+					const uint obj = i / 2;
+					std::vector<uint> ids;
+					if (i % 2 == 0)
+					{
+						for (uint f = m.prefix_faces[obj]; f < m.prefix_faces[obj + 1]; f++) ids.push_back(f);
+						S.face_bvh[obj] = std::make_unique<CachedBVH>();
+						S.face_bvh[obj]->build(ids, m, true);
+					}
+					else
+					{
+						for (uint e = m.prefix_edges[obj]; e < m.prefix_edges[obj + 1]; e++) ids.push_back(e);
+						S.edge_bvh[obj] = std::make_unique<CachedBVH>();
+						S.edge_bvh[obj]->build(ids, m, false);
+					} }, 1);
+		}
+		std::vector<uint> active;
+		for (uint c = 0; c < nc && c < S.p.max_contours; c++)
+			active.push_back(c);
+		const uint bs = std::max(1u, S.p.batch_size);
+		for (size_t b0 = 0; b0 < active.size(); b0 += bs)
+		{
+			std::vector<uint> batch(active.begin() + b0, active.begin() + std::min(active.size(), b0 + bs));
+			parallel_for(uint(batch.size()), [&](uint i)
+				{ init_runtime(S, S.rt[batch[i]], batch[i]); }, 1);
+			evaluate_directions(S, batch);
+			// select_runtime_best_results + pre-finalize merge capture + finalize
+			for (uint c : batch)
+			{
+				Runtime& r = S.rt[c];
+				S.processed[c] = 1;
+				int sel = -1;
+				for (size_t ci = 0; ci < r.results.size(); ci++)
+				{
+					if (!has_valid(r.results[ci]))
+						continue;
+					if (sel < 0 || response_is_better(r.results[ci], r.results[sel]))
+						sel = int(ci);
+				}
+				ComboInfo best;
+				if (sel >= 0)
+					best = r.results[sel];
+				S.selected[c] = best;
+				S.pre_area[c] = best.area;
+				std::set<uint> adjc;
+				for (const Hit& h : best.hits)
+				{
+					std::set<uint> t;
+					adj_contours(S, h, c, t);
+					for (uint o : t)
+					{
+						// same unordered object pair; a contour whose runtime was never built
+						// (a later batch, or past max_contours) has no object ids yet and
+						// never matches (contour_object_ids sentinel, resolver2.cpp:472-481)
+						if (o == c || o >= nc || o >= b0 + batch.size())
+							continue;
+						const Runtime& ro = S.rt[o];
+						if (std::min(ro.object_ids[0], ro.object_ids[1]) == std::min(r.object_ids[0], r.object_ids[1])
+							&& std::max(ro.object_ids[0], ro.object_ids[1]) == std::max(r.object_ids[0], r.object_ids[1]))
+							adjc.insert(o);
+					}
+				}
+				S.merge_adj[c].assign(adjc.begin(), adjc.end());
+				// finalize: re-evaluate the selected support (identical arithmetic here)
+				if (sel >= 0)
+					fill_metrics(S, r, S.selected[c]);
+			}
+			for (uint c : batch)
+			{
+				Runtime& r = S.rt[c];
+				r.hop[0].clear();
+				r.hop[1].clear();
+				r.geo[0].clear();
+				r.geo[1].clear();
+				r.cur_dist[0].clear();
+				r.cur_dist[1].clear();
+			}
+		}
+		// suppression (prp_select_pre_finalize_contours_to_suppress)
+		std::vector<uint> conflicting;
+		for (uint c : active)
+			if (!S.merge_adj[c].empty())
+				conflicting.push_back(c);
+		std::sort(conflicting.begin(), conflicting.end(), [&](uint a, uint b)
+			{
+				if (S.pre_area[a] != S.pre_area[b]) return S.pre_area[a] > S.pre_area[b];
+				return a < b; });
+		std::vector<uint8_t> is_active(nc, 0);
+		for (uint c : active)
+			is_active[c] = 1;
+		for (uint owner : conflicting)
+		{
+			if (S.suppressed[owner])
+				continue;
+			for (uint a : S.merge_adj[owner])
+				if (a != owner && is_active[a])
+					S.suppressed[a] = 1;
+		}
+		for (uint c = 0; c < nc; c++)
+			if (S.suppressed[c])
+				S.selected[c] = ComboInfo{};
+	}
+} // namespace
+
+// ---- C ABI of the oracle (ctypes) --------------------------------------------------
+struct OraclePrpResult
+{
+	uint contour_idx, contour_type, num_pairs, combo_idx;
+	uint num_dirs, hit_count, unculled_hit_count, covered_anchor_count;
+	uint boundary_anchor_count, eval_k_src, eval_k_dst, max_frontier_hop_src;
+	uint max_frontier_hop_dst, expansion_level_count, flags, object_id0;
+	uint object_id1, init_k_src, init_k_dst, diam_src;
+	uint diam_dst, num_boundary_src, num_boundary_dst, reserved;
+	float dir[3];
+	float depth, volume, objective, area, displacement_cost, coverage, normalized_objective, pre_finalize_area;
+	float reserved_f;
+};
+static_assert(sizeof(OraclePrpResult) == 24 * 4 + 12 * 4, "result record");
+
+struct OracleHitRec
+{
+	uint type, src_id, dst_id, sv[3], dv[3];
+	float bary[2], dist;
+};
+static_assert(sizeof(OracleHitRec) == 48, "hit record");
+
+extern "C"
+{
+	void* oracle_prp_run(const MeshIn* mesh, const void* ef_pairs, const uint* ef_indices, uint num_pairs, const Params* params)
+	{
+		Scene* S = new Scene();
+		S->m = *mesh;
+		S->p = *params;
+		const EfPair* e = static_cast<const EfPair*>(ef_pairs);
+		S->ef.assign(e, e + num_pairs);
+		for (uint i = 0; i < num_pairs; i++)
+		{
+			S->ef_e.push_back(ef_indices[2 * i]);
+			S->ef_f.push_back(ef_indices[2 * i + 1]);
+		}
+		run(*S);
+		return S;
+	}
+	void oracle_prp_free(void* h) { delete static_cast<Scene*>(h); }
+	uint oracle_prp_num_pairs(void* h) { return uint(static_cast<Scene*>(h)->ef.size()); }
+	uint oracle_prp_num_orig_pairs(void* h) { return static_cast<Scene*>(h)->num_orig_pairs; }
+	void oracle_prp_pairs(void* h, void* out_pairs, uint* out_idx, uint* out_mesh_index, uint* out_contour_index, float* out_len)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		for (size_t i = 0; i < S->ef.size(); i++)
+		{
+			static_cast<EfPair*>(out_pairs)[i] = S->ef[i];
+			out_idx[2 * i] = S->ef_e[i];
+			out_idx[2 * i + 1] = S->ef_f[i];
+			out_mesh_index[i] = S->mesh_index[i];
+			out_contour_index[i] = S->contour_index[i];
+			out_len[i] = S->length[i];
+		}
+	}
+	uint oracle_prp_num_contours(void* h) { return uint(static_cast<Scene*>(h)->contours.size()); }
+	uint oracle_prp_contour(void* h, uint c, uint* out)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		const auto& v = S->contours[c];
+		if (out)
+			std::copy(v.begin(), v.end(), out);
+		return uint(v.size());
+	}
+	void oracle_prp_result(void* h, uint c, OraclePrpResult* out)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		OraclePrpResult r{};
+		const ComboInfo& s = S->selected[c];
+		r.contour_idx = c;
+		r.contour_type = S->contour_type[c];
+		r.num_pairs = uint(S->contours[c].size());
+		r.combo_idx = s.present && !s.hits.empty() ? s.combo_idx : 0xFFFFFFFFu;
+		r.hit_count = uint(s.hits.size());
+		r.unculled_hit_count = s.unculled;
+		r.covered_anchor_count = s.covered;
+		r.boundary_anchor_count = s.anchors;
+		r.eval_k_src = s.eval_k_src;
+		r.eval_k_dst = s.eval_k_dst;
+		r.max_frontier_hop_src = s.max_front_src;
+		r.max_frontier_hop_dst = s.max_front_dst;
+		r.expansion_level_count = s.levels;
+		const bool processed = c < S->processed.size() && S->processed[c];
+		const Runtime& rt = S->rt[c];
+		r.flags = (s.eligible ? 1u : 0u) | (processed && rt.no_response ? 2u : 0u) | (S->suppressed[c] ? 4u : 0u) | (s.full_mesh ? 8u : 0u) | (processed ? 16u : 0u);
+		if (processed)
+		{
+			r.num_dirs = uint(rt.dirs.size());
+			r.object_id0 = rt.object_ids[0];
+			r.object_id1 = rt.object_ids[1];
+			r.init_k_src = rt.init_k[0];
+			r.init_k_dst = rt.init_k[1];
+			r.diam_src = rt.diam[0];
+			r.diam_dst = rt.diam[1];
+			r.num_boundary_src = uint(rt.boundary[0].size());
+			r.num_boundary_dst = uint(rt.boundary[1].size());
+		}
+		r.dir[0] = s.dir.x;
+		r.dir[1] = s.dir.y;
+		r.dir[2] = s.dir.z;
+		r.depth = s.depth;
+		r.volume = s.volume;
+		r.objective = s.objective;
+		r.area = s.area;
+		r.displacement_cost = s.cost;
+		r.coverage = s.coverage;
+		r.normalized_objective = response_objective(s);
+		r.pre_finalize_area = S->pre_area[c];
+		*out = r;
+	}
+	uint oracle_prp_hits(void* h, uint c, OracleHitRec* out)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		const auto& hits = S->selected[c].hits;
+		if (out)
+			for (size_t i = 0; i < hits.size(); i++)
+			{
+				OracleHitRec& o = out[i];
+				o.type = hits[i].type;
+				o.src_id = hits[i].src_id;
+				o.dst_id = hits[i].dst_id;
+				for (int k = 0; k < 3; k++)
+				{
+					o.sv[k] = hits[i].sv[k];
+					o.dv[k] = hits[i].dv[k];
+				}
+				o.bary[0] = hits[i].bary[0];
+				o.bary[1] = hits[i].bary[1];
+				o.dist = hits[i].dist;
+			}
+		return uint(hits.size());
+	}
+	uint oracle_prp_directions(void* h, uint c, float* out)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		const auto& d = S->rt[c].dirs;
+		if (out)
+			for (size_t i = 0; i < d.size(); i++)
+			{
+				out[3 * i] = d[i].x;
+				out[3 * i + 1] = d[i].y;
+				out[3 * i + 2] = d[i].z;
+			}
+		return uint(d.size());
+	}
+	void oracle_prp_stats(void* h, uint64_t* out2)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		out2[0] = S->tested;
+		out2[1] = S->requests;
+	}
+	void oracle_eigen3(const float* S9, float* out9)
+	{
+		Mat3 S;
+		for (int c = 0; c < 3; c++)
+			S.c[c] = v3(S9[3 * c], S9[3 * c + 1], S9[3 * c + 2]);
+		V3 ev[3];
+		all_eigenvectors(S, ev);
+		for (int k = 0; k < 3; k++)
+		{
+			out9[3 * k] = ev[k].x;
+			out9[3 * k + 1] = ev[k].y;
+			out9[3 * k + 2] = ev[k].z;
+		}
+	}
+}

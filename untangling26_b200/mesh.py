@@ -16,7 +16,27 @@ them. Ordering matters because later stages iterate adjacency lists in order:
 
 Adjacency lists are CSR pairs (offsets[n+1], data[...]) of uint32 numpy arrays.
 """
+import ctypes
+
 import numpy as np
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f32p = ctypes.POINTER(ctypes.c_float)
+
+
+class MeshDesc(ctypes.Structure):
+    """u26_mesh_desc of include/u26.h: host pointers to the mesh tables."""
+    _fields_ = [
+        ("num_verts", ctypes.c_uint32), ("num_edges", ctypes.c_uint32), ("num_faces", ctypes.c_uint32),
+        ("num_objects", ctypes.c_uint32),
+        ("x", _f32p), ("rest_x", _f32p), ("edges", _u32p), ("faces", _u32p), ("face_adj_edges", _u32p),
+        ("vav_off", _u32p), ("vav", _u32p), ("vae_off", _u32p), ("vae", _u32p), ("vaf_off", _u32p), ("vaf", _u32p),
+        ("eaf_off", _u32p), ("eaf", _u32p), ("eae_off", _u32p), ("eae", _u32p),
+        ("prefix_verts", _u32p), ("prefix_edges", _u32p), ("prefix_faces", _u32p),
+        ("vert_object", _u32p), ("vert_component", _u32p),
+        ("rest_vert_area", _f32p), ("rest_edge_area", _f32p), ("rest_face_area", _f32p), ("vert_mass", _f32p),
+        ("mesh_orientation", _u32p),
+    ]
 
 
 class CSR:
@@ -123,6 +143,76 @@ class Mesh:
         for j in range(3):
             np.add.at(ea, fae[:, j], fa64 / 3.0)
         self.rest_edge_area = ea.astype(np.float32)
+
+        # per-object primitive ranges (edges and faces come grouped by object)
+        eobj = self.object_of_vert[self.edges[:, 0]] if ne else np.zeros(0, np.uint32)
+        fobj = self.object_of_vert[self.faces[:, 0]] if nf else np.zeros(0, np.uint32)
+        self.prefix_num_edges = np.searchsorted(eobj, np.arange(self.num_objects + 1)).astype(np.uint32)
+        self.prefix_num_faces = np.searchsorted(fobj, np.arange(self.num_objects + 1)).astype(np.uint32)
+        if not (np.all(np.diff(eobj.astype(np.int64)) >= 0) and np.all(np.diff(fobj.astype(np.int64)) >= 0)):
+            raise ValueError("edges and faces must be grouped by object (objects own contiguous vertex ranges)")
+        # unit density and thickness: vertex mass = rest vertex area
+        self.vert_mass = self.rest_vert_area.copy()
+        self.mesh_orientation = np.zeros(max(self.num_objects, 1), np.uint32)
+        self.vert_component = self._components()
+
+    def _components(self):
+        """Connected components of the vertex graph, numbered per object in vertex order."""
+        from scipy.sparse import csr_matrix
+        from scipy.sparse.csgraph import connected_components
+        nv = self.num_verts
+        off, data = self.vert_adj_verts.offsets.astype(np.int64), self.vert_adj_verts.data.astype(np.int64)
+        g = csr_matrix((np.ones(len(data), np.int8), data, off), shape=(nv, nv))
+        _, labels = connected_components(g, directed=False)
+        # relabel by first vertex so that components count up in vertex order inside an object
+        first = np.full(labels.max() + 1 if nv else 0, nv, np.int64)
+        np.minimum.at(first, labels, np.arange(nv))
+        order = np.argsort(first, kind="stable")
+        rank = np.empty_like(order)
+        rank[order] = np.arange(len(order))
+        lab = rank[labels]
+        comp = np.zeros(nv, np.uint32)
+        for obj in range(self.num_objects):
+            lo, hi = int(self.prefix_num_verts[obj]), int(self.prefix_num_verts[obj + 1])
+            if hi > lo:
+                comp[lo:hi] = (lab[lo:hi] - lab[lo:hi].min()).astype(np.uint32)
+        return comp
+
+    def desc(self, x=None):
+        """ctypes MeshDesc over this mesh's host arrays (keeps references alive)."""
+        d = MeshDesc()
+        keep = []
+
+        def p(a, t=ctypes.c_uint32):
+            a = np.ascontiguousarray(a)
+            keep.append(a)
+            return a.ctypes.data_as(ctypes.POINTER(t))
+
+        xx = self.x if x is None else np.ascontiguousarray(x, dtype=np.float32)
+        d.num_verts, d.num_edges, d.num_faces, d.num_objects = self.num_verts, self.num_edges, self.num_faces, self.num_objects
+        d.x = p(xx, ctypes.c_float)
+        d.rest_x = p(self.rest_x, ctypes.c_float)
+        d.edges = p(self.edges)
+        d.faces = p(self.faces)
+        d.face_adj_edges = p(self.face_adj_edges)
+        for name in ("vert_adj_verts", "vert_adj_edges", "vert_adj_faces", "edge_adj_faces_ext", "edge_adj_edges_ext"):
+            csr = getattr(self, name)
+            short = {"vert_adj_verts": "vav", "vert_adj_edges": "vae", "vert_adj_faces": "vaf",
+                     "edge_adj_faces_ext": "eaf", "edge_adj_edges_ext": "eae"}[name]
+            setattr(d, short + "_off", p(csr.offsets))
+            setattr(d, short, p(csr.data))
+        d.prefix_verts = p(self.prefix_num_verts)
+        d.prefix_edges = p(self.prefix_num_edges)
+        d.prefix_faces = p(self.prefix_num_faces)
+        d.vert_object = p(self.object_of_vert)
+        d.vert_component = p(self.vert_component)
+        d.rest_vert_area = p(self.rest_vert_area, ctypes.c_float)
+        d.rest_edge_area = p(self.rest_edge_area, ctypes.c_float)
+        d.rest_face_area = p(self.rest_face_area, ctypes.c_float)
+        d.vert_mass = p(self.vert_mass, ctypes.c_float)
+        d.mesh_orientation = p(self.mesh_orientation)
+        d._keep = keep
+        return d
 
     def device_arrays(self, device="cuda"):
         """torch tensors of the arrays the kernels read."""
