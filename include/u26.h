@@ -103,7 +103,6 @@ U26_API u26_status u26_lbvh_update_and_refit(u26_lbvh* tree, const float* thickn
 U26_API u26_status u26_lbvh_query(u26_lbvh* tree, int mode, const float* x_begin, const float* x_end,
 	const uint32_t* edges, uint32_t num_queries, const float* d_hat, const float* thickness, uint32_t* count,
 	uint32_t* pairs, uint32_t max_pairs);
-/* LBVH::check_health (lbvh.cpp:1081-1085). Synchronises. *healthy = 1 or 0. */
 /* Tree options (no reference counterpart; defaults reproduce the reference):
  *   U26_LBVH_OPT_FULL_GLOBAL_AABB = 1: normalise Morton codes by the AABB of ALL leaves
  *   instead of the reference's first ceil(num_verts/256) blocks (lbvh.cpp:999-1021).
@@ -111,6 +110,7 @@ U26_API u26_status u26_lbvh_query(u26_lbvh* tree, int mode, const float* x_begin
  *   traversal stack overflows); the tree is better balanced in space. */
 #define U26_LBVH_OPT_FULL_GLOBAL_AABB 1
 U26_API u26_status u26_lbvh_set_option(u26_lbvh* tree, int option, int value);
+/* LBVH::check_health (lbvh.cpp:1081-1085). Synchronises. *healthy = 1 or 0. */
 U26_API u26_status u26_lbvh_check_health(u26_lbvh* tree, int* healthy);
 
 typedef struct u26_lbvh_arrays
@@ -156,5 +156,110 @@ U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint
  * host value; num_edges/num_faces bound the key. Pairs and indices are permuted in place. */
 U26_API u26_status u26_ef_canonicalize(u26_ctx* ctx, uint32_t count, void* ef_pairs, uint32_t* ef_indices,
 	uint32_t num_edges, uint32_t num_faces);
+
+/* ---- PRP contour evaluation ---------------------------------------------------------
+ * The reference's IntersectionResolver::host_resolve with the PRP method
+ * (intersection_resolver.cpp:2131-2218 -> host_resolve_intersections_PRP,
+ * intersection_resolver2.cpp:2750-4072, or device_resolve_intersections_PRP,
+ * intersection_resolver_gpu.cpp:2792-4460): EF preprocessing and contours, per-contour
+ * runtime (hop/geodesic distances, candidate directions), adaptive k-ring evaluation of
+ * every (contour, direction) with VF/EE/FV ray casting, product-complex cluster culling
+ * and J(r), selection, cross-contour suppression.
+ *
+ * Mesh tables are HOST pointers in the reference's conventions (MeshData, built once per
+ * scene by its initialiser, init_mesh_data.cpp:294-835); u26_scene_create uploads them. */
+typedef struct u26_mesh_desc
+{
+	uint32_t num_verts, num_edges, num_faces, num_objects;
+	const float* x;				  /* [V][3] current positions (used only by host-side stages) */
+	const float* rest_x;		  /* [V][3] rest positions (geodesic distances) */
+	const uint32_t* edges;		  /* [E][2] sorted unique, grouped by object */
+	const uint32_t* faces;		  /* [F][3] grouped by object */
+	const uint32_t* face_adj_edges; /* [F][3] edge of (face[j], face[j+1]) */
+	const uint32_t *vert_adj_verts_offsets, *vert_adj_verts; /* CSR, edge-id order */
+	const uint32_t *vert_adj_edges_offsets, *vert_adj_edges; /* CSR, ascending */
+	const uint32_t *vert_adj_faces_offsets, *vert_adj_faces; /* CSR, ascending */
+	const uint32_t *edge_adj_faces_offsets, *edge_adj_faces; /* CSR, edge_adj_faces_ext */
+	const uint32_t *edge_adj_edges_offsets, *edge_adj_edges; /* CSR, edge_adj_edges_ext */
+	const uint32_t *prefix_num_verts, *prefix_num_edges, *prefix_num_faces; /* [objects+1] */
+	const uint32_t* vert_object;	/* sa_vert_mesh_id */
+	const uint32_t* vert_component; /* vert_topology_component_id */
+	const float *rest_vert_area, *rest_edge_area, *rest_face_area, *vert_mass;
+	const uint32_t* mesh_orientation; /* [objects] 0: normals along the triangle winding */
+} u26_mesh_desc;
+
+typedef struct u26_scene u26_scene;
+U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* mesh, u26_scene** out);
+U26_API void u26_scene_destroy(u26_scene* scene);
+
+/* SceneParams fields of the PRP path (scene_params.h:65-81). */
+typedef struct u26_prp_params
+{
+	uint32_t max_contours;		/* untangling_process_contours_count (256) */
+	uint32_t direction_mode;	/* 0: the reference's seed directions (resolver2.cpp:1488-1569); 1: 26 lattice directions */
+	uint32_t use_ccr;			/* PRP_use_intrinsic_contour_side_candidates (1) */
+	float ccr_tau;				/* PRP_intrinsic_tau (0.25) */
+	uint32_t ccr_use_rest;		/* PRP_use_rest_geodesic_distance_for_intrinsic_candidates (1) */
+	uint32_t ccr_use_current;	/* PRP_use_deformed_boundary_distance_for_intrinsic_candidates (1) */
+	uint32_t batch_size;		/* PRP_cpu_contour_batch_size; results do not depend on it */
+	uint32_t reserved;
+} u26_prp_params;
+
+/* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:
+ * 1 response_eligible, 2 no_response_terminal, 4 suppressed, 8 full_mesh_evaluated,
+ * 16 processed (contour index < max_contours). combo_idx = ~0 when there is no response. */
+typedef struct u26_prp_result
+{
+	uint32_t contour_idx, contour_type, num_pairs, combo_idx;
+	uint32_t num_dirs, hit_count, unculled_hit_count, covered_anchor_count;
+	uint32_t boundary_anchor_count, eval_k_src, eval_k_dst, max_frontier_hop_src;
+	uint32_t max_frontier_hop_dst, expansion_level_count, flags, object_id0;
+	uint32_t object_id1, init_k_src, init_k_dst, diam_src;
+	uint32_t diam_dst, num_boundary_src, num_boundary_dst, reserved;
+	float dir[3];
+	float depth, volume, objective, area, displacement_cost, coverage, normalized_objective, pre_finalize_area;
+	float reserved_f;
+} u26_prp_result;
+
+/* One hit of a selected support S(r) (RayCasting::HitInfo, intersection_resolver_helper.h:260-449,
+ * without the group and direction fields). type 0 VF, 1 EE, 2 FV; unused vertex slots ~0. */
+typedef struct u26_prp_hit
+{
+	uint32_t type, src_id, dst_id, src_verts[3], dst_verts[3];
+	float bary[2], dist;
+} u26_prp_hit;
+
+typedef struct u26_prp_output u26_prp_output;
+typedef struct u26_prp_output_view
+{
+	uint32_t num_pairs, num_orig_pairs, num_contours, num_hits;
+	const void* pairs;				 /* [num_pairs] 48-B EF pairs, loop-vertex pairs appended */
+	const uint32_t* pair_indices;	 /* [num_pairs][2] (eid, fid) */
+	const uint32_t* mesh_index;		 /* [num_pairs] ef_pair_mesh_index */
+	const uint32_t* contour_index;	 /* [num_pairs] ef_pair_contour_index */
+	const float* pair_length;		 /* [num_pairs] ef_pair_length */
+	const uint32_t* contour_offsets; /* [num_contours+1] into contour_pairs */
+	const uint32_t* contour_pairs;	 /* pair ids of each contour in flood-fill order */
+	const u26_prp_result* results;	 /* [num_contours] */
+	const uint32_t* hit_offsets;	 /* [num_contours+1] into hits */
+	const u26_prp_hit* hits;		 /* selected supports, canonical (type, src, dst) order */
+	const float* directions;		 /* [num_contours][26][3] candidate directions (num_dirs used) */
+	uint64_t ray_tests;				 /* leaf primitive tests of all ray casts */
+	uint64_t ray_requests;			 /* VF + EE + FV ray requests */
+	uint32_t levels;				 /* k-ring levels evaluated (max over batches) */
+	uint32_t device_error_flags;
+	double stage_ms[8];				 /* host wall time per stage: preprocess, runtime, candidates, raycast, cull, control, finalize, total */
+} u26_prp_output_view;
+
+/* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any
+ * thickness >= 0; ray casting only needs boxes that contain the primitives). x: DEVICE
+ * positions [V][3]; ef_pairs / ef_indices: DEVICE canonical EF list (u26_ef_canonicalize)
+ * of num_pairs entries. Synchronises; *out owns the host-side results until
+ * u26_prp_output_destroy. */
+U26_API u26_status u26_prp_resolve(u26_scene* scene, u26_lbvh* face_tree, u26_lbvh* edge_tree, const float* x,
+	const void* ef_pairs, const uint32_t* ef_indices, uint32_t num_pairs, const u26_prp_params* params,
+	u26_prp_output** out);
+U26_API u26_status u26_prp_output_view_get(const u26_prp_output* out, u26_prp_output_view* view);
+U26_API void u26_prp_output_destroy(u26_prp_output* out);
 
 #endif /* U26_H */

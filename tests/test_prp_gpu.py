@@ -1,0 +1,76 @@
+"""PRP contour evaluation on the GPU (C ABI u26_prp_resolve) against the CPU oracle.
+
+Bit-exact: augmented EF list (loop-vertex pairs), contour flood fill and mesh parity,
+candidate directions, per-contour results (selected direction, k-ring levels, J, depth,
+volume, area, displacement cost, coverage, flags) and the selected hit sets S(r).
+"""
+import numpy as np
+import pytest
+
+from untangling26_b200 import synthetic
+from untangling26_b200.intersection_resolver import CollisionScene
+from untangling26_b200.prp import prp_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_both(oracle, ctx, mesh, **kw):
+    sc = CollisionScene(ctx, mesh, d_hat=1e-3, thickness=0.0)
+    sc.construct_lbvh()
+    res = sc.untangle_pass(prp_params(**kw))
+    ef_ref, idx_ref = oracle.detect_ef(mesh)
+    ref = oracle.PrpRun(mesh, ef_ref, idx_ref, oracle.prp_params(**kw))
+    sc.close()
+    return res, ref
+
+
+def _compare(res, ref):
+    assert res.num_orig_pairs == ref.num_orig_pairs
+    assert res.pairs.tobytes() == ref.pairs.tobytes()
+    assert np.array_equal(res.pair_indices, ref.pair_indices)
+    assert np.array_equal(res.mesh_index, ref.mesh_index)
+    assert np.array_equal(res.contour_index, ref.contour_index)
+    assert res.pair_length.tobytes() == ref.pair_length.tobytes()
+    assert len(res.contours) == len(ref.contours)
+    for a, b in zip(res.contours, ref.contours):
+        assert np.array_equal(a, b)
+    for c in range(len(ref.contours)):
+        ra, rb = res.results[c], ref.results[c]
+        for name in ref.results.dtype.names:
+            if name.startswith("reserved"):
+                continue
+            assert np.array_equal(ra[name], rb[name]), f"contour {c} field {name}: gpu {ra[name]} oracle {rb[name]}"
+        assert res.directions[c].tobytes() == ref.directions[c].tobytes(), f"contour {c} directions"
+        assert res.hits[c].tobytes() == ref.hits[c].tobytes(), f"contour {c} hit set"
+
+
+@pytest.mark.parametrize("n,seed", [(32, 0), (64, 0), (64, 3)])
+def test_prp_two_sheets(oracle, u26ctx, n, seed):
+    m = synthetic.two_sheets(n, seed=seed)
+    res, ref = _run_both(oracle, u26ctx, m)
+    assert len(ref.contours) > 0
+    assert any(r["hit_count"] > 0 for r in ref.results)
+    _compare(res, ref)
+    assert res.device_error_flags == 0
+
+
+def test_prp_two_sheets_26_directions(oracle, u26ctx):
+    m = synthetic.two_sheets(32, seed=1)
+    res, ref = _run_both(oracle, u26ctx, m, direction_mode=1)
+    assert all(r["num_dirs"] == 26 for r in ref.results if r["flags"] & 16)
+    _compare(res, ref)
+
+
+@pytest.mark.parametrize("ccr", [(1, 1, 1), (1, 1, 0), (0, 0, 0)])
+def test_prp_folded_sheet(oracle, u26ctx, ccr):
+    m = synthetic.folded_sheet(48, seed=2)
+    res, ref = _run_both(oracle, u26ctx, m, use_ccr=ccr[0], ccr_use_rest=ccr[1], ccr_use_current=ccr[2], max_contours=64)
+    assert len(ref.contours) > 1
+    _compare(res, ref)
+
+
+def test_prp_no_intersections(oracle, u26ctx):
+    m = synthetic.two_sheets(16, seed=0)
+    m.x[m.num_verts // 2:, 2] += 3.0
+    res, ref = _run_both(oracle, u26ctx, m)
+    assert len(res.contours) == 0 and len(ref.contours) == 0

@@ -64,6 +64,11 @@ _SIGS = {
     "u26_ef_narrow_phase": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32]),
     "u26_ef_detect": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "u26_lbvh_set_option": (c_int, [c_vp, c_int, c_int]),
+    "u26_scene_create": (c_int, [c_vp, c_vp, ctypes.POINTER(c_vp)]),
+    "u26_scene_destroy": (None, [c_vp]),
+    "u26_prp_resolve": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp, ctypes.POINTER(c_vp)]),
+    "u26_prp_output_view_get": (c_int, [c_vp, c_vp]),
+    "u26_prp_output_destroy": (None, [c_vp]),
     "u26_ef_canonicalize": (c_int, [c_vp, c_u32, c_vp, c_vp, c_u32, c_u32]),
 }
 

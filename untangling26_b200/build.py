@@ -17,7 +17,7 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
-    "-Xcompiler", "-fPIC,-fvisibility=hidden,-O2",
+    "-Xcompiler", "-fPIC,-fvisibility=hidden,-O2,-ffp-contract=off",
     "-shared",
 ]
 

@@ -148,3 +148,50 @@ class CollisionScene:
         """Canonical EF pairs (numpy) of the last detection."""
         n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
         return self.resolver.download(n)
+
+    # ---- PRP contour evaluation (IntersectionResolver::host_resolve, intersection_resolver.cpp:2131-2218)
+    def _ensure_prp_scene(self):
+        if getattr(self, "prp_scene", None) is None:
+            desc = self.mesh.desc()
+            h = ctypes.c_void_p()
+            self.ctx.check(self.ctx.lib.u26_scene_create(self.ctx.handle, ctypes.byref(desc), ctypes.byref(h)), "scene_create")
+            self.prp_scene = h
+            self._desc = desc
+
+    def host_resolve(self, params=None, num_pairs=None):
+        """PRP pass over the canonical EF list of the last detection (call ef_pairs() or
+        canonicalize first). Returns a PrpResult."""
+        from .prp import PrpResult, prp_params
+        self._ensure_prp_scene()
+        params = params or prp_params()
+        n = int(self.resolver.ef_count.item()) if num_pairs is None else num_pairs
+        # the edge tree is refit at x for the EE ray casts (the face tree already is)
+        self.edge_tree.update_and_refit(self.thickness, self.x, self.x, self.edges)
+        out = ctypes.c_void_p()
+        self.ctx.check(self.ctx.lib.u26_prp_resolve(
+            self.prp_scene, self.face_tree.handle, self.edge_tree.handle, ptr(self.x), ptr(self.resolver.ef_list),
+            ptr(self.resolver.ef_indices), n, ctypes.byref(params), ctypes.byref(out)), "prp_resolve")
+        try:
+            return PrpResult(self.ctx.lib, out)
+        finally:
+            self.ctx.lib.u26_prp_output_destroy(out)
+
+    def untangle_pass(self, params=None):
+        """One untangling pass at the current positions: refit, fused EF detection,
+        canonical EF order, PRP contour evaluation."""
+        self.detect_ef_fused()
+        n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
+        return self.host_resolve(params, num_pairs=n)
+
+    def close(self):
+        if getattr(self, "prp_scene", None) is not None:
+            self.ctx.lib.u26_scene_destroy(self.prp_scene)
+            self.prp_scene = None
+        self.face_tree.close()
+        self.edge_tree.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

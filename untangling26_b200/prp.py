@@ -1,0 +1,102 @@
+"""PRP contour evaluation: Python side of u26_prp_resolve (include/u26.h).
+
+``PrpParams`` mirrors the SceneParams fields of the PRP path (scene_params.h:65-81);
+``PrpResult`` holds one pass's outputs (augmented EF list, contours, per-contour results
+and selected supports S(r)) as numpy arrays.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native as nat
+
+c_u32, c_f32, c_u64, c_vp = ctypes.c_uint32, ctypes.c_float, ctypes.c_uint64, ctypes.c_void_p
+
+
+class PrpParams(ctypes.Structure):
+    _fields_ = [
+        ("max_contours", c_u32),      # untangling_process_contours_count
+        ("direction_mode", c_u32),    # 0 reference seed directions, 1 the 26 lattice directions
+        ("use_ccr", c_u32),           # PRP_use_intrinsic_contour_side_candidates
+        ("ccr_tau", c_f32),           # PRP_intrinsic_tau
+        ("ccr_use_rest", c_u32),      # PRP_use_rest_geodesic_distance_for_intrinsic_candidates
+        ("ccr_use_current", c_u32),   # PRP_use_deformed_boundary_distance_for_intrinsic_candidates
+        ("batch_size", c_u32),        # PRP_cpu_contour_batch_size
+        ("reserved", c_u32),
+    ]
+
+
+def prp_params(**kw):
+    p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
+                  batch_size=32, reserved=0)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+RESULT_DTYPE = np.dtype([
+    ("contour_idx", np.uint32), ("contour_type", np.uint32), ("num_pairs", np.uint32), ("combo_idx", np.uint32),
+    ("num_dirs", np.uint32), ("hit_count", np.uint32), ("unculled_hit_count", np.uint32), ("covered_anchor_count", np.uint32),
+    ("boundary_anchor_count", np.uint32), ("eval_k_src", np.uint32), ("eval_k_dst", np.uint32),
+    ("max_frontier_hop_src", np.uint32), ("max_frontier_hop_dst", np.uint32), ("expansion_level_count", np.uint32),
+    ("flags", np.uint32), ("object_id0", np.uint32), ("object_id1", np.uint32), ("init_k_src", np.uint32),
+    ("init_k_dst", np.uint32), ("diam_src", np.uint32), ("diam_dst", np.uint32), ("num_boundary_src", np.uint32),
+    ("num_boundary_dst", np.uint32), ("reserved", np.uint32),
+    ("dir", np.float32, 3), ("depth", np.float32), ("volume", np.float32), ("objective", np.float32),
+    ("area", np.float32), ("displacement_cost", np.float32), ("coverage", np.float32),
+    ("normalized_objective", np.float32), ("pre_finalize_area", np.float32), ("reserved_f", np.float32)])
+HIT_DTYPE = np.dtype([("type", np.uint32), ("src_id", np.uint32), ("dst_id", np.uint32), ("sv", np.uint32, 3),
+                      ("dv", np.uint32, 3), ("bary", np.float32, 2), ("dist", np.float32)])
+EF_PAIR_DTYPE = np.dtype([("idx", np.uint32, 5), ("bary", np.float32, 3), ("grad", np.float32, 3), ("stiff", np.float32)])
+assert RESULT_DTYPE.itemsize == 144 and HIT_DTYPE.itemsize == 48
+
+STAGES = ("preprocess", "runtime", "candidates", "raycast", "cull", "control", "finalize", "total")
+
+
+class PrpOutputView(ctypes.Structure):
+    _fields_ = [
+        ("num_pairs", c_u32), ("num_orig_pairs", c_u32), ("num_contours", c_u32), ("num_hits", c_u32),
+        ("pairs", c_vp), ("pair_indices", c_vp), ("mesh_index", c_vp), ("contour_index", c_vp), ("pair_length", c_vp),
+        ("contour_offsets", c_vp), ("contour_pairs", c_vp), ("results", c_vp), ("hit_offsets", c_vp), ("hits", c_vp),
+        ("directions", c_vp), ("ray_tests", c_u64), ("ray_requests", c_u64), ("levels", c_u32),
+        ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8),
+    ]
+
+
+def _host_array(p, count, dtype):
+    if count == 0 or not p:
+        return np.zeros(0, dtype)
+    nbytes = count * np.dtype(dtype).itemsize
+    buf = (ctypes.c_char * nbytes).from_address(p)
+    return np.frombuffer(bytes(buf), dtype=dtype, count=count).copy()
+
+
+class PrpResult:
+    """One pass's outputs, copied out of the u26_prp_output handle."""
+
+    def __init__(self, lib, handle):
+        v = PrpOutputView()
+        st = lib.u26_prp_output_view_get(handle, ctypes.byref(v))
+        if st != 0:
+            raise nat.U26Error(st, "u26_prp_output_view_get")
+        n, nc, nh = v.num_pairs, v.num_contours, v.num_hits
+        self.num_orig_pairs = v.num_orig_pairs
+        self.pairs = _host_array(v.pairs, n, EF_PAIR_DTYPE)
+        self.pair_indices = _host_array(v.pair_indices, 2 * n, np.uint32).reshape(-1, 2)
+        self.mesh_index = _host_array(v.mesh_index, n, np.uint32)
+        self.contour_index = _host_array(v.contour_index, n, np.uint32)
+        self.pair_length = _host_array(v.pair_length, n, np.float32)
+        coff = _host_array(v.contour_offsets, nc + 1, np.uint32)
+        cp = _host_array(v.contour_pairs, int(coff[-1]) if nc else 0, np.uint32)
+        self.contours = [cp[coff[c]:coff[c + 1]] for c in range(nc)]
+        self.results = _host_array(v.results, nc, RESULT_DTYPE)
+        hoff = _host_array(v.hit_offsets, nc + 1, np.uint32)
+        hits = _host_array(v.hits, nh, HIT_DTYPE)
+        self.hits = [hits[hoff[c]:hoff[c + 1]] for c in range(nc)]
+        dirs = _host_array(v.directions, nc * 26 * 3, np.float32).reshape(nc, 26, 3)
+        self.directions = [dirs[c, :self.results[c]["num_dirs"]] for c in range(nc)]
+        self.tested = int(v.ray_tests)
+        self.requests = int(v.ray_requests)
+        self.levels = int(v.levels)
+        self.device_error_flags = int(v.device_error_flags)
+        self.stage_ms = dict(zip(STAGES, list(v.stage_ms)))
