@@ -157,6 +157,21 @@ U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint
 U26_API u26_status u26_ef_canonicalize(u26_ctx* ctx, uint32_t count, void* ef_pairs, uint32_t* ef_indices,
 	uint32_t num_edges, uint32_t num_faces);
 
+/* Allocation-free variant of u26_ef_canonicalize (no counterpart in the reference, which
+ * sorts on the host). For callers that cannot let the library allocate device memory: a
+ * solver that owns all GPU memory in its own arena, or a loop that must not run
+ * cudaMalloc / cudaFree because they can synchronise the device. Same result as
+ * u26_ef_canonicalize. Its scratch is a fixed array of U26_NOALLOC_SCRATCH_BYTES in
+ * the library's static device memory, held on every GPU that loads the library until the
+ * process exits; count above U26_NOALLOC_MAX_EF_PAIRS returns U26_ERR_CAPACITY. The
+ * first call on each device looks up the array's device address (make that first call
+ * before any stream capture). All calls share the one array: calls that overlap on the
+ * GPU (other streams or contexts) race and must be ordered by the caller. */
+#define U26_NOALLOC_MAX_EF_PAIRS 32768u
+#define U26_NOALLOC_SCRATCH_BYTES 2637824u
+U26_API u26_status u26_ef_canonicalize_noalloc(u26_ctx* ctx, uint32_t count, void* ef_pairs, uint32_t* ef_indices,
+	uint32_t num_edges, uint32_t num_faces);
+
 /* ---- PRP contour evaluation ---------------------------------------------------------
  * The reference's IntersectionResolver::host_resolve with the PRP method
  * (intersection_resolver.cpp:2131-2218 -> host_resolve_intersections_PRP,

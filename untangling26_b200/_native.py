@@ -64,6 +64,7 @@ _SIGS = {
     "u26_ef_narrow_phase": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32]),
     "u26_ef_detect": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp]),
     "u26_lbvh_set_option": (c_int, [c_vp, c_int, c_int]),
+    "u26_ef_canonicalize_noalloc": (c_int, [c_vp, c_u32, c_vp, c_vp, c_u32, c_u32]),
     "u26_scene_create": (c_int, [c_vp, c_vp, ctypes.POINTER(c_vp)]),
     "u26_scene_destroy": (None, [c_vp]),
     "u26_prp_resolve": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_vp, ctypes.POINTER(c_vp)]),

@@ -175,4 +175,35 @@ namespace u26
 		}
 		return U26_OK;
 	}
+
+	u26_status RadixSorter::sort_into(u26_ctx* ctx, uint64_t* keys, uint32_t* vals, uint32_t n, int bit_lo, int bit_hi,
+		uint64_t* keys_alt, uint32_t* vals_alt, uint32_t* counts)
+	{
+		if (n <= 1 || bit_hi <= bit_lo)
+			return U26_OK;
+		const uint32_t num_tiles = div_up(n, kTile);
+		uint64_t* k_src = keys;
+		uint32_t* v_src = vals;
+		uint64_t* k_dst = keys_alt;
+		uint32_t* v_dst = vals_alt;
+		for (int shift = bit_lo; shift < bit_hi; shift += 8)
+		{
+			const int bits = min(8, bit_hi - shift);
+			const uint32_t mask = (1u << bits) - 1u;
+			radix_hist_kernel<<<num_tiles, kThreads, 0, ctx->stream>>>(k_src, n, shift, mask, counts, num_tiles);
+			U26_TRY(after_launch(ctx, "radix_hist_kernel"));
+			radix_scan_kernel<<<1, 1024, 0, ctx->stream>>>(counts, 256u * num_tiles);
+			U26_TRY(after_launch(ctx, "radix_scan_kernel"));
+			radix_scatter_kernel<<<num_tiles, kThreads, 0, ctx->stream>>>(k_src, v_src, k_dst, v_dst, n, shift, mask, counts, num_tiles);
+			U26_TRY(after_launch(ctx, "radix_scatter_kernel"));
+			std::swap(k_src, k_dst);
+			std::swap(v_src, v_dst);
+		}
+		if (k_src != keys)
+		{
+			U26_CUDA(ctx, cudaMemcpyAsync(keys, k_src, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+			U26_CUDA(ctx, cudaMemcpyAsync(vals, v_src, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, ctx->stream));
+		}
+		return U26_OK;
+	}
 } // namespace u26

@@ -83,6 +83,10 @@ namespace u26
 	{
 		DevBuf keys_alt, vals_alt, counts;
 		u26_status sort(u26_ctx* ctx, uint64_t* keys, uint32_t* vals, uint32_t n, int bit_lo, int bit_hi);
+		// Same passes over caller-provided scratch (allocates nothing): keys_alt/vals_alt hold
+		// n entries, counts holds 256 * ceil(n / 2048) words. The result ends in keys/vals.
+		static u26_status sort_into(u26_ctx* ctx, uint64_t* keys, uint32_t* vals, uint32_t n, int bit_lo, int bit_hi,
+			uint64_t* keys_alt, uint32_t* vals_alt, uint32_t* counts);
 		void release()
 		{
 			keys_alt.release();
