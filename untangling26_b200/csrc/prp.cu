@@ -32,6 +32,8 @@
 //   gather_kernel             selected supports S(r) compacted for the host
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -1869,6 +1871,37 @@ static double ms_since(std::chrono::steady_clock::time_point t0)
 	return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// GPU-timeline markers of one level (read only when U26_PRP_TRACE is set)
+struct LevelEvents
+{
+	cudaEvent_t e[8] = {};
+	bool on = false;
+	explicit LevelEvents(bool enable) : on(enable)
+	{
+		if (on)
+			for (auto& x : e)
+				cudaEventCreate(&x);
+	}
+	~LevelEvents()
+	{
+		if (on)
+			for (auto& x : e)
+				cudaEventDestroy(x);
+	}
+	void mark(int i, cudaStream_t st)
+	{
+		if (on)
+			cudaEventRecord(e[i], st);
+	}
+	float ms(int a, int b) const
+	{
+		float t = 0.0f;
+		if (on)
+			cudaEventElapsedTime(&t, e[a], e[b]);
+		return t;
+	}
+};
+
 static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree, const float* d_x, const void* d_pairs,
 	const uint32_t* d_idx, uint32_t num_pairs, const u26_prp_params* P, u26_prp_output* out)
 {
@@ -2038,6 +2071,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	};
 	uint32_t hit_cap = 1u << 20;
 	uint32_t level = 0;
+	const bool trace = std::getenv("U26_PRP_TRACE") != nullptr;
+	LevelEvents ev(trace);
 	for (; !remaining.empty() && level < 65; level++)
 	{
 		auto tl = std::chrono::steady_clock::now();
@@ -2112,6 +2147,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			U26_CUDA(ctx, S->d_hitcount.reserve(sizeof(uint32_t)));
 			U26_CUDA(ctx, cudaMemsetAsync(S->d_hitcount.ptr, 0, sizeof(uint32_t), st));
 			HitSink sink{ S->d_keys.as<uint64_t>(), S->d_vals.as<uint32_t>(), S->d_pay_in.as<float>(), S->d_hitcount.as<uint32_t>(), hit_cap, b };
+			ev.mark(0, st);
 			if (total_req)
 			{
 				raycast_kernel<<<div_up(total_req, 128), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
@@ -2132,7 +2168,9 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->stage_ms[3] += ms_since(tl);
 		tl = std::chrono::steady_clock::now();
 		// sort hits by (task, type, source, target)
+		ev.mark(1, st);
 		U26_TRY(S->sorter.sort(ctx, S->d_keys.as<uint64_t>(), S->d_vals.as<uint32_t>(), nh, 0, 2 + 2 * b + tb));
+		ev.mark(2, st);
 		const HitKeyCodec cd{ b };
 		U26_CUDA(ctx, S->d_seg.reserve(sizeof(uint32_t) * (nt + 1)));
 		segments_kernel<<<div_up(nt + 1, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, nt, S->d_seg.as<uint32_t>());
@@ -2164,6 +2202,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				S->d_catt.as<uint32_t>(), S->d_root.as<uint32_t>());
 			U26_TRY(after_launch(ctx, "compress_kernel"));
 		}
+		ev.mark(3, st);
 		// support entries of boundary-attached components
 		std::vector<uint32_t> seg_h;
 		U26_TRY(download(ctx, seg_h, S->d_seg.ptr, nt + 1));
@@ -2192,6 +2231,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			ne_entries = std::min(*ctx->host_word, ecap);
 			U26_TRY(S->esorter.sort(ctx, S->d_ekeys.as<uint64_t>(), S->d_evals.as<uint32_t>(), ne_entries, 0, tb + 1 + vb + rb));
 		}
+		ev.mark(4, st);
 		U26_CUDA(ctx, S->d_out.reserve(sizeof(TaskOut) * nt));
 		task_kernel<<<nt, 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_keys.as<uint64_t>(), cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
 			S->d_csize.as<uint32_t>(), S->d_catt.as<uint32_t>(), S->d_pay.as<float>(), S->d_anchor_off.as<uint32_t>(),
@@ -2200,6 +2240,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			S->d_vmass.as<float>(), S->d_vn.as<float>(), S->d_en.as<float>(), S->d_fn.as<float>(), S->d_slots.as<Slot>(),
 			S->d_hop.as<uint32_t>(), vs, S->d_out.as<TaskOut>());
 		U26_TRY(after_launch(ctx, "task_kernel"));
+		ev.mark(5, st);
 		U26_TRY(download(ctx, tout, S->d_out.ptr, nt));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
 		for (uint32_t t = 0; t < nt; t++)
@@ -2216,8 +2257,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				S->d_pay.as<float>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_sel.as<u26_prp_hit>());
 			U26_TRY(after_launch(ctx, "gather_kernel"));
 			U26_TRY(download(ctx, sel, S->d_sel.ptr, nsel));
-			U26_CUDA(ctx, cudaStreamSynchronize(st));
 		}
+		ev.mark(6, st);
+		U26_CUDA(ctx, cudaStreamSynchronize(st));
+		if (trace)
+			fprintf(stderr, "[u26 prp] level %u tasks %u requests %u hits %u entries %u selected %u | raycast %.2f sort %.2f union %.2f entries %.2f task %.2f gather %.2f ms\n",
+				level, nt, total_req, nh, ne_entries, nsel, ev.ms(0, 1), ev.ms(1, 2), ev.ms(2, 3), ev.ms(3, 4), ev.ms(4, 5), ev.ms(5, 6));
 		out->stage_ms[4] += ms_since(tl);
 		tl = std::chrono::steady_clock::now();
 		// ---- k-ring control (evaluate_current_runtime_directions_template)
