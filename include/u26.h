@@ -261,6 +261,8 @@ typedef struct u26_prp_output_view
 	const float* directions;		 /* [num_contours][26][3] candidate directions (num_dirs used) */
 	uint64_t ray_tests;				 /* leaf primitive tests of all ray casts */
 	uint64_t ray_requests;			 /* VF + EE + FV ray requests */
+	uint64_t ray_pairs;				 /* (request, candidate target) pairs decided: the
+									  * implementation-independent ray-primitive test count */
 	uint32_t levels;				 /* k-ring levels evaluated (max over batches) */
 	uint32_t device_error_flags;
 	double stage_ms[8];				 /* host wall time per stage: preprocess, runtime, candidates, raycast, cull, control, finalize, total */

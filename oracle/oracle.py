@@ -283,9 +283,9 @@ class PrpRun:
                     self.directions.append(db[:nd])
                 else:
                     self.directions.append(np.zeros((0, 3), np.float32))
-            st = np.zeros(2, np.uint64)
+            st = np.zeros(3, np.uint64)
             L.oracle_prp_stats(h, _p(st, _u64p))
-            self.tested, self.requests = int(st[0]), int(st[1])
+            self.tested, self.requests, self.pairs_tested = int(st[0]), int(st[1]), int(st[2])
         finally:
             L.oracle_prp_free(h)
 

@@ -716,7 +716,7 @@ namespace
 		std::vector<uint8_t> processed, suppressed;
 		std::vector<float> pre_area;
 		std::vector<std::vector<uint>> merge_adj;
-		uint64_t tested = 0, requests = 0;
+		uint64_t tested = 0, requests = 0, pairs = 0;
 		// per-object BVHs (faces, edges)
 		std::vector<std::unique_ptr<CachedBVH>> face_bvh, edge_bvh;
 		std::mutex mtx;
@@ -1478,7 +1478,7 @@ namespace
 			cnt = mx - mn + 1;
 		};
 		std::vector<Hit> hits;
-		uint64_t tested = 0, requests = 0;
+		uint64_t tested = 0, requests = 0, pairs = 0;
 		const bool brute = S.p.brute_force_raycast != 0;
 		const CachedBVH* fb_dst = brute ? nullptr : S.face_bvh[r.object_ids[1]].get();
 		const CachedBVH* eb_dst = brute ? nullptr : S.edge_bvh[r.object_ids[1]].get();
@@ -1498,6 +1498,7 @@ namespace
 				q.vid = v;
 				cast_vert(m, fb_dst, q, hits, tested);
 				requests++;
+				pairs += r.cand_f[1].size();
 			}
 		}
 		// EE
@@ -1529,6 +1530,7 @@ namespace
 				}
 				cast_edge(m, eb_dst, q, hits, tested);
 				requests++;
+				pairs += r.cand_e[1].size();
 			}
 		}
 		// FV
@@ -1546,12 +1548,14 @@ namespace
 				q.vid = v;
 				cast_vert(m, fb_src, q, hits, tested);
 				requests++;
+				pairs += r.cand_f[0].size();
 			}
 		}
 		{
 			std::lock_guard<std::mutex> lock(S.mtx);
 			S.tested += tested;
 			S.requests += requests;
+			S.pairs += pairs;
 		}
 		info.unculled = uint(hits.size());
 		if (hits.empty())
@@ -2052,6 +2056,7 @@ extern "C"
 		Scene* S = static_cast<Scene*>(h);
 		out2[0] = S->tested;
 		out2[1] = S->requests;
+		out2[2] = S->pairs;
 	}
 	void oracle_eigen3(const float* S9, float* out9)
 	{

@@ -26,6 +26,9 @@ def _run_both(oracle, ctx, mesh, **kw):
 
 def _compare(res, ref):
     assert res.num_orig_pairs == ref.num_orig_pairs
+    # the ray-primitive pair count (the bench metric's unit) is the same work on both sides
+    assert res.pairs_tested == ref.pairs_tested
+    assert res.requests == ref.requests
     assert res.pairs.tobytes() == ref.pairs.tobytes()
     assert np.array_equal(res.pair_indices, ref.pair_indices)
     assert np.array_equal(res.mesh_index, ref.mesh_index)

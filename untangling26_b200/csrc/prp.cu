@@ -275,6 +275,21 @@ namespace u26
 			}
 		}
 
+		// per-slot bitmap of the contour-boundary vertices (object-local index)
+		__global__ void bnd_bits_kernel(const Slot* __restrict__ slots, const uint32_t* __restrict__ bnd, uint32_t v_stride,
+			uint32_t* __restrict__ bits)
+		{
+			const uint32_t s = blockIdx.x;
+			const Slot sl = slots[s];
+			uint32_t* b = bits + size_t(s) * (v_stride / 32 + 1);
+			for (uint32_t j = threadIdx.x; j < sl.bnd_cnt; j += blockDim.x)
+			{
+				const uint32_t v = bnd[sl.bnd_off + j] - sl.v_lo;
+				if (v < sl.v_cnt)
+					atomicOr(b + (v >> 5), 1u << (v & 31));
+			}
+		}
+
 		// ------------------------------------------------------------ candidates
 		__device__ __forceinline__ bool owns1(float own, float opp, float tau)
 		{
@@ -294,10 +309,12 @@ namespace u26
 			uint32_t f_stride, const uint32_t* __restrict__ hop, const float* __restrict__ geo, const uint32_t* __restrict__ order,
 			const uint32_t* __restrict__ level_end, uint32_t use_ccr, uint32_t ccr_rest, uint32_t ccr_current, float tau,
 			uint8_t* __restrict__ owns, uint32_t* __restrict__ cand_v, uint32_t* __restrict__ cand_e, uint32_t* __restrict__ cand_f,
-			uint32_t* __restrict__ counts, uint32_t* __restrict__ bits_e, uint32_t* __restrict__ bits_f)
+			uint32_t* __restrict__ counts, uint32_t* __restrict__ bits_e, uint32_t* __restrict__ bits_f, float* __restrict__ slot_box)
 		{
 			const uint32_t s = slot_ids[blockIdx.x];
 			const uint32_t o = s ^ 1u; // the other side of the same contour
+			// AABB of the candidate faces / edges (targets of the rays cast at this slot)
+			f3 fmn = mk3(INFINITY), fmx = mk3(-INFINITY), emn = mk3(INFINITY), emx = mk3(-INFINITY);
 			const Slot sl = slots[s];
 			const Slot so = slots[o];
 			const uint32_t lo = sl.v_lo;
@@ -371,6 +388,9 @@ namespace u26
 						continue;
 					cand_e[size_t(s) * e_stride + atomicAdd(&nec, 1u)] = e;
 					atomicOr(be + ((e - sl.e_lo) >> 5), 1u << ((e - sl.e_lo) & 31));
+					const f3 pa = ld3(x, ev.x), pb = ld3(x, ev.y);
+					emn = vmin(emn, vmin(pa, pb));
+					emx = vmax(emx, vmax(pa, pb));
 				}
 				for (uint32_t kk = vaf_off[gv]; kk < vaf_off[gv + 1]; kk++)
 				{
@@ -384,9 +404,38 @@ namespace u26
 						continue;
 					cand_f[size_t(s) * f_stride + atomicAdd(&nfc, 1u)] = f;
 					atomicOr(bf + ((f - sl.f_lo) >> 5), 1u << ((f - sl.f_lo) & 31));
+					const f3 pa = ld3(x, a), pb = ld3(x, b), pc = ld3(x, c);
+					fmn = vmin(fmn, vmin(pa, vmin(pb, pc)));
+					fmx = vmax(fmx, vmax(pa, vmax(pb, pc)));
 				}
 			}
+			// block min / max of the candidate boxes
+			__shared__ float red[12][8];
+			float v12[12] = { fmn.x, fmn.y, fmn.z, fmx.x, fmx.y, fmx.z, emn.x, emn.y, emn.z, emx.x, emx.y, emx.z };
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+			for (int q = 0; q < 12; q++)
+			{
+				float v = v12[q];
+				const bool is_min = (q % 6) < 3;
+				for (int off = 16; off > 0; off >>= 1)
+				{
+					const float w = __shfl_xor_sync(0xFFFFFFFFu, v, off);
+					v = is_min ? fminf(v, w) : fmaxf(v, w);
+				}
+				if (lane == 0)
+					red[q][warp] = v;
+			}
 			__syncthreads();
+			if (threadIdx.x < 12)
+			{
+				const int q = threadIdx.x;
+				const bool is_min = (q % 6) < 3;
+				float v = red[q][0];
+				for (int w = 1; w < 8; w++)
+					v = is_min ? fminf(v, red[q][w]) : fmaxf(v, red[q][w]);
+				slot_box[12 * size_t(s) + q] = v;
+			}
 			if (threadIdx.x == 0)
 			{
 				counts[3 * s] = nvc;
@@ -452,10 +501,42 @@ namespace u26
 			return (__ldg(bits + (l >> 5)) >> (l & 31)) & 1u;
 		}
 
-		// conservative ray / box test against a box grown by eps
-		__device__ __forceinline__ bool ray_box(f3 o, f3 d, float tmax_ray, const NodeBox& b)
+		// conservative ray / box test against a box grown by eps, over [t_lo, t_hi]
+		__device__ __forceinline__ bool ray_box_range(f3 o, f3 d, float t_lo, float t_hi, const float* lo, const float* hi, float& out_lo,
+			float& out_hi)
 		{
-			float tmin = 0.0f, tmax = tmax_ray;
+			float tmin = t_lo, tmax = t_hi;
+			const float oo[3] = { o.x, o.y, o.z }, dd[3] = { d.x, d.y, d.z };
+#pragma unroll
+			for (int a = 0; a < 3; a++)
+			{
+				const float eps = 1e-5f * (1.0f + fmaxf(fabsf(lo[a]), fabsf(hi[a])));
+				const float l = lo[a] - eps, h = hi[a] + eps;
+				if (fabsf(dd[a]) < 1e-30f)
+				{
+					if (oo[a] < l || oo[a] > h)
+						return false;
+					continue;
+				}
+				const float inv = 1.0f / dd[a];
+				float t0 = (l - oo[a]) * inv, t1 = (h - oo[a]) * inv;
+				if (t0 > t1)
+				{
+					const float t = t0;
+					t0 = t1;
+					t1 = t;
+				}
+				tmin = fmaxf(tmin, t0);
+				tmax = fminf(tmax, t1);
+			}
+			out_lo = tmin;
+			out_hi = tmax;
+			return tmin <= tmax;
+		}
+
+		__device__ __forceinline__ bool ray_box(f3 o, f3 d, float t_lo, float tmax_ray, const NodeBox& b)
+		{
+			float tmin = t_lo, tmax = tmax_ray;
 			const float lo[3] = { b.mn.x, b.mn.y, b.mn.z }, hi[3] = { b.mx.x, b.mx.y, b.mx.z };
 			const float oo[3] = { o.x, o.y, o.z }, dd[3] = { d.x, d.y, d.z };
 #pragma unroll
@@ -517,7 +598,7 @@ namespace u26
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
 			TreeView ftree, TreeView etree, const float* __restrict__ x, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces,
-			HitSink sink, unsigned long long* __restrict__ stats, uint32_t* __restrict__ dev_err)
+			const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats, uint32_t* __restrict__ dev_err)
 		{
 			const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
 			uint32_t tested = 0;
@@ -551,8 +632,12 @@ namespace u26
 					const f3 cast = fv ? -dir : dir;
 					const f3 orig = ld3(x, vid);
 					const f3 end = orig + cast * 1.0f;
+					// clip the ray to the grown AABB of the candidate target faces
+					const float* tb = slot_box + 12 * size_t(fv ? tk.slot0 : tk.slot1);
+					float t_lo = 0.0f, t_hi = 1.0f;
 					int sp = 0;
-					stack[sp++] = 0u;
+					if (ray_box_range(orig, cast, 0.0f, 1.0f, tb, tb + 3, t_lo, t_hi))
+						stack[sp++] = 0u;
 					uint32_t loop = 0;
 					while (sp > 0)
 					{
@@ -560,7 +645,7 @@ namespace u26
 						NodeBox b;
 						b.mn = __ldg(&ftree.boxes[node].mn);
 						b.mx = __ldg(&ftree.boxes[node].mx);
-						if (!ray_box(orig, cast, 1.0f, b))
+						if (!ray_box(orig, cast, t_lo, t_hi, b))
 							continue;
 						const uint32_t fid = __ldg(ftree.object_idx + node);
 						if (fid != kInvalid)
@@ -619,10 +704,20 @@ namespace u26
 							pd = dot(pn, p0);
 						}
 						const f3 a_end = p0 + dir * ray_max, b_end = p1 + dir * ray_max;
-						const f3 smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
-						const f3 smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
+						f3 smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
+						f3 smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
+						// intersect the swept box with the grown AABB of the candidate target edges
+						const float* tb = slot_box + 12 * size_t(tk.slot1) + 6;
+						{
+							const float e0 = 1e-5f * (1.0f + fmaxf(fabsf(tb[0]), fabsf(tb[3])));
+							const float e1 = 1e-5f * (1.0f + fmaxf(fabsf(tb[1]), fabsf(tb[4])));
+							const float e2 = 1e-5f * (1.0f + fmaxf(fabsf(tb[2]), fabsf(tb[5])));
+							smn = vmax(smn, mk3(tb[0] - e0, tb[1] - e1, tb[2] - e2));
+							smx = vmin(smx, mk3(tb[3] + e0, tb[4] + e1, tb[5] + e2));
+						}
 						int sp = 0;
-						stack[sp++] = 0u;
+						if (smn.x <= smx.x && smn.y <= smx.y && smn.z <= smx.z)
+							stack[sp++] = 0u;
 						uint32_t loop = 0;
 						while (sp > 0)
 						{
@@ -942,10 +1037,13 @@ namespace u26
 		}
 
 		// support entries (side, vertex, component) of hits in boundary-attached components
+		// Only contour-boundary vertices are entered: the coverage test queries (side, v)
+		// for v in the contour's side-`side` anchors, which are that side's boundary verts.
 		__global__ void entries_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, const uint32_t* __restrict__ seg,
 			const uint32_t* __restrict__ root, const uint32_t* __restrict__ comp_att, const uint2* __restrict__ edges,
 			const uint32_t* __restrict__ faces, int vb, int rb, uint64_t* __restrict__ ekeys, uint32_t* __restrict__ evals,
-			uint32_t* __restrict__ ecount, uint32_t cap)
+			uint32_t* __restrict__ ecount, uint32_t cap, const Task* __restrict__ tasks, const Slot* __restrict__ slots,
+			const uint32_t* __restrict__ bnd_bits, uint32_t v_stride)
 		{
 			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 			if (i >= n)
@@ -958,11 +1056,16 @@ namespace u26
 			const uint32_t rl = r - seg[t];
 			uint32_t sv[3], dv[3];
 			hit_verts(cd.type(k), cd.src(k), cd.dst(k), edges, faces, sv, dv);
+			const Task tk = tasks[t];
 			for (int side = 0; side < 2; side++)
 				for (int q = 0; q < 3; q++)
 				{
 					const uint32_t v = side == 0 ? sv[q] : dv[q];
 					if (v == kInf)
+						continue;
+					const uint32_t sl_id = side == 0 ? tk.slot0 : tk.slot1;
+					const uint32_t lv = v - slots[sl_id].v_lo;
+					if (!((bnd_bits[size_t(sl_id) * (v_stride / 32 + 1) + (lv >> 5)] >> (lv & 31)) & 1u))
 						continue;
 					const uint32_t slot = atomicAdd(ecount, 1u);
 					if (slot < cap)
@@ -972,14 +1075,6 @@ namespace u26
 					}
 				}
 		}
-
-		struct TaskOut
-		{
-			uint32_t hit_begin, hit_end, best_root, hit_count;
-			uint32_t unculled, covered, anchors, max_front_src;
-			uint32_t max_front_dst, sel_offset, ncand, pad;
-			float depth, volume, area, kappa;
-		};
 
 		__device__ __forceinline__ bool entry_exists(const uint64_t* ek, uint32_t n, uint64_t key)
 		{
@@ -998,45 +1093,36 @@ namespace u26
 			return false;
 		}
 
-		// One CTA per task: candidate components, coverage, best component, metrics.
-		__global__ void __launch_bounds__(256) task_kernel(const Task* __restrict__ tasks, uint32_t ntasks, const uint64_t* __restrict__ keys,
-			HitKeyCodec cd, const uint32_t* __restrict__ seg, const uint32_t* __restrict__ root, const uint32_t* __restrict__ comp_size,
-			const uint32_t* __restrict__ comp_att, const float* __restrict__ pay, const uint32_t* __restrict__ anchor_off,
-			const uint32_t* __restrict__ anchors, const uint64_t* __restrict__ ekeys, uint32_t nentries, int vb, int rb,
-			uint32_t* __restrict__ cand_roots, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces,
-			const float* __restrict__ vert_area, const float* __restrict__ edge_area, const float* __restrict__ face_area,
-			const float* __restrict__ vert_mass, const float* __restrict__ vn, const float* __restrict__ en, const float* __restrict__ fnn,
-			const Slot* __restrict__ slots, const uint32_t* __restrict__ hop, uint32_t v_stride, TaskOut* __restrict__ out)
+		// boundary-attached component roots of each task (order does not matter: the
+		// selection rule below is a strict total order)
+		__global__ void cand_roots_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, const uint32_t* __restrict__ seg,
+			const uint32_t* __restrict__ root, const uint32_t* __restrict__ comp_att, uint32_t* __restrict__ ncand,
+			uint32_t* __restrict__ cand_roots)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n || root[i] != i || !comp_att[i])
+				return;
+			const uint32_t t = cd.task(keys[i]);
+			cand_roots[seg[t] + atomicAdd(ncand + t, 1u)] = i;
+		}
+
+		// One CTA per task: EF-anchor coverage of each candidate component (one warp per
+		// component, lanes over the contour's anchors), then the best component: maximal
+		// coverage, then more hits, then the smaller canonical key (= smaller root index).
+		__global__ void __launch_bounds__(256) coverage_kernel(const Task* __restrict__ tasks, uint32_t ntasks, const uint32_t* __restrict__ seg,
+			const uint32_t* __restrict__ ncand_arr, const uint32_t* __restrict__ cand_roots, const uint32_t* __restrict__ comp_size,
+			const uint32_t* __restrict__ anchor_off, const uint32_t* __restrict__ anchors, const uint64_t* __restrict__ ekeys,
+			uint32_t nentries, int vb, int rb, uint32_t* __restrict__ best_out, uint32_t* __restrict__ bestcov_out)
 		{
 			const uint32_t t = blockIdx.x;
 			if (t >= ntasks)
 				return;
 			const Task tk = tasks[t];
-			const uint32_t lo = seg[t], hi = seg[t + 1];
+			const uint32_t lo = seg[t];
+			const uint32_t ncand = ncand_arr[t];
 			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-			__shared__ uint32_t s_ncand, s_best, s_bestcov;
-			__shared__ uint32_t s_cov[256];
-			// 1) boundary-attached component roots (in key order)
-			if (warp == 0)
-			{
-				uint32_t nc = 0;
-				for (uint32_t base = lo; base < hi; base += 32)
-				{
-					const uint32_t i = base + lane;
-					const bool is = i < hi && root[i] == i && comp_att[i];
-					const uint32_t m = __ballot_sync(0xFFFFFFFFu, is);
-					if (is)
-						cand_roots[lo + nc + __popc(m & ((1u << lane) - 1u))] = i;
-					nc += __popc(m);
-				}
-				if (lane == 0)
-					s_ncand = nc;
-			}
-			__syncthreads();
-			const uint32_t ncand = s_ncand;
-			const uint32_t c = tk.contour_local;
-			const uint32_t a_lo = anchor_off[c], a_hi = anchor_off[c + 1];
-			// 2) EF-anchor coverage of each candidate component (one warp per component)
+			const uint32_t a_lo = anchor_off[tk.contour_local], a_hi = anchor_off[tk.contour_local + 1];
+			__shared__ uint32_t s_cov[8];
 			uint32_t best = kInf, best_cov = 0, best_n = 0;
 			for (uint32_t j0 = 0; j0 < ncand; j0 += 8)
 			{
@@ -1068,7 +1154,6 @@ namespace u26
 					{
 						const uint32_t r = cand_roots[lo + j0 + w];
 						const uint32_t cv = s_cov[w], nh = comp_size[r];
-						// max coverage, then more hits, then the smaller canonical key (= smaller root)
 						const bool better = best == kInf || cv > best_cov || (cv == best_cov && nh > best_n) || (cv == best_cov && nh == best_n && r < best);
 						if (better)
 						{
@@ -1082,176 +1167,288 @@ namespace u26
 			}
 			if (threadIdx.x == 0)
 			{
-				s_best = best;
-				s_bestcov = best_cov;
-			}
-			__syncthreads();
-			best = s_best;
-			// 3) metrics over the selected hits in canonical order (warp 0)
-			if (warp == 0)
-			{
-				__shared__ float buf_a[32], buf_v[32], buf_k[32];
-				__shared__ uint32_t buf_f[32];
-				float sa = 0.0f, sv = 0.0f, sk = 0.0f, depth = 0.0f;
-				uint32_t mfs = 0, mfd = 0, run = 0;
-				const f3 dir = mk3(tk.dir[0], tk.dir[1], tk.dir[2]);
-				const Slot s0 = slots[tk.slot0], s1 = slots[tk.slot1];
-				const uint32_t* h0 = hop + size_t(tk.slot0) * v_stride;
-				const uint32_t* h1 = hop + size_t(tk.slot1) * v_stride;
-				if (best != kInf)
-				{
-					for (uint32_t base = lo; base < hi; base += 32)
-					{
-						const uint32_t i = base + lane;
-						const bool sel = i < hi && root[i] == best;
-						const uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
-						buf_f[lane] = 0u;
-						__syncwarp();
-						if (sel)
-						{
-							const uint64_t k = keys[i];
-							const uint32_t ty = cd.type(k), s = cd.src(k), d = cd.dst(k);
-							const float b0 = pay[3 * i], b1 = pay[3 * i + 1], dist = pay[3 * i + 2];
-							float area, alpha;
-							if (ty == 0u)
-							{
-								area = vert_area[s];
-								alpha = fabsf(dot(mk3(vn[3 * s], vn[3 * s + 1], vn[3 * s + 2]), dir));
-							}
-							else if (ty == 1u)
-							{
-								area = edge_area[s];
-								alpha = fabsf(dot(mk3(en[3 * s], en[3 * s + 1], en[3 * s + 2]), dir));
-							}
-							else
-							{
-								area = face_area[s];
-								alpha = fabsf(dot(mk3(fnn[3 * s], fnn[3 * s + 1], fnn[3 * s + 2]), dir));
-							}
-							uint32_t sv3[3], dv3[3];
-							hit_verts(ty, s, d, edges, faces, sv3, dv3);
-							auto im = [&](uint32_t v)
-							{ return 1.0f / fmaxf(vert_mass[v], 1e-8f); };
-							float e;
-							if (ty == 0u)
-							{
-								const float bx = b0, by = b1, bz = 1.0f - b0 - b1;
-								e = ((im(sv3[0]) + bx * bx * im(dv3[0])) + by * by * im(dv3[1])) + bz * bz * im(dv3[2]);
-							}
-							else if (ty == 2u)
-							{
-								const float bx = b0, by = b1, bz = 1.0f - b0 - b1;
-								e = ((bx * bx * im(sv3[0]) + by * by * im(sv3[1])) + bz * bz * im(sv3[2])) + im(dv3[0]);
-							}
-							else
-							{
-								const float a0 = b0, a1 = 1.0f - b0, c0 = b1, c1 = 1.0f - b1;
-								e = ((a0 * a0 * im(sv3[0]) + a1 * a1 * im(sv3[1])) + c0 * c0 * im(dv3[0])) + c1 * c1 * im(dv3[1]);
-							}
-							const float sd = dist + 3e-3f;
-							const float kap = e > 1e-8f ? (sd * sd) / e : 0.0f;
-							const uint32_t dl = (run + __popc(m & ((1u << lane) - 1u))) & 31u;
-							buf_a[dl] = area;
-							buf_v[dl] = (area * alpha) * dist;
-							buf_k[dl] = kap;
-							buf_f[dl] = 1u;
-							depth = fmaxf(depth, dist);
-							for (int q = 0; q < 3; q++)
-							{
-								if (sv3[q] != kInf)
-								{
-									const uint32_t hv = h0[sv3[q] - s0.v_lo];
-									if (hv != kInf)
-										mfs = max(mfs, hv);
-								}
-								if (dv3[q] != kInf)
-								{
-									const uint32_t hv = h1[dv3[q] - s1.v_lo];
-									if (hv != kInf)
-										mfd = max(mfd, hv);
-								}
-							}
-						}
-						__syncwarp();
-						if (buf_f[lane])
-						{
-							sa = sa + buf_a[lane];
-							sv = sv + buf_v[lane];
-							sk = sk + buf_k[lane];
-						}
-						run += __popc(m);
-						__syncwarp();
-					}
-				}
-				for (int off = 16; off >= 1; off >>= 1)
-				{
-					sa = sa + __shfl_xor_sync(0xFFFFFFFFu, sa, off);
-					sv = sv + __shfl_xor_sync(0xFFFFFFFFu, sv, off);
-					sk = sk + __shfl_xor_sync(0xFFFFFFFFu, sk, off);
-				}
-				for (int off = 16; off >= 1; off >>= 1)
-				{
-					depth = fmaxf(depth, __shfl_xor_sync(0xFFFFFFFFu, depth, off));
-					mfs = max(mfs, __shfl_xor_sync(0xFFFFFFFFu, mfs, off));
-					mfd = max(mfd, __shfl_xor_sync(0xFFFFFFFFu, mfd, off));
-				}
-				if (lane == 0)
-				{
-					TaskOut o;
-					o.hit_begin = lo;
-					o.hit_end = hi;
-					o.best_root = best;
-					o.hit_count = best != kInf ? comp_size[best] : 0u;
-					o.unculled = hi - lo;
-					o.covered = best != kInf ? s_bestcov : 0u;
-					o.anchors = a_hi - a_lo;
-					o.max_front_src = mfs;
-					o.max_front_dst = mfd;
-					o.sel_offset = 0u;
-					o.ncand = ncand;
-					o.pad = 0u;
-					o.depth = depth;
-					o.volume = sv;
-					o.area = sa;
-					o.kappa = sk;
-					out[t] = o;
-				}
+				best_out[t] = best;
+				bestcov_out[t] = best_cov;
 			}
 		}
 
-		// selected supports, compacted in task order at the offsets in out[t].sel_offset
-		__global__ void gather_kernel(const TaskOut* __restrict__ out, uint32_t ntasks, const uint64_t* __restrict__ keys, HitKeyCodec cd,
-			const uint32_t* __restrict__ root, const float* __restrict__ pay, const uint2* __restrict__ edges,
-			const uint32_t* __restrict__ faces, u26_prp_hit* __restrict__ dst)
+		__device__ __forceinline__ uint32_t selected_flag(const uint64_t* keys, const uint32_t* root, const uint32_t* best, HitKeyCodec cd,
+			uint32_t i, uint32_t n)
 		{
-			const uint32_t t = blockIdx.x;
+			if (i >= n)
+				return 0u;
+			return root[i] == best[cd.task(keys[i])] ? 1u : 0u;
+		}
+
+		// exclusive scan of the "selected" flags (hits of each task's best component), in
+		// three phases over blocks of 1024 hits
+		__global__ void __launch_bounds__(256) sel_block_sums_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ root,
+			const uint32_t* __restrict__ best, HitKeyCodec cd, uint32_t n, uint32_t* __restrict__ bsum)
+		{
+			const uint32_t base = blockIdx.x * 1024u;
+			uint32_t c = 0;
+			for (uint32_t k = threadIdx.x; k < 1024u; k += 256u)
+				c += selected_flag(keys, root, best, cd, base + k, n);
+			c = __reduce_add_sync(0xFFFFFFFFu, c);
+			__shared__ uint32_t w[8];
+			if ((threadIdx.x & 31) == 0)
+				w[threadIdx.x >> 5] = c;
+			__syncthreads();
+			if (threadIdx.x == 0)
+			{
+				uint32_t t = 0;
+				for (int q = 0; q < 8; q++)
+					t += w[q];
+				bsum[blockIdx.x] = t;
+			}
+		}
+
+		__global__ void __launch_bounds__(1024) scan_one_block_kernel(uint32_t* __restrict__ v, uint32_t n, uint32_t* __restrict__ total)
+		{
+			__shared__ uint32_t ws[32];
+			const uint32_t per = (n + blockDim.x - 1) / blockDim.x;
+			const uint32_t b = threadIdx.x * per, e = min(n, b + per);
+			uint32_t local = 0;
+			for (uint32_t i = b; i < e; i++)
+				local += v[i];
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+			uint32_t x = local;
+			for (int o = 1; o < 32; o <<= 1)
+			{
+				const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+				if (lane >= o)
+					x += y;
+			}
+			if (lane == 31)
+				ws[warp] = x;
+			__syncthreads();
+			if (warp == 0)
+			{
+				uint32_t y = ws[lane];
+				for (int o = 1; o < 32; o <<= 1)
+				{
+					const uint32_t z = __shfl_up_sync(0xFFFFFFFFu, y, o);
+					if (lane >= o)
+						y += z;
+				}
+				ws[lane] = y;
+			}
+			__syncthreads();
+			uint32_t run = x - local + (warp > 0 ? ws[warp - 1] : 0u);
+			for (uint32_t i = b; i < e; i++)
+			{
+				const uint32_t c = v[i];
+				v[i] = run;
+				run += c;
+			}
+			if (threadIdx.x == blockDim.x - 1)
+				*total = run;
+		}
+
+		// position of every selected hit in the compact canonical order, and its metric terms
+		__global__ void __launch_bounds__(256) sel_terms_kernel(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ root,
+			const uint32_t* __restrict__ best, HitKeyCodec cd, uint32_t n, const uint32_t* __restrict__ bsum, const Task* __restrict__ tasks,
+			const float* __restrict__ pay, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const float* __restrict__ vert_area,
+			const float* __restrict__ edge_area, const float* __restrict__ face_area, const float* __restrict__ vert_mass,
+			const float* __restrict__ vn, const float* __restrict__ en, const float* __restrict__ fnn, const Slot* __restrict__ slots,
+			const uint32_t* __restrict__ hop, uint32_t v_stride, uint32_t* __restrict__ pos, float* __restrict__ terms,
+			uint32_t* __restrict__ task_max, u26_prp_hit* __restrict__ out_hits)
+		{
+			__shared__ uint32_t wsum[8];
+			const uint32_t base = blockIdx.x * 1024u;
+			uint32_t f[4];
+			uint32_t loc = 0;
+#pragma unroll
+			for (int q = 0; q < 4; q++)
+			{
+				f[q] = selected_flag(keys, root, best, cd, base + 4 * threadIdx.x + q, n);
+				loc += f[q];
+			}
+			// exclusive scan of per-thread counts across the block
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+			uint32_t x = loc;
+			for (int o = 1; o < 32; o <<= 1)
+			{
+				const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+				if (lane >= o)
+					x += y;
+			}
+			if (lane == 31)
+				wsum[warp] = x;
+			__syncthreads();
+			uint32_t wbase = 0;
+			for (int q = 0; q < warp; q++)
+				wbase += wsum[q];
+			uint32_t p = bsum[blockIdx.x] + wbase + x - loc;
+#pragma unroll
+			for (int q = 0; q < 4; q++)
+			{
+				const uint32_t i = base + 4 * threadIdx.x + q;
+				if (!f[q])
+					continue;
+				pos[i] = p;
+				const uint64_t k = keys[i];
+				const uint32_t t = cd.task(k), ty = cd.type(k), sid = cd.src(k), did = cd.dst(k);
+				const Task tk = tasks[t];
+				const f3 dir = mk3(tk.dir[0], tk.dir[1], tk.dir[2]);
+				const float b0 = pay[3 * i], b1 = pay[3 * i + 1], dist = pay[3 * i + 2];
+				float area, alpha;
+				if (ty == 0u)
+				{
+					area = vert_area[sid];
+					alpha = fabsf(dot(mk3(vn[3 * sid], vn[3 * sid + 1], vn[3 * sid + 2]), dir));
+				}
+				else if (ty == 1u)
+				{
+					area = edge_area[sid];
+					alpha = fabsf(dot(mk3(en[3 * sid], en[3 * sid + 1], en[3 * sid + 2]), dir));
+				}
+				else
+				{
+					area = face_area[sid];
+					alpha = fabsf(dot(mk3(fnn[3 * sid], fnn[3 * sid + 1], fnn[3 * sid + 2]), dir));
+				}
+				uint32_t sv3[3], dv3[3];
+				hit_verts(ty, sid, did, edges, faces, sv3, dv3);
+				auto im = [&](uint32_t v)
+				{ return 1.0f / fmaxf(vert_mass[v], 1e-8f); };
+				float e;
+				if (ty == 0u)
+				{
+					const float bx = b0, by = b1, bz = 1.0f - b0 - b1;
+					e = ((im(sv3[0]) + bx * bx * im(dv3[0])) + by * by * im(dv3[1])) + bz * bz * im(dv3[2]);
+				}
+				else if (ty == 2u)
+				{
+					const float bx = b0, by = b1, bz = 1.0f - b0 - b1;
+					e = ((bx * bx * im(sv3[0]) + by * by * im(sv3[1])) + bz * bz * im(sv3[2])) + im(dv3[0]);
+				}
+				else
+				{
+					const float a0 = b0, a1 = 1.0f - b0, c0 = b1, c1 = 1.0f - b1;
+					e = ((a0 * a0 * im(sv3[0]) + a1 * a1 * im(sv3[1])) + c0 * c0 * im(dv3[0])) + c1 * c1 * im(dv3[1]);
+				}
+				const float sd = dist + 3e-3f;
+				terms[3 * size_t(p)] = area;
+				terms[3 * size_t(p) + 1] = (area * alpha) * dist;
+				terms[3 * size_t(p) + 2] = e > 1e-8f ? (sd * sd) / e : 0.0f;
+				// depth (non-negative float bits order like uints) and frontier hops
+				atomicMax(task_max + 3 * t, __float_as_uint(dist));
+				const Slot s0 = slots[tk.slot0], s1 = slots[tk.slot1];
+				const uint32_t* h0 = hop + size_t(tk.slot0) * v_stride;
+				const uint32_t* h1 = hop + size_t(tk.slot1) * v_stride;
+				uint32_t mfs = 0, mfd = 0;
+				for (int q2 = 0; q2 < 3; q2++)
+				{
+					if (sv3[q2] != kInf)
+					{
+						const uint32_t hv = h0[sv3[q2] - s0.v_lo];
+						if (hv != kInf)
+							mfs = max(mfs, hv);
+					}
+					if (dv3[q2] != kInf)
+					{
+						const uint32_t hv = h1[dv3[q2] - s1.v_lo];
+						if (hv != kInf)
+							mfd = max(mfd, hv);
+					}
+				}
+				atomicMax(task_max + 3 * t + 1, mfs);
+				atomicMax(task_max + 3 * t + 2, mfd);
+				if (out_hits)
+				{
+					u26_prp_hit h;
+					h.type = ty;
+					h.src_id = sid;
+					h.dst_id = did;
+					for (int q2 = 0; q2 < 3; q2++)
+					{
+						h.src_verts[q2] = sv3[q2];
+						h.dst_verts[q2] = dv3[q2];
+					}
+					h.bary[0] = b0;
+					h.bary[1] = b1;
+					h.dist = dist;
+					out_hits[p] = h;
+				}
+				p++;
+			}
+		}
+
+		struct TaskOut
+		{
+			uint32_t hit_begin, hit_end, best_root, hit_count;
+			uint32_t unculled, covered, anchors, max_front_src;
+			uint32_t max_front_dst, sel_offset, ncand, pad;
+			float depth, volume, area, kappa;
+		};
+
+		// one warp per task: canonical 32-lane strided sums over its contiguous selected terms
+		__global__ void task_sum_kernel(uint32_t ntasks, const Task* __restrict__ tasks, const uint32_t* __restrict__ seg,
+			const uint32_t* __restrict__ best, const uint32_t* __restrict__ bestcov, const uint32_t* __restrict__ comp_size,
+			const uint32_t* __restrict__ ncand, const uint32_t* __restrict__ sel_begin, const float* __restrict__ terms,
+			const uint32_t* __restrict__ task_max, const uint32_t* __restrict__ anchor_off, TaskOut* __restrict__ out)
+		{
+			const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const int lane = threadIdx.x & 31;
 			if (t >= ntasks)
 				return;
-			const TaskOut o = out[t];
-			if (o.best_root == kInf)
-				return;
-			const int lane = threadIdx.x;
-			uint32_t run = 0;
-			for (uint32_t base = o.hit_begin; base < o.hit_end; base += 32)
+			const uint32_t b = best[t];
+			const uint32_t cnt = b != kInf ? comp_size[b] : 0u;
+			const uint32_t p0 = sel_begin[t];
+			float sa = 0.0f, sv = 0.0f, sk = 0.0f;
+			for (uint32_t i = lane; i < cnt; i += 32)
 			{
-				const uint32_t i = base + lane;
-				const bool sel = i < o.hit_end && root[i] == o.best_root;
-				const uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
-				if (sel)
-				{
-					const uint64_t k = keys[i];
-					u26_prp_hit h;
-					h.type = cd.type(k);
-					h.src_id = cd.src(k);
-					h.dst_id = cd.dst(k);
-					hit_verts(h.type, h.src_id, h.dst_id, edges, faces, h.src_verts, h.dst_verts);
-					h.bary[0] = pay[3 * i];
-					h.bary[1] = pay[3 * i + 1];
-					h.dist = pay[3 * i + 2];
-					dst[o.sel_offset + run + __popc(m & ((1u << lane) - 1u))] = h;
-				}
-				run += __popc(m);
+				const float* tt = terms + 3 * size_t(p0 + i);
+				sa = sa + tt[0];
+				sv = sv + tt[1];
+				sk = sk + tt[2];
 			}
+			for (int off = 16; off >= 1; off >>= 1)
+			{
+				sa = sa + __shfl_xor_sync(0xFFFFFFFFu, sa, off);
+				sv = sv + __shfl_xor_sync(0xFFFFFFFFu, sv, off);
+				sk = sk + __shfl_xor_sync(0xFFFFFFFFu, sk, off);
+			}
+			if (lane == 0)
+			{
+				const Task tk = tasks[t];
+				TaskOut o;
+				o.hit_begin = seg[t];
+				o.hit_end = seg[t + 1];
+				o.best_root = b;
+				o.hit_count = cnt;
+				o.unculled = seg[t + 1] - seg[t];
+				o.covered = b != kInf ? bestcov[t] : 0u;
+				o.anchors = anchor_off[tk.contour_local + 1] - anchor_off[tk.contour_local];
+				o.max_front_src = task_max[3 * t + 1];
+				o.max_front_dst = task_max[3 * t + 2];
+				o.sel_offset = p0;
+				o.ncand = ncand[t];
+				o.pad = 0u;
+				o.depth = __uint_as_float(task_max[3 * t]);
+				o.volume = sv;
+				o.area = sa;
+				o.kappa = sk;
+				out[t] = o;
+			}
+		}
+
+		// selected-hit offset of each task: the scanned position of its first hit
+		__global__ void sel_begin_kernel(uint32_t ntasks, const uint32_t* __restrict__ seg, const uint32_t* __restrict__ bsum_scanned,
+			const uint64_t* __restrict__ keys, const uint32_t* __restrict__ root, const uint32_t* __restrict__ best, HitKeyCodec cd,
+			uint32_t n, uint32_t* __restrict__ sel_begin)
+		{
+			const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+			if (t >= ntasks)
+				return;
+			// count selected flags in [block start, seg[t]) on top of the block prefix
+			const uint32_t i0 = seg[t];
+			const uint32_t blk = i0 / 1024u;
+			uint32_t p = bsum_scanned[blk];
+			for (uint32_t i = blk * 1024u; i < i0; i++)
+				p += selected_flag(keys, root, best, cd, i, n);
+			sel_begin[t] = p;
 		}
 	} // namespace
 } // namespace u26
@@ -1352,7 +1549,7 @@ namespace
 
 	inline bool usable(const ComboState& c)
 	{
-		return !c.hits.empty() && c.covered > 0 && std::isfinite(c.objective) && std::isfinite(c.coverage) && c.coverage > 0.0f;
+		return c.hit_count > 0 && c.covered > 0 && std::isfinite(c.objective) && std::isfinite(c.coverage) && c.coverage > 0.0f;
 	}
 	inline bool valid_resp(const ComboState& c) { return c.eligible && usable(c); }
 	inline float resp_obj(const ComboState& c)
@@ -1422,6 +1619,7 @@ struct u26_scene
 	DevBuf d_cand_v, d_cand_e, d_cand_f, d_counts, d_bits_e, d_bits_f;
 	DevBuf d_tasks, d_keys, d_vals, d_pay_in, d_pay, d_hitcount, d_stats, d_seg, d_parent, d_root, d_att, d_csize, d_catt;
 	DevBuf d_ekeys, d_evals, d_ecount, d_cand_roots, d_vf_off, d_vf, d_anchor_off, d_anchors, d_out, d_sel;
+	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	RadixSorter sorter, esorter;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 };
@@ -1434,7 +1632,7 @@ struct u26_prp_output
 	std::vector<u26_prp_result> results;
 	std::vector<u26_prp_hit> hits;
 	uint32_t num_orig_pairs = 0, levels = 0, dev_err = 0;
-	uint64_t ray_tests = 0, ray_requests = 0;
+	uint64_t ray_tests = 0, ray_requests = 0, ray_pairs = 0;
 	double stage_ms[8] = { 0 };
 };
 
@@ -1547,7 +1745,8 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_geo, &s->d_order, &s->d_level_end, &s->d_work, &s->d_mark, &s->d_owns, &s->d_cand_v, &s->d_cand_e, &s->d_cand_f,
 		&s->d_counts, &s->d_bits_e, &s->d_bits_f, &s->d_tasks, &s->d_keys, &s->d_vals, &s->d_pay_in, &s->d_pay, &s->d_hitcount,
 		&s->d_stats, &s->d_seg, &s->d_parent, &s->d_root, &s->d_att, &s->d_csize, &s->d_catt, &s->d_ekeys, &s->d_evals,
-		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel };
+		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
+		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
@@ -2061,6 +2260,15 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 2));
 	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 2, st));
 	const TreeView ftv = tree_view(face_tree), etv = tree_view(edge_tree);
+	const uint32_t bnd_words = vs / 32 + 1;
+	if (nslots)
+	{
+		U26_CUDA(ctx, S->d_bnd_bits.reserve(sizeof(uint32_t) * size_t(nslots) * bnd_words));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_bnd_bits.ptr, 0, sizeof(uint32_t) * size_t(nslots) * bnd_words, st));
+		bnd_bits_kernel<<<nslots, 256, 0, st>>>(S->d_slots.as<Slot>(), S->d_bnd.as<uint32_t>(), vs, S->d_bnd_bits.as<uint32_t>());
+		U26_TRY(after_launch(ctx, "bnd_bits_kernel"));
+		U26_CUDA(ctx, S->d_slot_box.reserve(sizeof(float) * 12 * size_t(nslots)));
+	}
 	std::vector<uint32_t> remaining(nact);
 	std::iota(remaining.begin(), remaining.end(), 0u);
 	auto grow = [](uint32_t cur, uint32_t diam) -> uint32_t
@@ -2073,17 +2281,11 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	uint32_t level = 0;
 	const bool trace = std::getenv("U26_PRP_TRACE") != nullptr;
 	LevelEvents ev(trace);
-	for (; !remaining.empty() && level < 65; level++)
+	uint64_t alg_tests = 0;
+
+	// candidates of the listed slots at slots[s].k
+	auto build_candidates = [&](const std::vector<uint32_t>& sids, std::vector<uint32_t>& counts) -> u26_status
 	{
-		auto tl = std::chrono::steady_clock::now();
-		// candidates of the remaining contours at their current k
-		std::vector<uint32_t> sids;
-		for (uint32_t c : remaining)
-			for (int sd = 0; sd < 2; sd++)
-			{
-				slots[2 * c + sd].k = R[c].k[sd];
-				sids.push_back(2 * c + sd);
-			}
 		U26_TRY(upload(ctx, S->d_slots, slots));
 		U26_TRY(upload(ctx, S->d_slot_ids, sids));
 		candidates_kernel<<<uint32_t(sids.size()), 256, 0, st>>>(S->d_slots.as<Slot>(), S->d_slot_ids.as<uint32_t>(), S->d_bnd.as<uint32_t>(),
@@ -2091,45 +2293,33 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			S->d_vaf_off.as<uint32_t>(), S->d_vaf.as<uint32_t>(), vs, es_, fs, S->d_hop.as<uint32_t>(), S->d_geo.as<float>(),
 			S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(), P->use_ccr, P->ccr_use_rest, P->ccr_use_current, P->ccr_tau,
 			S->d_owns.as<uint8_t>(), S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), S->d_cand_f.as<uint32_t>(),
-			S->d_counts.as<uint32_t>(), S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>());
+			S->d_counts.as<uint32_t>(), S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(), S->d_slot_box.as<float>());
 		U26_TRY(after_launch(ctx, "candidates_kernel"));
-		std::vector<uint32_t> counts;
 		U26_TRY(download(ctx, counts, S->d_counts.ptr, 3 * size_t(nslots)));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
-		out->stage_ms[2] += ms_since(tl);
-		tl = std::chrono::steady_clock::now();
-		// tasks
-		std::vector<Task> tasks;
+		return U26_OK;
+	};
+
+	// ray casting, hit sort, product adjacency, coverage, best component and metrics of
+	// the given tasks; with hits_out, also the selected supports in canonical order
+	auto evaluate = [&](std::vector<Task>& tasks, const std::vector<uint32_t>& counts, std::vector<TaskOut>& tout,
+						std::vector<u26_prp_hit>* hits_out) -> u26_status
+	{
+		auto tl = std::chrono::steady_clock::now();
 		uint32_t total_req = 0;
-		for (uint32_t c : remaining)
+		for (Task& t : tasks)
 		{
-			const ContourRT& r = R[c];
-			for (uint32_t d = 0; d < r.dirs.size(); d++)
-			{
-				if (r.conv[d] || r.pruned[d])
-					continue;
-				Task t{};
-				t.slot0 = 2 * c;
-				t.slot1 = 2 * c + 1;
-				t.contour_local = c;
-				t.contour_global = c;
-				t.combo = d;
-				t.dir[0] = r.dirs[d].x;
-				t.dir[1] = r.dirs[d].y;
-				t.dir[2] = r.dirs[d].z;
-				const uint32_t v0 = counts[3 * t.slot0], e0 = counts[3 * t.slot0 + 1], f0 = counts[3 * t.slot0 + 2];
-				const uint32_t v1 = counts[3 * t.slot1], e1 = counts[3 * t.slot1 + 1], f1 = counts[3 * t.slot1 + 2];
-				t.n_vf = f1 ? v0 : 0;
-				t.n_ee = e1 ? e0 : 0;
-				t.n_fv = f0 ? v1 : 0;
-				t.req_begin = total_req;
-				total_req += t.n_vf + t.n_ee + t.n_fv;
-				tasks.push_back(t);
-			}
+			const uint32_t v0 = counts[3 * t.slot0], e0 = counts[3 * t.slot0 + 1], f0 = counts[3 * t.slot0 + 2];
+			const uint32_t v1 = counts[3 * t.slot1], e1 = counts[3 * t.slot1 + 1], f1 = counts[3 * t.slot1 + 2];
+			t.n_vf = f1 ? v0 : 0;
+			t.n_ee = e1 ? e0 : 0;
+			t.n_fv = f0 ? v1 : 0;
+			t.req_begin = total_req;
+			total_req += t.n_vf + t.n_ee + t.n_fv;
+			if (!hits_out)
+				alg_tests += uint64_t(t.n_vf) * f1 + uint64_t(t.n_ee) * e1 + uint64_t(t.n_fv) * f0;
 		}
 		const uint32_t nt = uint32_t(tasks.size());
-		if (nt == 0)
-			break;
 		const int tb = bits_for(nt + 1);
 		if (2 + 2 * b + tb > 64)
 			return set_error(ctx, U26_ERR_CAPACITY, "PRP hit key needs %d bits", 2 + 2 * b + tb);
@@ -2137,13 +2327,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		proj_bounds_kernel<<<nt, 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_counts.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), es_,
 			S->d_edges.as<uint2>(), d_x);
 		U26_TRY(after_launch(ctx, "proj_bounds_kernel"));
-		// ray casting with a capacity retry
 		uint32_t nh = 0;
 		for (int attempt = 0; attempt < 8; attempt++)
 		{
 			U26_CUDA(ctx, S->d_keys.reserve(sizeof(uint64_t) * hit_cap));
 			U26_CUDA(ctx, S->d_vals.reserve(sizeof(uint32_t) * hit_cap));
-			U26_CUDA(ctx, S->d_pay_in.reserve(sizeof(float) * 3 * hit_cap));
+			U26_CUDA(ctx, S->d_pay_in.reserve(sizeof(float) * 3 * size_t(hit_cap)));
 			U26_CUDA(ctx, S->d_hitcount.reserve(sizeof(uint32_t)));
 			U26_CUDA(ctx, cudaMemsetAsync(S->d_hitcount.ptr, 0, sizeof(uint32_t), st));
 			HitSink sink{ S->d_keys.as<uint64_t>(), S->d_vals.as<uint32_t>(), S->d_pay_in.as<float>(), S->d_hitcount.as<uint32_t>(), hit_cap, b };
@@ -2152,8 +2341,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			{
 				raycast_kernel<<<div_up(total_req, 128), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
 					S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(),
-					ftv, etv, d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), sink,
-					attempt == 0 ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
+					ftv, etv, d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
+					(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
 				U26_TRY(after_launch(ctx, "raycast_kernel"));
 			}
 			U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_hitcount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -2161,13 +2350,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			nh = *ctx->host_word;
 			if (nh <= hit_cap)
 				break;
-			hit_cap = std::max(hit_cap * 2, nh + nh / 4);
+			hit_cap = uint32_t(std::min<uint64_t>(0xFFFFFFF0ull, std::max<uint64_t>(uint64_t(hit_cap) * 2, uint64_t(nh) + nh / 4)));
 			if (attempt == 7)
 				return set_error(ctx, U26_ERR_CAPACITY, "PRP hit capacity");
 		}
 		out->stage_ms[3] += ms_since(tl);
 		tl = std::chrono::steady_clock::now();
-		// sort hits by (task, type, source, target)
 		ev.mark(1, st);
 		U26_TRY(S->sorter.sort(ctx, S->d_keys.as<uint64_t>(), S->d_vals.as<uint32_t>(), nh, 0, 2 + 2 * b + tb));
 		ev.mark(2, st);
@@ -2176,15 +2364,13 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		segments_kernel<<<div_up(nt + 1, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, nt, S->d_seg.as<uint32_t>());
 		U26_TRY(after_launch(ctx, "segments_kernel"));
 		const uint32_t nh1 = std::max(nh, 1u);
-		U26_CUDA(ctx, S->d_pay.reserve(sizeof(float) * 3 * nh1));
+		U26_CUDA(ctx, S->d_pay.reserve(sizeof(float) * 3 * size_t(nh1)));
 		U26_CUDA(ctx, S->d_parent.reserve(sizeof(uint32_t) * nh1));
 		U26_CUDA(ctx, S->d_root.reserve(sizeof(uint32_t) * nh1));
 		U26_CUDA(ctx, S->d_att.reserve(nh1));
 		U26_CUDA(ctx, S->d_csize.reserve(sizeof(uint32_t) * nh1));
 		U26_CUDA(ctx, S->d_catt.reserve(sizeof(uint32_t) * nh1));
 		U26_CUDA(ctx, S->d_cand_roots.reserve(sizeof(uint32_t) * nh1));
-		std::vector<TaskOut> tout(nt);
-		uint32_t nsel = 0;
 		if (nh)
 		{
 			init_hits_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), S->d_vals.as<uint32_t>(), S->d_pay_in.as<float>(),
@@ -2203,7 +2389,6 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			U26_TRY(after_launch(ctx, "compress_kernel"));
 		}
 		ev.mark(3, st);
-		// support entries of boundary-attached components
 		std::vector<uint32_t> seg_h;
 		U26_TRY(download(ctx, seg_h, S->d_seg.ptr, nt + 1));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
@@ -2214,59 +2399,129 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		const int vb = bits_for(std::max(S->nv, 2u));
 		if (tb + 1 + vb + rb > 64)
 			return set_error(ctx, U26_ERR_CAPACITY, "PRP support key needs %d bits", tb + 1 + vb + rb);
-		const uint32_t ecap = 6u * nh1;
-		U26_CUDA(ctx, S->d_ekeys.reserve(sizeof(uint64_t) * ecap));
-		U26_CUDA(ctx, S->d_evals.reserve(sizeof(uint32_t) * ecap));
+		const uint32_t ecap = uint32_t(std::min<uint64_t>(0xFFFFFFF0ull, 6ull * nh1));
+		U26_CUDA(ctx, S->d_ekeys.reserve(sizeof(uint64_t) * size_t(ecap)));
+		U26_CUDA(ctx, S->d_evals.reserve(sizeof(uint32_t) * size_t(ecap)));
 		U26_CUDA(ctx, S->d_ecount.reserve(sizeof(uint32_t)));
 		U26_CUDA(ctx, cudaMemsetAsync(S->d_ecount.ptr, 0, sizeof(uint32_t), st));
+		U26_CUDA(ctx, S->d_ncand.reserve(sizeof(uint32_t) * 3 * (nt + 1)));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_ncand.ptr, 0, sizeof(uint32_t) * 3 * (nt + 1), st));
+		uint32_t* d_ncand = S->d_ncand.as<uint32_t>();
 		uint32_t ne_entries = 0;
 		if (nh)
 		{
 			entries_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
 				S->d_catt.as<uint32_t>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), vb, rb, S->d_ekeys.as<uint64_t>(),
-				S->d_evals.as<uint32_t>(), S->d_ecount.as<uint32_t>(), ecap);
+				S->d_evals.as<uint32_t>(), S->d_ecount.as<uint32_t>(), ecap, S->d_tasks.as<Task>(), S->d_slots.as<Slot>(),
+				S->d_bnd_bits.as<uint32_t>(), vs);
 			U26_TRY(after_launch(ctx, "entries_kernel"));
+			cand_roots_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
+				S->d_catt.as<uint32_t>(), d_ncand, S->d_cand_roots.as<uint32_t>());
+			U26_TRY(after_launch(ctx, "cand_roots_kernel"));
 			U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_ecount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
 			U26_CUDA(ctx, cudaStreamSynchronize(st));
 			ne_entries = std::min(*ctx->host_word, ecap);
 			U26_TRY(S->esorter.sort(ctx, S->d_ekeys.as<uint64_t>(), S->d_evals.as<uint32_t>(), ne_entries, 0, tb + 1 + vb + rb));
 		}
 		ev.mark(4, st);
+		// best component per task, selected-hit scan, metric terms, canonical sums
+		U26_CUDA(ctx, S->d_best.reserve(sizeof(uint32_t) * 2 * (nt + 1)));
+		uint32_t* d_best = S->d_best.as<uint32_t>();
+		uint32_t* d_bestcov = d_best + (nt + 1);
+		coverage_kernel<<<nt, 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_seg.as<uint32_t>(), d_ncand, S->d_cand_roots.as<uint32_t>(),
+			S->d_csize.as<uint32_t>(), S->d_anchor_off.as<uint32_t>(), S->d_anchors.as<uint32_t>(), S->d_ekeys.as<uint64_t>(), ne_entries, vb,
+			rb, d_best, d_bestcov);
+		U26_TRY(after_launch(ctx, "coverage_kernel"));
+		const uint32_t nblk = div_up(nh1, 1024);
+		U26_CUDA(ctx, S->d_bsum.reserve(sizeof(uint32_t) * (nblk + 2)));
+		U26_CUDA(ctx, S->d_task_max.reserve(sizeof(uint32_t) * 3 * (nt + 1)));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_task_max.ptr, 0, sizeof(uint32_t) * 3 * (nt + 1), st));
+		U26_CUDA(ctx, S->d_selbegin.reserve(sizeof(uint32_t) * (nt + 1)));
+		uint32_t nsel = 0;
+		if (nh)
+		{
+			sel_block_sums_kernel<<<nblk, 256, 0, st>>>(S->d_keys.as<uint64_t>(), S->d_root.as<uint32_t>(), d_best, cd, nh, S->d_bsum.as<uint32_t>());
+			U26_TRY(after_launch(ctx, "sel_block_sums_kernel"));
+			scan_one_block_kernel<<<1, 1024, 0, st>>>(S->d_bsum.as<uint32_t>(), nblk, S->d_bsum.as<uint32_t>() + nblk + 1);
+			U26_TRY(after_launch(ctx, "scan_one_block_kernel"));
+			U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_bsum.as<uint32_t>() + nblk + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+			U26_CUDA(ctx, cudaStreamSynchronize(st));
+			nsel = *ctx->host_word;
+			U26_CUDA(ctx, S->d_pos.reserve(sizeof(uint32_t) * nh1));
+			U26_CUDA(ctx, S->d_terms.reserve(sizeof(float) * 3 * size_t(std::max(nsel, 1u))));
+			if (hits_out)
+				U26_CUDA(ctx, S->d_sel.reserve(sizeof(u26_prp_hit) * size_t(std::max(nsel, 1u))));
+			sel_terms_kernel<<<nblk, 256, 0, st>>>(S->d_keys.as<uint64_t>(), S->d_root.as<uint32_t>(), d_best, cd, nh, S->d_bsum.as<uint32_t>(),
+				S->d_tasks.as<Task>(), S->d_pay.as<float>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_varea.as<float>(),
+				S->d_earea.as<float>(), S->d_farea.as<float>(), S->d_vmass.as<float>(), S->d_vn.as<float>(), S->d_en.as<float>(),
+				S->d_fn.as<float>(), S->d_slots.as<Slot>(), S->d_hop.as<uint32_t>(), vs, S->d_pos.as<uint32_t>(), S->d_terms.as<float>(),
+				S->d_task_max.as<uint32_t>(), hits_out ? S->d_sel.as<u26_prp_hit>() : nullptr);
+			U26_TRY(after_launch(ctx, "sel_terms_kernel"));
+			sel_begin_kernel<<<div_up(nt, 256), 256, 0, st>>>(nt, S->d_seg.as<uint32_t>(), S->d_bsum.as<uint32_t>(), S->d_keys.as<uint64_t>(),
+				S->d_root.as<uint32_t>(), d_best, cd, nh, S->d_selbegin.as<uint32_t>());
+			U26_TRY(after_launch(ctx, "sel_begin_kernel"));
+		}
+		else
+			U26_CUDA(ctx, cudaMemsetAsync(S->d_selbegin.ptr, 0, sizeof(uint32_t) * (nt + 1), st));
 		U26_CUDA(ctx, S->d_out.reserve(sizeof(TaskOut) * nt));
-		task_kernel<<<nt, 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_keys.as<uint64_t>(), cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
-			S->d_csize.as<uint32_t>(), S->d_catt.as<uint32_t>(), S->d_pay.as<float>(), S->d_anchor_off.as<uint32_t>(),
-			S->d_anchors.as<uint32_t>(), S->d_ekeys.as<uint64_t>(), ne_entries, vb, rb, S->d_cand_roots.as<uint32_t>(),
-			S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_varea.as<float>(), S->d_earea.as<float>(), S->d_farea.as<float>(),
-			S->d_vmass.as<float>(), S->d_vn.as<float>(), S->d_en.as<float>(), S->d_fn.as<float>(), S->d_slots.as<Slot>(),
-			S->d_hop.as<uint32_t>(), vs, S->d_out.as<TaskOut>());
-		U26_TRY(after_launch(ctx, "task_kernel"));
+		task_sum_kernel<<<div_up(32 * nt, 256), 256, 0, st>>>(nt, S->d_tasks.as<Task>(), S->d_seg.as<uint32_t>(), d_best, d_bestcov,
+			S->d_csize.as<uint32_t>(), d_ncand, S->d_selbegin.as<uint32_t>(), S->d_terms.as<float>(), S->d_task_max.as<uint32_t>(),
+			S->d_anchor_off.as<uint32_t>(), S->d_out.as<TaskOut>());
+		U26_TRY(after_launch(ctx, "task_sum_kernel"));
 		ev.mark(5, st);
 		U26_TRY(download(ctx, tout, S->d_out.ptr, nt));
-		U26_CUDA(ctx, cudaStreamSynchronize(st));
-		for (uint32_t t = 0; t < nt; t++)
-		{
-			tout[t].sel_offset = nsel;
-			nsel += tout[t].hit_count;
-		}
-		std::vector<u26_prp_hit> sel;
-		if (nsel)
-		{
-			U26_TRY(upload(ctx, S->d_out, tout));
-			U26_CUDA(ctx, S->d_sel.reserve(sizeof(u26_prp_hit) * nsel));
-			gather_kernel<<<nt, 32, 0, st>>>(S->d_out.as<TaskOut>(), nt, S->d_keys.as<uint64_t>(), cd, S->d_root.as<uint32_t>(),
-				S->d_pay.as<float>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_sel.as<u26_prp_hit>());
-			U26_TRY(after_launch(ctx, "gather_kernel"));
-			U26_TRY(download(ctx, sel, S->d_sel.ptr, nsel));
-		}
+		if (hits_out)
+			U26_TRY(download(ctx, *hits_out, S->d_sel.ptr, nsel));
 		ev.mark(6, st);
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
 		if (trace)
-			fprintf(stderr, "[u26 prp] level %u tasks %u requests %u hits %u entries %u selected %u | raycast %.2f sort %.2f union %.2f entries %.2f task %.2f gather %.2f ms\n",
-				level, nt, total_req, nh, ne_entries, nsel, ev.ms(0, 1), ev.ms(1, 2), ev.ms(2, 3), ev.ms(3, 4), ev.ms(4, 5), ev.ms(5, 6));
+			fprintf(stderr, "[u26 prp] %s tasks %u requests %u hits %u entries %u selected %u | raycast %.2f sort %.2f union %.2f entries %.2f select %.2f download %.2f ms\n",
+				hits_out ? "materialize" : "level", nt, total_req, nh, ne_entries, nsel, ev.ms(0, 1), ev.ms(1, 2), ev.ms(2, 3), ev.ms(3, 4), ev.ms(4, 5),
+				ev.ms(5, 6));
 		out->stage_ms[4] += ms_since(tl);
+		return U26_OK;
+	};
+
+	for (; !remaining.empty() && level < 65; level++)
+	{
+		auto tl = std::chrono::steady_clock::now();
+		std::vector<uint32_t> sids;
+		for (uint32_t c : remaining)
+			for (int sd = 0; sd < 2; sd++)
+			{
+				slots[2 * c + sd].k = R[c].k[sd];
+				sids.push_back(2 * c + sd);
+			}
+		std::vector<uint32_t> counts;
+		U26_TRY(build_candidates(sids, counts));
+		out->stage_ms[2] += ms_since(tl);
+		std::vector<Task> tasks;
+		for (uint32_t c : remaining)
+		{
+			const ContourRT& r = R[c];
+			for (uint32_t d = 0; d < r.dirs.size(); d++)
+			{
+				if (r.conv[d] || r.pruned[d])
+					continue;
+				Task t{};
+				t.slot0 = 2 * c;
+				t.slot1 = 2 * c + 1;
+				t.contour_local = c;
+				t.contour_global = c;
+				t.combo = d;
+				t.dir[0] = r.dirs[d].x;
+				t.dir[1] = r.dirs[d].y;
+				t.dir[2] = r.dirs[d].z;
+				tasks.push_back(t);
+			}
+		}
+		if (tasks.empty())
+			break;
+		std::vector<TaskOut> tout;
+		U26_TRY(evaluate(tasks, counts, tout, nullptr));
 		tl = std::chrono::steady_clock::now();
 		// ---- k-ring control (evaluate_current_runtime_directions_template)
-		for (uint32_t t = 0; t < nt; t++)
+		for (size_t t = 0; t < tasks.size(); t++)
 		{
 			const Task& tk = tasks[t];
 			ContourRT& r = R[tk.contour_local];
@@ -2280,7 +2535,6 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			cs.anchors = o.anchors;
 			if (o.best_root != kInfH)
 			{
-				cs.hits.assign(sel.begin() + o.sel_offset, sel.begin() + o.sel_offset + o.hit_count);
 				cs.hit_count = o.hit_count;
 				cs.covered = o.covered;
 				cs.depth = o.depth;
@@ -2349,10 +2603,65 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	}
 	out->levels = level;
 
+	// ---- materialize the winners: re-evaluate each contour's selected (direction, k) once
+	// more with the supports gathered (the evaluation is deterministic, so these are the
+	// hits the selected metrics were computed on)
+	std::vector<int> chosen_idx(nc, -1);
+	{
+		auto tl = std::chrono::steady_clock::now();
+		std::vector<uint32_t> sids;
+		std::vector<Task> tasks;
+		for (uint32_t c = 0; c < nact; c++)
+		{
+			ContourRT& r = R[c];
+			int sel = -1;
+			for (size_t d = 0; d < r.res.size(); d++)
+			{
+				if (!valid_resp(r.res[d]))
+					continue;
+				if (sel < 0 || better_resp(r.res[d], uint32_t(d), r.res[sel], uint32_t(sel)))
+					sel = int(d);
+			}
+			chosen_idx[c] = sel;
+			if (sel < 0)
+				continue;
+			slots[2 * c].k = r.res[sel].eval_k_src;
+			slots[2 * c + 1].k = r.res[sel].eval_k_dst;
+			sids.push_back(2 * c);
+			sids.push_back(2 * c + 1);
+			Task t{};
+			t.slot0 = 2 * c;
+			t.slot1 = 2 * c + 1;
+			t.contour_local = c;
+			t.contour_global = c;
+			t.combo = uint32_t(sel);
+			t.dir[0] = r.dirs[sel].x;
+			t.dir[1] = r.dirs[sel].y;
+			t.dir[2] = r.dirs[sel].z;
+			tasks.push_back(t);
+		}
+		if (!tasks.empty())
+		{
+			std::vector<uint32_t> counts;
+			U26_TRY(build_candidates(sids, counts));
+			std::vector<TaskOut> tout;
+			std::vector<u26_prp_hit> hits;
+			U26_TRY(evaluate(tasks, counts, tout, &hits));
+			for (size_t t = 0; t < tasks.size(); t++)
+			{
+				ComboState& cs = R[tasks[t].contour_local].res[tasks[t].combo];
+				const TaskOut& o = tout[t];
+				if (o.hit_count != cs.hit_count || o.area != cs.area || o.depth != cs.depth || o.covered != cs.covered)
+					return set_error(ctx, U26_ERR_INVALID_INPUT, "PRP winner re-evaluation of contour %u differs", tasks[t].contour_local);
+				cs.hits.assign(hits.begin() + o.sel_offset, hits.begin() + o.sel_offset + o.hit_count);
+			}
+		}
+		out->stage_ms[6] += ms_since(tl);
+	}
+
 	// ---- 4. selection, merge capture, suppression, output
 	t0 = std::chrono::steady_clock::now();
 	std::vector<ComboState> chosen(nc);
-	std::vector<int> chosen_idx(nc, -1);
 	std::vector<std::vector<uint32_t>> merge(nc);
 	std::vector<float> pre_area(nc, 0.0f);
 	auto flags_of = [&](uint32_t v)
@@ -2360,15 +2669,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	for (uint32_t c = 0; c < nact; c++)
 	{
 		ContourRT& r = R[c];
-		int sel = -1;
-		for (size_t d = 0; d < r.res.size(); d++)
-		{
-			if (!valid_resp(r.res[d]))
-				continue;
-			if (sel < 0 || better_resp(r.res[d], uint32_t(d), r.res[sel], uint32_t(sel)))
-				sel = int(d);
-		}
-		chosen_idx[c] = sel;
+		const int sel = chosen_idx[c];
 		if (sel >= 0)
 			chosen[c] = r.res[sel];
 		pre_area[c] = chosen[c].area;
@@ -2525,6 +2826,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	U26_CUDA(ctx, cudaStreamSynchronize(st));
 	out->ray_tests = stats[0];
 	out->ray_requests = stats[1];
+	out->ray_pairs = alg_tests;
 	out->dev_err = *ctx->host_word;
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
@@ -2575,6 +2877,7 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->directions = o->directions.data();
 	v->ray_tests = o->ray_tests;
 	v->ray_requests = o->ray_requests;
+	v->ray_pairs = o->ray_pairs;
 	v->levels = o->levels;
 	v->device_error_flags = o->dev_err;
 	for (int i = 0; i < 8; i++)

@@ -58,7 +58,7 @@ class PrpOutputView(ctypes.Structure):
         ("num_pairs", c_u32), ("num_orig_pairs", c_u32), ("num_contours", c_u32), ("num_hits", c_u32),
         ("pairs", c_vp), ("pair_indices", c_vp), ("mesh_index", c_vp), ("contour_index", c_vp), ("pair_length", c_vp),
         ("contour_offsets", c_vp), ("contour_pairs", c_vp), ("results", c_vp), ("hit_offsets", c_vp), ("hits", c_vp),
-        ("directions", c_vp), ("ray_tests", c_u64), ("ray_requests", c_u64), ("levels", c_u32),
+        ("directions", c_vp), ("ray_tests", c_u64), ("ray_requests", c_u64), ("ray_pairs", c_u64), ("levels", c_u32),
         ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8),
     ]
 
@@ -97,6 +97,7 @@ class PrpResult:
         self.directions = [dirs[c, :self.results[c]["num_dirs"]] for c in range(nc)]
         self.tested = int(v.ray_tests)
         self.requests = int(v.ray_requests)
+        self.pairs_tested = int(v.ray_pairs)
         self.levels = int(v.levels)
         self.device_error_flags = int(v.device_error_flags)
         self.stage_ms = dict(zip(STAGES, list(v.stage_ms)))
