@@ -266,6 +266,9 @@ typedef struct u26_prp_output_view
 	uint32_t levels;				 /* k-ring levels evaluated (max over batches) */
 	uint32_t device_error_flags;
 	double stage_ms[8];				 /* host wall time per stage: preprocess, runtime, candidates, raycast, cull, control, finalize, total */
+	uint64_t ray_nodes;				 /* BVH nodes visited by the ray casts */
+	uint64_t ray_edge_tests;		 /* leaf tests of the EE (edge-edge) casts, included in ray_tests */
+	double gpu_ms[6];				 /* GPU time (CUDA events): ray casting, hit sort, union-find, support entries, selection + metrics, download */
 } u26_prp_output_view;
 
 /* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any

@@ -601,7 +601,7 @@ namespace u26
 			const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats, uint32_t* __restrict__ dev_err)
 		{
 			const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-			uint32_t tested = 0;
+			uint32_t tested = 0, visited = 0, etested = 0;
 			if (r < total)
 			{
 				// task of this request: last task with req_begin <= r
@@ -642,6 +642,7 @@ namespace u26
 					while (sp > 0)
 					{
 						const uint32_t node = stack[--sp];
+						visited++;
 						NodeBox b;
 						b.mn = __ldg(&ftree.boxes[node].mn);
 						b.mx = __ldg(&ftree.boxes[node].mx);
@@ -722,6 +723,7 @@ namespace u26
 						while (sp > 0)
 						{
 							const uint32_t node = stack[--sp];
+							visited++;
 							NodeBox b;
 							b.mn = __ldg(&etree.boxes[node].mn);
 							b.mx = __ldg(&etree.boxes[node].mx);
@@ -731,6 +733,7 @@ namespace u26
 							if (e2 != kInvalid)
 							{
 								tested++;
+								etested++;
 								if (!bit_test(bits, s1.e_lo, s1.e_cnt, e2))
 									continue;
 								const uint2 qv = edges[e2];
@@ -783,10 +786,15 @@ namespace u26
 				const uint32_t mask = __activemask();
 				const uint32_t tsum = __reduce_add_sync(mask, tested);
 				const uint32_t rsum = __reduce_add_sync(mask, r < total ? 1u : 0u);
+				const uint32_t vsum = __reduce_add_sync(mask, visited);
+				const uint32_t esum = __reduce_add_sync(mask, etested);
 				if ((threadIdx.x & 31) == uint32_t(__ffs(mask) - 1))
 				{
+					// [0] leaf primitive tests, [1] requests, [2] nodes visited, [3] edge leaf tests
 					atomicAdd(stats + 0, (unsigned long long)tsum);
 					atomicAdd(stats + 1, (unsigned long long)rsum);
+					atomicAdd(stats + 2, (unsigned long long)vsum);
+					atomicAdd(stats + 3, (unsigned long long)esum);
 				}
 			}
 		}
@@ -1622,6 +1630,7 @@ struct u26_scene
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	RadixSorter sorter, esorter;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
+	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 };
 
 struct u26_prp_output
@@ -1634,6 +1643,8 @@ struct u26_prp_output
 	uint32_t num_orig_pairs = 0, levels = 0, dev_err = 0;
 	uint64_t ray_tests = 0, ray_requests = 0, ray_pairs = 0;
 	double stage_ms[8] = { 0 };
+	double gpu_ms[6] = { 0 };
+	uint64_t ray_nodes = 0, ray_edge_tests = 0;
 };
 
 template <typename T>
@@ -2257,8 +2268,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 
 	// ---- 3. adaptive k-ring levels, every active (contour, direction) task batched
 	const int b = bits_for(std::max({ S->nv, S->ne, S->nf, 2u }));
-	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 2));
-	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 2, st));
+	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 4));
+	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 4, st));
 	const TreeView ftv = tree_view(face_tree), etv = tree_view(edge_tree);
 	const uint32_t bnd_words = vs / 32 + 1;
 	if (nslots)
@@ -2277,10 +2288,11 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			return cur;
 		return uint32_t(std::min<uint64_t>(diam, std::max<uint64_t>(1u, uint64_t(cur) * 2u)));
 	};
-	uint32_t hit_cap = 1u << 20;
+	// hit capacity kept by the scene across passes; grows by 1.5x the count that overflowed
+	uint32_t hit_cap = std::max<uint32_t>(S->hit_cap, 1u << 22);
 	uint32_t level = 0;
 	const bool trace = std::getenv("U26_PRP_TRACE") != nullptr;
-	LevelEvents ev(trace);
+	LevelEvents ev(true);
 	uint64_t alg_tests = 0;
 
 	// candidates of the listed slots at slots[s].k
@@ -2350,7 +2362,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			nh = *ctx->host_word;
 			if (nh <= hit_cap)
 				break;
-			hit_cap = uint32_t(std::min<uint64_t>(0xFFFFFFF0ull, std::max<uint64_t>(uint64_t(hit_cap) * 2, uint64_t(nh) + nh / 4)));
+			hit_cap = uint32_t(std::min<uint64_t>(0xFFFFFFF0ull, std::max<uint64_t>(uint64_t(hit_cap) * 2, uint64_t(nh) + nh / 2)));
+			S->hit_cap = hit_cap;
 			if (attempt == 7)
 				return set_error(ctx, U26_ERR_CAPACITY, "PRP hit capacity");
 		}
@@ -2399,28 +2412,38 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		const int vb = bits_for(std::max(S->nv, 2u));
 		if (tb + 1 + vb + rb > 64)
 			return set_error(ctx, U26_ERR_CAPACITY, "PRP support key needs %d bits", tb + 1 + vb + rb);
-		const uint32_t ecap = uint32_t(std::min<uint64_t>(0xFFFFFFF0ull, 6ull * nh1));
-		U26_CUDA(ctx, S->d_ekeys.reserve(sizeof(uint64_t) * size_t(ecap)));
-		U26_CUDA(ctx, S->d_evals.reserve(sizeof(uint32_t) * size_t(ecap)));
 		U26_CUDA(ctx, S->d_ecount.reserve(sizeof(uint32_t)));
-		U26_CUDA(ctx, cudaMemsetAsync(S->d_ecount.ptr, 0, sizeof(uint32_t), st));
 		U26_CUDA(ctx, S->d_ncand.reserve(sizeof(uint32_t) * 3 * (nt + 1)));
 		U26_CUDA(ctx, cudaMemsetAsync(S->d_ncand.ptr, 0, sizeof(uint32_t) * 3 * (nt + 1), st));
 		uint32_t* d_ncand = S->d_ncand.as<uint32_t>();
 		uint32_t ne_entries = 0;
 		if (nh)
 		{
-			entries_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
-				S->d_catt.as<uint32_t>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), vb, rb, S->d_ekeys.as<uint64_t>(),
-				S->d_evals.as<uint32_t>(), S->d_ecount.as<uint32_t>(), ecap, S->d_tasks.as<Task>(), S->d_slots.as<Slot>(),
-				S->d_bnd_bits.as<uint32_t>(), vs);
-			U26_TRY(after_launch(ctx, "entries_kernel"));
 			cand_roots_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
 				S->d_catt.as<uint32_t>(), d_ncand, S->d_cand_roots.as<uint32_t>());
 			U26_TRY(after_launch(ctx, "cand_roots_kernel"));
-			U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_ecount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-			U26_CUDA(ctx, cudaStreamSynchronize(st));
-			ne_entries = std::min(*ctx->host_word, ecap);
+			// support entries, with a capacity kept across levels (re-run once on overflow)
+			uint32_t ecap = std::max<uint32_t>(S->e_cap, 1u << 20);
+			for (int attempt = 0; attempt < 4; attempt++)
+			{
+				U26_CUDA(ctx, S->d_ekeys.reserve(sizeof(uint64_t) * size_t(ecap)));
+				U26_CUDA(ctx, S->d_evals.reserve(sizeof(uint32_t) * size_t(ecap)));
+				U26_CUDA(ctx, cudaMemsetAsync(S->d_ecount.ptr, 0, sizeof(uint32_t), st));
+				entries_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_root.as<uint32_t>(),
+					S->d_catt.as<uint32_t>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), vb, rb, S->d_ekeys.as<uint64_t>(),
+					S->d_evals.as<uint32_t>(), S->d_ecount.as<uint32_t>(), ecap, S->d_tasks.as<Task>(), S->d_slots.as<Slot>(),
+					S->d_bnd_bits.as<uint32_t>(), vs);
+				U26_TRY(after_launch(ctx, "entries_kernel"));
+				U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_ecount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+				U26_CUDA(ctx, cudaStreamSynchronize(st));
+				ne_entries = *ctx->host_word;
+				if (ne_entries <= ecap)
+					break;
+				ecap = uint32_t(std::min<uint64_t>(0xFFFFFFF0ull, uint64_t(ne_entries) + ne_entries / 2));
+				S->e_cap = ecap;
+				if (attempt == 3)
+					return set_error(ctx, U26_ERR_CAPACITY, "PRP support entry capacity");
+			}
 			U26_TRY(S->esorter.sort(ctx, S->d_ekeys.as<uint64_t>(), S->d_evals.as<uint32_t>(), ne_entries, 0, tb + 1 + vb + rb));
 		}
 		ev.mark(4, st);
@@ -2478,6 +2501,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			fprintf(stderr, "[u26 prp] %s tasks %u requests %u hits %u entries %u selected %u | raycast %.2f sort %.2f union %.2f entries %.2f select %.2f download %.2f ms\n",
 				hits_out ? "materialize" : "level", nt, total_req, nh, ne_entries, nsel, ev.ms(0, 1), ev.ms(1, 2), ev.ms(2, 3), ev.ms(3, 4), ev.ms(4, 5),
 				ev.ms(5, 6));
+		for (int q = 0; q < 6; q++)
+			out->gpu_ms[q] += ev.ms(q, q + 1);
 		out->stage_ms[4] += ms_since(tl);
 		return U26_OK;
 	};
@@ -2821,12 +2846,14 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->hits.insert(out->hits.end(), cs.hits.begin(), cs.hits.end());
 	}
 	std::vector<unsigned long long> stats;
-	U26_TRY(download(ctx, stats, S->d_stats.ptr, 2));
+	U26_TRY(download(ctx, stats, S->d_stats.ptr, 4));
 	U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, ctx->dev_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
 	U26_CUDA(ctx, cudaStreamSynchronize(st));
 	out->ray_tests = stats[0];
 	out->ray_requests = stats[1];
 	out->ray_pairs = alg_tests;
+	out->ray_nodes = stats[2];
+	out->ray_edge_tests = stats[3];
 	out->dev_err = *ctx->host_word;
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
@@ -2878,6 +2905,10 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->ray_tests = o->ray_tests;
 	v->ray_requests = o->ray_requests;
 	v->ray_pairs = o->ray_pairs;
+	v->ray_nodes = o->ray_nodes;
+	v->ray_edge_tests = o->ray_edge_tests;
+	for (int i = 0; i < 6; i++)
+		v->gpu_ms[i] = o->gpu_ms[i];
 	v->levels = o->levels;
 	v->device_error_flags = o->dev_err;
 	for (int i = 0; i < 8; i++)

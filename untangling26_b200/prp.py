@@ -59,8 +59,11 @@ class PrpOutputView(ctypes.Structure):
         ("pairs", c_vp), ("pair_indices", c_vp), ("mesh_index", c_vp), ("contour_index", c_vp), ("pair_length", c_vp),
         ("contour_offsets", c_vp), ("contour_pairs", c_vp), ("results", c_vp), ("hit_offsets", c_vp), ("hits", c_vp),
         ("directions", c_vp), ("ray_tests", c_u64), ("ray_requests", c_u64), ("ray_pairs", c_u64), ("levels", c_u32),
-        ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8),
+        ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8), ("ray_nodes", c_u64),
+        ("ray_edge_tests", c_u64), ("gpu_ms", ctypes.c_double * 6),
     ]
+
+GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
 
 
 def _host_array(p, count, dtype):
@@ -101,3 +104,6 @@ class PrpResult:
         self.levels = int(v.levels)
         self.device_error_flags = int(v.device_error_flags)
         self.stage_ms = dict(zip(STAGES, list(v.stage_ms)))
+        self.gpu_ms = dict(zip(GPU_PHASES, list(v.gpu_ms)))
+        self.nodes_visited = int(v.ray_nodes)
+        self.edge_tests = int(v.ray_edge_tests)
