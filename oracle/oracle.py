@@ -207,12 +207,13 @@ class PrpParams(ctypes.Structure):
         ("ccr_use_current", ctypes.c_uint32),   # PRP_use_deformed_boundary_distance_for_intrinsic_candidates
         ("batch_size", ctypes.c_uint32),        # PRP_cpu_contour_batch_size
         ("brute_force_raycast", ctypes.c_uint32),
+        ("contour_stride", ctypes.c_uint32),    # timing sample: contours c with c % stride == 0 only
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
-                  batch_size=32, brute_force_raycast=0)
+                  batch_size=32, brute_force_raycast=0, contour_stride=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -81,6 +81,7 @@ namespace
 		uint ccr_use_current;
 		uint batch_size;
 		uint brute_force_raycast;
+		uint contour_stride; // sampling option for timing: evaluate contours c with c % stride == 0 (0 or 1: all)
 	};
 
 	struct EfPair
@@ -679,6 +680,7 @@ namespace
 	struct Runtime
 	{
 		uint contour_idx = 0;
+		bool inited = false; // runtime identity built (its batch has started)
 		std::vector<uint> contour;
 		uint object_ids[2] = { 0, 0 };
 		uint comp_ids[2] = { kInf, kInf };
@@ -1130,6 +1132,7 @@ namespace
 	{
 		const MeshIn& m = S.m;
 		r.contour_idx = c;
+		r.inited = true;
 		r.contour = S.contours[c];
 		const uint first = r.contour.front();
 		const EfPair& fp = S.ef[first];
@@ -1819,8 +1822,10 @@ namespace
 					} }, 1);
 		}
 		std::vector<uint> active;
+		const uint stride = std::max(1u, S.p.contour_stride);
 		for (uint c = 0; c < nc && c < S.p.max_contours; c++)
-			active.push_back(c);
+			if (c % stride == 0)
+				active.push_back(c);
 		const uint bs = std::max(1u, S.p.batch_size);
 		for (size_t b0 = 0; b0 < active.size(); b0 += bs)
 		{
@@ -1856,7 +1861,7 @@ namespace
 						// same unordered object pair; a contour whose runtime was never built
 						// (a later batch, or past max_contours) has no object ids yet and
 						// never matches (contour_object_ids sentinel, resolver2.cpp:472-481)
-						if (o == c || o >= nc || o >= b0 + batch.size())
+						if (o == c || o >= nc || !S.rt[o].inited)
 							continue;
 						const Runtime& ro = S.rt[o];
 						if (std::min(ro.object_ids[0], ro.object_ids[1]) == std::min(r.object_ids[0], r.object_ids[1])
