@@ -216,8 +216,11 @@ typedef struct u26_prp_params
 	float ccr_tau;				/* PRP_intrinsic_tau (0.25) */
 	uint32_t ccr_use_rest;		/* PRP_use_rest_geodesic_distance_for_intrinsic_candidates (1) */
 	uint32_t ccr_use_current;	/* PRP_use_deformed_boundary_distance_for_intrinsic_candidates (1) */
-	uint32_t batch_size;		/* PRP_cpu_contour_batch_size; results do not depend on it */
-	uint32_t reserved;
+	uint32_t batch_size;		/* PRP_cpu_contour_batch_size (32): a contour's merge partners are limited to its own or earlier batches */
+	uint32_t opt_iterations;	/* PRP_direction_optimization_iterations (0 = off): projected Newton / Cauchy steps of the
+								 * selected direction on S^2 (intersection_resolver2.cpp:1232-1486) */
+	uint32_t ccr_blend;			/* PRP_use_blended_intrinsic_coordinates (0): one blended ownership coordinate */
+	float ccr_blend_weight;		/* PRP_intrinsic_blend_weight (0.5): rest-coordinate weight of the blend */
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:
@@ -230,10 +233,10 @@ typedef struct u26_prp_result
 	uint32_t boundary_anchor_count, eval_k_src, eval_k_dst, max_frontier_hop_src;
 	uint32_t max_frontier_hop_dst, expansion_level_count, flags, object_id0;
 	uint32_t object_id1, init_k_src, init_k_dst, diam_src;
-	uint32_t diam_dst, num_boundary_src, num_boundary_dst, reserved;
+	uint32_t diam_dst, num_boundary_src, num_boundary_dst, opt_attempted;
 	float dir[3];
 	float depth, volume, objective, area, displacement_cost, coverage, normalized_objective, pre_finalize_area;
-	float reserved_f;
+	uint32_t opt_accepted; /* direction refinement: trial steps taken / accepted (direction_optimization_*_count) */
 } u26_prp_result;
 
 /* One hit of a selected support S(r) (RayCasting::HitInfo, intersection_resolver_helper.h:260-449,

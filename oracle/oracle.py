@@ -208,12 +208,16 @@ class PrpParams(ctypes.Structure):
         ("batch_size", ctypes.c_uint32),        # PRP_cpu_contour_batch_size
         ("brute_force_raycast", ctypes.c_uint32),
         ("contour_stride", ctypes.c_uint32),    # timing sample: contours c with c % stride == 0 only
+        ("opt_iterations", ctypes.c_uint32),    # PRP_direction_optimization_iterations
+        ("ccr_blend", ctypes.c_uint32),         # PRP_use_blended_intrinsic_coordinates
+        ("ccr_blend_weight", ctypes.c_float),   # PRP_intrinsic_blend_weight
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
-                  batch_size=32, brute_force_raycast=0, contour_stride=0)
+                  batch_size=32, brute_force_raycast=0, contour_stride=0, opt_iterations=0, ccr_blend=0,
+                  ccr_blend_weight=0.5)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -226,10 +230,10 @@ RESULT_DTYPE = np.dtype([
     ("max_frontier_hop_src", np.uint32), ("max_frontier_hop_dst", np.uint32), ("expansion_level_count", np.uint32),
     ("flags", np.uint32), ("object_id0", np.uint32), ("object_id1", np.uint32), ("init_k_src", np.uint32),
     ("init_k_dst", np.uint32), ("diam_src", np.uint32), ("diam_dst", np.uint32), ("num_boundary_src", np.uint32),
-    ("num_boundary_dst", np.uint32), ("reserved", np.uint32),
+    ("num_boundary_dst", np.uint32), ("opt_attempted", np.uint32),
     ("dir", np.float32, 3), ("depth", np.float32), ("volume", np.float32), ("objective", np.float32),
     ("area", np.float32), ("displacement_cost", np.float32), ("coverage", np.float32),
-    ("normalized_objective", np.float32), ("pre_finalize_area", np.float32), ("reserved_f", np.float32)])
+    ("normalized_objective", np.float32), ("pre_finalize_area", np.float32), ("opt_accepted", np.uint32)])
 HIT_DTYPE = np.dtype([("type", np.uint32), ("src_id", np.uint32), ("dst_id", np.uint32), ("sv", np.uint32, 3),
                       ("dv", np.uint32, 3), ("bary", np.float32, 2), ("dist", np.float32)])
 assert RESULT_DTYPE.itemsize == 144 and HIT_DTYPE.itemsize == 48

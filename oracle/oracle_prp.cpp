@@ -82,6 +82,9 @@ namespace
 		uint batch_size;
 		uint brute_force_raycast;
 		uint contour_stride; // sampling option for timing: evaluate contours c with c % stride == 0 (0 or 1: all)
+		uint opt_iterations; // PRP_direction_optimization_iterations (scene_params.h:65), 0 = off
+		uint ccr_blend;		 // PRP_use_blended_intrinsic_coordinates (scene_params.h:72)
+		float ccr_blend_weight; // PRP_intrinsic_blend_weight (scene_params.h:73)
 	};
 
 	struct EfPair
@@ -138,6 +141,7 @@ namespace
 		uint eval_k_src = kInf, eval_k_dst = kInf;
 		uint levels = 0;
 		bool eligible = false, full_mesh = false;
+		uint opt_attempted = 0, opt_accepted = 0; // direction_optimization_{iteration,accepted}_count
 		std::vector<Hit> hits;
 	};
 
@@ -691,6 +695,7 @@ namespace
 		std::vector<V3> dirs;
 		std::vector<ComboInfo> results;
 		std::vector<uint8_t> converged, pruned, present;
+		std::vector<uint8_t> active; // active_combos as a mask (all directions, or the one under refinement)
 		uint init_k[2] = { 0, 0 }, k[2] = { 0, 0 };
 		bool finished = false, no_response = false;
 		std::vector<uint> cand_v[2], cand_e[2], cand_f[2];
@@ -1160,6 +1165,7 @@ namespace
 		r.converged.assign(nd, 0);
 		r.pruned.assign(nd, 0);
 		r.present.assign(nd, 0);
+		r.active.assign(nd, 1);
 		for (int s = 0; s < 2; s++)
 		{
 			r.init_k[s] = kring_init(uint(r.boundary[s].size()), r.diam[s]);
@@ -1167,17 +1173,78 @@ namespace
 		}
 	}
 
-	// ---- candidates at level k with contour-side restriction (CCR)
+	// ---- candidates at level k with contour-side restriction (CCR, intersection_resolver2.h:405-506)
+	inline bool reachable(float d) { return finitef(d) && d < std::numeric_limits<float>::max() * 0.5f; }
+
+	// compute_normalized_phi
+	inline float normalized_phi(float own, float opp, float eps = 1e-6f)
+	{
+		const bool g0 = reachable(own), g1 = reachable(opp);
+		if (!g0 && !g1)
+			return 0.0f;
+		if (!g0)
+			return 1.0f;
+		if (!g1)
+			return -1.0f;
+		return (own - opp) / (own + opp + eps);
+	}
+
+	// prp_intrinsic_contour_side_owns_vertex
 	inline bool owns_1(float own, float opp, float tau)
 	{
-		const float unreach = std::numeric_limits<float>::max() * 0.5f;
-		if (!finitef(own) || own >= unreach)
+		if (!reachable(own))
 			return false;
-		if (!finitef(opp) || opp >= unreach)
+		if (!reachable(opp))
 			return true;
-		// compute_normalized_phi with both reachable
-		const float phi = (own - opp) / (own + opp + 1e-6f);
-		return phi <= tau;
+		return normalized_phi(own, opp) <= tau;
+	}
+
+	// prp_dual_metric_contour_side_owns_vertex: each enabled metric passes on its own
+	inline bool owns_dual(float ro, float rp, float co, float cp, float tau, bool use_rest, bool use_cur)
+	{
+		return (!use_rest || owns_1(ro, rp, tau)) && (!use_cur || owns_1(co, cp, tau));
+	}
+
+	// prp_intrinsic_contour_side_blended_phi / _owns_vertex_blended
+	inline float blended_phi(float ro, float rp, float co, float cp, float w, float eps = 1e-6f)
+	{
+		if (!finitef(w) || (!reachable(ro) && !reachable(co)))
+			return std::numeric_limits<float>::infinity();
+		const float pr = normalized_phi(ro, rp, eps), pc = normalized_phi(co, cp, eps);
+		if (!(reachable(ro) && reachable(rp)))
+			return pc;
+		if (!(reachable(co) && reachable(cp)))
+			return pr;
+		const float wc = std::fmin(std::fmax(w, 0.0f), 1.0f);
+		return wc * pr + (1.0f - wc) * pc;
+	}
+	inline bool owns_blended(float ro, float rp, float co, float cp, float tau, float w) { return blended_phi(ro, rp, co, cp, w) <= tau; }
+
+	// prp_contour_roles_share_topology / prp_intrinsic_contour_side_restriction_applies
+	inline bool roles_share_topology(const uint obj[2], const uint comp[2])
+	{
+		return obj[0] == obj[1] && comp[0] != kInf && comp[0] == comp[1];
+	}
+	inline bool ccr_applies(bool enabled, const uint obj[2], const uint comp[2], bool use_deformed)
+	{
+		if (!enabled)
+			return false;
+		if (use_deformed)
+			return obj[0] != kInf && obj[1] != kInf;
+		return roles_share_topology(obj, comp);
+	}
+
+	// the owner test of one vertex for a role (resolver2.cpp:1750-1772)
+	inline bool owns_vertex(const Params& p, float ro, float rp, float co, float cp)
+	{
+		const bool rest = p.ccr_use_rest != 0, cur = p.ccr_use_current != 0;
+		if (p.ccr_blend && rest && cur)
+			return owns_blended(ro, rp, co, cp, p.ccr_tau, p.ccr_blend_weight);
+		if (rest && !owns_1(ro, rp, p.ccr_tau))
+			return false;
+		if (!cur)
+			return true;
+		return owns_dual(ro, rp, co, cp, p.ccr_tau, rest, true);
 	}
 
 	void build_candidates(const Scene& S, Runtime& r)
@@ -1204,15 +1271,7 @@ namespace
 				if (d[face_of(m, f, 0)] <= k && d[face_of(m, f, 1)] <= k && d[face_of(m, f, 2)] <= k)
 					cf.push_back(f);
 		}
-		if (!S.p.use_ccr || !(S.p.ccr_use_rest || S.p.ccr_use_current))
-			return;
-		// restriction applies: deformed distance on -> both object ids valid; else shared topology
-		bool applies;
-		if (S.p.ccr_use_current)
-			applies = true;
-		else
-			applies = r.object_ids[0] == r.object_ids[1] && r.comp_ids[0] != kInf && r.comp_ids[0] == r.comp_ids[1];
-		if (!applies)
+		if (!ccr_applies(S.p.use_ccr && (S.p.ccr_use_rest || S.p.ccr_use_current), r.object_ids, r.comp_ids, S.p.ccr_use_current != 0))
 			return;
 		auto cur = [&](int role, uint v)
 		{
@@ -1231,12 +1290,13 @@ namespace
 			auto owns = [&](uint v)
 			{
 				const float ro = r.geo[role][v], rp = r.geo[role ^ 1][v];
-				const float tau = S.p.ccr_tau;
-				if (S.p.ccr_use_rest && !owns_1(ro, rp, tau))
+				const bool rest = S.p.ccr_use_rest != 0, cur_on = S.p.ccr_use_current != 0;
+				// the current-space distances are only computed where the rule reads them
+				if (!(S.p.ccr_blend && rest && cur_on) && rest && !owns_1(ro, rp, S.p.ccr_tau))
 					return false;
-				if (!S.p.ccr_use_current)
+				if (!cur_on)
 					return true;
-				return (!S.p.ccr_use_rest || owns_1(ro, rp, tau)) && owns_1(cur(role, v), cur(role ^ 1, v), tau);
+				return owns_vertex(S.p, ro, rp, cur(role, v), cur(role ^ 1, v));
 			};
 			auto& cv = r.cand_v[role];
 			cv.erase(std::remove_if(cv.begin(), cv.end(), [&](uint v)
@@ -1670,10 +1730,14 @@ namespace
 			r.finished = false;
 			r.no_response = false;
 			max_combo = std::max(max_combo, uint(r.dirs.size()));
-			std::fill(r.converged.begin(), r.converged.end(), 0);
-			std::fill(r.pruned.begin(), r.pruned.end(), 0);
-			std::fill(r.present.begin(), r.present.end(), 0);
-			std::fill(r.results.begin(), r.results.end(), ComboInfo{});
+			for (size_t ci = 0; ci < r.dirs.size(); ci++)
+				if (r.active[ci])
+				{
+					r.converged[ci] = 0;
+					r.pruned[ci] = 0;
+					r.present[ci] = 0;
+					r.results[ci] = ComboInfo{};
+				}
 		}
 		auto grow = [](uint cur, uint diam) -> uint
 		{
@@ -1692,7 +1756,7 @@ namespace
 				for (uint c : remaining)
 				{
 					const Runtime& r = S.rt[c];
-					if (combo < r.dirs.size() && !r.converged[combo] && !r.pruned[combo])
+					if (combo < r.dirs.size() && r.active[combo] && !r.converged[combo] && !r.pruned[combo])
 						active.push_back(c);
 				}
 				parallel_for(uint(active.size()), [&](uint i)
@@ -1716,19 +1780,19 @@ namespace
 				bool has = false;
 				float best = std::numeric_limits<float>::infinity();
 				for (size_t ci = 0; ci < r.dirs.size(); ci++)
-					if (has_valid(r.results[ci]))
+					if (r.active[ci] && has_valid(r.results[ci]))
 					{
 						has = true;
 						best = std::fmin(best, response_objective(r.results[ci]));
 					}
 				if (has)
 					for (size_t ci = 0; ci < r.dirs.size(); ci++)
-						if (!r.converged[ci] && r.present[ci] && response_objective(r.results[ci]) >= best)
+						if (r.active[ci] && !r.converged[ci] && r.present[ci] && response_objective(r.results[ci]) >= best)
 							r.pruned[ci] = 1;
 				bool pending = false, gs = false, gd = false;
 				for (size_t ci = 0; ci < r.dirs.size(); ci++)
 				{
-					if (r.converged[ci] || r.pruned[ci])
+					if (!r.active[ci] || r.converged[ci] || r.pruned[ci])
 						continue;
 					pending = true;
 					const ComboInfo& info = r.results[ci];
@@ -1753,6 +1817,254 @@ namespace
 				next.push_back(c);
 			}
 			remaining.swap(next);
+		}
+	}
+
+	// ---- S^2 direction refinement (prp_optimize_runtime_directions, resolver2.cpp:1232-1486)
+
+	// compute_effective_inverse_mass_weight (intersection_resolver_helper.cpp:611-645)
+	float eff_inv_mass(const MeshIn& m, const Hit& h)
+	{
+		auto inv_mass = [&](uint v)
+		{ return 1.0f / std::fmax(m.vert_mass[v], 1e-8f); };
+		if (h.type == VF)
+		{
+			const float bx = h.bary[0], by = h.bary[1], bz = 1.0f - h.bary[0] - h.bary[1];
+			return ((inv_mass(h.sv[0]) + bx * bx * inv_mass(h.dv[0])) + by * by * inv_mass(h.dv[1])) + bz * bz * inv_mass(h.dv[2]);
+		}
+		if (h.type == FV)
+		{
+			const float bx = h.bary[0], by = h.bary[1], bz = 1.0f - h.bary[0] - h.bary[1];
+			return ((bx * bx * inv_mass(h.sv[0]) + by * by * inv_mass(h.sv[1])) + bz * bz * inv_mass(h.sv[2])) + inv_mass(h.dv[0]);
+		}
+		const float a0 = h.bary[0], a1 = 1.0f - h.bary[0], b0 = h.bary[1], b1 = 1.0f - h.bary[1];
+		return ((a0 * a0 * inv_mass(h.sv[0]) + a1 * a1 * inv_mass(h.sv[1])) + b0 * b0 * inv_mass(h.dv[0])) + b1 * b1 * inv_mass(h.dv[1]);
+	}
+
+	// get_hit_characteristic_normal (resolver2.cpp:1232-1256), at the current positions
+	V3 hit_normal(const MeshIn& m, const Hit& h)
+	{
+		auto X = [&](uint v)
+		{ return v3(m.x[3 * v], m.x[3 * v + 1], m.x[3 * v + 2]); };
+		if (h.type == VF)
+			return cross(X(h.dv[1]) - X(h.dv[0]), X(h.dv[2]) - X(h.dv[0]));
+		if (h.type == FV)
+			return cross(X(h.sv[1]) - X(h.sv[0]), X(h.sv[2]) - X(h.sv[0]));
+		const V3 p0 = X(h.sv[0]), p1 = X(h.sv[1]), q0 = X(h.dv[0]), q1 = X(h.dv[1]);
+		V3 c = cross(p1 - p0, q1 - q0);
+		if (length(c) < 1e-8f)
+			c = (q0 * h.bary[1] + q1 * (1.0f - h.bary[1])) - (p0 * h.bary[0] + p1 * (1.0f - h.bary[0]));
+		return c;
+	}
+
+	struct DirStep
+	{
+		V3 dir = v3(0.0f);
+		float predicted = 0.0f, gnorm = 0.0f;
+		bool valid = false;
+	};
+
+	// prp_compute_direction_optimization_step (resolver2.cpp:1268-1368). The gradient and
+	// Hessian sums run in the canonical 32-lane strided order over the hits in key order.
+	DirStep direction_step(const MeshIn& m, const std::vector<Hit>& hits, V3 input_dir, float trust)
+	{
+		DirStep out;
+		if (hits.empty() || !valid_dir(input_dir))
+			return out;
+		const V3 r = normalize(input_dir);
+		const float off = 3e-3f; // prp_response_depth_offset (intersection_resolver2.h:98)
+		const uint n = uint(hits.size());
+		// per-hit terms: g[3], H[9] (row-major), contributes
+		std::vector<float> T(size_t(n) * 13, 0.0f);
+		uint contributing = 0;
+		for (uint i = 0; i < n; i++)
+		{
+			const Hit& h = hits[i];
+			const V3 raw = hit_normal(m, h);
+			const float nl = length(raw);
+			if (!finitef(nl) || nl < 1e-8f)
+				continue;
+			const V3 nn = raw / nl;
+			const float ndr = dot(nn, r);
+			if (!finitef(ndr) || std::fabs(ndr) < 1e-6f)
+				continue;
+			const float e = eff_inv_mass(m, h);
+			if (!finitef(e) || e <= 1e-8f)
+				continue;
+			const float w = 1.0f / e;
+			const float d = h.dist;
+			const V3 dd = (nn * (-d)) / ndr;
+			const V3 g = dd * ((2.0f * w) * (d + off));
+			const float hs = ((2.0f * w) / (ndr * ndr)) * ((3.0f * d) * d + (2.0f * d) * off);
+			float* t = &T[size_t(i) * 13];
+			t[0] = g.x;
+			t[1] = g.y;
+			t[2] = g.z;
+			const float nv[3] = { nn.x, nn.y, nn.z };
+			for (int a = 0; a < 3; a++)
+				for (int b2 = 0; b2 < 3; b2++)
+					t[3 + 3 * a + b2] = hs * (nv[a] * nv[b2]);
+			t[12] = 1.0f;
+			contributing++;
+		}
+		if (contributing == 0)
+			return out;
+		float G[3], H[9];
+		for (int q = 0; q < 3; q++)
+			G[q] = lane_sum(n, [&](uint i)
+				{ return T[size_t(i) * 13 + q]; });
+		for (int q = 0; q < 9; q++)
+			H[q] = lane_sum(n, [&](uint i)
+				{ return T[size_t(i) * 13 + 3 + q]; });
+		const V3 grad = v3(G[0], G[1], G[2]);
+		auto Hmul = [&](V3 v)
+		{
+			return v3((H[0] * v.x + H[1] * v.y) + H[2] * v.z, (H[3] * v.x + H[4] * v.y) + H[5] * v.z,
+				(H[6] * v.x + H[7] * v.y) + H[8] * v.z);
+		};
+		const V3 tg = grad - r * dot(r, grad);
+		const V3 axis = std::fabs(r.y) < 0.9f ? v3(0.0f, 1.0f, 0.0f) : v3(1.0f, 0.0f, 0.0f);
+		const V3 e1 = normalize(cross(axis, r));
+		const V3 e2 = normalize(cross(r, e1));
+		const float g0 = dot(e1, tg), g1 = dot(e2, tg);
+		const float gnorm = std::sqrt(g0 * g0 + g1 * g1);
+		if (!finitef(gnorm) || gnorm < 1e-6f)
+			return out;
+		const float h00 = dot(e1, Hmul(e1)), h01 = dot(e1, Hmul(e2)), h10 = dot(e2, Hmul(e1)), h11 = dot(e2, Hmul(e2));
+		const float det = h00 * h11 - h01 * h10;
+		float d0, d1;
+		if (finitef(det) && det > 1e-10f && h00 > 0.0f)
+		{
+			d0 = -(h11 * g0 - h01 * g1) / det;
+			d1 = -(h00 * g1 - h10 * g0) / det;
+		}
+		else
+		{
+			const float gg = g0 * g0 + g1 * g1;
+			const float ghg = g0 * (h00 * g0 + h01 * g1) + g1 * (h10 * g0 + h11 * g1);
+			const float alpha = ghg > 1e-10f ? gg / ghg : trust / (gnorm + 1e-20f);
+			d0 = -alpha * g0;
+			d1 = -alpha * g1;
+		}
+		const float sn = std::sqrt(d0 * d0 + d1 * d1);
+		if (!finitef(sn) || sn < 1e-7f)
+			return out;
+		if (sn > trust)
+		{
+			const float sc = trust / sn;
+			d0 = d0 * sc;
+			d1 = d1 * sc;
+		}
+		const V3 trial = (r + e1 * d0) + e2 * d1;
+		if (!valid_dir(trial))
+			return out;
+		out.dir = normalize(trial);
+		out.predicted = std::fmax(0.0f, -(g0 * d0 + g1 * d1));
+		out.gnorm = gnorm;
+		out.valid = true;
+		return out;
+	}
+
+	int select_best(const Runtime& r)
+	{
+		int sel = -1;
+		for (size_t ci = 0; ci < r.results.size(); ci++)
+		{
+			if (!has_valid(r.results[ci]))
+				continue;
+			if (sel < 0 || response_is_better(r.results[ci], r.results[sel]))
+				sel = int(ci);
+		}
+		return sel;
+	}
+
+	// trust-region loop over the batch's contours; each trial re-runs the k-ring
+	// evaluation of the one refined direction from the initial level
+	void optimize_directions(Scene& S, const std::vector<uint>& batch, uint iterations)
+	{
+		if (iterations == 0 || batch.empty())
+			return;
+		struct St
+		{
+			int combo = -1;
+			uint attempted = 0, accepted = 0;
+			float trust = 0.3f;
+			bool done = false;
+		};
+		std::vector<St> st(batch.size());
+		for (size_t i = 0; i < batch.size(); i++)
+		{
+			const Runtime& r = S.rt[batch[i]];
+			const int sel = select_best(r);
+			if (sel < 0 || r.results[sel].hits.empty())
+				st[i].done = true;
+			else
+				st[i].combo = sel;
+		}
+		for (uint it = 0; it < iterations; it++)
+		{
+			std::vector<ComboInfo> acc(batch.size());
+			std::vector<V3> acc_dir(batch.size(), v3(0.0f));
+			std::vector<float> pred(batch.size(), 0.0f), gn(batch.size(), 0.0f);
+			std::vector<uint> trials;
+			std::vector<size_t> trial_slot;
+			for (size_t i = 0; i < batch.size(); i++)
+			{
+				St& s = st[i];
+				Runtime& r = S.rt[batch[i]];
+				if (s.done)
+					continue;
+				const ComboInfo& a = r.results[s.combo];
+				const DirStep step = direction_step(S.m, a.hits, a.dir, s.trust);
+				if (!step.valid)
+				{
+					s.done = true;
+					continue;
+				}
+				s.attempted++;
+				acc[i] = a;
+				acc_dir[i] = r.dirs[s.combo];
+				pred[i] = step.predicted;
+				gn[i] = step.gnorm;
+				r.dirs[s.combo] = step.dir;
+				std::fill(r.active.begin(), r.active.end(), 0);
+				r.active[s.combo] = 1;
+				trials.push_back(batch[i]);
+				trial_slot.push_back(i);
+			}
+			if (trials.empty())
+				break;
+			evaluate_directions(S, trials);
+			for (size_t j = 0; j < trials.size(); j++)
+			{
+				const size_t i = trial_slot[j];
+				St& s = st[i];
+				Runtime& r = S.rt[trials[j]];
+				std::fill(r.active.begin(), r.active.end(), 1);
+				ComboInfo& trial = r.results[s.combo];
+				// prp_select_response over {accepted, trial}: the trial wins only if strictly better
+				const bool take = has_valid(trial) && (!has_valid(acc[i]) || response_is_better(trial, acc[i]));
+				if (take)
+				{
+					s.accepted++;
+					trial.opt_attempted = s.attempted;
+					trial.opt_accepted = s.accepted;
+					r.dirs[s.combo] = trial.dir;
+					const float actual = response_objective(acc[i]) - response_objective(trial);
+					if (pred[i] > 1e-20f && actual / pred[i] > 0.75f)
+						s.trust = std::fmin(1.0f, s.trust * 2.0f);
+				}
+				else
+				{
+					r.results[s.combo] = acc[i];
+					r.results[s.combo].opt_attempted = s.attempted;
+					r.results[s.combo].opt_accepted = s.accepted;
+					r.dirs[s.combo] = acc_dir[i];
+					s.trust = std::fmax(0.01f, s.trust * 0.5f);
+					if (s.trust <= 0.01f || gn[i] < 1e-6f)
+						s.done = true;
+				}
+			}
 		}
 	}
 
@@ -1833,6 +2145,7 @@ namespace
 			parallel_for(uint(batch.size()), [&](uint i)
 				{ init_runtime(S, S.rt[batch[i]], batch[i]); }, 1);
 			evaluate_directions(S, batch);
+			optimize_directions(S, batch, S.p.opt_iterations);
 			// select_runtime_best_results + pre-finalize merge capture + finalize
 			for (uint c : batch)
 			{
@@ -1919,10 +2232,10 @@ struct OraclePrpResult
 	uint boundary_anchor_count, eval_k_src, eval_k_dst, max_frontier_hop_src;
 	uint max_frontier_hop_dst, expansion_level_count, flags, object_id0;
 	uint object_id1, init_k_src, init_k_dst, diam_src;
-	uint diam_dst, num_boundary_src, num_boundary_dst, reserved;
+	uint diam_dst, num_boundary_src, num_boundary_dst, opt_attempted;
 	float dir[3];
 	float depth, volume, objective, area, displacement_cost, coverage, normalized_objective, pre_finalize_area;
-	float reserved_f;
+	uint opt_accepted;
 };
 static_assert(sizeof(OraclePrpResult) == 24 * 4 + 12 * 4, "result record");
 
@@ -2019,6 +2332,8 @@ extern "C"
 		r.coverage = s.coverage;
 		r.normalized_objective = response_objective(s);
 		r.pre_finalize_area = S->pre_area[c];
+		r.opt_attempted = s.opt_attempted;
+		r.opt_accepted = s.opt_accepted;
 		*out = r;
 	}
 	uint oracle_prp_hits(void* h, uint c, OracleHitRec* out)

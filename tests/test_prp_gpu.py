@@ -64,11 +64,22 @@ def test_prp_two_sheets_26_directions(oracle, u26ctx):
     _compare(res, ref)
 
 
-@pytest.mark.parametrize("ccr", [(1, 1, 1), (1, 1, 0), (0, 0, 0)])
+@pytest.mark.parametrize("ccr", [(1, 1, 1, 0), (1, 1, 0, 0), (1, 0, 1, 0), (0, 0, 0, 0), (1, 1, 1, 1)])
 def test_prp_folded_sheet(oracle, u26ctx, ccr):
+    """Contour-side restriction modes: rest AND current (default), rest only, current only,
+    off, and the blended coordinate (weight 0.5)."""
     m = synthetic.folded_sheet(48, seed=2)
-    res, ref = _run_both(oracle, u26ctx, m, use_ccr=ccr[0], ccr_use_rest=ccr[1], ccr_use_current=ccr[2], max_contours=64)
+    res, ref = _run_both(oracle, u26ctx, m, use_ccr=ccr[0], ccr_use_rest=ccr[1], ccr_use_current=ccr[2], ccr_blend=ccr[3],
+                         max_contours=64)
     assert len(ref.contours) > 1
+    _compare(res, ref)
+
+
+def test_prp_two_objects_rest_only_restriction(oracle, u26ctx):
+    # rest-geodesic ownership only applies when both sides share an object and component;
+    # across two sheets the candidates stay unrestricted
+    m = synthetic.two_sheets(32, seed=2)
+    res, ref = _run_both(oracle, u26ctx, m, ccr_use_current=0)
     _compare(res, ref)
 
 
@@ -77,3 +88,25 @@ def test_prp_no_intersections(oracle, u26ctx):
     m.x[m.num_verts // 2:, 2] += 3.0
     res, ref = _run_both(oracle, u26ctx, m)
     assert len(res.contours) == 0 and len(ref.contours) == 0
+
+
+@pytest.mark.parametrize("iters", [1, 8])
+def test_prp_direction_refinement(oracle, u26ctx, iters):
+    """Projected Newton / Cauchy refinement of the selected direction on S^2: the steps,
+    the trial evaluations from the initial k-ring level and the accept / reject decisions
+    (trial and accepted counts) match the oracle bit for bit."""
+    m = synthetic.folded_sheet(48, seed=2)
+    res, ref = _run_both(oracle, u26ctx, m, opt_iterations=iters, max_contours=64)
+    assert any(r["opt_accepted"] > 0 for r in ref.results)
+    assert all(r["opt_attempted"] <= iters for r in ref.results)
+    _compare(res, ref)
+    assert res.device_error_flags == 0
+
+
+def test_prp_direction_refinement_flat_supports(oracle, u26ctx):
+    # two flat sheets: the supports' normals are parallel to the selected direction, the
+    # tangent gradient vanishes and no trial is taken
+    m = synthetic.two_sheets(32, seed=0)
+    res, ref = _run_both(oracle, u26ctx, m, opt_iterations=4)
+    assert all(r["opt_attempted"] == 0 for r in ref.results)
+    _compare(res, ref)

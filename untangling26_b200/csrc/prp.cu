@@ -291,14 +291,41 @@ namespace u26
 		}
 
 		// ------------------------------------------------------------ candidates
+		// contour-side ownership (intersection_resolver2.h:431-506)
+		__device__ __forceinline__ bool reachable(float d) { return isfinite(d) && d < 3.402823466e+38f * 0.5f; }
+		__device__ __forceinline__ float normalized_phi(float own, float opp)
+		{
+			const bool g0 = reachable(own), g1 = reachable(opp);
+			if (!g0 && !g1)
+				return 0.0f;
+			if (!g0)
+				return 1.0f;
+			if (!g1)
+				return -1.0f;
+			return (own - opp) / (own + opp + 1e-6f);
+		}
 		__device__ __forceinline__ bool owns1(float own, float opp, float tau)
 		{
-			const float unreach = 3.402823466e+38f * 0.5f;
-			if (!isfinite(own) || own >= unreach)
+			if (!reachable(own))
 				return false;
-			if (!isfinite(opp) || opp >= unreach)
+			if (!reachable(opp))
 				return true;
-			const float phi = (own - opp) / (own + opp + 1e-6f);
+			return normalized_phi(own, opp) <= tau;
+		}
+		__device__ __forceinline__ bool owns_blended(float ro, float rp, float co, float cp, float tau, float w)
+		{
+			float phi;
+			if (!isfinite(w) || (!reachable(ro) && !reachable(co)))
+				phi = INFINITY;
+			else if (!(reachable(ro) && reachable(rp)))
+				phi = normalized_phi(co, cp);
+			else if (!(reachable(co) && reachable(cp)))
+				phi = normalized_phi(ro, rp);
+			else
+			{
+				const float wc = fminf(fmaxf(w, 0.0f), 1.0f);
+				phi = wc * normalized_phi(ro, rp) + (1.0f - wc) * normalized_phi(co, cp);
+			}
 			return phi <= tau;
 		}
 
@@ -307,8 +334,8 @@ namespace u26
 			const uint32_t* __restrict__ faces, const uint32_t* __restrict__ vae_off, const uint32_t* __restrict__ vae,
 			const uint32_t* __restrict__ vaf_off, const uint32_t* __restrict__ vaf, uint32_t v_stride, uint32_t e_stride,
 			uint32_t f_stride, const uint32_t* __restrict__ hop, const float* __restrict__ geo, const uint32_t* __restrict__ order,
-			const uint32_t* __restrict__ level_end, uint32_t use_ccr, uint32_t ccr_rest, uint32_t ccr_current, float tau,
-			uint8_t* __restrict__ owns, uint32_t* __restrict__ cand_v, uint32_t* __restrict__ cand_e, uint32_t* __restrict__ cand_f,
+			const uint32_t* __restrict__ level_end, uint32_t ccr_rest, uint32_t ccr_current, uint32_t ccr_blend, float tau,
+			float blend_w, uint8_t* __restrict__ owns, uint32_t* __restrict__ cand_v, uint32_t* __restrict__ cand_e, uint32_t* __restrict__ cand_f,
 			uint32_t* __restrict__ counts, uint32_t* __restrict__ bits_e, uint32_t* __restrict__ bits_f, float* __restrict__ slot_box)
 		{
 			const uint32_t s = slot_ids[blockIdx.x];
@@ -340,7 +367,8 @@ namespace u26
 			const uint32_t k = sl.k;
 			const uint32_t nk = le[min(k, sl.diam)];
 			__syncthreads();
-			const bool applies = use_ccr && (ccr_rest || ccr_current);
+			const bool applies = sl.pad[0] != 0u; // prp_intrinsic_contour_side_restriction_applies, per contour
+			const bool blend = ccr_blend && ccr_rest && ccr_current;
 			for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x)
 			{
 				const uint32_t v = os[i];
@@ -352,7 +380,7 @@ namespace u26
 					float rp = kGeoInf;
 					if (gv >= so.v_lo && gv < so.v_lo + so.v_cnt)
 						rp = go[gv - so.v_lo];
-					if (ccr_rest && !owns1(ro, rp, tau))
+					if (!blend && ccr_rest && !owns1(ro, rp, tau))
 						own = false;
 					else if (ccr_current)
 					{
@@ -362,7 +390,7 @@ namespace u26
 							co = fminf(co, length(xv - ld3(x, bnd[sl.bnd_off + j])));
 						for (uint32_t j = 0; j < so.bnd_cnt; j++)
 							cp = fminf(cp, length(xv - ld3(x, bnd[so.bnd_off + j])));
-						own = (!ccr_rest || owns1(ro, rp, tau)) && owns1(co, cp, tau);
+						own = blend ? owns_blended(ro, rp, co, cp, tau, blend_w) : ((!ccr_rest || owns1(ro, rp, tau)) && owns1(co, cp, tau));
 					}
 				}
 				ow[v] = own ? 1 : 0;
@@ -1442,6 +1470,215 @@ namespace u26
 			}
 		}
 
+		// ------------------------------------------------------------ S^2 direction step
+		struct StepIn
+		{
+			float dir[3];
+			float trust;
+			uint32_t hit_begin, hit_count;
+		};
+		struct StepOut
+		{
+			float dir[3];
+			float predicted, gnorm;
+			uint32_t valid, contributing, pad;
+		};
+
+		__device__ __forceinline__ bool valid_dir(f3 v)
+		{
+			return isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && length_sq(v) > 1e-12f;
+		}
+
+		// compute_effective_inverse_mass_weight (intersection_resolver_helper.cpp:611-645)
+		__device__ __forceinline__ float hit_eff_inv_mass(const u26_prp_hit& h, const float* __restrict__ vert_mass)
+		{
+			auto im = [&](uint32_t v)
+			{ return 1.0f / fmaxf(vert_mass[v], 1e-8f); };
+			const float b0 = h.bary[0], b1 = h.bary[1];
+			if (h.type == 0u)
+			{
+				const float bz = 1.0f - b0 - b1;
+				return ((im(h.src_verts[0]) + b0 * b0 * im(h.dst_verts[0])) + b1 * b1 * im(h.dst_verts[1])) + bz * bz * im(h.dst_verts[2]);
+			}
+			if (h.type == 2u)
+			{
+				const float bz = 1.0f - b0 - b1;
+				return ((b0 * b0 * im(h.src_verts[0]) + b1 * b1 * im(h.src_verts[1])) + bz * bz * im(h.src_verts[2])) + im(h.dst_verts[0]);
+			}
+			const float a1 = 1.0f - b0, c1 = 1.0f - b1;
+			return ((b0 * b0 * im(h.src_verts[0]) + a1 * a1 * im(h.src_verts[1])) + b1 * b1 * im(h.dst_verts[0])) + c1 * c1 * im(h.dst_verts[1]);
+		}
+
+		// get_hit_characteristic_normal (intersection_resolver2.cpp:1232-1256) at x
+		__device__ __forceinline__ f3 hit_normal(const u26_prp_hit& h, const float* __restrict__ x)
+		{
+			if (h.type == 0u)
+			{
+				const f3 A = ld3(x, h.dst_verts[0]), B = ld3(x, h.dst_verts[1]), C = ld3(x, h.dst_verts[2]);
+				return cross(B - A, C - A);
+			}
+			if (h.type == 2u)
+			{
+				const f3 A = ld3(x, h.src_verts[0]), B = ld3(x, h.src_verts[1]), C = ld3(x, h.src_verts[2]);
+				return cross(B - A, C - A);
+			}
+			const f3 p0 = ld3(x, h.src_verts[0]), p1 = ld3(x, h.src_verts[1]), q0 = ld3(x, h.dst_verts[0]), q1 = ld3(x, h.dst_verts[1]);
+			f3 c = cross(p1 - p0, q1 - q0);
+			if (length(c) < 1e-8f)
+				c = (q0 * h.bary[1] + q1 * (1.0f - h.bary[1])) - (p0 * h.bary[0] + p1 * (1.0f - h.bary[0]));
+			return c;
+		}
+
+		// One warp per contour under refinement: the gradient and Gauss-Newton Hessian of
+		// sum_h w_h (delta_h + delta_0)^2 with respect to the direction r over the accepted
+		// support (delta_h' = -delta_h n_h / (n_h . r)), projected to the tangent plane of S^2,
+		// then a Newton step when the 2x2 tangent Hessian is positive definite, else a Cauchy
+		// step, clipped to the trust radius (prp_compute_direction_optimization_step,
+		// intersection_resolver2.cpp:1268-1368). Sums: canonical 32-lane strided order over
+		// the hits in key order; a skipped hit adds zeros.
+		__global__ void dir_step_kernel(uint32_t n, const StepIn* __restrict__ in, const u26_prp_hit* __restrict__ hits,
+			const float* __restrict__ x, const float* __restrict__ vert_mass, StepOut* __restrict__ out)
+		{
+			const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const int lane = threadIdx.x & 31;
+			if (t >= n)
+				return;
+			const StepIn si = in[t];
+			const f3 r0 = mk3(si.dir[0], si.dir[1], si.dir[2]);
+			StepOut o{};
+			if (si.hit_count == 0u || !valid_dir(r0))
+			{
+				if (lane == 0)
+					out[t] = o;
+				return;
+			}
+			const f3 r = normalize(r0);
+			const float off = 3e-3f; // prp_response_depth_offset (intersection_resolver2.h:98)
+			float acc[12];
+#pragma unroll
+			for (int q = 0; q < 12; q++)
+				acc[q] = 0.0f;
+			uint32_t contributing = 0;
+			for (uint32_t i = lane; i < si.hit_count; i += 32)
+			{
+				const u26_prp_hit h = hits[si.hit_begin + i];
+				float term[12];
+#pragma unroll
+				for (int q = 0; q < 12; q++)
+					term[q] = 0.0f;
+				const f3 raw = hit_normal(h, x);
+				const float nl = length(raw);
+				bool use = isfinite(nl) && !(nl < 1e-8f);
+				f3 nn = mk3(0.0f);
+				float ndr = 0.0f, e = 0.0f;
+				if (use)
+				{
+					nn = raw / nl;
+					ndr = dot(nn, r);
+					use = isfinite(ndr) && !(fabsf(ndr) < 1e-6f);
+				}
+				if (use)
+				{
+					e = hit_eff_inv_mass(h, vert_mass);
+					use = isfinite(e) && !(e <= 1e-8f);
+				}
+				if (use)
+				{
+					const float w = 1.0f / e;
+					const float d = h.dist;
+					const f3 dd = (nn * (-d)) / ndr;
+					const f3 g = dd * ((2.0f * w) * (d + off));
+					const float hs = ((2.0f * w) / (ndr * ndr)) * ((3.0f * d) * d + (2.0f * d) * off);
+					const float nv[3] = { nn.x, nn.y, nn.z };
+					term[0] = g.x;
+					term[1] = g.y;
+					term[2] = g.z;
+#pragma unroll
+					for (int a = 0; a < 3; a++)
+#pragma unroll
+						for (int b2 = 0; b2 < 3; b2++)
+							term[3 + 3 * a + b2] = hs * (nv[a] * nv[b2]);
+					contributing++;
+				}
+#pragma unroll
+				for (int q = 0; q < 12; q++)
+					acc[q] = acc[q] + term[q];
+			}
+#pragma unroll
+			for (int q = 0; q < 12; q++)
+				for (int sh = 16; sh >= 1; sh >>= 1)
+					acc[q] = acc[q] + __shfl_xor_sync(0xFFFFFFFFu, acc[q], sh);
+			contributing = __reduce_add_sync(0xFFFFFFFFu, contributing);
+			if (lane != 0)
+				return;
+			o.contributing = contributing;
+			if (contributing == 0u)
+			{
+				out[t] = o;
+				return;
+			}
+			const float* H = acc + 3;
+			auto hmul = [&](f3 v)
+			{
+				return mk3((H[0] * v.x + H[1] * v.y) + H[2] * v.z, (H[3] * v.x + H[4] * v.y) + H[5] * v.z,
+					(H[6] * v.x + H[7] * v.y) + H[8] * v.z);
+			};
+			const f3 grad = mk3(acc[0], acc[1], acc[2]);
+			const f3 tg = grad - r * dot(r, grad);
+			const f3 axis = fabsf(r.y) < 0.9f ? mk3(0.0f, 1.0f, 0.0f) : mk3(1.0f, 0.0f, 0.0f);
+			const f3 e1 = normalize(cross(axis, r));
+			const f3 e2 = normalize(cross(r, e1));
+			const float g0 = dot(e1, tg), g1 = dot(e2, tg);
+			const float gnorm = sqrtf(g0 * g0 + g1 * g1);
+			if (!isfinite(gnorm) || gnorm < 1e-6f)
+			{
+				out[t] = o;
+				return;
+			}
+			const float h00 = dot(e1, hmul(e1)), h01 = dot(e1, hmul(e2)), h10 = dot(e2, hmul(e1)), h11 = dot(e2, hmul(e2));
+			const float det = h00 * h11 - h01 * h10;
+			float d0, d1;
+			if (isfinite(det) && det > 1e-10f && h00 > 0.0f)
+			{
+				d0 = -(h11 * g0 - h01 * g1) / det;
+				d1 = -(h00 * g1 - h10 * g0) / det;
+			}
+			else
+			{
+				const float gg = g0 * g0 + g1 * g1;
+				const float ghg = g0 * (h00 * g0 + h01 * g1) + g1 * (h10 * g0 + h11 * g1);
+				const float alpha = ghg > 1e-10f ? gg / ghg : si.trust / (gnorm + 1e-20f);
+				d0 = -alpha * g0;
+				d1 = -alpha * g1;
+			}
+			const float sn = sqrtf(d0 * d0 + d1 * d1);
+			if (!isfinite(sn) || sn < 1e-7f)
+			{
+				out[t] = o;
+				return;
+			}
+			if (sn > si.trust)
+			{
+				const float sc = si.trust / sn;
+				d0 = d0 * sc;
+				d1 = d1 * sc;
+			}
+			const f3 trial = (r + e1 * d0) + e2 * d1;
+			if (!valid_dir(trial))
+			{
+				out[t] = o;
+				return;
+			}
+			const f3 nd = normalize(trial);
+			o.dir[0] = nd.x;
+			o.dir[1] = nd.y;
+			o.dir[2] = nd.z;
+			o.predicted = fmaxf(0.0f, -(g0 * d0 + g1 * d1));
+			o.gnorm = gnorm;
+			o.valid = 1u;
+			out[t] = o;
+		}
+
 		// selected-hit offset of each task: the scanned position of its first hit
 		__global__ void sel_begin_kernel(uint32_t ntasks, const uint32_t* __restrict__ seg, const uint32_t* __restrict__ bsum_scanned,
 			const uint64_t* __restrict__ keys, const uint32_t* __restrict__ root, const uint32_t* __restrict__ best, HitKeyCodec cd,
@@ -1552,6 +1789,7 @@ namespace
 		uint32_t levels = 0, eval_k_src = kInfH, eval_k_dst = kInfH;
 		uint32_t hit_count = 0, unculled = 0, covered = 0, anchors = 0, mfs = 0, mfd = 0;
 		float depth = 0, volume = 0, area = 0, cost = 0, objective = 0, coverage = 0;
+		uint32_t opt_attempted = 0, opt_accepted = 0; // direction_optimization_{iteration,accepted}_count
 		std::vector<u26_prp_hit> hits;
 	};
 
@@ -1605,6 +1843,7 @@ namespace
 		std::vector<V3h> dirs;
 		std::vector<ComboState> res;
 		std::vector<uint8_t> conv, pruned, present;
+		std::vector<uint8_t> active; // active_combos as a mask: all directions, or the one under refinement
 		uint32_t diam[2] = { 0, 0 }, k0[2] = { 0, 0 }, k[2] = { 0, 0 };
 		bool finished = false, no_resp = false;
 		uint32_t levels = 0;
@@ -1628,6 +1867,7 @@ struct u26_scene
 	DevBuf d_tasks, d_keys, d_vals, d_pay_in, d_pay, d_hitcount, d_stats, d_seg, d_parent, d_root, d_att, d_csize, d_catt;
 	DevBuf d_ekeys, d_evals, d_ecount, d_cand_roots, d_vf_off, d_vf, d_anchor_off, d_anchors, d_out, d_sel;
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
+	DevBuf d_step_in, d_step_hits, d_step_out;
 	RadixSorter sorter, esorter;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
@@ -1757,7 +1997,8 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_counts, &s->d_bits_e, &s->d_bits_f, &s->d_tasks, &s->d_keys, &s->d_vals, &s->d_pay_in, &s->d_pay, &s->d_hitcount,
 		&s->d_stats, &s->d_seg, &s->d_parent, &s->d_root, &s->d_att, &s->d_csize, &s->d_catt, &s->d_ekeys, &s->d_evals,
 		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
-		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms };
+		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
+		&s->d_step_hits, &s->d_step_out };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
@@ -2178,6 +2419,15 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		const uint32_t es = G.mesh_index[first];
 		r.obj[es] = S->vobj[G.ef[first].idx[0]];
 		r.obj[es ^ 1] = S->vobj[G.ef[first].idx[2]];
+		uint32_t comp[2];
+		comp[es] = S->vcomp[G.ef[first].idx[0]];
+		comp[es ^ 1] = S->vcomp[G.ef[first].idx[2]];
+		// prp_intrinsic_contour_side_restriction_applies (intersection_resolver2.h:415-429)
+		bool ccr_on = P->use_ccr && (P->ccr_use_rest || P->ccr_use_current);
+		if (ccr_on && P->ccr_use_current)
+			ccr_on = r.obj[0] != kInfH && r.obj[1] != kInfH;
+		else if (ccr_on)
+			ccr_on = r.obj[0] == r.obj[1] && comp[0] != kInfH && comp[0] == comp[1];
 		std::vector<uint32_t> b[2];
 		for (uint32_t p : G.contours[c])
 		{
@@ -2206,6 +2456,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			sl.bnd_cnt = uint32_t(b[sd].size());
 			sl.k = 0;
 			sl.diam = 0;
+			sl.pad[0] = ccr_on ? 1u : 0u;
+			sl.pad[1] = 0u;
 			bnd.insert(bnd.end(), b[sd].begin(), b[sd].end());
 		}
 		r.dirs = directions(*S, x, G, r, P->direction_mode, gc, gc_valid);
@@ -2214,6 +2466,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		r.conv.assign(nd, 0);
 		r.pruned.assign(nd, 0);
 		r.present.assign(nd, 0);
+		r.active.assign(nd, 1);
 	}
 	const uint32_t nslots = 2 * nact;
 	const uint32_t vs = std::max(1u, S->vmax_obj), es_ = std::max(1u, S->emax_obj), fs = std::max(1u, S->fmax_obj);
@@ -2280,8 +2533,6 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_TRY(after_launch(ctx, "bnd_bits_kernel"));
 		U26_CUDA(ctx, S->d_slot_box.reserve(sizeof(float) * 12 * size_t(nslots)));
 	}
-	std::vector<uint32_t> remaining(nact);
-	std::iota(remaining.begin(), remaining.end(), 0u);
 	auto grow = [](uint32_t cur, uint32_t diam) -> uint32_t
 	{
 		if (cur >= diam)
@@ -2290,7 +2541,6 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	};
 	// hit capacity kept by the scene across passes; grows by 1.5x the count that overflowed
 	uint32_t hit_cap = std::max<uint32_t>(S->hit_cap, 1u << 22);
-	uint32_t level = 0;
 	const bool trace = std::getenv("U26_PRP_TRACE") != nullptr;
 	LevelEvents ev(true);
 	uint64_t alg_tests = 0;
@@ -2303,7 +2553,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		candidates_kernel<<<uint32_t(sids.size()), 256, 0, st>>>(S->d_slots.as<Slot>(), S->d_slot_ids.as<uint32_t>(), S->d_bnd.as<uint32_t>(),
 			d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_vae_off.as<uint32_t>(), S->d_vae.as<uint32_t>(),
 			S->d_vaf_off.as<uint32_t>(), S->d_vaf.as<uint32_t>(), vs, es_, fs, S->d_hop.as<uint32_t>(), S->d_geo.as<float>(),
-			S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(), P->use_ccr, P->ccr_use_rest, P->ccr_use_current, P->ccr_tau,
+			S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(), P->ccr_use_rest, P->ccr_use_current, P->ccr_blend, P->ccr_tau,
+			P->ccr_blend_weight,
 			S->d_owns.as<uint8_t>(), S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), S->d_cand_f.as<uint32_t>(),
 			S->d_counts.as<uint32_t>(), S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(), S->d_slot_box.as<float>());
 		U26_TRY(after_launch(ctx, "candidates_kernel"));
@@ -2507,151 +2758,170 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		return U26_OK;
 	};
 
-	for (; !remaining.empty() && level < 65; level++)
+	// evaluate_current_runtime_directions_template for the listed contours: k from the
+	// initial level, the active directions reset, levels until every active direction has
+	// converged or been pruned
+	auto run_levels = [&](std::vector<uint32_t> remaining) -> u26_status
 	{
+		for (uint32_t c : remaining)
+		{
+			ContourRT& r = R[c];
+			r.k[0] = r.k0[0];
+			r.k[1] = r.k0[1];
+			r.finished = false;
+			r.no_resp = false;
+			for (size_t d = 0; d < r.dirs.size(); d++)
+				if (r.active[d])
+				{
+					r.conv[d] = 0;
+					r.pruned[d] = 0;
+					r.present[d] = 0;
+					r.res[d] = ComboState{};
+				}
+		}
+		uint32_t level = 0;
+		for (; !remaining.empty() && level < 65; level++)
+		{
+			auto tl = std::chrono::steady_clock::now();
+			std::vector<uint32_t> sids;
+			for (uint32_t c : remaining)
+				for (int sd = 0; sd < 2; sd++)
+				{
+					slots[2 * c + sd].k = R[c].k[sd];
+					sids.push_back(2 * c + sd);
+				}
+			std::vector<uint32_t> counts;
+			U26_TRY(build_candidates(sids, counts));
+			out->stage_ms[2] += ms_since(tl);
+			std::vector<Task> tasks;
+			for (uint32_t c : remaining)
+			{
+				const ContourRT& r = R[c];
+				for (uint32_t d = 0; d < r.dirs.size(); d++)
+				{
+					if (!r.active[d] || r.conv[d] || r.pruned[d])
+						continue;
+					Task t{};
+					t.slot0 = 2 * c;
+					t.slot1 = 2 * c + 1;
+					t.contour_local = c;
+					t.contour_global = c;
+					t.combo = d;
+					t.dir[0] = r.dirs[d].x;
+					t.dir[1] = r.dirs[d].y;
+					t.dir[2] = r.dirs[d].z;
+					tasks.push_back(t);
+				}
+			}
+			if (tasks.empty())
+				break;
+			std::vector<TaskOut> tout;
+			U26_TRY(evaluate(tasks, counts, tout, nullptr));
+			tl = std::chrono::steady_clock::now();
+			// ---- k-ring control (evaluate_current_runtime_directions_template)
+			for (size_t t = 0; t < tasks.size(); t++)
+			{
+				const Task& tk = tasks[t];
+				ContourRT& r = R[tk.contour_local];
+				const TaskOut& o = tout[t];
+				ComboState cs;
+				cs.present = true;
+				cs.levels = level + 1;
+				cs.eval_k_src = r.k[0];
+				cs.eval_k_dst = r.k[1];
+				cs.unculled = o.unculled;
+				cs.anchors = o.anchors;
+				if (o.best_root != kInfH)
+				{
+					cs.hit_count = o.hit_count;
+					cs.covered = o.covered;
+					cs.depth = o.depth;
+					cs.volume = o.volume;
+					cs.area = o.area;
+					cs.cost = o.kappa;
+					cs.objective = (o.area * o.depth) * o.depth;
+					cs.coverage = o.anchors > 0 ? float(o.covered) / float(o.anchors) : 0.0f;
+					cs.mfs = o.max_front_src;
+					cs.mfd = o.max_front_dst;
+				}
+				cs.full_mesh = r.k[0] >= r.diam[0] && r.k[1] >= r.diam[1];
+				const bool src_ok = cs.mfs < r.k[0] || r.k[0] >= r.diam[0];
+				const bool dst_ok = cs.mfd < r.k[1] || r.k[1] >= r.diam[1];
+				cs.eligible = usable(cs) && src_ok && dst_ok;
+				r.conv[tk.combo] = (cs.eligible || cs.full_mesh) ? 1 : 0;
+				r.present[tk.combo] = 1;
+				r.res[tk.combo] = std::move(cs);
+			}
+			std::vector<uint32_t> next;
+			for (uint32_t c : remaining)
+			{
+				ContourRT& r = R[c];
+				r.levels = level + 1;
+				bool has = false;
+				float best = std::numeric_limits<float>::infinity();
+				for (size_t d = 0; d < r.dirs.size(); d++)
+					if (r.active[d] && valid_resp(r.res[d]))
+					{
+						has = true;
+						best = std::fmin(best, resp_obj(r.res[d]));
+					}
+				if (has)
+					for (size_t d = 0; d < r.dirs.size(); d++)
+						if (r.active[d] && !r.conv[d] && r.present[d] && resp_obj(r.res[d]) >= best)
+							r.pruned[d] = 1;
+				bool pending = false, gs = false, gd = false;
+				for (size_t d = 0; d < r.dirs.size(); d++)
+				{
+					if (!r.active[d] || r.conv[d] || r.pruned[d])
+						continue;
+					pending = true;
+					const ComboState& cs = r.res[d];
+					gs = gs || (r.k[0] < r.diam[0] && (!usable(cs) || cs.mfs >= r.k[0]));
+					gd = gd || (r.k[1] < r.diam[1] && (!usable(cs) || cs.mfd >= r.k[1]));
+				}
+				if (!pending)
+				{
+					r.finished = true;
+					r.no_resp = !has;
+					continue;
+				}
+				const uint32_t ns = gs ? grow(r.k[0], r.diam[0]) : r.k[0];
+				const uint32_t nd = gd ? grow(r.k[1], r.diam[1]) : r.k[1];
+				if (ns <= r.k[0] && nd <= r.k[1])
+				{
+					r.finished = true;
+					continue;
+				}
+				r.k[0] = ns;
+				r.k[1] = nd;
+				next.push_back(c);
+			}
+			remaining.swap(next);
+			out->stage_ms[5] += ms_since(tl);
+		}
+		out->levels = std::max(out->levels, level);
+		return U26_OK;
+	};
+	{
+		std::vector<uint32_t> all(nact);
+		std::iota(all.begin(), all.end(), 0u);
+		U26_TRY(run_levels(all));
+	}
+	// ---- materialize: re-evaluate the listed (contour, direction) results once more with
+	// the supports gathered (the evaluation is deterministic, so these are the hits the
+	// stored metrics were computed on)
+	auto materialize = [&](const std::vector<std::pair<uint32_t, uint32_t>>& cc) -> u26_status
+	{
+		if (cc.empty())
+			return U26_OK;
 		auto tl = std::chrono::steady_clock::now();
 		std::vector<uint32_t> sids;
-		for (uint32_t c : remaining)
-			for (int sd = 0; sd < 2; sd++)
-			{
-				slots[2 * c + sd].k = R[c].k[sd];
-				sids.push_back(2 * c + sd);
-			}
-		std::vector<uint32_t> counts;
-		U26_TRY(build_candidates(sids, counts));
-		out->stage_ms[2] += ms_since(tl);
 		std::vector<Task> tasks;
-		for (uint32_t c : remaining)
+		for (const auto& [c, d] : cc)
 		{
 			const ContourRT& r = R[c];
-			for (uint32_t d = 0; d < r.dirs.size(); d++)
-			{
-				if (r.conv[d] || r.pruned[d])
-					continue;
-				Task t{};
-				t.slot0 = 2 * c;
-				t.slot1 = 2 * c + 1;
-				t.contour_local = c;
-				t.contour_global = c;
-				t.combo = d;
-				t.dir[0] = r.dirs[d].x;
-				t.dir[1] = r.dirs[d].y;
-				t.dir[2] = r.dirs[d].z;
-				tasks.push_back(t);
-			}
-		}
-		if (tasks.empty())
-			break;
-		std::vector<TaskOut> tout;
-		U26_TRY(evaluate(tasks, counts, tout, nullptr));
-		tl = std::chrono::steady_clock::now();
-		// ---- k-ring control (evaluate_current_runtime_directions_template)
-		for (size_t t = 0; t < tasks.size(); t++)
-		{
-			const Task& tk = tasks[t];
-			ContourRT& r = R[tk.contour_local];
-			const TaskOut& o = tout[t];
-			ComboState cs;
-			cs.present = true;
-			cs.levels = level + 1;
-			cs.eval_k_src = r.k[0];
-			cs.eval_k_dst = r.k[1];
-			cs.unculled = o.unculled;
-			cs.anchors = o.anchors;
-			if (o.best_root != kInfH)
-			{
-				cs.hit_count = o.hit_count;
-				cs.covered = o.covered;
-				cs.depth = o.depth;
-				cs.volume = o.volume;
-				cs.area = o.area;
-				cs.cost = o.kappa;
-				cs.objective = (o.area * o.depth) * o.depth;
-				cs.coverage = o.anchors > 0 ? float(o.covered) / float(o.anchors) : 0.0f;
-				cs.mfs = o.max_front_src;
-				cs.mfd = o.max_front_dst;
-			}
-			cs.full_mesh = r.k[0] >= r.diam[0] && r.k[1] >= r.diam[1];
-			const bool src_ok = cs.mfs < r.k[0] || r.k[0] >= r.diam[0];
-			const bool dst_ok = cs.mfd < r.k[1] || r.k[1] >= r.diam[1];
-			cs.eligible = usable(cs) && src_ok && dst_ok;
-			r.conv[tk.combo] = (cs.eligible || cs.full_mesh) ? 1 : 0;
-			r.present[tk.combo] = 1;
-			r.res[tk.combo] = std::move(cs);
-		}
-		std::vector<uint32_t> next;
-		for (uint32_t c : remaining)
-		{
-			ContourRT& r = R[c];
-			r.levels = level + 1;
-			bool has = false;
-			float best = std::numeric_limits<float>::infinity();
-			for (size_t d = 0; d < r.dirs.size(); d++)
-				if (valid_resp(r.res[d]))
-				{
-					has = true;
-					best = std::fmin(best, resp_obj(r.res[d]));
-				}
-			if (has)
-				for (size_t d = 0; d < r.dirs.size(); d++)
-					if (!r.conv[d] && r.present[d] && resp_obj(r.res[d]) >= best)
-						r.pruned[d] = 1;
-			bool pending = false, gs = false, gd = false;
-			for (size_t d = 0; d < r.dirs.size(); d++)
-			{
-				if (r.conv[d] || r.pruned[d])
-					continue;
-				pending = true;
-				const ComboState& cs = r.res[d];
-				gs = gs || (r.k[0] < r.diam[0] && (!usable(cs) || cs.mfs >= r.k[0]));
-				gd = gd || (r.k[1] < r.diam[1] && (!usable(cs) || cs.mfd >= r.k[1]));
-			}
-			if (!pending)
-			{
-				r.finished = true;
-				r.no_resp = !has;
-				continue;
-			}
-			const uint32_t ns = gs ? grow(r.k[0], r.diam[0]) : r.k[0];
-			const uint32_t nd = gd ? grow(r.k[1], r.diam[1]) : r.k[1];
-			if (ns <= r.k[0] && nd <= r.k[1])
-			{
-				r.finished = true;
-				continue;
-			}
-			r.k[0] = ns;
-			r.k[1] = nd;
-			next.push_back(c);
-		}
-		remaining.swap(next);
-		out->stage_ms[5] += ms_since(tl);
-	}
-	out->levels = level;
-
-	// ---- materialize the winners: re-evaluate each contour's selected (direction, k) once
-	// more with the supports gathered (the evaluation is deterministic, so these are the
-	// hits the selected metrics were computed on)
-	std::vector<int> chosen_idx(nc, -1);
-	{
-		auto tl = std::chrono::steady_clock::now();
-		std::vector<uint32_t> sids;
-		std::vector<Task> tasks;
-		for (uint32_t c = 0; c < nact; c++)
-		{
-			ContourRT& r = R[c];
-			int sel = -1;
-			for (size_t d = 0; d < r.res.size(); d++)
-			{
-				if (!valid_resp(r.res[d]))
-					continue;
-				if (sel < 0 || better_resp(r.res[d], uint32_t(d), r.res[sel], uint32_t(sel)))
-					sel = int(d);
-			}
-			chosen_idx[c] = sel;
-			if (sel < 0)
-				continue;
-			slots[2 * c].k = r.res[sel].eval_k_src;
-			slots[2 * c + 1].k = r.res[sel].eval_k_dst;
+			slots[2 * c].k = r.res[d].eval_k_src;
+			slots[2 * c + 1].k = r.res[d].eval_k_dst;
 			sids.push_back(2 * c);
 			sids.push_back(2 * c + 1);
 			Task t{};
@@ -2659,29 +2929,178 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			t.slot1 = 2 * c + 1;
 			t.contour_local = c;
 			t.contour_global = c;
-			t.combo = uint32_t(sel);
-			t.dir[0] = r.dirs[sel].x;
-			t.dir[1] = r.dirs[sel].y;
-			t.dir[2] = r.dirs[sel].z;
+			t.combo = d;
+			t.dir[0] = r.dirs[d].x;
+			t.dir[1] = r.dirs[d].y;
+			t.dir[2] = r.dirs[d].z;
 			tasks.push_back(t);
 		}
-		if (!tasks.empty())
+		std::vector<uint32_t> counts;
+		U26_TRY(build_candidates(sids, counts));
+		std::vector<TaskOut> tout;
+		std::vector<u26_prp_hit> hits;
+		U26_TRY(evaluate(tasks, counts, tout, &hits));
+		for (size_t t = 0; t < tasks.size(); t++)
 		{
-			std::vector<uint32_t> counts;
-			U26_TRY(build_candidates(sids, counts));
-			std::vector<TaskOut> tout;
-			std::vector<u26_prp_hit> hits;
-			U26_TRY(evaluate(tasks, counts, tout, &hits));
-			for (size_t t = 0; t < tasks.size(); t++)
-			{
-				ComboState& cs = R[tasks[t].contour_local].res[tasks[t].combo];
-				const TaskOut& o = tout[t];
-				if (o.hit_count != cs.hit_count || o.area != cs.area || o.depth != cs.depth || o.covered != cs.covered)
-					return set_error(ctx, U26_ERR_INVALID_INPUT, "PRP winner re-evaluation of contour %u differs", tasks[t].contour_local);
-				cs.hits.assign(hits.begin() + o.sel_offset, hits.begin() + o.sel_offset + o.hit_count);
-			}
+			ComboState& cs = R[tasks[t].contour_local].res[tasks[t].combo];
+			const TaskOut& o = tout[t];
+			if (o.hit_count != cs.hit_count || o.area != cs.area || o.depth != cs.depth || o.covered != cs.covered)
+				return set_error(ctx, U26_ERR_INVALID_INPUT, "PRP re-evaluation of contour %u direction %u differs", tasks[t].contour_local,
+					tasks[t].combo);
+			cs.hits.assign(hits.begin() + o.sel_offset, hits.begin() + o.sel_offset + o.hit_count);
 		}
 		out->stage_ms[6] += ms_since(tl);
+		return U26_OK;
+	};
+	// prp_select_response over a contour's results
+	auto select_best = [&](const ContourRT& r) -> int
+	{
+		int sel = -1;
+		for (size_t d = 0; d < r.res.size(); d++)
+		{
+			if (!valid_resp(r.res[d]))
+				continue;
+			if (sel < 0 || better_resp(r.res[d], uint32_t(d), r.res[sel], uint32_t(sel)))
+				sel = int(d);
+		}
+		return sel;
+	};
+	std::vector<int> chosen_idx(nc, -1);
+	{
+		std::vector<std::pair<uint32_t, uint32_t>> cc;
+		for (uint32_t c = 0; c < nact; c++)
+		{
+			chosen_idx[c] = select_best(R[c]);
+			if (chosen_idx[c] >= 0)
+				cc.emplace_back(c, uint32_t(chosen_idx[c]));
+		}
+		U26_TRY(materialize(cc));
+	}
+
+	// ---- S^2 direction refinement (prp_optimize_runtime_directions,
+	// intersection_resolver2.cpp:1371-1486): per iteration, the steps of all open contours
+	// in one launch, then every trial direction evaluated from the initial k-ring level in
+	// the batched levels, accepted only when strictly better (trust radius x2 / x0.5)
+	if (P->opt_iterations > 0 && nact > 0)
+	{
+		struct OptState
+		{
+			int combo = -1;
+			uint32_t attempted = 0, accepted = 0;
+			float trust = 0.3f;
+			bool done = false;
+		};
+		std::vector<OptState> os(nact);
+		for (uint32_t c = 0; c < nact; c++)
+		{
+			if (chosen_idx[c] < 0 || R[c].res[chosen_idx[c]].hits.empty())
+				os[c].done = true;
+			else
+				os[c].combo = chosen_idx[c];
+		}
+		std::vector<ComboState> acc(nact);
+		std::vector<V3h> acc_dir(nact);
+		std::vector<float> pred(nact, 0.0f), gn(nact, 0.0f);
+		for (uint32_t it = 0; it < P->opt_iterations; it++)
+		{
+			std::vector<uint32_t> open;
+			std::vector<StepIn> sin;
+			std::vector<u26_prp_hit> shits;
+			for (uint32_t c = 0; c < nact; c++)
+			{
+				if (os[c].done)
+					continue;
+				const ContourRT& r = R[c];
+				const ComboState& a = r.res[os[c].combo];
+				StepIn si{};
+				si.dir[0] = r.dirs[os[c].combo].x;
+				si.dir[1] = r.dirs[os[c].combo].y;
+				si.dir[2] = r.dirs[os[c].combo].z;
+				si.trust = os[c].trust;
+				si.hit_begin = uint32_t(shits.size());
+				si.hit_count = uint32_t(a.hits.size());
+				shits.insert(shits.end(), a.hits.begin(), a.hits.end());
+				open.push_back(c);
+				sin.push_back(si);
+			}
+			if (open.empty())
+				break;
+			const uint32_t no = uint32_t(open.size());
+			U26_TRY(upload(ctx, S->d_step_in, sin));
+			U26_TRY(upload(ctx, S->d_step_hits, shits));
+			U26_CUDA(ctx, S->d_step_out.reserve(sizeof(StepOut) * no));
+			dir_step_kernel<<<div_up(32 * no, 256), 256, 0, st>>>(no, S->d_step_in.as<StepIn>(), S->d_step_hits.as<u26_prp_hit>(), d_x,
+				S->d_vmass.as<float>(), S->d_step_out.as<StepOut>());
+			U26_TRY(after_launch(ctx, "dir_step_kernel"));
+			std::vector<StepOut> so;
+			U26_TRY(download(ctx, so, S->d_step_out.ptr, no));
+			U26_CUDA(ctx, cudaStreamSynchronize(st));
+			std::vector<uint32_t> trials;
+			for (uint32_t i = 0; i < no; i++)
+			{
+				const uint32_t c = open[i];
+				ContourRT& r = R[c];
+				const uint32_t d = uint32_t(os[c].combo);
+				if (!so[i].valid)
+				{
+					os[c].done = true;
+					continue;
+				}
+				os[c].attempted++;
+				acc[c] = r.res[d];
+				acc_dir[c] = r.dirs[d];
+				pred[c] = so[i].predicted;
+				gn[c] = so[i].gnorm;
+				r.dirs[d] = mkv(so[i].dir[0], so[i].dir[1], so[i].dir[2]);
+				std::fill(r.active.begin(), r.active.end(), 0);
+				r.active[d] = 1;
+				trials.push_back(c);
+			}
+			if (trials.empty())
+				break;
+			U26_TRY(run_levels(trials));
+			std::vector<std::pair<uint32_t, uint32_t>> taken;
+			for (uint32_t c : trials)
+			{
+				ContourRT& r = R[c];
+				OptState& o = os[c];
+				const uint32_t d = uint32_t(o.combo);
+				std::fill(r.active.begin(), r.active.end(), 1);
+				ComboState& trial = r.res[d];
+				const bool take = valid_resp(trial) && (!valid_resp(acc[c]) || better_resp(trial, d, acc[c], d));
+				if (take)
+				{
+					o.accepted++;
+					trial.opt_attempted = o.attempted;
+					trial.opt_accepted = o.accepted;
+					const float actual = resp_obj(acc[c]) - resp_obj(trial);
+					if (pred[c] > 1e-20f && actual / pred[c] > 0.75f)
+						o.trust = std::fmin(1.0f, o.trust * 2.0f);
+					taken.emplace_back(c, d);
+				}
+				else
+				{
+					r.res[d] = std::move(acc[c]);
+					r.res[d].opt_attempted = o.attempted;
+					r.res[d].opt_accepted = o.accepted;
+					r.dirs[d] = acc_dir[c];
+					o.trust = std::fmax(0.01f, o.trust * 0.5f);
+					if (o.trust <= 0.01f || gn[c] < 1e-6f)
+						o.done = true;
+				}
+				acc[c] = ComboState{};
+			}
+			// the accepted trials' supports feed the next step and the output
+			U26_TRY(materialize(taken));
+		}
+		std::vector<std::pair<uint32_t, uint32_t>> cc;
+		for (uint32_t c = 0; c < nact; c++)
+		{
+			chosen_idx[c] = select_best(R[c]);
+			if (chosen_idx[c] >= 0 && R[c].res[chosen_idx[c]].hits.size() != R[c].res[chosen_idx[c]].hit_count)
+				cc.emplace_back(c, uint32_t(chosen_idx[c]));
+		}
+		U26_TRY(materialize(cc));
 	}
 
 	// ---- 4. selection, merge capture, suppression, output
@@ -2842,6 +3261,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		rr.coverage = cs.coverage;
 		rr.normalized_objective = resp_obj(cs);
 		rr.pre_finalize_area = processed ? pre_area[c] : 0.0f;
+		rr.opt_attempted = cs.opt_attempted;
+		rr.opt_accepted = cs.opt_accepted;
 		out->hit_offsets[c + 1] = out->hit_offsets[c] + rr.hit_count;
 		out->hits.insert(out->hits.end(), cs.hits.begin(), cs.hits.end());
 	}
