@@ -310,3 +310,180 @@ def detect_ef(mesh, d_hat=1e-3, thickness=0.0):
     lbvh_refit(tree, mesh.x, mesh.x, th, mesh.faces)
     broad, _, _ = lbvh_query(tree, QUERY_EDGES_UNCULLED, mesh.x, mesh.x, mesh.edges, dh, th)
     return ef_narrow(broad, mesh.x, mesh.edges, mesh.faces, dh, mesh.vert_property)
+
+
+# ---- unit entry points of the PRP decision rules (intersection_resolver2.h:405-506, 807-912;
+# intersection_resolver2.cpp:311-375, 453-592, 1058-1230, 1268-1368, 1488-1569, 1883-1954)
+
+_F, _U, _I = ctypes.c_float, ctypes.c_uint32, ctypes.c_int
+
+
+def _sig(name, restype, argtypes):
+    f = getattr(lib(), name)
+    f.restype = restype
+    f.argtypes = argtypes
+    return f
+
+
+def ccr_owns(own, opp, tau=0.25):
+    """prp_intrinsic_contour_side_owns_vertex"""
+    return bool(_sig("oracle_ccr_owns", _I, [_F, _F, _F])(own, opp, tau))
+
+
+def ccr_owns_dual(rest_own, rest_opp, cur_own, cur_opp, tau=0.25, use_rest=True, use_current=True):
+    """prp_dual_metric_contour_side_owns_vertex"""
+    f = _sig("oracle_ccr_owns_dual", _I, [_F, _F, _F, _F, _F, _I, _I])
+    return bool(f(rest_own, rest_opp, cur_own, cur_opp, tau, int(use_rest), int(use_current)))
+
+
+def ccr_owns_blended(rest_own, rest_opp, cur_own, cur_opp, tau, weight):
+    """prp_intrinsic_contour_side_owns_vertex_blended"""
+    return bool(_sig("oracle_ccr_owns_blended", _I, [_F] * 6)(rest_own, rest_opp, cur_own, cur_opp, tau, weight))
+
+
+def ccr_blended_phi(rest_own, rest_opp, cur_own, cur_opp, weight):
+    """prp_intrinsic_contour_side_blended_phi"""
+    return _sig("oracle_ccr_blended_phi", _F, [_F] * 5)(rest_own, rest_opp, cur_own, cur_opp, weight)
+
+
+def ccr_roles_share(obj, comp):
+    """prp_contour_roles_share_topology"""
+    return bool(_sig("oracle_ccr_roles_share", _I, [_U] * 4)(obj[0], obj[1], comp[0], comp[1]))
+
+
+def ccr_applies(enabled, obj, comp, use_deformed=False):
+    """prp_intrinsic_contour_side_restriction_applies"""
+    f = _sig("oracle_ccr_applies", _I, [_I, _U, _U, _U, _U, _I])
+    return bool(f(int(enabled), obj[0], obj[1], comp[0], comp[1], int(use_deformed)))
+
+
+RESP_DTYPE = np.dtype([("objective", np.float32), ("coverage", np.float32), ("depth", np.float32), ("cost", np.float32),
+                       ("hit_count", np.uint32), ("covered", np.uint32), ("eligible", np.uint32), ("pad", np.uint32)])
+
+
+def response(objective, coverage, eligible=True, depth=1.0, cost=1.0, hit_count=1, covered=1):
+    """One candidate response record (the fields the comparator reads)."""
+    return (objective, coverage, depth, cost, hit_count, covered, int(eligible), 0)
+
+
+def select_response(responses):
+    """prp_select_response: index of the best valid response, or -1."""
+    a = np.array(responses, RESP_DTYPE)
+    return _sig("oracle_select_response", _I, [_U, ctypes.c_void_p])(len(a), a.ctypes.data_as(ctypes.c_void_p))
+
+
+def response_objective(objective, coverage):
+    """prp_penetration_objective_divided_by_squared_coverage"""
+    return _sig("oracle_response_objective", _F, [_F, _F])(objective, coverage)
+
+
+def classify_contour(is_loop, is_boundary, adj_degree, mesh_index):
+    """classify_contour_type over one contour's pairs (ContourType value)."""
+    il = np.ascontiguousarray(is_loop, np.uint8)
+    ib = np.ascontiguousarray(is_boundary, np.uint8)
+    dg = np.ascontiguousarray(adj_degree, np.uint32)
+    mi = np.ascontiguousarray(mesh_index, np.uint32)
+    f = _sig("oracle_classify_contour", _U, [_U, ctypes.c_void_p, ctypes.c_void_p, _u32p, _u32p])
+    return f(len(il), il.ctypes.data_as(ctypes.c_void_p), ib.ctypes.data_as(ctypes.c_void_p), _p(dg, _u32p), _p(mi, _u32p))
+
+
+def suppress(adjacency, pre_area, active):
+    """prp_select_pre_finalize_contours_to_suppress: sorted suppressed contour ids."""
+    nc = len(adjacency)
+    off = np.zeros(nc + 1, np.uint32)
+    for c, a in enumerate(adjacency):
+        off[c + 1] = off[c] + len(a)
+    adj = np.array([x for a in adjacency for x in a] or [0], np.uint32)
+    area = np.ascontiguousarray(pre_area, np.float32)
+    act = np.array(list(active) or [0], np.uint32)
+    out = np.zeros(nc, np.uint8)
+    f = _sig("oracle_suppress", None, [_U, _u32p, _u32p, _f32p, _U, _u32p, ctypes.c_void_p])
+    f(nc, _p(off, _u32p), _p(adj, _u32p), _p(area, _f32p), len(active), _p(act, _u32p), out.ctypes.data_as(ctypes.c_void_p))
+    return [int(c) for c in np.nonzero(out)[0]]
+
+
+def penetration(hits, direction, vert_area, edge_area, face_area, vert_mass, vn, en, fn):
+    """prp_eval_penetration_v2: dict of depth, volume, area, objective, cost."""
+    h = np.ascontiguousarray(hits, HIT_DTYPE)
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (direction, vert_area, edge_area, face_area, vert_mass, vn, en, fn)]
+    out = np.zeros(5, np.float32)
+    f = _sig("oracle_penetration", None, [_U, ctypes.c_void_p, _f32p, _U, _U, _U] + [_f32p] * 7 + [_f32p])
+    d, va, ea, fa, vm, vn_, en_, fn_ = arrs
+    f(len(h), h.ctypes.data_as(ctypes.c_void_p), _p(d, _f32p), len(va), len(ea), len(fa), _p(va, _f32p), _p(ea, _f32p), _p(fa, _f32p),
+      _p(vm, _f32p), _p(vn_, _f32p), _p(en_, _f32p), _p(fn_, _f32p), _p(out, _f32p))
+    return dict(zip(("depth", "volume", "area", "objective", "cost"), out.tolist()))
+
+
+def seed_directions(points, weights, boundary0, boundary1, x, vert_area, mode=0):
+    """get_raycasting_direction on explicit inputs: (n, 3) float32."""
+    P = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    W = np.ascontiguousarray(weights, np.float32)
+    b0 = np.array(list(boundary0) or [0], np.uint32)
+    b1 = np.array(list(boundary1) or [0], np.uint32)
+    X = np.ascontiguousarray(x, np.float32).reshape(-1, 3)
+    A = np.ascontiguousarray(vert_area, np.float32)
+    out = np.zeros((26, 3), np.float32)
+    f = _sig("oracle_seed_directions", _U, [_U, _U, _f32p, _f32p, _U, _u32p, _U, _u32p, _U, _f32p, _f32p, _f32p])
+    n = f(mode, len(P), _p(P, _f32p), _p(W, _f32p), len(boundary0), _p(b0, _u32p), len(boundary1), _p(b1, _u32p), len(X), _p(X, _f32p),
+          _p(A, _f32p), _p(out, _f32p))
+    return out[:n]
+
+
+class KInfo(ctypes.Structure):
+    _fields_ = [("hit_count", _U), ("covered", _U), ("anchors", _U), ("mfs", _U), ("mfd", _U), ("eligible", _U),
+                ("objective", _F), ("coverage", _F)]
+
+
+_KEVAL = ctypes.CFUNCTYPE(_I, _U, _U, _U, _U, ctypes.POINTER(KInfo))
+
+
+def kring_trace(init_k, diam, evaluate, active=None, cached=None, max_levels=70):
+    """evaluate_current_runtime_directions_template for one runtime with a scripted evaluator.
+
+    evaluate(level, k_src, k_dst, combo) -> dict of KInfo fields (empty dict: no hits).
+    Returns dict(trace=[(k_src, k_dst) per level], finished, no_response, evaluations, eligible)."""
+    n = len(active) if active is not None else 1
+    act = np.ascontiguousarray(active if active is not None else [1], np.uint8)
+    cache = None
+    if cached is not None:
+        cache = (KInfo * n)()
+        for i, c in enumerate(cached):
+            for k, v in (c or {}).items():
+                setattr(cache[i], k, v)
+
+    def cb(level, ks, kd, combo, out):
+        for k, v in evaluate(level, ks, kd, combo).items():
+            setattr(out[0], k, v)
+        return 0
+
+    trace = np.zeros(2 * max_levels, np.uint32)
+    state = np.zeros(4, np.uint32)
+    elig = np.zeros(n, np.uint8)
+    ik = np.array(init_k, np.uint32)
+    dm = np.array(diam, np.uint32)
+    f = _sig("oracle_kring_trace", None, [_u32p, _u32p, _U, ctypes.c_void_p, ctypes.c_void_p, _KEVAL, _u32p, _U, _u32p, ctypes.c_void_p])
+    keep = _KEVAL(cb)
+    f(_p(ik, _u32p), _p(dm, _u32p), n, act.ctypes.data_as(ctypes.c_void_p), ctypes.cast(cache, ctypes.c_void_p) if cache is not None else None,
+      keep, _p(trace, _u32p), max_levels, _p(state, _u32p), elig.ctypes.data_as(ctypes.c_void_p))
+    lv = int(state[3])
+    return dict(trace=[(int(trace[2 * i]), int(trace[2 * i + 1])) for i in range(min(lv, max_levels))], finished=bool(state[0]),
+                no_response=bool(state[1]), evaluations=int(state[2]), eligible=[bool(e) for e in elig])
+
+
+def direction_step(hits, x, vert_mass, direction, trust):
+    """prp_compute_direction_optimization_step: (dir, predicted_reduction, gradient_norm, valid)."""
+    h = np.ascontiguousarray(hits, HIT_DTYPE)
+    X = np.ascontiguousarray(x, np.float32).reshape(-1, 3)
+    M = np.ascontiguousarray(vert_mass, np.float32)
+    d = np.ascontiguousarray(direction, np.float32)
+    out = np.zeros(6, np.float32)
+    f = _sig("oracle_direction_step", None, [_U, ctypes.c_void_p, _U, _f32p, _f32p, _f32p, _F, _f32p])
+    f(len(h), h.ctypes.data_as(ctypes.c_void_p), len(X), _p(X, _f32p), _p(M, _f32p), _p(d, _f32p), trust, _p(out, _f32p))
+    return out[:3].copy(), float(out[3]), float(out[4]), bool(out[5])
+
+
+def hit(type_, src_id, dst_id, src_verts, dst_verts, bary, dist):
+    """One HIT_DTYPE record; unused vertex slots ~0."""
+    sv = list(src_verts) + [0xFFFFFFFF] * (3 - len(src_verts))
+    dv = list(dst_verts) + [0xFFFFFFFF] * (3 - len(dst_verts))
+    return np.array([(type_, src_id, dst_id, sv, dv, bary, dist)], HIT_DTYPE)

@@ -830,6 +830,51 @@ namespace
 	}
 
 	// ---- contours + classification
+	// classify_contour_type (intersection_resolver2.cpp:311-375) over one contour's pairs in
+	// flood-fill order: loop-vertex pairs, boundary-edge pairs, EF-adjacency degree, mesh side.
+	// ContourType (intersection_resolver2.h:27-37): 0 Undefined, 1 Closed, 2 Eight, 3 LL,
+	// 4 BLI, 5 Cross, 6 BIBI (boundary pairs on both sides), 7 BBII (both on one side)
+	uint classify_contour(uint n, const uint8_t* is_loop, const uint8_t* is_bnd, const uint* adj_deg, const uint* mesh_index)
+	{
+		std::vector<uint> bnd, loops;
+		bool closed = true;
+		for (uint i = 0; i < n; i++)
+		{
+			if (is_loop[i])
+				loops.push_back(i);
+			if (is_bnd[i])
+			{
+				bnd.push_back(i);
+				closed = false;
+			}
+			if (!is_loop[i] && adj_deg[i] == 1)
+				closed = false;
+		}
+		uint t = 0;
+		if (bnd.empty())
+		{
+			if (loops.empty() && closed)
+				t = 1;
+			else if (loops.size() == 1 && closed)
+				t = 2;
+			else if (loops.size() == 2 && closed)
+				t = 3;
+		}
+		else if (loops.empty())
+		{
+			if (bnd.size() == 2)
+				t = mesh_index[bnd.front()] == mesh_index[bnd.back()] ? 7 : 6;
+		}
+		else if (loops.size() == 1)
+		{
+			if (bnd.size() == 1)
+				t = 4;
+			else if (bnd.size() == 2)
+				t = 5;
+		}
+		return t;
+	}
+
 	void contours(Scene& S)
 	{
 		const uint n = uint(S.ef.size());
@@ -882,44 +927,18 @@ namespace
 		S.contour_type.resize(S.contours.size());
 		for (uint c = 0; c < S.contours.size(); c++)
 		{
-			std::vector<uint> bnd, loops;
-			bool closed = true;
-			for (uint p : S.contours[c])
+			const auto& C = S.contours[c];
+			std::vector<uint8_t> is_loop(C.size()), is_bnd(C.size());
+			std::vector<uint> deg(C.size()), mi(C.size());
+			for (size_t i = 0; i < C.size(); i++)
 			{
-				const bool is_bnd = (m.eaf_off[S.ef_e[p] + 1] - m.eaf_off[S.ef_e[p]]) <= 1;
-				if (S.ef[p].is_loop())
-					loops.push_back(p);
-				if (is_bnd)
-				{
-					bnd.push_back(p);
-					closed = false;
-				}
-				if (!S.ef[p].is_loop() && S.adj[p].size() == 1)
-					closed = false;
+				const uint p = C[i];
+				is_loop[i] = S.ef[p].is_loop() ? 1 : 0;
+				is_bnd[i] = (m.eaf_off[S.ef_e[p] + 1] - m.eaf_off[S.ef_e[p]]) <= 1 ? 1 : 0;
+				deg[i] = uint(S.adj[p].size());
+				mi[i] = S.mesh_index[p];
 			}
-			uint t = 0;
-			if (bnd.empty())
-			{
-				if (loops.empty() && closed)
-					t = 1;
-				else if (loops.size() == 1 && closed)
-					t = 2;
-				else if (loops.size() == 2 && closed)
-					t = 3;
-			}
-			else if (loops.empty())
-			{
-				if (bnd.size() == 2)
-					t = S.mesh_index[bnd.front()] == S.mesh_index[bnd.back()] ? 7 : 6;
-			}
-			else if (loops.size() == 1)
-			{
-				if (bnd.size() == 1)
-					t = 4;
-				else if (bnd.size() == 2)
-					t = 5;
-			}
-			S.contour_type[c] = t;
+			S.contour_type[c] = classify_contour(uint(C.size()), is_loop.data(), is_bnd.data(), deg.data(), mi.data());
 		}
 		// vertex boundary flags
 		S.vflags.assign(m.num_verts, {});
@@ -1039,11 +1058,15 @@ namespace
 		}
 	}
 
-	std::vector<V3> ray_directions(const Scene& S, const Runtime& r)
+	// get_raycasting_direction (intersection_resolver2.cpp:1488-1569): +-e0, +-e1, +-e2 of the
+	// area-weighted scatter of both sides' anchors about the weighted contour centre
+	// (ascending eigenvalues), centre - side centroid for each side (fallback e1 / e2),
+	// +-(centre - global area-weighted centroid); mode 1: the 26 lattice directions
+	std::vector<V3> seed_directions(uint direction_mode, const std::vector<V3>& pts, const std::vector<float>& pw,
+		const std::vector<uint>* boundary, const float* x, const float* vert_area, uint num_verts)
 	{
-		const MeshIn& m = S.m;
 		std::vector<V3> dirs;
-		if (S.p.direction_mode == 1)
+		if (direction_mode == 1)
 		{
 			for (int dx = -1; dx <= 1; dx++)
 				for (int dy = -1; dy <= 1; dy++)
@@ -1066,27 +1089,27 @@ namespace
 		// weighted mean of the contour points (helper.h:199-228)
 		V3 ws = v3(0.0f), us = v3(0.0f);
 		float sw = 0.0f;
-		for (uint p : r.contour)
+		for (size_t i = 0; i < pts.size(); i++)
 		{
-			const float w = S.length[p];
-			us = us + S.pos3[p];
-			ws = ws + S.pos3[p] * w;
+			const float w = pw[i];
+			us = us + pts[i];
+			ws = ws + pts[i] * w;
 			sw += w;
 		}
-		const V3 center = sw == 0.0f ? us / float(r.contour.size()) : ws / sw;
+		const V3 center = sw == 0.0f ? us / float(pts.size()) : ws / sw;
 		V3 mc[2] = { v3(0.0f), v3(0.0f) };
 		Mat3 Sw = mat_zero();
 		for (int side = 0; side < 2; side++)
 		{
 			float wsum = 0.0f;
 			std::vector<float> wts;
-			for (uint v : r.boundary[side])
+			for (uint v : boundary[side])
 			{
-				const V3 x = load3(m.x, v);
-				const float w = std::fmax(m.rest_vert_area[v], 1e-8f);
+				const V3 xv = load3(x, v);
+				const float w = std::fmax(vert_area[v], 1e-8f);
 				wts.push_back(w);
-				mc[side] = mc[side] + x * w;
-				const V3 c = x - center;
+				mc[side] = mc[side] + xv * w;
+				const V3 c = xv - center;
 				Sw = madd(Sw, mscale(w, outer(c, c)));
 			}
 			for (float w : wts)
@@ -1106,10 +1129,10 @@ namespace
 		}
 		V3 gc = v3(0.0f);
 		float tm = 0.0f;
-		for (uint v = 0; v < m.num_verts; v++)
+		for (uint v = 0; v < num_verts; v++)
 		{
-			const float w = std::fmax(m.rest_vert_area[v], 1e-8f);
-			gc = gc + load3(m.x, v) * w;
+			const float w = std::fmax(vert_area[v], 1e-8f);
+			gc = gc + load3(x, v) * w;
 			tm += w;
 		}
 		if (tm > 1e-8f)
@@ -1122,6 +1145,18 @@ namespace
 		if (dirs.empty())
 			add_signed(v3(0, 1, 0));
 		return dirs;
+	}
+
+	std::vector<V3> ray_directions(const Scene& S, const Runtime& r)
+	{
+		std::vector<V3> pts;
+		std::vector<float> pw;
+		for (uint p : r.contour)
+		{
+			pts.push_back(S.pos3[p]);
+			pw.push_back(S.length[p]);
+		}
+		return seed_directions(S.p.direction_mode, pts, pw, r.boundary, S.m.x, S.m.rest_vert_area, S.m.num_verts);
 	}
 
 	inline uint kring_init(uint boundary_count, uint diam)
@@ -1412,13 +1447,23 @@ namespace
 		return s[0];
 	}
 
-	// prp_eval_penetration_v2 + prp_fill_combo_eval_info over hits in canonical order
-	void fill_metrics(const Scene& S, const Runtime& r, ComboInfo& c)
+	struct PenMetrics
 	{
-		const MeshIn& m = S.m;
-		std::sort(c.hits.begin(), c.hits.end(), [](const Hit& a, const Hit& b)
-			{ return a.key() < b.key(); });
-		const uint n = uint(c.hits.size());
+		float depth = 0, volume = 0, area = 0, objective = 0, cost = 0;
+	};
+
+	// prp_eval_penetration_v2 (intersection_resolver2.cpp:1883-1954) over hits in key order:
+	// A = rest area of the source primitive, alpha = |n_src . r|, delta = dist; depth = max
+	// delta, volume = sum A alpha delta, J = (sum A) depth^2, displacement cost = sum
+	// (delta + 3e-3)^2 / kappa_h. Sums in the canonical 32-lane strided order.
+	PenMetrics penetration_metrics(const MeshIn& m, const V3* vn, const V3* en, const V3* fn, V3 dir, const std::vector<Hit>& hits)
+	{
+		struct HitsRef
+		{
+			V3 dir;
+			const std::vector<Hit>& hits;
+		} c{ dir, hits };
+		const uint n = uint(hits.size());
 		auto inv_mass = [&](uint v)
 		{ return 1.0f / std::fmax(m.vert_mass[v], 1e-8f); };
 		auto area_alpha = [&](const Hit& h, float& area, float& alpha)
@@ -1427,17 +1472,17 @@ namespace
 			if (h.type == VF)
 			{
 				area = m.rest_vert_area[h.src_id];
-				alpha = std::fabs(dot(S.vn[h.src_id], d));
+				alpha = std::fabs(dot(vn[h.src_id], d));
 			}
 			else if (h.type == EE)
 			{
 				area = m.rest_edge_area[h.src_id];
-				alpha = std::fabs(dot(S.en[h.src_id], d));
+				alpha = std::fabs(dot(en[h.src_id], d));
 			}
 			else
 			{
 				area = m.rest_face_area[h.src_id];
-				alpha = std::fabs(dot(S.fn[h.src_id], d));
+				alpha = std::fabs(dot(fn[h.src_id], d));
 			}
 		};
 		auto eff_inv = [&](const Hit& h)
@@ -1467,12 +1512,27 @@ namespace
 				const float sd = c.hits[i].dist + 3e-3f;
 				const float e = eff_inv(c.hits[i]);
 				return e > 1e-8f ? (sd * sd) / e : 0.0f; });
-		c.depth = depth;
-		c.volume = volume;
-		c.area = area;
-		c.objective = (area * depth) * depth;
-		c.cost = kappa;
-		c.hit_count = n;
+		PenMetrics pm;
+		pm.depth = depth;
+		pm.volume = volume;
+		pm.area = area;
+		pm.objective = (area * depth) * depth;
+		pm.cost = kappa;
+		return pm;
+	}
+
+	// prp_eval_penetration_v2 + prp_fill_combo_eval_info over hits in canonical order
+	void fill_metrics(const Scene& S, const Runtime& r, ComboInfo& c)
+	{
+		std::sort(c.hits.begin(), c.hits.end(), [](const Hit& a, const Hit& b)
+			{ return a.key() < b.key(); });
+		const PenMetrics pm = penetration_metrics(S.m, S.vn.data(), S.en.data(), S.fn.data(), c.dir, c.hits);
+		c.depth = pm.depth;
+		c.volume = pm.volume;
+		c.area = pm.area;
+		c.objective = pm.objective;
+		c.cost = pm.cost;
+		c.hit_count = uint(c.hits.size());
 		// EF-anchor coverage
 		std::set<uint> sup[2];
 		for (const Hit& h : c.hits)
@@ -1719,12 +1779,20 @@ namespace
 	}
 
 	// evaluate_current_runtime_directions_template (intersection_resolver2.cpp:1058-1230)
-	void evaluate_directions(Scene& S, std::vector<uint>& batch)
+	// evaluate_current_runtime_directions_template (intersection_resolver2.cpp:1058-1230) over
+	// the listed runtimes: k from the initial level, the active directions reset; per level
+	// build(remaining) prepares the candidates and eval(runtime, combo) evaluates one active,
+	// unconverged, unpruned direction at the runtime's current k. A response is eligible
+	// when usable and detached (frontier hop below k, or k at the diameter, on both roles);
+	// directions whose objective is not below the best valid one are pruned; only the roles
+	// that touch the frontier grow (k <- min(2k, diameter)).
+	template <typename Build, typename Eval>
+	void kring_levels(const std::vector<Runtime*>& batch, Build&& build, Eval&& eval, bool parallel)
 	{
 		uint max_combo = 0;
-		for (uint c : batch)
+		for (Runtime* rp : batch)
 		{
-			Runtime& r = S.rt[c];
+			Runtime& r = *rp;
 			r.k[0] = r.init_k[0];
 			r.k[1] = r.init_k[1];
 			r.finished = false;
@@ -1745,38 +1813,43 @@ namespace
 				return cur;
 			return uint(std::min<uint64_t>(diam, std::max<uint64_t>(1u, uint64_t(cur) * 2u)));
 		};
-		std::vector<uint> remaining = batch;
+		std::vector<Runtime*> remaining = batch;
 		for (uint level = 0; !remaining.empty() && level < 65; level++)
 		{
-			parallel_for(uint(remaining.size()), [&](uint i)
-				{ build_candidates(S, S.rt[remaining[i]]); }, 1);
+			build(remaining);
 			for (uint combo = 0; combo < max_combo; combo++)
 			{
-				std::vector<uint> active;
-				for (uint c : remaining)
+				std::vector<Runtime*> active;
+				for (Runtime* rp : remaining)
 				{
-					const Runtime& r = S.rt[c];
+					const Runtime& r = *rp;
 					if (combo < r.dirs.size() && r.active[combo] && !r.converged[combo] && !r.pruned[combo])
-						active.push_back(c);
+						active.push_back(rp);
 				}
-				parallel_for(uint(active.size()), [&](uint i)
-					{
-						Runtime& r = S.rt[active[i]];
-						ComboInfo info = eval_combo(S, r, combo);
-						info.levels = level + 1;
-						info.full_mesh = r.k[0] >= r.diam[0] && r.k[1] >= r.diam[1];
-						const bool usable = has_usable(info);
-						const bool src_ok = info.max_front_src < r.k[0] || r.k[0] >= r.diam[0];
-						const bool dst_ok = info.max_front_dst < r.k[1] || r.k[1] >= r.diam[1];
-						info.eligible = usable && src_ok && dst_ok;
-						r.converged[combo] = (info.eligible || info.full_mesh) ? 1 : 0;
-						r.present[combo] = 1;
-						r.results[combo] = std::move(info); }, 1);
+				auto one = [&](uint i)
+				{
+					Runtime& r = *active[i];
+					ComboInfo info = eval(r, combo);
+					info.levels = level + 1;
+					info.full_mesh = r.k[0] >= r.diam[0] && r.k[1] >= r.diam[1];
+					const bool usable = has_usable(info);
+					const bool src_ok = info.max_front_src < r.k[0] || r.k[0] >= r.diam[0];
+					const bool dst_ok = info.max_front_dst < r.k[1] || r.k[1] >= r.diam[1];
+					info.eligible = usable && src_ok && dst_ok;
+					r.converged[combo] = (info.eligible || info.full_mesh) ? 1 : 0;
+					r.present[combo] = 1;
+					r.results[combo] = std::move(info);
+				};
+				if (parallel)
+					parallel_for(uint(active.size()), one, 1);
+				else
+					for (uint i = 0; i < active.size(); i++)
+						one(i);
 			}
-			std::vector<uint> next;
-			for (uint c : remaining)
+			std::vector<Runtime*> next;
+			for (Runtime* rp : remaining)
 			{
-				Runtime& r = S.rt[c];
+				Runtime& r = *rp;
 				bool has = false;
 				float best = std::numeric_limits<float>::infinity();
 				for (size_t ci = 0; ci < r.dirs.size(); ci++)
@@ -1814,10 +1887,24 @@ namespace
 				}
 				r.k[0] = ns;
 				r.k[1] = nd;
-				next.push_back(c);
+				next.push_back(rp);
 			}
 			remaining.swap(next);
 		}
+	}
+
+	void evaluate_directions(Scene& S, const std::vector<uint>& batch)
+	{
+		std::vector<Runtime*> rts;
+		for (uint c : batch)
+			rts.push_back(&S.rt[c]);
+		kring_levels(
+			rts, [&](const std::vector<Runtime*>& rem)
+			{ parallel_for(uint(rem.size()), [&](uint i)
+				  { build_candidates(S, *rem[i]); }, 1); },
+			[&](Runtime& r, uint combo)
+			{ return eval_combo(S, r, combo); },
+			true);
 	}
 
 	// ---- S^2 direction refinement (prp_optimize_runtime_directions, resolver2.cpp:1232-1486)
@@ -2099,6 +2186,33 @@ namespace
 					out.insert(a / 2);
 	}
 
+	// prp_select_pre_finalize_contours_to_suppress (intersection_resolver2.cpp:453-592):
+	// contours with merge partners, by pre-finalize area (descending, then index), each
+	// unsuppressed owner suppresses the active contours its support reaches
+	void suppress_contours(const std::vector<std::vector<uint>>& merge_adj, const std::vector<float>& pre_area,
+		const std::vector<uint>& active, std::vector<uint8_t>& suppressed)
+	{
+		std::vector<uint> conflicting;
+		for (uint c : active)
+			if (!merge_adj[c].empty())
+				conflicting.push_back(c);
+		std::sort(conflicting.begin(), conflicting.end(), [&](uint a, uint b)
+			{
+				if (pre_area[a] != pre_area[b]) return pre_area[a] > pre_area[b];
+				return a < b; });
+		std::vector<uint8_t> is_active(merge_adj.size(), 0);
+		for (uint c : active)
+			is_active[c] = 1;
+		for (uint owner : conflicting)
+		{
+			if (suppressed[owner])
+				continue;
+			for (uint a : merge_adj[owner])
+				if (a != owner && is_active[a])
+					suppressed[a] = 1;
+		}
+	}
+
 	void run(Scene& S)
 	{
 		const MeshIn& m = S.m;
@@ -2198,26 +2312,7 @@ namespace
 				r.cur_dist[1].clear();
 			}
 		}
-		// suppression (prp_select_pre_finalize_contours_to_suppress)
-		std::vector<uint> conflicting;
-		for (uint c : active)
-			if (!S.merge_adj[c].empty())
-				conflicting.push_back(c);
-		std::sort(conflicting.begin(), conflicting.end(), [&](uint a, uint b)
-			{
-				if (S.pre_area[a] != S.pre_area[b]) return S.pre_area[a] > S.pre_area[b];
-				return a < b; });
-		std::vector<uint8_t> is_active(nc, 0);
-		for (uint c : active)
-			is_active[c] = 1;
-		for (uint owner : conflicting)
-		{
-			if (S.suppressed[owner])
-				continue;
-			for (uint a : S.merge_adj[owner])
-				if (a != owner && is_active[a])
-					S.suppressed[a] = 1;
-		}
+		suppress_contours(S.merge_adj, S.pre_area, active, S.suppressed);
 		for (uint c = 0; c < nc; c++)
 			if (S.suppressed[c])
 				S.selected[c] = ComboInfo{};
@@ -2391,5 +2486,245 @@ extern "C"
 			out9[3 * k + 1] = ev[k].y;
 			out9[3 * k + 2] = ev[k].z;
 		}
+	}
+
+	// ---- unit entry points of the PRP decision rules (known-answer tests) ----
+
+	int oracle_ccr_owns(float own, float opp, float tau) { return owns_1(own, opp, tau) ? 1 : 0; }
+	int oracle_ccr_owns_dual(float ro, float rp, float co, float cp, float tau, int use_rest, int use_cur)
+	{
+		return owns_dual(ro, rp, co, cp, tau, use_rest != 0, use_cur != 0) ? 1 : 0;
+	}
+	int oracle_ccr_owns_blended(float ro, float rp, float co, float cp, float tau, float w) { return owns_blended(ro, rp, co, cp, tau, w) ? 1 : 0; }
+	float oracle_ccr_blended_phi(float ro, float rp, float co, float cp, float w) { return blended_phi(ro, rp, co, cp, w); }
+	int oracle_ccr_roles_share(uint o0, uint o1, uint c0, uint c1)
+	{
+		const uint o[2] = { o0, o1 }, c[2] = { c0, c1 };
+		return roles_share_topology(o, c) ? 1 : 0;
+	}
+	int oracle_ccr_applies(int enabled, uint o0, uint o1, uint c0, uint c1, int use_deformed)
+	{
+		const uint o[2] = { o0, o1 }, c[2] = { c0, c1 };
+		return ccr_applies(enabled != 0, o, c, use_deformed != 0) ? 1 : 0;
+	}
+
+	struct OracleResp
+	{
+		float objective, coverage, depth, cost;
+		uint hit_count, covered, eligible, pad;
+	};
+	static ComboInfo combo_from(const OracleResp& q, uint idx)
+	{
+		ComboInfo c;
+		c.present = true;
+		c.combo_idx = idx;
+		c.objective = q.objective;
+		c.coverage = q.coverage;
+		c.depth = q.depth;
+		c.cost = q.cost;
+		c.hit_count = q.hit_count;
+		c.hits.resize(q.hit_count);
+		c.covered = q.covered;
+		c.anchors = q.covered;
+		c.eligible = q.eligible != 0;
+		return c;
+	}
+	// prp_select_response: index of the best valid response, -1 when none
+	int oracle_select_response(uint n, const OracleResp* q)
+	{
+		std::vector<ComboInfo> v;
+		for (uint i = 0; i < n; i++)
+			v.push_back(combo_from(q[i], i));
+		int sel = -1;
+		for (uint i = 0; i < n; i++)
+		{
+			if (!has_valid(v[i]))
+				continue;
+			if (sel < 0 || response_is_better(v[i], v[sel]))
+				sel = int(i);
+		}
+		return sel;
+	}
+	float oracle_response_objective(float objective, float coverage) { return objective_div_cov2(objective, coverage); }
+
+	uint oracle_classify_contour(uint n, const uint8_t* is_loop, const uint8_t* is_bnd, const uint* deg, const uint* mesh_index)
+	{
+		return classify_contour(n, is_loop, is_bnd, deg, mesh_index);
+	}
+
+	void oracle_suppress(uint nc, const uint* adj_off, const uint* adj, const float* pre_area, uint nactive, const uint* active, uint8_t* out)
+	{
+		std::vector<std::vector<uint>> m(nc);
+		for (uint c = 0; c < nc; c++)
+			m[c].assign(adj + adj_off[c], adj + adj_off[c + 1]);
+		std::vector<float> area(pre_area, pre_area + nc);
+		std::vector<uint> act(active, active + nactive);
+		std::vector<uint8_t> sup(nc, 0);
+		suppress_contours(m, area, act, sup);
+		std::memcpy(out, sup.data(), nc);
+	}
+
+	static std::vector<Hit> hits_from(uint n, const OracleHitRec* h)
+	{
+		std::vector<Hit> v(n);
+		for (uint i = 0; i < n; i++)
+		{
+			v[i].type = h[i].type;
+			v[i].src_id = h[i].src_id;
+			v[i].dst_id = h[i].dst_id;
+			for (int k = 0; k < 3; k++)
+			{
+				v[i].sv[k] = h[i].sv[k];
+				v[i].dv[k] = h[i].dv[k];
+			}
+			v[i].bary[0] = h[i].bary[0];
+			v[i].bary[1] = h[i].bary[1];
+			v[i].dist = h[i].dist;
+		}
+		return v;
+	}
+
+	// prp_eval_penetration_v2 on a hit list: out = depth, volume, area, objective, cost
+	void oracle_penetration(uint n, const OracleHitRec* hits, const float* dir, uint nv, uint ne, uint nf, const float* vert_area,
+		const float* edge_area, const float* face_area, const float* vert_mass, const float* vn, const float* en, const float* fn, float* out5)
+	{
+		MeshIn m{};
+		m.num_verts = nv;
+		m.num_edges = ne;
+		m.num_faces = nf;
+		m.rest_vert_area = vert_area;
+		m.rest_edge_area = edge_area;
+		m.rest_face_area = face_area;
+		m.vert_mass = vert_mass;
+		auto v3s = [](const float* p, uint k)
+		{
+			std::vector<V3> r(k);
+			for (uint i = 0; i < k; i++)
+				r[i] = v3(p[3 * i], p[3 * i + 1], p[3 * i + 2]);
+			return r;
+		};
+		const std::vector<V3> VN = v3s(vn, nv), EN = v3s(en, ne), FN = v3s(fn, nf);
+		std::vector<Hit> H = hits_from(n, hits);
+		std::sort(H.begin(), H.end(), [](const Hit& a, const Hit& b)
+			{ return a.key() < b.key(); });
+		const PenMetrics pm = penetration_metrics(m, VN.data(), EN.data(), FN.data(), v3(dir[0], dir[1], dir[2]), H);
+		out5[0] = pm.depth;
+		out5[1] = pm.volume;
+		out5[2] = pm.area;
+		out5[3] = pm.objective;
+		out5[4] = pm.cost;
+	}
+
+	// get_raycasting_direction on explicit inputs; returns the direction count (<= 26)
+	uint oracle_seed_directions(uint mode, uint npts, const float* pts, const float* w, uint nb0, const uint* b0, uint nb1, const uint* b1,
+		uint nv, const float* x, const float* vert_area, float* out)
+	{
+		std::vector<V3> P(npts);
+		std::vector<float> W(w, w + npts);
+		for (uint i = 0; i < npts; i++)
+			P[i] = v3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]);
+		std::vector<uint> B[2] = { std::vector<uint>(b0, b0 + nb0), std::vector<uint>(b1, b1 + nb1) };
+		const std::vector<V3> d = seed_directions(mode, P, W, B, x, vert_area, nv);
+		for (size_t i = 0; i < d.size() && i < 26; i++)
+		{
+			out[3 * i] = d[i].x;
+			out[3 * i + 1] = d[i].y;
+			out[3 * i + 2] = d[i].z;
+		}
+		return uint(std::min<size_t>(d.size(), 26));
+	}
+
+	struct OracleKInfo
+	{
+		uint hit_count, covered, anchors, mfs, mfd, eligible;
+		float objective, coverage;
+	};
+	typedef int (*OracleKEval)(uint level, uint k_src, uint k_dst, uint combo, OracleKInfo* out);
+
+	// The adaptive k-ring control of one runtime with a scripted evaluator (cb). cached holds
+	// the stored results of inactive directions (or null). trace receives (k_src, k_dst) of
+	// every level; state = finished, no_response, evaluations, levels; eligible per direction.
+	void oracle_kring_trace(const uint* init_k, const uint* diam, uint ndirs, const uint8_t* active, const OracleKInfo* cached, OracleKEval cb,
+		uint* trace, uint max_levels, uint* state, uint8_t* eligible)
+	{
+		Runtime r;
+		r.dirs.assign(ndirs, v3(0.0f, 1.0f, 0.0f));
+		r.results.assign(ndirs, ComboInfo{});
+		r.converged.assign(ndirs, 0);
+		r.pruned.assign(ndirs, 0);
+		r.present.assign(ndirs, 0);
+		r.active.assign(active, active + ndirs);
+		r.init_k[0] = init_k[0];
+		r.init_k[1] = init_k[1];
+		r.diam[0] = diam[0];
+		r.diam[1] = diam[1];
+		auto to_info = [](const OracleKInfo& q, uint combo)
+		{
+			ComboInfo c;
+			c.present = true;
+			c.combo_idx = combo;
+			c.hit_count = q.hit_count;
+			c.hits.resize(q.hit_count);
+			c.covered = q.covered;
+			c.anchors = q.anchors;
+			c.max_front_src = q.mfs;
+			c.max_front_dst = q.mfd;
+			c.objective = q.objective;
+			c.coverage = q.coverage;
+			c.eligible = q.eligible != 0;
+			return c;
+		};
+		if (cached)
+			for (uint d = 0; d < ndirs; d++)
+				if (!r.active[d])
+				{
+					r.results[d] = to_info(cached[d], d);
+					r.present[d] = 1;
+				}
+		uint levels = 0, evals = 0;
+		std::vector<Runtime*> rts{ &r };
+		kring_levels(
+			rts, [&](const std::vector<Runtime*>&)
+			{
+				if (levels < max_levels)
+				{
+					trace[2 * levels] = r.k[0];
+					trace[2 * levels + 1] = r.k[1];
+				}
+				levels++; },
+			[&](Runtime& rr, uint combo)
+			{
+				OracleKInfo q{};
+				cb(levels - 1, rr.k[0], rr.k[1], combo, &q);
+				evals++;
+				return to_info(q, combo);
+			},
+			false);
+		state[0] = r.finished ? 1 : 0;
+		state[1] = r.no_response ? 1 : 0;
+		state[2] = evals;
+		state[3] = levels;
+		for (uint d = 0; d < ndirs; d++)
+			eligible[d] = r.results[d].eligible ? 1 : 0;
+	}
+
+	// prp_compute_direction_optimization_step: out = dir[3], predicted reduction, gradient norm, valid
+	void oracle_direction_step(uint n, const OracleHitRec* hits, uint nv, const float* x, const float* vert_mass, const float* dir, float trust,
+		float* out6)
+	{
+		MeshIn m{};
+		m.num_verts = nv;
+		m.x = x;
+		m.vert_mass = vert_mass;
+		std::vector<Hit> H = hits_from(n, hits);
+		std::sort(H.begin(), H.end(), [](const Hit& a, const Hit& b)
+			{ return a.key() < b.key(); });
+		const DirStep st = direction_step(m, H, v3(dir[0], dir[1], dir[2]), trust);
+		out6[0] = st.dir.x;
+		out6[1] = st.dir.y;
+		out6[2] = st.dir.z;
+		out6[3] = st.predicted;
+		out6[4] = st.gnorm;
+		out6[5] = st.valid ? 1.0f : 0.0f;
 	}
 }
