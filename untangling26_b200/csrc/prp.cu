@@ -42,7 +42,11 @@
 #include <set>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "lbvh_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace u26
 {
@@ -329,6 +333,73 @@ namespace u26
 			return phi <= tau;
 		}
 
+		// Current-space distance of each k-ring vertex to the nearest boundary anchor of its own
+		// side and of the opposite side (deformed_boundary_distance, intersection_resolver2.cpp:
+		// 1706-1738), cached across the levels of a pass (NaN = not yet computed). One warp per
+		// vertex, lanes over the anchors; min over squared distances, then one sqrt (sqrt is
+		// monotone and correctly rounded, so this equals the min of the lengths). Only the
+		// vertices whose ownership test reads the current distances are computed.
+		__global__ void __launch_bounds__(256) ccr_current_kernel(const Slot* __restrict__ slots, const uint32_t* __restrict__ slot_ids,
+			const uint32_t* __restrict__ bnd, const float* __restrict__ x, uint32_t v_stride, const float* __restrict__ geo,
+			const uint32_t* __restrict__ order, const uint32_t* __restrict__ level_end, uint32_t ccr_rest, uint32_t ccr_blend, float tau,
+			uint32_t blocks_per_slot, float* __restrict__ cur_own, float* __restrict__ cur_opp)
+		{
+			const uint32_t s = slot_ids[blockIdx.x / blocks_per_slot];
+			const uint32_t o = s ^ 1u;
+			const Slot sl = slots[s];
+			if (sl.pad[0] == 0u)
+				return;
+			const Slot so = slots[o];
+			const uint32_t nk = level_end[size_t(s) * (v_stride + 1) + min(sl.k, sl.diam)];
+			const float* gs = geo + size_t(s) * v_stride;
+			const float* go = geo + size_t(o) * v_stride;
+			const uint32_t* os = order + size_t(s) * v_stride;
+			float* co_out = cur_own + size_t(s) * v_stride;
+			float* cp_out = cur_opp + size_t(s) * v_stride;
+			const int lane = threadIdx.x & 31;
+			const uint32_t wid = (blockIdx.x % blocks_per_slot) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+			const uint32_t nw = blocks_per_slot * (blockDim.x >> 5);
+			const bool blend = ccr_blend && ccr_rest;
+			for (uint32_t i = wid; i < nk; i += nw)
+			{
+				const uint32_t v = os[i];
+				if (!isnan(co_out[v]))
+					continue;
+				const uint32_t gv = sl.v_lo + v;
+				if (!blend && ccr_rest)
+				{
+					float rp = kGeoInf;
+					if (gv >= so.v_lo && gv < so.v_lo + so.v_cnt)
+						rp = go[gv - so.v_lo];
+					if (!owns1(gs[v], rp, tau))
+						continue;
+				}
+				const f3 xv = ld3(x, gv);
+				float m_own = INFINITY, m_opp = INFINITY;
+				for (uint32_t j = lane; j < sl.bnd_cnt; j += 32)
+				{
+					const f3 d = xv - ld3(x, bnd[sl.bnd_off + j]);
+					m_own = fminf(m_own, dot(d, d));
+				}
+				for (uint32_t j = lane; j < so.bnd_cnt; j += 32)
+				{
+					const f3 d = xv - ld3(x, bnd[so.bnd_off + j]);
+					m_opp = fminf(m_opp, dot(d, d));
+				}
+#pragma unroll
+				for (int off = 16; off >= 1; off >>= 1)
+				{
+					m_own = fminf(m_own, __shfl_xor_sync(0xFFFFFFFFu, m_own, off));
+					m_opp = fminf(m_opp, __shfl_xor_sync(0xFFFFFFFFu, m_opp, off));
+				}
+				if (lane == 0)
+				{
+					co_out[v] = fminf(3.402823466e+38f, sqrtf(m_own));
+					cp_out[v] = fminf(3.402823466e+38f, sqrtf(m_opp));
+				}
+			}
+		}
+
 		__global__ void __launch_bounds__(256) candidates_kernel(const Slot* __restrict__ slots, const uint32_t* __restrict__ slot_ids,
 			const uint32_t* __restrict__ bnd, const float* __restrict__ x, const uint2* __restrict__ edges,
 			const uint32_t* __restrict__ faces, const uint32_t* __restrict__ vae_off, const uint32_t* __restrict__ vae,
@@ -336,7 +407,8 @@ namespace u26
 			uint32_t f_stride, const uint32_t* __restrict__ hop, const float* __restrict__ geo, const uint32_t* __restrict__ order,
 			const uint32_t* __restrict__ level_end, uint32_t ccr_rest, uint32_t ccr_current, uint32_t ccr_blend, float tau,
 			float blend_w, uint8_t* __restrict__ owns, uint32_t* __restrict__ cand_v, uint32_t* __restrict__ cand_e, uint32_t* __restrict__ cand_f,
-			uint32_t* __restrict__ counts, uint32_t* __restrict__ bits_e, uint32_t* __restrict__ bits_f, float* __restrict__ slot_box)
+			uint32_t* __restrict__ counts, uint32_t* __restrict__ bits_e, uint32_t* __restrict__ bits_f, float* __restrict__ slot_box,
+			const float* __restrict__ cur_own, const float* __restrict__ cur_opp)
 		{
 			const uint32_t s = slot_ids[blockIdx.x];
 			const uint32_t o = s ^ 1u; // the other side of the same contour
@@ -384,12 +456,7 @@ namespace u26
 						own = false;
 					else if (ccr_current)
 					{
-						const f3 xv = ld3(x, gv);
-						float co = 3.402823466e+38f, cp = 3.402823466e+38f;
-						for (uint32_t j = 0; j < sl.bnd_cnt; j++)
-							co = fminf(co, length(xv - ld3(x, bnd[sl.bnd_off + j])));
-						for (uint32_t j = 0; j < so.bnd_cnt; j++)
-							cp = fminf(cp, length(xv - ld3(x, bnd[so.bnd_off + j])));
+						const float co = cur_own[size_t(s) * v_stride + v], cp = cur_opp[size_t(s) * v_stride + v];
 						own = blend ? owns_blended(ro, rp, co, cp, tau, blend_w) : ((!ccr_rest || owns1(ro, rp, tau)) && owns1(co, cp, tau));
 					}
 				}
@@ -562,40 +629,113 @@ namespace u26
 			return tmin <= tmax;
 		}
 
-		__device__ __forceinline__ bool ray_box(f3 o, f3 d, float t_lo, float tmax_ray, const NodeBox& b)
+		// Conservative node margins, applied to every node once per pass so that the traversals
+		// read grown boxes: eps = 1e-5 (1 + max |bound|) per axis for the ray slab tests, one eps
+		// from all six bounds for the swept-edge box tests (the epsilon-grown node tests that
+		// keep the traversal a superset of the exact primitive tests).
+		__global__ void grow_boxes_kernel(const NodeBox* __restrict__ boxes, uint32_t n, int isotropic, NodeBox* __restrict__ out)
 		{
-			float tmin = t_lo, tmax = tmax_ray;
-			const float lo[3] = { b.mn.x, b.mn.y, b.mn.z }, hi[3] = { b.mx.x, b.mx.y, b.mx.z };
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			const NodeBox b = boxes[i];
+			NodeBox g;
+			if (isotropic)
+			{
+				const float e = 1e-5f * (1.0f + fmaxf(fmaxf(fabsf(b.mn.x), fabsf(b.mx.x)), fmaxf(fmaxf(fabsf(b.mn.y), fabsf(b.mx.y)), fmaxf(fabsf(b.mn.z), fabsf(b.mx.z)))));
+				g.mn = make_float4(b.mn.x - e, b.mn.y - e, b.mn.z - e, 0.0f);
+				g.mx = make_float4(b.mx.x + e, b.mx.y + e, b.mx.z + e, 0.0f);
+			}
+			else
+			{
+				const float ex = 1e-5f * (1.0f + fmaxf(fabsf(b.mn.x), fabsf(b.mx.x)));
+				const float ey = 1e-5f * (1.0f + fmaxf(fabsf(b.mn.y), fabsf(b.mx.y)));
+				const float ez = 1e-5f * (1.0f + fmaxf(fabsf(b.mn.z), fabsf(b.mx.z)));
+				g.mn = make_float4(b.mn.x - ex, b.mn.y - ey, b.mn.z - ez, 0.0f);
+				g.mx = make_float4(b.mx.x + ex, b.mx.y + ey, b.mx.z + ez, 0.0f);
+			}
+			out[i] = g;
+		}
+
+		// The subtree roots that split one traversal across kSplit threads: the nodes at
+		// depth log2(kSplit) below the root, or shallower leaves; unused entries ~0.
+		constexpr uint32_t kSplit = 8;
+		__global__ void frontier_kernel(const uint2* __restrict__ children, const uint32_t* __restrict__ object_idx, uint32_t n_nodes,
+			uint32_t* __restrict__ out)
+		{
+			if (threadIdx.x != 0 || blockIdx.x != 0)
+				return;
+			uint32_t cur[kSplit], nxt[kSplit];
+			uint32_t nc = 0;
+			if (n_nodes > 0)
+				cur[nc++] = 0u;
+			for (uint32_t d = 1; d < kSplit; d <<= 1)
+			{
+				uint32_t nn = 0;
+				for (uint32_t i = 0; i < nc; i++)
+				{
+					const uint32_t v = cur[i];
+					if (object_idx[v] != kInvalid)
+						nxt[nn++] = v;
+					else
+					{
+						nxt[nn++] = children[v].x;
+						nxt[nn++] = children[v].y;
+					}
+				}
+				for (uint32_t i = 0; i < nn; i++)
+					cur[i] = nxt[i];
+				nc = nn;
+			}
+			for (uint32_t i = 0; i < kSplit; i++)
+				out[i] = i < nc ? cur[i] : kInvalid;
+		}
+
+		// slab test of a grown box with the ray's reciprocals hoisted (same values as ray_box:
+		// t0 <= t1 follows from the reciprocal's sign)
+		struct RaySlab
+		{
+			float o[3], inv[3];
+			uint32_t par; // bit a: |d_a| < 1e-30 (the ray is parallel to slab a)
+		};
+		__device__ __forceinline__ RaySlab make_slab(f3 o, f3 d)
+		{
+			RaySlab r;
 			const float oo[3] = { o.x, o.y, o.z }, dd[3] = { d.x, d.y, d.z };
+			r.par = 0;
 #pragma unroll
 			for (int a = 0; a < 3; a++)
 			{
-				const float eps = 1e-5f * (1.0f + fmaxf(fabsf(lo[a]), fabsf(hi[a])));
-				const float l = lo[a] - eps, h = hi[a] + eps;
+				r.o[a] = oo[a];
 				if (fabsf(dd[a]) < 1e-30f)
 				{
-					if (oo[a] < l || oo[a] > h)
+					r.par |= 1u << a;
+					r.inv[a] = 0.0f;
+				}
+				else
+					r.inv[a] = 1.0f / dd[a];
+			}
+			return r;
+		}
+		__device__ __forceinline__ bool ray_grown_box(const RaySlab& r, float t_lo, float t_hi, const NodeBox& g)
+		{
+			float tmin = t_lo, tmax = t_hi;
+			const float lo[3] = { g.mn.x, g.mn.y, g.mn.z }, hi[3] = { g.mx.x, g.mx.y, g.mx.z };
+#pragma unroll
+			for (int a = 0; a < 3; a++)
+			{
+				if (r.par & (1u << a))
+				{
+					if (r.o[a] < lo[a] || r.o[a] > hi[a])
 						return false;
 					continue;
 				}
-				const float inv = 1.0f / dd[a];
-				float t0 = (l - oo[a]) * inv, t1 = (h - oo[a]) * inv;
-				if (t0 > t1)
-				{
-					const float t = t0;
-					t0 = t1;
-					t1 = t;
-				}
-				tmin = fmaxf(tmin, t0);
-				tmax = fminf(tmax, t1);
+				const float ta = (lo[a] - r.o[a]) * r.inv[a], tb = (hi[a] - r.o[a]) * r.inv[a];
+				const bool pos = r.inv[a] >= 0.0f;
+				tmin = fmaxf(tmin, pos ? ta : tb);
+				tmax = fminf(tmax, pos ? tb : ta);
 			}
 			return tmin <= tmax;
-		}
-
-		__device__ __forceinline__ bool box_box(f3 mn, f3 mx, const NodeBox& b)
-		{
-			const float e = 1e-5f * (1.0f + fmaxf(fmaxf(fabsf(b.mn.x), fabsf(b.mx.x)), fmaxf(fmaxf(fabsf(b.mn.y), fabsf(b.mx.y)), fmaxf(fabsf(b.mn.z), fabsf(b.mx.z)))));
-			return (mn.x <= b.mx.x + e) & (mx.x >= b.mn.x - e) & (mn.y <= b.mx.y + e) & (mx.y >= b.mn.y - e) & (mn.z <= b.mx.z + e) & (mx.z >= b.mn.z - e);
 		}
 
 		struct HitSink
@@ -608,10 +748,16 @@ namespace u26
 			int b;
 		};
 
+		// one counter atomic per group of lanes emitting together (slot order does not matter:
+		// hit keys are unique and sorted afterwards)
 		__device__ __forceinline__ void emit(const HitSink& hs, uint32_t task, uint32_t type, uint32_t src, uint32_t dst, float b0, float b1,
 			float dist)
 		{
-			const uint32_t slot = atomicAdd(hs.count, 1u);
+			cg::coalesced_group g = cg::coalesced_threads();
+			uint32_t base = 0;
+			if (g.thread_rank() == 0)
+				base = atomicAdd(hs.count, g.size());
+			const uint32_t slot = g.shfl(base, 0) + g.thread_rank();
 			if (slot >= hs.cap)
 				return;
 			const uint64_t key = (uint64_t(task) << (2 + 2 * hs.b)) | (uint64_t(type) << (2 * hs.b)) | (uint64_t(src) << hs.b) | uint64_t(dst);
@@ -622,14 +768,47 @@ namespace u26
 			hs.payload[3 * slot + 2] = dist;
 		}
 
+		// Packet traversal: a warp takes 32 consecutive requests (one task's candidate vertices
+		// or edges in BFS order: one direction, nearby origins) and walks the union of their
+		// paths with one shared stack, every lane testing its own ray against each popped node
+		// (one broadcast load per node) and its own leaf primitives. Face-tree requests (VF,
+		// FV) and edge-tree requests (EE) of a warp take one packet walk each. The grid is
+		// kSplit parts x the requests rounded up to warps; part p starts at frontier node p,
+		// so every (ray, leaf) pair is decided once.
+		constexpr int kStack = 64;
 		__global__ void __launch_bounds__(128) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
-			TreeView ftree, TreeView etree, const float* __restrict__ x, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces,
-			const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats, uint32_t* __restrict__ dev_err)
+			TreeView ftree, TreeView etree, const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow,
+			const uint32_t* __restrict__ ffront, const uint32_t* __restrict__ efront, const float* __restrict__ x, const uint2* __restrict__ edges,
+			const uint32_t* __restrict__ faces, const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats,
+			uint32_t* __restrict__ dev_err)
 		{
-			const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+			__shared__ uint32_t s_stack[4][kStack];
+			const int lane = threadIdx.x & 31;
+			uint32_t* stack = s_stack[threadIdx.x >> 5];
+			const uint32_t warps_per_part = (total + 31u) >> 5;
+			const uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const uint32_t part = wi / warps_per_part; // warp-uniform
+			if (part >= kSplit)
+				return; // whole warps only
+			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
 			uint32_t tested = 0, visited = 0, etested = 0;
+
+			// ---- per-lane request
+			int kind = 0; // 1: VF / FV ray on the face tree, 2: EE swept edge on the edge tree
+			uint32_t t = 0, vid = 0, eid = 0;
+			bool fv = false;
+			const uint32_t* bits = nullptr;
+			uint32_t tgt_lo = 0, tgt_cnt = 0;
+			f3 dir = mk3(0.0f), orig = mk3(0.0f), sray = mk3(0.0f);
+			float slen = 0.0f, inv_len = 0.0f, t_lo = 0.0f, t_hi = 1.0f;
+			bool seg_ok = false;
+			RaySlab slab{};
+			uint2 ev = make_uint2(0u, 0u);
+			f3 p0 = mk3(0.0f), e1 = mk3(0.0f), pn = mk3(0.0f), smn = mk3(0.0f), smx = mk3(0.0f);
+			float pd = 0.0f, ray_max = 0.0f;
+			bool plane = false;
 			if (r < total)
 			{
 				// task of this request: last task with req_begin <= r
@@ -642,79 +821,49 @@ namespace u26
 					else
 						hi = mid;
 				}
-				const uint32_t t = lo;
+				t = lo;
 				const Task tk = tasks[t];
 				const uint32_t local = r - tk.req_begin;
-				const f3 dir = mk3(tk.dir[0], tk.dir[1], tk.dir[2]);
-				const Slot s0 = slots[tk.slot0], s1 = slots[tk.slot1];
-				uint32_t stack[64];
+				dir = mk3(tk.dir[0], tk.dir[1], tk.dir[2]);
 				if (local < tk.n_vf + tk.n_ee + tk.n_fv && (local < tk.n_vf || local >= tk.n_vf + tk.n_ee))
 				{
 					// VF: vertex of side 0 along +dir onto faces of side 1;
 					// FV: vertex of side 1 along -dir onto faces of side 0
-					const bool fv = local >= tk.n_vf;
-					const uint32_t vid = fv ? cand_v[size_t(tk.slot1) * v_stride + (local - tk.n_vf - tk.n_ee)]
-											: cand_v[size_t(tk.slot0) * v_stride + local];
-					const Slot& tgt = fv ? s0 : s1;
-					const uint32_t* bits = bits_f + size_t(fv ? tk.slot0 : tk.slot1) * (f_stride / 32 + 1);
+					fv = local >= tk.n_vf;
+					vid = fv ? cand_v[size_t(tk.slot1) * v_stride + (local - tk.n_vf - tk.n_ee)] : cand_v[size_t(tk.slot0) * v_stride + local];
+					const Slot tgt = slots[fv ? tk.slot0 : tk.slot1];
+					tgt_lo = tgt.f_lo;
+					tgt_cnt = tgt.f_cnt;
+					bits = bits_f + size_t(fv ? tk.slot0 : tk.slot1) * (f_stride / 32 + 1);
 					const f3 cast = fv ? -dir : dir;
-					const f3 orig = ld3(x, vid);
+					orig = ld3(x, vid);
 					const f3 end = orig + cast * 1.0f;
+					// segment constants of seg_tri, once per ray
+					const f3 sd = end - orig;
+					const float len_sq = length_sq(sd);
+					seg_ok = !(len_sq < 1e-6f * 1e-6f);
+					slen = sqrtf(len_sq);
+					inv_len = 1.0f / slen;
+					sray = sd * inv_len;
+					slab = make_slab(orig, cast);
 					// clip the ray to the grown AABB of the candidate target faces
 					const float* tb = slot_box + 12 * size_t(fv ? tk.slot0 : tk.slot1);
-					float t_lo = 0.0f, t_hi = 1.0f;
-					int sp = 0;
 					if (ray_box_range(orig, cast, 0.0f, 1.0f, tb, tb + 3, t_lo, t_hi))
-						stack[sp++] = 0u;
-					uint32_t loop = 0;
-					while (sp > 0)
-					{
-						const uint32_t node = stack[--sp];
-						visited++;
-						NodeBox b;
-						b.mn = __ldg(&ftree.boxes[node].mn);
-						b.mx = __ldg(&ftree.boxes[node].mx);
-						if (!ray_box(orig, cast, t_lo, t_hi, b))
-							continue;
-						const uint32_t fid = __ldg(ftree.object_idx + node);
-						if (fid != kInvalid)
-						{
-							tested++;
-							if (!bit_test(bits, tgt.f_lo, tgt.f_cnt, fid))
-								continue;
-							const uint32_t f0 = faces[3 * fid], f1 = faces[3 * fid + 1], f2 = faces[3 * fid + 2];
-							if (vid == f0 || vid == f1 || vid == f2)
-								continue;
-							f3 bary;
-							float tt;
-							if (seg_tri(orig, end, ld3(x, f0), ld3(x, f1), ld3(x, f2), bary, tt) && tt >= 0.0f && tt <= 1.0f)
-								emit(sink, t, fv ? 2u : 0u, fv ? fid : vid, fv ? vid : fid, bary.x, bary.y, tt * 1.0f);
-							continue;
-						}
-						const uint2 ch = __ldg(ftree.children + node);
-						if (sp + 2 > 64)
-						{
-							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
-							break;
-						}
-						stack[sp++] = ch.y;
-						stack[sp++] = ch.x;
-						if (++loop > 4000000u)
-						{
-							atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
-							break;
-						}
-					}
+						kind = 1;
 				}
 				else if (local < tk.n_vf + tk.n_ee)
 				{
 					// EE: swept edge of side 0 along dir onto edges of side 1
-					const uint32_t eid = cand_e[size_t(tk.slot0) * e_stride + (local - tk.n_vf)];
-					const uint32_t* bits = bits_e + size_t(tk.slot1) * (e_stride / 32 + 1);
-					const uint2 ev = edges[eid];
-					const f3 p0 = ld3(x, ev.x), p1 = ld3(x, ev.y);
+					eid = cand_e[size_t(tk.slot0) * e_stride + (local - tk.n_vf)];
+					bits = bits_e + size_t(tk.slot1) * (e_stride / 32 + 1);
+					const Slot s1 = slots[tk.slot1];
+					tgt_lo = s1.e_lo;
+					tgt_cnt = s1.e_cnt;
+					ev = edges[eid];
+					p0 = ld3(x, ev.x);
+					const f3 p1 = ld3(x, ev.y);
 					const float dl2 = dot(dir, dir);
-					float ray_max = 1.0f;
+					ray_max = 1.0f;
 					if (!(dl2 <= 1e-12f))
 					{
 						const float smin = fminf(dot(p0, dir), dot(p1, dir));
@@ -722,103 +871,199 @@ namespace u26
 					}
 					if (ray_max > 0.0f)
 					{
-						const f3 e1 = p1 - p0;
-						f3 pn = cross(e1, dir);
+						e1 = p1 - p0;
+						pn = cross(e1, dir);
 						const float nl = length(pn);
-						const bool plane = nl >= 1e-10f;
-						float pd = 0.0f;
+						plane = nl >= 1e-10f;
 						if (plane)
 						{
 							pn = pn / nl;
 							pd = dot(pn, p0);
 						}
 						const f3 a_end = p0 + dir * ray_max, b_end = p1 + dir * ray_max;
-						f3 smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
-						f3 smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
+						smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
+						smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
 						// intersect the swept box with the grown AABB of the candidate target edges
 						const float* tb = slot_box + 12 * size_t(tk.slot1) + 6;
-						{
-							const float e0 = 1e-5f * (1.0f + fmaxf(fabsf(tb[0]), fabsf(tb[3])));
-							const float e1 = 1e-5f * (1.0f + fmaxf(fabsf(tb[1]), fabsf(tb[4])));
-							const float e2 = 1e-5f * (1.0f + fmaxf(fabsf(tb[2]), fabsf(tb[5])));
-							smn = vmax(smn, mk3(tb[0] - e0, tb[1] - e1, tb[2] - e2));
-							smx = vmin(smx, mk3(tb[3] + e0, tb[4] + e1, tb[5] + e2));
-						}
-						int sp = 0;
+						const float g0 = 1e-5f * (1.0f + fmaxf(fabsf(tb[0]), fabsf(tb[3])));
+						const float g1 = 1e-5f * (1.0f + fmaxf(fabsf(tb[1]), fabsf(tb[4])));
+						const float g2 = 1e-5f * (1.0f + fmaxf(fabsf(tb[2]), fabsf(tb[5])));
+						smn = vmax(smn, mk3(tb[0] - g0, tb[1] - g1, tb[2] - g2));
+						smx = vmin(smx, mk3(tb[3] + g0, tb[4] + g1, tb[5] + g2));
 						if (smn.x <= smx.x && smn.y <= smx.y && smn.z <= smx.z)
-							stack[sp++] = 0u;
-						uint32_t loop = 0;
-						while (sp > 0)
+							kind = 2;
+					}
+				}
+			}
+
+			// ---- face tree: VF / FV rays of the warp
+			bool on = kind == 1;
+			const uint32_t fstart = ffront[part];
+			if (__any_sync(0xFFFFFFFFu, on) && fstart != kInvalid)
+			{
+				int sp = 1;
+				if (lane == 0)
+					stack[0] = fstart;
+				__syncwarp();
+				uint32_t loop = 0;
+				while (sp > 0)
+				{
+					const uint32_t node = stack[--sp];
+					NodeBox b;
+					b.mn = __ldg(&fgrow[node].mn);
+					b.mx = __ldg(&fgrow[node].mx);
+					visited += on ? 1u : 0u;
+					const bool hit = on && ray_grown_box(slab, t_lo, t_hi, b);
+					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
+						continue;
+					const uint32_t fid = __ldg(ftree.object_idx + node);
+					if (fid != kInvalid)
+					{
+						if (hit)
 						{
-							const uint32_t node = stack[--sp];
-							visited++;
-							NodeBox b;
-							b.mn = __ldg(&etree.boxes[node].mn);
-							b.mx = __ldg(&etree.boxes[node].mx);
-							if (!box_box(smn, smx, b))
-								continue;
-							const uint32_t e2 = __ldg(etree.object_idx + node);
-							if (e2 != kInvalid)
+							tested++;
+							if (bit_test(bits, tgt_lo, tgt_cnt, fid))
 							{
-								tested++;
-								etested++;
-								if (!bit_test(bits, s1.e_lo, s1.e_cnt, e2))
-									continue;
-								const uint2 qv = edges[e2];
-								if (ev.x == qv.x || ev.x == qv.y || ev.y == qv.x || ev.y == qv.y)
-									continue;
-								const f3 q0 = ld3(x, qv.x), q1 = ld3(x, qv.y);
-								if (plane)
+								const uint32_t f0 = faces[3 * fid], f1 = faces[3 * fid + 1], f2 = faces[3 * fid + 2];
+								if (vid != f0 && vid != f1 && vid != f2)
 								{
-									const float d0 = dot(pn, q0) - pd;
-									const float d1 = dot(pn, q1) - pd;
-									if ((d0 > 1e-6f && d1 > 1e-6f) || (d0 < -1e-6f && d1 < -1e-6f))
-										continue;
+									f3 bary;
+									float tt;
+									if (seg_ok && ray_tri(orig, sray, slen, ld3(x, f0), ld3(x, f1), ld3(x, f2), tt, bary))
+									{
+										tt = tt * inv_len;
+										if (tt >= 0.0f && tt <= 1.0f)
+											emit(sink, t, fv ? 2u : 0u, fv ? fid : vid, fv ? vid : fid, bary.x, bary.y, tt * 1.0f);
+									}
 								}
-								const f3 e2v = q1 - q0;
-								const f3 rr = q0 - p0;
-								const f3 n = cross(e1, e2v);
-								const float det = -dot(dir, n);
-								if (fabsf(det) < 1e-10f)
-									continue;
-								const float inv = 1.0f / det;
-								const float d_r_e1_e2 = dot(rr, cross(e1, e2v));
-								const float d_dir_r_e2 = dot(dir, cross(rr, e2v));
-								const float d_dir_e1_r = dot(dir, cross(e1, rr));
-								const float sv = -d_r_e1_e2 * inv;
-								const float t1 = -d_dir_r_e2 * inv;
-								const float t2 = d_dir_e1_r * inv;
-								if (sv >= 0.0f && sv <= ray_max && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f)
-									emit(sink, t, 1u, eid, e2, 1.0f - t1, 1.0f - t2, sv);
-								continue;
-							}
-							const uint2 ch = __ldg(etree.children + node);
-							if (sp + 2 > 64)
-							{
-								atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
-								break;
-							}
-							stack[sp++] = ch.y;
-							stack[sp++] = ch.x;
-							if (++loop > 4000000u)
-							{
-								atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
-								break;
 							}
 						}
+						__syncwarp();
+						continue;
+					}
+					if (sp + 2 > kStack)
+					{
+						if (lane == 0)
+							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
+						break;
+					}
+					const uint2 ch = __ldg(ftree.children + node);
+					__syncwarp();
+					if (lane == 0)
+					{
+						stack[sp] = ch.y;
+						stack[sp + 1] = ch.x;
+					}
+					sp += 2;
+					__syncwarp();
+					if (++loop > 4000000u)
+					{
+						if (lane == 0)
+							atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
+						break;
+					}
+				}
+				__syncwarp();
+			}
+
+			// ---- edge tree: EE swept edges of the warp
+			on = kind == 2;
+			const uint32_t estart = efront[part];
+			if (__any_sync(0xFFFFFFFFu, on) && estart != kInvalid)
+			{
+				int sp = 1;
+				if (lane == 0)
+					stack[0] = estart;
+				__syncwarp();
+				uint32_t loop = 0;
+				while (sp > 0)
+				{
+					const uint32_t node = stack[--sp];
+					NodeBox g;
+					g.mn = __ldg(&egrow[node].mn);
+					g.mx = __ldg(&egrow[node].mx);
+					visited += on ? 1u : 0u;
+					const bool hit = on && (smn.x <= g.mx.x) & (smx.x >= g.mn.x) & (smn.y <= g.mx.y) & (smx.y >= g.mn.y) & (smn.z <= g.mx.z) &
+						(smx.z >= g.mn.z);
+					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
+						continue;
+					const uint32_t e2 = __ldg(etree.object_idx + node);
+					if (e2 != kInvalid)
+					{
+						if (hit)
+						{
+							tested++;
+							etested++;
+							if (bit_test(bits, tgt_lo, tgt_cnt, e2))
+							{
+								const uint2 qv = edges[e2];
+								if (!(ev.x == qv.x || ev.x == qv.y || ev.y == qv.x || ev.y == qv.y))
+								{
+									const f3 q0 = ld3(x, qv.x), q1 = ld3(x, qv.y);
+									bool sep = false;
+									if (plane)
+									{
+										const float d0 = dot(pn, q0) - pd;
+										const float d1 = dot(pn, q1) - pd;
+										sep = (d0 > 1e-6f && d1 > 1e-6f) || (d0 < -1e-6f && d1 < -1e-6f);
+									}
+									if (!sep)
+									{
+										const f3 e2v = q1 - q0;
+										const f3 rr = q0 - p0;
+										const f3 n = cross(e1, e2v);
+										const float det = -dot(dir, n);
+										if (!(fabsf(det) < 1e-10f))
+										{
+											const float inv = 1.0f / det;
+											const float d_r_e1_e2 = dot(rr, cross(e1, e2v));
+											const float d_dir_r_e2 = dot(dir, cross(rr, e2v));
+											const float d_dir_e1_r = dot(dir, cross(e1, rr));
+											const float sv = -d_r_e1_e2 * inv;
+											const float t1 = -d_dir_r_e2 * inv;
+											const float t2 = d_dir_e1_r * inv;
+											if (sv >= 0.0f && sv <= ray_max && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f)
+												emit(sink, t, 1u, eid, e2, 1.0f - t1, 1.0f - t2, sv);
+										}
+									}
+								}
+							}
+						}
+						__syncwarp();
+						continue;
+					}
+					if (sp + 2 > kStack)
+					{
+						if (lane == 0)
+							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
+						break;
+					}
+					const uint2 ch = __ldg(etree.children + node);
+					__syncwarp();
+					if (lane == 0)
+					{
+						stack[sp] = ch.y;
+						stack[sp + 1] = ch.x;
+					}
+					sp += 2;
+					__syncwarp();
+					if (++loop > 4000000u)
+					{
+						if (lane == 0)
+							atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
+						break;
 					}
 				}
 			}
 			if (stats)
 			{
-				const uint32_t mask = __activemask();
-				const uint32_t tsum = __reduce_add_sync(mask, tested);
-				const uint32_t rsum = __reduce_add_sync(mask, r < total ? 1u : 0u);
-				const uint32_t vsum = __reduce_add_sync(mask, visited);
-				const uint32_t esum = __reduce_add_sync(mask, etested);
-				if ((threadIdx.x & 31) == uint32_t(__ffs(mask) - 1))
+				const uint32_t tsum = __reduce_add_sync(0xFFFFFFFFu, tested);
+				const uint32_t rsum = __reduce_add_sync(0xFFFFFFFFu, (part == 0 && r < total) ? 1u : 0u);
+				const uint32_t vsum = __reduce_add_sync(0xFFFFFFFFu, visited);
+				const uint32_t esum = __reduce_add_sync(0xFFFFFFFFu, etested);
+				if (lane == 0)
 				{
-					// [0] leaf primitive tests, [1] requests, [2] nodes visited, [3] edge leaf tests
+					// [0] leaf primitive tests, [1] requests, [2] ray-node tests, [3] edge leaf tests
 					atomicAdd(stats + 0, (unsigned long long)tsum);
 					atomicAdd(stats + 1, (unsigned long long)rsum);
 					atomicAdd(stats + 2, (unsigned long long)vsum);
@@ -1056,20 +1301,40 @@ namespace u26
 			uint32_t* __restrict__ comp_size, uint32_t* __restrict__ comp_att, uint32_t* __restrict__ root)
 		{
 			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-			if (i >= n)
-				return;
-			uint32_t r = i;
-			for (int it = 0; it < 1 << 22; it++)
+			const bool valid = i < n;
+			uint32_t r = kInf;
+			bool att = false;
+			if (valid)
 			{
-				const uint32_t p = parent[r];
-				if (p == r)
-					break;
-				r = p;
+				r = i;
+				for (int it = 0; it < 1 << 22; it++)
+				{
+					const uint32_t p = parent[r];
+					if (p == r)
+						break;
+					r = p;
+				}
+				// path compression: every pointer on the walked path now names the root
+				// (concurrent readers see an old ancestor or the root, both valid)
+				uint32_t v = i;
+				for (int it = 0; it < 1 << 22 && v != r; it++)
+				{
+					const uint32_t p = parent[v];
+					parent[v] = r;
+					v = p;
+				}
+				root[i] = r;
+				att = attached[i] != 0;
 			}
-			root[i] = r;
-			atomicAdd(comp_size + r, 1u);
-			if (attached[i])
-				atomicOr(comp_att + r, 1u);
+			// one atomic per (warp, component): hits of a task's large components are adjacent
+			const uint32_t peers = __match_any_sync(0xFFFFFFFFu, r);
+			const uint32_t att_peers = __ballot_sync(0xFFFFFFFFu, att) & peers;
+			if (valid && (threadIdx.x & 31) == uint32_t(__ffs(peers) - 1))
+			{
+				atomicAdd(comp_size + r, uint32_t(__popc(peers)));
+				if (att_peers)
+					atomicOr(comp_att + r, 1u);
+			}
 		}
 
 		// support entries (side, vertex, component) of hits in boundary-attached components
@@ -1103,7 +1368,12 @@ namespace u26
 					const uint32_t lv = v - slots[sl_id].v_lo;
 					if (!((bnd_bits[size_t(sl_id) * (v_stride / 32 + 1) + (lv >> 5)] >> (lv & 31)) & 1u))
 						continue;
-					const uint32_t slot = atomicAdd(ecount, 1u);
+					// one counter atomic per group of lanes (entries are sorted afterwards)
+					cg::coalesced_group g = cg::coalesced_threads();
+					uint32_t base = 0;
+					if (g.thread_rank() == 0)
+						base = atomicAdd(ecount, g.size());
+					const uint32_t slot = g.shfl(base, 0) + g.thread_rank();
 					if (slot < cap)
 					{
 						ekeys[slot] = (uint64_t(t) << (1 + vb + rb)) | (uint64_t(side) << (vb + rb)) | (uint64_t(v) << rb) | uint64_t(rl);
@@ -1112,25 +1382,8 @@ namespace u26
 				}
 		}
 
-		__device__ __forceinline__ bool entry_exists(const uint64_t* ek, uint32_t n, uint64_t key)
-		{
-			uint32_t lo = 0, hi = n;
-			while (lo < hi)
-			{
-				const uint32_t mid = (lo + hi) >> 1;
-				const uint64_t v = ek[mid];
-				if (v == key)
-					return true;
-				if (v < key)
-					lo = mid + 1;
-				else
-					hi = mid;
-			}
-			return false;
-		}
-
 		// boundary-attached component roots of each task (order does not matter: the
-		// selection rule below is a strict total order)
+		// selection rule is a strict total order)
 		__global__ void cand_roots_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, const uint32_t* __restrict__ seg,
 			const uint32_t* __restrict__ root, const uint32_t* __restrict__ comp_att, uint32_t* __restrict__ ncand,
 			uint32_t* __restrict__ cand_roots)
@@ -1142,69 +1395,147 @@ namespace u26
 			cand_roots[seg[t] + atomicAdd(ncand + t, 1u)] = i;
 		}
 
-		// One CTA per task: EF-anchor coverage of each candidate component (one warp per
-		// component, lanes over the contour's anchors), then the best component: maximal
-		// coverage, then more hits, then the smaller canonical key (= smaller root index).
-		__global__ void __launch_bounds__(256) coverage_kernel(const Task* __restrict__ tasks, uint32_t ntasks, const uint32_t* __restrict__ seg,
-			const uint32_t* __restrict__ ncand_arr, const uint32_t* __restrict__ cand_roots, const uint32_t* __restrict__ comp_size,
-			const uint32_t* __restrict__ anchor_off, const uint32_t* __restrict__ anchors, const uint64_t* __restrict__ ekeys,
-			uint32_t nentries, int vb, int rb, uint32_t* __restrict__ best_out, uint32_t* __restrict__ bestcov_out)
+		__device__ __forceinline__ uint32_t lower_bound64(const uint64_t* __restrict__ a, uint32_t n, uint64_t key)
 		{
-			const uint32_t t = blockIdx.x;
+			uint32_t lo = 0, hi = n;
+			while (lo < hi)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (a[mid] < key)
+					lo = mid + 1;
+				else
+					hi = mid;
+			}
+			return lo;
+		}
+
+		// The component ids (root - segment start) entered for one (task, side, vertex): a
+		// sorted run of the support entries (with repeats).
+		struct EntryRun
+		{
+			uint32_t b, e;
+		};
+		__device__ __forceinline__ EntryRun entry_run(const uint64_t* __restrict__ ek, uint32_t n, uint64_t prefix, int rb)
+		{
+			const uint32_t b = lower_bound64(ek, n, prefix);
+			uint32_t e = b;
+			const uint64_t hi = prefix + (uint64_t(1) << rb);
+			while (e < n && ek[e] < hi)
+				e++;
+			return EntryRun{ b, e };
+		}
+		__device__ __forceinline__ bool run_has(const uint64_t* __restrict__ ek, EntryRun r, uint64_t key)
+		{
+			uint32_t lo = r.b, hi = r.e;
+			while (lo < hi)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (ek[mid] < key)
+					lo = mid + 1;
+				else
+					hi = mid;
+			}
+			return lo < r.e && ek[lo] == key;
+		}
+
+		// EF-anchor coverage counted per anchor (prp_fill_combo_eval_info, intersection_
+		// resolver2.cpp:1806-1881): one thread per (task, anchor); every boundary-attached
+		// component that holds a vertex of the anchor's edge on side m and a vertex of its face
+		// on side m^1 gains one covered anchor (cov[] is indexed by the component's root).
+		__global__ void coverage_count_kernel(const Task* __restrict__ tasks, uint32_t ntasks, const uint32_t* __restrict__ task_anchor_begin,
+			const uint32_t* __restrict__ anchor_off, const uint32_t* __restrict__ anchors, const uint64_t* __restrict__ ekeys, uint32_t nentries,
+			int vb, int rb, const uint32_t* __restrict__ seg, uint32_t* __restrict__ cov)
+		{
+			const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+			if (g >= task_anchor_begin[ntasks])
+				return;
+			uint32_t lo = 0, hi = ntasks;
+			while (hi - lo > 1)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (task_anchor_begin[mid] <= g)
+					lo = mid;
+				else
+					hi = mid;
+			}
+			const uint32_t t = lo;
+			const uint32_t c = tasks[t].contour_local;
+			const uint32_t* A = anchors + 6 * size_t(anchor_off[c] + (g - task_anchor_begin[t]));
+			const uint32_t m = A[0];
+			const uint64_t tb = uint64_t(t) << (1 + vb + rb);
+			auto prefix = [&](uint32_t side, uint32_t v)
+			{ return tb | (uint64_t(side) << (vb + rb)) | (uint64_t(v) << rb); };
+			const EntryRun E0 = entry_run(ekeys, nentries, prefix(m, A[1]), rb);
+			const EntryRun E1 = entry_run(ekeys, nentries, prefix(m, A[2]), rb);
+			if (E0.b == E0.e && E1.b == E1.e)
+				return;
+			const EntryRun F[3] = { entry_run(ekeys, nentries, prefix(m ^ 1u, A[3]), rb), entry_run(ekeys, nentries, prefix(m ^ 1u, A[4]), rb),
+				entry_run(ekeys, nentries, prefix(m ^ 1u, A[5]), rb) };
+			if (F[0].b == F[0].e && F[1].b == F[1].e && F[2].b == F[2].e)
+				return;
+			const uint64_t rmask = (uint64_t(1) << rb) - 1u;
+			const uint32_t s0 = seg[t];
+			// distinct components of E0 u E1 in increasing order (two-pointer merge)
+			uint32_t i0 = E0.b, i1 = E1.b;
+			uint32_t last = kInf;
+			for (int it = 0; it < (1 << 22) && (i0 < E0.e || i1 < E1.e); it++)
+			{
+				uint32_t rl;
+				if (i1 >= E1.e || (i0 < E0.e && (ekeys[i0] & rmask) <= (ekeys[i1] & rmask)))
+					rl = uint32_t(ekeys[i0++] & rmask);
+				else
+					rl = uint32_t(ekeys[i1++] & rmask);
+				if (rl == last)
+					continue;
+				last = rl;
+				bool in_f = false;
+				for (int q = 0; q < 3 && !in_f; q++)
+					in_f = run_has(ekeys, F[q], prefix(m ^ 1u, A[3 + q]) | rl);
+				if (in_f)
+					atomicAdd(cov + s0 + rl, 1u);
+			}
+		}
+
+		// One warp per task: the best candidate component, maximal coverage, then more hits,
+		// then the smaller canonical key (= smaller root index).
+		__global__ void best_component_kernel(uint32_t ntasks, const uint32_t* __restrict__ seg, const uint32_t* __restrict__ ncand_arr,
+			const uint32_t* __restrict__ cand_roots, const uint32_t* __restrict__ comp_size, const uint32_t* __restrict__ cov,
+			uint32_t* __restrict__ best_out, uint32_t* __restrict__ bestcov_out)
+		{
+			const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const int lane = threadIdx.x & 31;
 			if (t >= ntasks)
 				return;
-			const Task tk = tasks[t];
-			const uint32_t lo = seg[t];
-			const uint32_t ncand = ncand_arr[t];
-			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-			const uint32_t a_lo = anchor_off[tk.contour_local], a_hi = anchor_off[tk.contour_local + 1];
-			__shared__ uint32_t s_cov[8];
-			uint32_t best = kInf, best_cov = 0, best_n = 0;
-			for (uint32_t j0 = 0; j0 < ncand; j0 += 8)
+			const uint32_t lo = seg[t], ncand = ncand_arr[t];
+			uint32_t best = kInf, bc = 0, bn = 0;
+			for (uint32_t j = lane; j < ncand; j += 32)
 			{
-				const uint32_t j = j0 + warp;
-				uint32_t cov = 0;
-				if (j < ncand)
+				const uint32_t r = cand_roots[lo + j];
+				const uint32_t cv = cov[r], nh = comp_size[r];
+				if (best == kInf || cv > bc || (cv == bc && (nh > bn || (nh == bn && r < best))))
 				{
-					const uint32_t r = cand_roots[lo + j];
-					const uint64_t tb = (uint64_t(t) << (1 + vb + rb));
-					const uint64_t rl = uint64_t(r - lo);
-					auto has = [&](uint32_t side, uint32_t v)
-					{ return entry_exists(ekeys, nentries, tb | (uint64_t(side) << (vb + rb)) | (uint64_t(v) << rb) | rl); };
-					for (uint32_t a = a_lo + lane; a < a_hi; a += 32)
-					{
-						const uint32_t* A = anchors + 6 * size_t(a);
-						const uint32_t m = A[0];
-						const bool eo = has(m, A[1]) || has(m, A[2]);
-						const bool fo = eo && (has(m ^ 1u, A[3]) || has(m ^ 1u, A[4]) || has(m ^ 1u, A[5]));
-						cov += (eo && fo) ? 1u : 0u;
-					}
-					cov = __reduce_add_sync(0xFFFFFFFFu, cov);
+					best = r;
+					bc = cv;
+					bn = nh;
 				}
-				if (lane == 0)
-					s_cov[warp] = cov;
-				__syncthreads();
-				if (threadIdx.x == 0)
-				{
-					for (uint32_t w = 0; w < 8 && j0 + w < ncand; w++)
-					{
-						const uint32_t r = cand_roots[lo + j0 + w];
-						const uint32_t cv = s_cov[w], nh = comp_size[r];
-						const bool better = best == kInf || cv > best_cov || (cv == best_cov && nh > best_n) || (cv == best_cov && nh == best_n && r < best);
-						if (better)
-						{
-							best = r;
-							best_cov = cv;
-							best_n = nh;
-						}
-					}
-				}
-				__syncthreads();
 			}
-			if (threadIdx.x == 0)
+#pragma unroll
+			for (int off = 16; off >= 1; off >>= 1)
+			{
+				const uint32_t ob = __shfl_xor_sync(0xFFFFFFFFu, best, off);
+				const uint32_t oc = __shfl_xor_sync(0xFFFFFFFFu, bc, off);
+				const uint32_t on = __shfl_xor_sync(0xFFFFFFFFu, bn, off);
+				if (ob != kInf && (best == kInf || oc > bc || (oc == bc && (on > bn || (on == bn && ob < best)))))
+				{
+					best = ob;
+					bc = oc;
+					bn = on;
+				}
+			}
+			if (lane == 0)
 			{
 				best_out[t] = best;
-				bestcov_out[t] = best_cov;
+				bestcov_out[t] = best == kInf ? 0u : bc;
 			}
 		}
 
@@ -1316,6 +1647,9 @@ namespace u26
 			for (int q = 0; q < warp; q++)
 				wbase += wsum[q];
 			uint32_t p = bsum[blockIdx.x] + wbase + x - loc;
+			// running maxima of depth (float bits) and frontier hops of the thread's current
+			// task; flushed when the task changes, then reduced across the warp by task segment
+			uint32_t cur_t = kInf, m_dist = 0u, m_fs = 0u, m_fd = 0u;
 #pragma unroll
 			for (int q = 0; q < 4; q++)
 			{
@@ -1369,7 +1703,18 @@ namespace u26
 				terms[3 * size_t(p) + 1] = (area * alpha) * dist;
 				terms[3 * size_t(p) + 2] = e > 1e-8f ? (sd * sd) / e : 0.0f;
 				// depth (non-negative float bits order like uints) and frontier hops
-				atomicMax(task_max + 3 * t, __float_as_uint(dist));
+				if (t != cur_t)
+				{
+					if (cur_t != kInf)
+					{
+						atomicMax(task_max + 3 * cur_t, m_dist);
+						atomicMax(task_max + 3 * cur_t + 1, m_fs);
+						atomicMax(task_max + 3 * cur_t + 2, m_fd);
+					}
+					cur_t = t;
+					m_dist = m_fs = m_fd = 0u;
+				}
+				m_dist = max(m_dist, __float_as_uint(dist));
 				const Slot s0 = slots[tk.slot0], s1 = slots[tk.slot1];
 				const uint32_t* h0 = hop + size_t(tk.slot0) * v_stride;
 				const uint32_t* h1 = hop + size_t(tk.slot1) * v_stride;
@@ -1389,8 +1734,8 @@ namespace u26
 							mfd = max(mfd, hv);
 					}
 				}
-				atomicMax(task_max + 3 * t + 1, mfs);
-				atomicMax(task_max + 3 * t + 2, mfd);
+				m_fs = max(m_fs, mfs);
+				m_fd = max(m_fd, mfd);
 				if (out_hits)
 				{
 					u26_prp_hit h;
@@ -1408,6 +1753,31 @@ namespace u26
 					out_hits[p] = h;
 				}
 				p++;
+			}
+			// segmented max across the warp: each lane's last task is non-decreasing along the
+			// lanes (lanes without selected hits carry kInf), a run's first lane holds the run's
+			// maxima after the shuffle steps and flushes them (max is idempotent, so a run that
+			// also reaches past an empty lane is harmless)
+#pragma unroll
+			for (int off = 1; off < 32; off <<= 1)
+			{
+				const uint32_t ot = __shfl_down_sync(0xFFFFFFFFu, cur_t, off);
+				const uint32_t od = __shfl_down_sync(0xFFFFFFFFu, m_dist, off);
+				const uint32_t of = __shfl_down_sync(0xFFFFFFFFu, m_fs, off);
+				const uint32_t og = __shfl_down_sync(0xFFFFFFFFu, m_fd, off);
+				if (lane + off < 32 && ot == cur_t)
+				{
+					m_dist = max(m_dist, od);
+					m_fs = max(m_fs, of);
+					m_fd = max(m_fd, og);
+				}
+			}
+			const uint32_t prev_t = __shfl_up_sync(0xFFFFFFFFu, cur_t, 1);
+			if (cur_t != kInf && (lane == 0 || prev_t != cur_t))
+			{
+				atomicMax(task_max + 3 * cur_t, m_dist);
+				atomicMax(task_max + 3 * cur_t + 1, m_fs);
+				atomicMax(task_max + 3 * cur_t + 2, m_fd);
 			}
 		}
 
@@ -1433,7 +1803,28 @@ namespace u26
 			const uint32_t cnt = b != kInf ? comp_size[b] : 0u;
 			const uint32_t p0 = sel_begin[t];
 			float sa = 0.0f, sv = 0.0f, sk = 0.0f;
-			for (uint32_t i = lane; i < cnt; i += 32)
+			// each lane adds its strided terms in order; the loads of 8 steps are issued ahead
+			uint32_t i = lane;
+			for (; i + 7u * 32u < cnt; i += 8u * 32u)
+			{
+				float ta[8], tv[8], tk8[8];
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+				{
+					const float* tt = terms + 3 * size_t(p0 + i + 32u * u);
+					ta[u] = tt[0];
+					tv[u] = tt[1];
+					tk8[u] = tt[2];
+				}
+#pragma unroll
+				for (int u = 0; u < 8; u++)
+				{
+					sa = sa + ta[u];
+					sv = sv + tv[u];
+					sk = sk + tk8[u];
+				}
+			}
+			for (; i < cnt; i += 32)
 			{
 				const float* tt = terms + 3 * size_t(p0 + i);
 				sa = sa + tt[0];
@@ -1868,6 +2259,7 @@ struct u26_scene
 	DevBuf d_ekeys, d_evals, d_ecount, d_cand_roots, d_vf_off, d_vf, d_anchor_off, d_anchors, d_out, d_sel;
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
+	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
 	RadixSorter sorter, esorter;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
@@ -1998,7 +2390,8 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_stats, &s->d_seg, &s->d_parent, &s->d_root, &s->d_att, &s->d_csize, &s->d_catt, &s->d_ekeys, &s->d_evals,
 		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
 		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
-		&s->d_step_hits, &s->d_step_out };
+		&s->d_step_hits, &s->d_step_out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
+		&s->d_cur_opp, &s->d_tab, &s->d_cov };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
@@ -2490,6 +2883,11 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_CUDA(ctx, S->d_counts.reserve(sizeof(uint32_t) * 3 * size_t(nslots)));
 		U26_CUDA(ctx, S->d_bits_e.reserve(sizeof(uint32_t) * size_t(nslots) * (es_ / 32 + 1)));
 		U26_CUDA(ctx, S->d_bits_f.reserve(sizeof(uint32_t) * size_t(nslots) * (fs / 32 + 1)));
+		// current-space anchor distances, computed lazily per level (NaN: not yet computed)
+		U26_CUDA(ctx, S->d_cur_own.reserve(sizeof(float) * size_t(nslots) * vs));
+		U26_CUDA(ctx, S->d_cur_opp.reserve(sizeof(float) * size_t(nslots) * vs));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_cur_own.ptr, 0xFF, sizeof(float) * size_t(nslots) * vs, st));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_cur_opp.ptr, 0xFF, sizeof(float) * size_t(nslots) * vs, st));
 		distances_kernel<<<nslots, 256, 0, st>>>(S->d_slots.as<Slot>(), S->d_slot_ids.as<uint32_t>(), S->d_bnd.as<uint32_t>(),
 			S->d_vav_off.as<uint32_t>(), S->d_vav.as<uint32_t>(), S->d_rest_x.as<float>(), vs, S->d_hop.as<uint32_t>(),
 			S->d_geo.as<float>(), S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(), S->d_work.as<uint32_t>(),
@@ -2524,6 +2922,27 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 4));
 	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 4, st));
 	const TreeView ftv = tree_view(face_tree), etv = tree_view(edge_tree);
+	// grown node boxes of this pass's trees and the subtree roots of the split traversal
+	{
+		const uint32_t fn_ = ftv.n ? 2 * ftv.n - 1 : 0, en_ = etv.n ? 2 * etv.n - 1 : 0;
+		U26_CUDA(ctx, S->d_fgrow.reserve(sizeof(NodeBox) * std::max(fn_, 1u)));
+		U26_CUDA(ctx, S->d_egrow.reserve(sizeof(NodeBox) * std::max(en_, 1u)));
+		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * kSplit));
+		if (fn_)
+		{
+			grow_boxes_kernel<<<div_up(fn_, 256), 256, 0, st>>>(ftv.boxes, fn_, 0, S->d_fgrow.as<NodeBox>());
+			U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
+		}
+		if (en_)
+		{
+			grow_boxes_kernel<<<div_up(en_, 256), 256, 0, st>>>(etv.boxes, en_, 1, S->d_egrow.as<NodeBox>());
+			U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
+		}
+		frontier_kernel<<<1, 32, 0, st>>>(ftv.children, ftv.object_idx, fn_, S->d_front.as<uint32_t>());
+		U26_TRY(after_launch(ctx, "frontier_kernel"));
+		frontier_kernel<<<1, 32, 0, st>>>(etv.children, etv.object_idx, en_, S->d_front.as<uint32_t>() + kSplit);
+		U26_TRY(after_launch(ctx, "frontier_kernel"));
+	}
 	const uint32_t bnd_words = vs / 32 + 1;
 	if (nslots)
 	{
@@ -2550,13 +2969,22 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	{
 		U26_TRY(upload(ctx, S->d_slots, slots));
 		U26_TRY(upload(ctx, S->d_slot_ids, sids));
+		if (P->use_ccr && P->ccr_use_current && !sids.empty())
+		{
+			constexpr uint32_t kBlocksPerSlot = 32;
+			ccr_current_kernel<<<uint32_t(sids.size()) * kBlocksPerSlot, 256, 0, st>>>(S->d_slots.as<Slot>(), S->d_slot_ids.as<uint32_t>(),
+				S->d_bnd.as<uint32_t>(), d_x, vs, S->d_geo.as<float>(), S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(),
+				P->ccr_use_rest, P->ccr_blend, P->ccr_tau, kBlocksPerSlot, S->d_cur_own.as<float>(), S->d_cur_opp.as<float>());
+			U26_TRY(after_launch(ctx, "ccr_current_kernel"));
+		}
 		candidates_kernel<<<uint32_t(sids.size()), 256, 0, st>>>(S->d_slots.as<Slot>(), S->d_slot_ids.as<uint32_t>(), S->d_bnd.as<uint32_t>(),
 			d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_vae_off.as<uint32_t>(), S->d_vae.as<uint32_t>(),
 			S->d_vaf_off.as<uint32_t>(), S->d_vaf.as<uint32_t>(), vs, es_, fs, S->d_hop.as<uint32_t>(), S->d_geo.as<float>(),
 			S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(), P->ccr_use_rest, P->ccr_use_current, P->ccr_blend, P->ccr_tau,
 			P->ccr_blend_weight,
 			S->d_owns.as<uint8_t>(), S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), S->d_cand_f.as<uint32_t>(),
-			S->d_counts.as<uint32_t>(), S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(), S->d_slot_box.as<float>());
+			S->d_counts.as<uint32_t>(), S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(), S->d_slot_box.as<float>(),
+			S->d_cur_own.as<float>(), S->d_cur_opp.as<float>());
 		U26_TRY(after_launch(ctx, "candidates_kernel"));
 		U26_TRY(download(ctx, counts, S->d_counts.ptr, 3 * size_t(nslots)));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
@@ -2583,6 +3011,20 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				alg_tests += uint64_t(t.n_vf) * f1 + uint64_t(t.n_ee) * e1 + uint64_t(t.n_fv) * f0;
 		}
 		const uint32_t nt = uint32_t(tasks.size());
+		if (trace && nt > 0)
+		{
+			std::vector<uint32_t> ord(nt);
+			std::iota(ord.begin(), ord.end(), 0u);
+			std::partial_sort(ord.begin(), ord.begin() + std::min<uint32_t>(nt, 5), ord.end(), [&](uint32_t a, uint32_t b)
+				{ return tasks[a].n_vf + tasks[a].n_ee + tasks[a].n_fv > tasks[b].n_vf + tasks[b].n_ee + tasks[b].n_fv; });
+			for (uint32_t q = 0; q < std::min<uint32_t>(nt, 5); q++)
+			{
+				const Task& t = tasks[ord[q]];
+				fprintf(stderr, "[u26 prp]   task contour %u dir %u k %u/%u requests vf %u ee %u fv %u cand faces %u/%u edges %u/%u\n", t.contour_local,
+					t.combo, slots[t.slot0].k, slots[t.slot1].k, t.n_vf, t.n_ee, t.n_fv, counts[3 * t.slot0 + 2], counts[3 * t.slot1 + 2],
+					counts[3 * t.slot0 + 1], counts[3 * t.slot1 + 1]);
+			}
+		}
 		const int tb = bits_for(nt + 1);
 		if (2 + 2 * b + tb > 64)
 			return set_error(ctx, U26_ERR_CAPACITY, "PRP hit key needs %d bits", 2 + 2 * b + tb);
@@ -2602,9 +3044,11 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			ev.mark(0, st);
 			if (total_req)
 			{
-				raycast_kernel<<<div_up(total_req, 128), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
+				const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * kSplit;
+				raycast_kernel<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
 					S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(),
-					ftv, etv, d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
+					ftv, etv, S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(), S->d_front.as<uint32_t>() + kSplit,
+					d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
 					(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
 				U26_TRY(after_launch(ctx, "raycast_kernel"));
 			}
@@ -2702,10 +3146,25 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_CUDA(ctx, S->d_best.reserve(sizeof(uint32_t) * 2 * (nt + 1)));
 		uint32_t* d_best = S->d_best.as<uint32_t>();
 		uint32_t* d_bestcov = d_best + (nt + 1);
-		coverage_kernel<<<nt, 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_seg.as<uint32_t>(), d_ncand, S->d_cand_roots.as<uint32_t>(),
-			S->d_csize.as<uint32_t>(), S->d_anchor_off.as<uint32_t>(), S->d_anchors.as<uint32_t>(), S->d_ekeys.as<uint64_t>(), ne_entries, vb,
-			rb, d_best, d_bestcov);
-		U26_TRY(after_launch(ctx, "coverage_kernel"));
+		{
+			// coverage per anchor, then the best component per task
+			std::vector<uint32_t> tab(nt + 1, 0u);
+			for (uint32_t q = 0; q < nt; q++)
+				tab[q + 1] = tab[q] + (anchor_off[tasks[q].contour_local + 1] - anchor_off[tasks[q].contour_local]);
+			U26_TRY(upload(ctx, S->d_tab, tab));
+			U26_CUDA(ctx, S->d_cov.reserve(sizeof(uint32_t) * std::max(nh, 1u)));
+			U26_CUDA(ctx, cudaMemsetAsync(S->d_cov.ptr, 0, sizeof(uint32_t) * std::max(nh, 1u), st));
+			if (tab[nt] && ne_entries)
+			{
+				coverage_count_kernel<<<div_up(tab[nt], 256), 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_tab.as<uint32_t>(),
+					S->d_anchor_off.as<uint32_t>(), S->d_anchors.as<uint32_t>(), S->d_ekeys.as<uint64_t>(), ne_entries, vb, rb,
+					S->d_seg.as<uint32_t>(), S->d_cov.as<uint32_t>());
+				U26_TRY(after_launch(ctx, "coverage_count_kernel"));
+			}
+			best_component_kernel<<<div_up(32 * nt, 256), 256, 0, st>>>(nt, S->d_seg.as<uint32_t>(), d_ncand, S->d_cand_roots.as<uint32_t>(),
+				S->d_csize.as<uint32_t>(), S->d_cov.as<uint32_t>(), d_best, d_bestcov);
+			U26_TRY(after_launch(ctx, "best_component_kernel"));
+		}
 		const uint32_t nblk = div_up(nh1, 1024);
 		U26_CUDA(ctx, S->d_bsum.reserve(sizeof(uint32_t) * (nblk + 2)));
 		U26_CUDA(ctx, S->d_task_max.reserve(sizeof(uint32_t) * 3 * (nt + 1)));

@@ -79,9 +79,12 @@ namespace u26
 
 	// Radix sort of (key64, value32) pairs over bits [bit_lo, bit_hi), stable.
 	// keys/vals are sorted in place (ping-pong through internal scratch).
+	// Exclusive scan of v[0, n) in place on ctx's stream; tmp is grown to the scratch it needs.
+	u26_status device_exclusive_scan(u26_ctx* ctx, uint32_t* v, uint32_t n, DevBuf& tmp);
+
 	struct RadixSorter
 	{
-		DevBuf keys_alt, vals_alt, counts;
+		DevBuf keys_alt, vals_alt, counts, scan_tmp;
 		u26_status sort(u26_ctx* ctx, uint64_t* keys, uint32_t* vals, uint32_t n, int bit_lo, int bit_hi);
 		// Same passes over caller-provided scratch (allocates nothing): keys_alt/vals_alt hold
 		// n entries, counts holds 256 * ceil(n / 2048) words. The result ends in keys/vals.
@@ -92,6 +95,7 @@ namespace u26
 			keys_alt.release();
 			vals_alt.release();
 			counts.release();
+			scan_tmp.release();
 		}
 	};
 } // namespace u26
