@@ -123,6 +123,10 @@ def make_workload(name):
         return synthetic.folded_sheet(128, seed=1), {"workload": "folded_sheet_128x128", "triangles": 32258, "seed": 1}
     if name == "two_sheets64":
         return synthetic.two_sheets(64, seed=0), {"workload": "two_sheets_64x64", "triangles": 15876, "seed": 0}
+    if name == "batch64":
+        m = synthetic.batch_scenes(64, seed=2)
+        return m, {"workload": "batch_64_two_body_scenes", "triangles": int(len(m.faces)), "scenes": 64, "seed": 2,
+                   "tris_per_scene": "U[2000, 60000]", "bodies": "icosphere-derived shells or bumped sheets"}
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -148,10 +152,21 @@ def cpu_pass(mesh, max_contours, stride):
     return n_broad + run.pairs_tested, time.perf_counter() - t0
 
 
+CPU_BATCH_SCENES = 8  # scenes of the batch workload in the CPU sample
+
+
 def run_cpu_baseline(mesh, max_contours, samples=1):
     from oracle import oracle as o
     o.build()
     tests, sec = 0, 0.0
+    if mesh.meta.get("kind") == "batch_scenes":
+        from untangling26_b200 import synthetic
+        for s_i in range(CPU_BATCH_SCENES):
+            t, s = cpu_pass(synthetic.scene_mesh(mesh, s_i), max_contours, 1)
+            tests += t
+            sec += s
+        return {"value": tests / sec, "unit": UNIT, "cores": o.threads(), "kind": "port",
+                "sample": f"the full pass of the first {CPU_BATCH_SCENES} of {mesh.meta['num']} scenes, {sec:.1f} s"}
     for _ in range(samples):
         t, s = cpu_pass(mesh, max_contours, CPU_BASELINE_STRIDE)
         tests += t
@@ -167,13 +182,23 @@ def reference_arm(args, mesh, config):
         return
     from oracle import oracle as o
     o.build()
-    for _ in range(max(args.warmup, 0)):
-        cpu_pass(mesh, args.max_contours, CPU_REFERENCE_STRIDE)
+    if mesh.meta.get("kind") == "batch_scenes":
+        # each step: the full pass of two scenes of the batch, in turn
+        from untangling26_b200 import synthetic
+        scenes = [synthetic.scene_mesh(mesh, s_i) for s_i in range(mesh.meta["num"])]
+        step = lambda i: [cpu_pass(scenes[(2 * i + k) % len(scenes)], args.max_contours, 1) for k in range(2)]
+        sample = "each step the full pass of two scenes of the batch"
+    else:
+        step = lambda i: [cpu_pass(mesh, args.max_contours, CPU_REFERENCE_STRIDE)]
+        sample = (f"each step the full EF detection + PRP of every {CPU_REFERENCE_STRIDE}th "
+                  f"of the first {args.max_contours} contours")
+    for i in range(max(args.warmup, 0)):
+        step(i)
     tests, sec = 0, 0.0
-    for _ in range(args.steps):
-        t, s = cpu_pass(mesh, args.max_contours, CPU_REFERENCE_STRIDE)
-        tests += t
-        sec += s
+    for i in range(args.steps):
+        for t, s in step(i):
+            tests += t
+            sec += s
     value = tests / sec
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -182,8 +207,7 @@ def reference_arm(args, mesh, config):
         "config": dict(config, parallelism="host threads", l2="n/a (CPU)", max_contours=args.max_contours,
                        directions="reference seeds (<=10 per contour)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": o.threads(), "kind": "port",
-                         "sample": f"{args.steps} steps, each the full EF detection + PRP of every {CPU_REFERENCE_STRIDE}th "
-                                   f"of the first {args.max_contours} contours "
+                         "sample": f"{args.steps} steps, {sample} "
                                    "(the reference's algorithm restated on the CPU; its LuisaCompute build is absent)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
@@ -197,9 +221,15 @@ def main():
     ap.add_argument("--workload", default="folded256")
     ap.add_argument("--max-contours", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain-steps", type=int, default=1, help="timed passes of the plain form (0: skip)")
     args = ap.parse_args()
     ws, rank, local = _dist_env()
     mesh, config = make_workload(args.workload)
+    batch = args.workload.startswith("batch")
+    if batch:
+        # every contour of every scene, one merge batch (contour indices shift between the
+        # batched and the per-scene runs; the results stay the same)
+        args.max_contours = 1 << 20
     if args.impl == "reference":
         return reference_arm(args, mesh, config)
 
@@ -217,7 +247,7 @@ def main():
     ctx = Context(local)
     sc = CollisionScene(ctx, mesh, d_hat=1e-3, thickness=0.0, max_ef_pairs=max(1 << 16, mesh.num_edges))
     sc.construct_lbvh()
-    params = prp_params(max_contours=args.max_contours)
+    params = prp_params(max_contours=args.max_contours, batch_size=(1 << 20) if batch else 32)
     dev = torch.device("cuda", local)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
@@ -307,6 +337,53 @@ def main():
             roof["traffic"] = tr.get(roof["kernel"])
             roof_ef["traffic"] = tr.get("ef_detect_kernel")
 
+    # ---- the plain form on the same input (same pairs and results): one thread per request
+    # from the tree root, per-contour launches; for a batch of scenes, one pass per scene
+    plain = None
+    if args.plain_steps > 0:
+        pparams = prp_params(max_contours=args.max_contours, batch_size=(1 << 20) if batch else 32, form=1)
+        if batch:
+            from untangling26_b200 import synthetic
+            pscs = []
+            for s_i in range(mesh.meta["num"]):
+                m_i = synthetic.scene_mesh(mesh, s_i)
+                sc_i = CollisionScene(ctx, m_i, d_hat=1e-3, thickness=0.0, max_ef_pairs=max(1 << 16, m_i.num_edges))
+                sc_i.construct_lbvh()
+                pscs.append((sc_i, m_i))
+        else:
+            pscs = [(sc, mesh)]
+
+        def plain_pass():
+            tests = 0
+            for sc_i, m_i in pscs:
+                sc_i.refit_face_tree()
+                sc_i.resolver.reset()
+                sc_i.stats.zero_()
+                sc_i.ef_detect(with_stats=True)
+                n_i = sc_i.resolver.canonicalize(m_i.num_edges, m_i.num_faces)
+                r_i = sc_i.host_resolve(pparams, num_pairs=n_i)
+                tests += int(sc_i.stats[1].item()) + r_i.pairs_tested
+            return tests
+
+        plain_pass()
+        torch.cuda.synchronize()
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.plain_steps)]
+        ptests = 0
+        for i in range(args.plain_steps):
+            flush.fill_(i & 0xFF)
+            pev[i][0].record(stream)
+            ptests = plain_pass()
+            pev[i][1].record(stream)
+        torch.cuda.synchronize()
+        p_ms = sum(a.elapsed_time(b) for a, b in pev) / args.plain_steps
+        plain = {"value": ptests / (p_ms / 1e3), "unit": UNIT, "ms_per_step": p_ms, "steps": args.plain_steps,
+                 "same_tests": ptests == tests_pass, "untangle_passes_per_s": 1e3 / p_ms,
+                 "chosen_over_plain": value / ws / (ptests / (p_ms / 1e3)),
+                 "form": "one thread per request from the tree root, per-contour launches" + (", one pass per scene" if batch else "")}
+        if batch:
+            for sc_i, _ in pscs:
+                sc_i.close()
+
     # ---- e2e through the public API with host buffers
     x_host = torch.from_numpy(mesh.x).pin_memory()
     e_ms = []
@@ -333,10 +410,12 @@ def main():
             "warmup": max(args.warmup, 3), "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(config, l2="flushed between steps (256 MB write)", parallelism=f"scene replica per GPU x{ws}",
-                           max_contours=args.max_contours, directions="reference seeds (<=10 per contour)"),
+                           max_contours=args.max_contours, directions="reference seeds (<=10 per contour)",
+                           form="batched packet ray casting clipped to candidate boxes, all scenes in one pass"),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(mesh.x.nbytes), "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
             "untangle_passes_per_s": 1e3 * args.steps / total_ms,
+            "plain_form": plain,
             "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
             "pass": {"ef_pairs": n_ef, "contours": len(r0.contours), "processed": int(len(proc)),
                      "responses": int((proc["combo_idx"] != 0xFFFFFFFF).sum()), "levels": r0.levels,

@@ -201,6 +201,9 @@ typedef struct u26_mesh_desc
 	const uint32_t* vert_component; /* vert_topology_component_id */
 	const float *rest_vert_area, *rest_edge_area, *rest_face_area, *vert_mass;
 	const uint32_t* mesh_orientation; /* [objects] 0: normals along the triangle winding */
+	const uint32_t* object_scene;	  /* [objects] independent scene of each object, or NULL (one scene): several
+									   * simulations evaluated in one batch keep their own global centroid
+									   * (the radial seed direction of get_raycasting_direction) */
 } u26_mesh_desc;
 
 typedef struct u26_scene u26_scene;
@@ -221,6 +224,10 @@ typedef struct u26_prp_params
 								 * selected direction on S^2 (intersection_resolver2.cpp:1232-1486) */
 	uint32_t ccr_blend;			/* PRP_use_blended_intrinsic_coordinates (0): one blended ownership coordinate */
 	float ccr_blend_weight;		/* PRP_intrinsic_blend_weight (0.5): rest-coordinate weight of the blend */
+	uint32_t form;				/* ray casting form: 0 batched packet traversal clipped to the candidate boxes (default),
+								 * 1 the plain form (one thread per request from the root, one launch per contour);
+								 * both decide the same pairs and return the same results */
+	uint32_t reserved;
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:

@@ -69,6 +69,7 @@ namespace
 		const uint* vert_component;
 		const float *rest_vert_area, *rest_edge_area, *rest_face_area, *vert_mass;
 		const uint* mesh_orientation;
+		const uint* object_scene; // [objects] or null: one scene
 	};
 
 	struct Params
@@ -1063,7 +1064,8 @@ namespace
 	// (ascending eigenvalues), centre - side centroid for each side (fallback e1 / e2),
 	// +-(centre - global area-weighted centroid); mode 1: the 26 lattice directions
 	std::vector<V3> seed_directions(uint direction_mode, const std::vector<V3>& pts, const std::vector<float>& pw,
-		const std::vector<uint>* boundary, const float* x, const float* vert_area, uint num_verts)
+		const std::vector<uint>* boundary, const float* x, const float* vert_area, uint num_verts,
+		const std::function<bool(uint)>& in_scene = nullptr)
 	{
 		std::vector<V3> dirs;
 		if (direction_mode == 1)
@@ -1131,6 +1133,8 @@ namespace
 		float tm = 0.0f;
 		for (uint v = 0; v < num_verts; v++)
 		{
+			if (in_scene && !in_scene(v))
+				continue;
 			const float w = std::fmax(vert_area[v], 1e-8f);
 			gc = gc + load3(x, v) * w;
 			tm += w;
@@ -1156,7 +1160,14 @@ namespace
 			pts.push_back(S.pos3[p]);
 			pw.push_back(S.length[p]);
 		}
-		return seed_directions(S.p.direction_mode, pts, pw, r.boundary, S.m.x, S.m.rest_vert_area, S.m.num_verts);
+		const MeshIn& m = S.m;
+		if (!m.object_scene)
+			return seed_directions(S.p.direction_mode, pts, pw, r.boundary, m.x, m.rest_vert_area, m.num_verts);
+		// independent scenes in one batch: the global centroid of the contour's own scene
+		const uint sc = m.object_scene[r.object_ids[0]];
+		return seed_directions(S.p.direction_mode, pts, pw, r.boundary, m.x, m.rest_vert_area, m.num_verts,
+			[&](uint v)
+			{ return m.object_scene[m.vert_object[v]] == sc; });
 	}
 
 	inline uint kring_init(uint boundary_count, uint diam)

@@ -110,3 +110,18 @@ def test_prp_direction_refinement_flat_supports(oracle, u26ctx):
     res, ref = _run_both(oracle, u26ctx, m, opt_iterations=4)
     assert all(r["opt_attempted"] == 0 for r in ref.results)
     _compare(res, ref)
+
+
+@pytest.mark.parametrize("mesh_fn", [lambda: synthetic.folded_sheet(48, seed=2), lambda: synthetic.two_sheets(64, seed=3)])
+def test_prp_plain_form_same_results(u26ctx, mesh_fn):
+    """The plain form (one thread per request from the tree root, per-contour launches, no
+    candidate-box clipping) decides the same pairs and returns the same results as the
+    batched packet form."""
+    m = mesh_fn()
+    sc = CollisionScene(u26ctx, m, d_hat=1e-3, thickness=0.0)
+    sc.construct_lbvh()
+    chosen = sc.untangle_pass(prp_params(max_contours=64))
+    plain = sc.untangle_pass(prp_params(max_contours=64, form=1))
+    sc.close()
+    assert plain.device_error_flags == 0 and chosen.device_error_flags == 0
+    _compare(plain, chosen)

@@ -633,7 +633,10 @@ namespace u26
 		// read grown boxes: eps = 1e-5 (1 + max |bound|) per axis for the ray slab tests, one eps
 		// from all six bounds for the swept-edge box tests (the epsilon-grown node tests that
 		// keep the traversal a superset of the exact primitive tests).
-		__global__ void grow_boxes_kernel(const NodeBox* __restrict__ boxes, uint32_t n, int isotropic, NodeBox* __restrict__ out)
+		// The w lanes carry the node's links, so one 32-byte load serves a visit: inner node
+		// (mn.w, mx.w) = (left, right child); leaf (mn.w, mx.w) = (primitive, ~0).
+		__global__ void grow_boxes_kernel(const NodeBox* __restrict__ boxes, const uint2* __restrict__ children,
+			const uint32_t* __restrict__ object_idx, uint32_t n, int isotropic, NodeBox* __restrict__ out)
 		{
 			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 			if (i >= n)
@@ -653,6 +656,18 @@ namespace u26
 				const float ez = 1e-5f * (1.0f + fmaxf(fabsf(b.mn.z), fabsf(b.mx.z)));
 				g.mn = make_float4(b.mn.x - ex, b.mn.y - ey, b.mn.z - ez, 0.0f);
 				g.mx = make_float4(b.mx.x + ex, b.mx.y + ey, b.mx.z + ez, 0.0f);
+			}
+			const uint32_t obj = object_idx[i];
+			if (obj != kInvalid)
+			{
+				g.mn.w = __uint_as_float(obj);
+				g.mx.w = __uint_as_float(kInvalid);
+			}
+			else
+			{
+				const uint2 ch = children[i];
+				g.mn.w = __uint_as_float(ch.x);
+				g.mx.w = __uint_as_float(ch.y);
 			}
 			out[i] = g;
 		}
@@ -776,7 +791,7 @@ namespace u26
 		// kSplit parts x the requests rounded up to warps; part p starts at frontier node p,
 		// so every (ray, leaf) pair is decided once.
 		constexpr int kStack = 64;
-		__global__ void __launch_bounds__(128) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
+		__global__ void __launch_bounds__(128, 8) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
 			TreeView ftree, TreeView etree, const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow,
@@ -916,9 +931,10 @@ namespace u26
 					const bool hit = on && ray_grown_box(slab, t_lo, t_hi, b);
 					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
 						continue;
-					const uint32_t fid = __ldg(ftree.object_idx + node);
-					if (fid != kInvalid)
+					const uint32_t link_a = __float_as_uint(b.mn.w), link_b = __float_as_uint(b.mx.w);
+					if (link_b == kInvalid)
 					{
+						const uint32_t fid = link_a;
 						if (hit)
 						{
 							tested++;
@@ -947,12 +963,11 @@ namespace u26
 							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
 						break;
 					}
-					const uint2 ch = __ldg(ftree.children + node);
 					__syncwarp();
 					if (lane == 0)
 					{
-						stack[sp] = ch.y;
-						stack[sp + 1] = ch.x;
+						stack[sp] = link_b;
+						stack[sp + 1] = link_a;
 					}
 					sp += 2;
 					__syncwarp();
@@ -987,9 +1002,10 @@ namespace u26
 						(smx.z >= g.mn.z);
 					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
 						continue;
-					const uint32_t e2 = __ldg(etree.object_idx + node);
-					if (e2 != kInvalid)
+					const uint32_t link_a = __float_as_uint(g.mn.w), link_b = __float_as_uint(g.mx.w);
+					if (link_b == kInvalid)
 					{
+						const uint32_t e2 = link_a;
 						if (hit)
 						{
 							tested++;
@@ -1038,12 +1054,11 @@ namespace u26
 							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
 						break;
 					}
-					const uint2 ch = __ldg(etree.children + node);
 					__syncwarp();
 					if (lane == 0)
 					{
-						stack[sp] = ch.y;
-						stack[sp + 1] = ch.x;
+						stack[sp] = link_b;
+						stack[sp + 1] = link_a;
 					}
 					sp += 2;
 					__syncwarp();
@@ -1064,6 +1079,215 @@ namespace u26
 				if (lane == 0)
 				{
 					// [0] leaf primitive tests, [1] requests, [2] ray-node tests, [3] edge leaf tests
+					atomicAdd(stats + 0, (unsigned long long)tsum);
+					atomicAdd(stats + 1, (unsigned long long)rsum);
+					atomicAdd(stats + 2, (unsigned long long)vsum);
+					atomicAdd(stats + 3, (unsigned long long)esum);
+				}
+			}
+		}
+
+		// ---- the plain form (the comparison baseline of the batched, filtered form above):
+		// one thread per request with a private stack from the root, the epsilon-grown node
+		// tests evaluated per visit, no clipping to the candidate boxes, one launch per contour.
+		// It decides the same (request, primitive) pairs with the same exact tests.
+		__device__ __forceinline__ bool ray_box_plain(f3 o, f3 d, const NodeBox& b)
+		{
+			float tmin = 0.0f, tmax = 1.0f;
+			const float lo[3] = { b.mn.x, b.mn.y, b.mn.z }, hi[3] = { b.mx.x, b.mx.y, b.mx.z };
+			const float oo[3] = { o.x, o.y, o.z }, dd[3] = { d.x, d.y, d.z };
+#pragma unroll
+			for (int a = 0; a < 3; a++)
+			{
+				const float eps = 1e-5f * (1.0f + fmaxf(fabsf(lo[a]), fabsf(hi[a])));
+				const float l = lo[a] - eps, h = hi[a] + eps;
+				if (fabsf(dd[a]) < 1e-30f)
+				{
+					if (oo[a] < l || oo[a] > h)
+						return false;
+					continue;
+				}
+				const float inv = 1.0f / dd[a];
+				float t0 = (l - oo[a]) * inv, t1 = (h - oo[a]) * inv;
+				if (t0 > t1)
+				{
+					const float tt = t0;
+					t0 = t1;
+					t1 = tt;
+				}
+				tmin = fmaxf(tmin, t0);
+				tmax = fminf(tmax, t1);
+			}
+			return tmin <= tmax;
+		}
+
+		__global__ void __launch_bounds__(128) raycast_plain_kernel(const Task* __restrict__ tasks, uint32_t t_first, uint32_t ntasks,
+			uint32_t r_first, uint32_t count, const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v,
+			const uint32_t* __restrict__ cand_e, uint32_t v_stride, uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e,
+			const uint32_t* __restrict__ bits_f, TreeView ftree, TreeView etree, const float* __restrict__ x, const uint2* __restrict__ edges,
+			const uint32_t* __restrict__ faces, HitSink sink, unsigned long long* __restrict__ stats, uint32_t* __restrict__ dev_err)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			uint32_t tested = 0, visited = 0, etested = 0;
+			if (i < count)
+			{
+				const uint32_t r = r_first + i;
+				uint32_t lo = t_first, hi = t_first + ntasks;
+				while (hi - lo > 1)
+				{
+					const uint32_t mid = (lo + hi) >> 1;
+					if (tasks[mid].req_begin <= r)
+						lo = mid;
+					else
+						hi = mid;
+				}
+				const uint32_t t = lo;
+				const Task tk = tasks[t];
+				const uint32_t local = r - tk.req_begin;
+				const f3 dir = mk3(tk.dir[0], tk.dir[1], tk.dir[2]);
+				uint32_t stack[64];
+				int sp = 0;
+				if (local < tk.n_vf || local >= tk.n_vf + tk.n_ee)
+				{
+					const bool fv = local >= tk.n_vf;
+					const uint32_t vid = fv ? cand_v[size_t(tk.slot1) * v_stride + (local - tk.n_vf - tk.n_ee)] : cand_v[size_t(tk.slot0) * v_stride + local];
+					const Slot tgt = slots[fv ? tk.slot0 : tk.slot1];
+					const uint32_t* bits = bits_f + size_t(fv ? tk.slot0 : tk.slot1) * (f_stride / 32 + 1);
+					const f3 cast = fv ? -dir : dir;
+					const f3 orig = ld3(x, vid);
+					const f3 end = orig + cast * 1.0f;
+					if (ftree.n)
+						stack[sp++] = 0u;
+					for (uint32_t loop = 0; sp > 0; loop++)
+					{
+						const uint32_t node = stack[--sp];
+						visited++;
+						NodeBox b;
+						b.mn = __ldg(&ftree.boxes[node].mn);
+						b.mx = __ldg(&ftree.boxes[node].mx);
+						if (!ray_box_plain(orig, cast, b))
+							continue;
+						const uint32_t fid = __ldg(ftree.object_idx + node);
+						if (fid != kInvalid)
+						{
+							tested++;
+							if (!bit_test(bits, tgt.f_lo, tgt.f_cnt, fid))
+								continue;
+							const uint32_t f0 = faces[3 * fid], f1 = faces[3 * fid + 1], f2 = faces[3 * fid + 2];
+							if (vid == f0 || vid == f1 || vid == f2)
+								continue;
+							f3 bary;
+							float tt;
+							if (seg_tri(orig, end, ld3(x, f0), ld3(x, f1), ld3(x, f2), bary, tt) && tt >= 0.0f && tt <= 1.0f)
+								emit(sink, t, fv ? 2u : 0u, fv ? fid : vid, fv ? vid : fid, bary.x, bary.y, tt * 1.0f);
+							continue;
+						}
+						if (sp + 2 > 64 || loop > 4000000u)
+						{
+							atomicOr(dev_err, sp + 2 > 64 ? U26_DEVERR_STACK_OVERFLOW : U26_DEVERR_ITERATION_CAP);
+							break;
+						}
+						const uint2 ch = __ldg(ftree.children + node);
+						stack[sp++] = ch.y;
+						stack[sp++] = ch.x;
+					}
+				}
+				else
+				{
+					const uint32_t eid = cand_e[size_t(tk.slot0) * e_stride + (local - tk.n_vf)];
+					const uint32_t* bits = bits_e + size_t(tk.slot1) * (e_stride / 32 + 1);
+					const Slot s1 = slots[tk.slot1];
+					const uint2 ev = edges[eid];
+					const f3 p0 = ld3(x, ev.x), p1 = ld3(x, ev.y);
+					const float dl2 = dot(dir, dir);
+					float ray_max = 1.0f;
+					if (!(dl2 <= 1e-12f))
+					{
+						const float smin = fminf(dot(p0, dir), dot(p1, dir));
+						ray_max = fminf(fmaxf((tk.ee_pmax - smin) / dl2 + 1e-5f, 0.0f), 1.0f);
+					}
+					const f3 e1 = p1 - p0;
+					f3 pn = cross(e1, dir);
+					const float nl = length(pn);
+					const bool plane = nl >= 1e-10f;
+					float pd = 0.0f;
+					if (plane)
+					{
+						pn = pn / nl;
+						pd = dot(pn, p0);
+					}
+					const f3 a_end = p0 + dir * ray_max, b_end = p1 + dir * ray_max;
+					const f3 smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
+					const f3 smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
+					if (ray_max > 0.0f && etree.n)
+						stack[sp++] = 0u;
+					for (uint32_t loop = 0; sp > 0; loop++)
+					{
+						const uint32_t node = stack[--sp];
+						visited++;
+						NodeBox b;
+						b.mn = __ldg(&etree.boxes[node].mn);
+						b.mx = __ldg(&etree.boxes[node].mx);
+						const float e = 1e-5f * (1.0f + fmaxf(fmaxf(fmaxf(fabsf(b.mn.x), fabsf(b.mx.x)), fmaxf(fabsf(b.mn.y), fabsf(b.mx.y))),
+															   fmaxf(fabsf(b.mn.z), fabsf(b.mx.z))));
+						if (!((smn.x <= b.mx.x + e) & (smx.x >= b.mn.x - e) & (smn.y <= b.mx.y + e) & (smx.y >= b.mn.y - e) & (smn.z <= b.mx.z + e) &
+								(smx.z >= b.mn.z - e)))
+							continue;
+						const uint32_t e2 = __ldg(etree.object_idx + node);
+						if (e2 != kInvalid)
+						{
+							tested++;
+							etested++;
+							if (!bit_test(bits, s1.e_lo, s1.e_cnt, e2))
+								continue;
+							const uint2 qv = edges[e2];
+							if (ev.x == qv.x || ev.x == qv.y || ev.y == qv.x || ev.y == qv.y)
+								continue;
+							const f3 q0 = ld3(x, qv.x), q1 = ld3(x, qv.y);
+							if (plane)
+							{
+								const float d0 = dot(pn, q0) - pd;
+								const float d1 = dot(pn, q1) - pd;
+								if ((d0 > 1e-6f && d1 > 1e-6f) || (d0 < -1e-6f && d1 < -1e-6f))
+									continue;
+							}
+							const f3 e2v = q1 - q0;
+							const f3 rr = q0 - p0;
+							const f3 n = cross(e1, e2v);
+							const float det = -dot(dir, n);
+							if (fabsf(det) < 1e-10f)
+								continue;
+							const float inv = 1.0f / det;
+							const float d_r_e1_e2 = dot(rr, cross(e1, e2v));
+							const float d_dir_r_e2 = dot(dir, cross(rr, e2v));
+							const float d_dir_e1_r = dot(dir, cross(e1, rr));
+							const float sv = -d_r_e1_e2 * inv;
+							const float t1 = -d_dir_r_e2 * inv;
+							const float t2 = d_dir_e1_r * inv;
+							if (sv >= 0.0f && sv <= ray_max && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f)
+								emit(sink, t, 1u, eid, e2, 1.0f - t1, 1.0f - t2, sv);
+							continue;
+						}
+						if (sp + 2 > 64 || loop > 4000000u)
+						{
+							atomicOr(dev_err, sp + 2 > 64 ? U26_DEVERR_STACK_OVERFLOW : U26_DEVERR_ITERATION_CAP);
+							break;
+						}
+						const uint2 ch = __ldg(etree.children + node);
+						stack[sp++] = ch.y;
+						stack[sp++] = ch.x;
+					}
+				}
+			}
+			if (stats)
+			{
+				const uint32_t mask = __activemask();
+				const uint32_t tsum = __reduce_add_sync(mask, tested);
+				const uint32_t rsum = __reduce_add_sync(mask, i < count ? 1u : 0u);
+				const uint32_t vsum = __reduce_add_sync(mask, visited);
+				const uint32_t esum = __reduce_add_sync(mask, etested);
+				if ((threadIdx.x & 31) == uint32_t(__ffs(mask) - 1))
+				{
 					atomicAdd(stats + 0, (unsigned long long)tsum);
 					atomicAdd(stats + 1, (unsigned long long)rsum);
 					atomicAdd(stats + 2, (unsigned long long)vsum);
@@ -2247,7 +2471,7 @@ struct u26_scene
 	uint32_t nv = 0, ne = 0, nf = 0, nobj = 0;
 	std::vector<float> rest_x;
 	std::vector<uint32_t> edges, faces, fae, vav_off, vav, vae_off, vae, vaf_off, vaf, eaf_off, eaf, eae_off, eae;
-	std::vector<uint32_t> pv, pe, pf, vobj, vcomp, orient;
+	std::vector<uint32_t> pv, pe, pf, vobj, vcomp, orient, oscene;
 	std::vector<float> varea, earea, farea, vmass;
 	DevBuf d_rest_x, d_edges, d_faces, d_fae, d_vav_off, d_vav, d_vae_off, d_vae, d_vaf_off, d_vaf, d_eaf_off, d_eaf, d_eae_off, d_eae;
 	DevBuf d_vobj, d_varea, d_earea, d_farea, d_vmass, d_orient;
@@ -2340,6 +2564,10 @@ U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* m, u26_sc
 		cp(s->orient, m->mesh_orientation, s->nobj);
 	else
 		s->orient.assign(std::max(1u, s->nobj), 0u);
+	if (m->object_scene)
+		cp(s->oscene, m->object_scene, s->nobj);
+	else
+		s->oscene.assign(std::max(1u, s->nobj), 0u);
 	cpf(s->varea, m->rest_vert_area, s->nv);
 	cpf(s->earea, m->rest_edge_area, s->ne);
 	cpf(s->farea, m->rest_face_area, s->nf);
@@ -2791,17 +3019,21 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	// ---- 2. runtime identity, anchors, boundary verts, distances
 	t0 = std::chrono::steady_clock::now();
 	std::vector<ContourRT> R(nact);
-	V3h gc = mkv(0, 0, 0);
-	float tm = 0.0f;
+	// global area-weighted centroid of each independent scene (one scene unless the mesh
+	// says otherwise), summed in vertex order
+	const uint32_t nscene = S->oscene.empty() ? 1u : *std::max_element(S->oscene.begin(), S->oscene.end()) + 1u;
+	std::vector<V3h> gcs(nscene, mkv(0, 0, 0));
+	std::vector<float> tms(nscene, 0.0f);
 	for (uint32_t v = 0; v < S->nv; v++)
 	{
+		const uint32_t sc = S->oscene[S->vobj[v]];
 		const float w = std::fmax(S->varea[v], 1e-8f);
-		gc = gc + mkv(x[3 * v], x[3 * v + 1], x[3 * v + 2]) * w;
-		tm += w;
+		gcs[sc] = gcs[sc] + mkv(x[3 * v], x[3 * v + 1], x[3 * v + 2]) * w;
+		tms[sc] += w;
 	}
-	const bool gc_valid = tm > 1e-8f;
-	if (gc_valid)
-		gc = gc / tm;
+	for (uint32_t sc = 0; sc < nscene; sc++)
+		if (tms[sc] > 1e-8f)
+			gcs[sc] = gcs[sc] / tms[sc];
 	std::vector<uint32_t> anchor_off(nact + 1, 0u), anchors, bnd;
 	std::vector<Slot> slots(2 * size_t(nact));
 	for (uint32_t c = 0; c < nact; c++)
@@ -2853,7 +3085,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			sl.pad[1] = 0u;
 			bnd.insert(bnd.end(), b[sd].begin(), b[sd].end());
 		}
-		r.dirs = directions(*S, x, G, r, P->direction_mode, gc, gc_valid);
+		const uint32_t rsc = S->oscene[r.obj[0]];
+		r.dirs = directions(*S, x, G, r, P->direction_mode, gcs[rsc], tms[rsc] > 1e-8f);
 		const size_t nd = r.dirs.size();
 		r.res.assign(nd, ComboState{});
 		r.conv.assign(nd, 0);
@@ -2930,12 +3163,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * kSplit));
 		if (fn_)
 		{
-			grow_boxes_kernel<<<div_up(fn_, 256), 256, 0, st>>>(ftv.boxes, fn_, 0, S->d_fgrow.as<NodeBox>());
+			grow_boxes_kernel<<<div_up(fn_, 256), 256, 0, st>>>(ftv.boxes, ftv.children, ftv.object_idx, fn_, 0, S->d_fgrow.as<NodeBox>());
 			U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
 		}
 		if (en_)
 		{
-			grow_boxes_kernel<<<div_up(en_, 256), 256, 0, st>>>(etv.boxes, en_, 1, S->d_egrow.as<NodeBox>());
+			grow_boxes_kernel<<<div_up(en_, 256), 256, 0, st>>>(etv.boxes, etv.children, etv.object_idx, en_, 1, S->d_egrow.as<NodeBox>());
 			U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
 		}
 		frontier_kernel<<<1, 32, 0, st>>>(ftv.children, ftv.object_idx, fn_, S->d_front.as<uint32_t>());
@@ -3042,7 +3275,27 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			U26_CUDA(ctx, cudaMemsetAsync(S->d_hitcount.ptr, 0, sizeof(uint32_t), st));
 			HitSink sink{ S->d_keys.as<uint64_t>(), S->d_vals.as<uint32_t>(), S->d_pay_in.as<float>(), S->d_hitcount.as<uint32_t>(), hit_cap, b };
 			ev.mark(0, st);
-			if (total_req)
+			if (total_req && P->form == 1)
+			{
+				// plain form: one launch per contour (its tasks are contiguous)
+				for (uint32_t q = 0; q < nt;)
+				{
+					uint32_t e = q;
+					while (e < nt && tasks[e].contour_local == tasks[q].contour_local)
+						e++;
+					const uint32_t r0 = tasks[q].req_begin, r1 = e < nt ? tasks[e].req_begin : total_req;
+					if (r1 > r0)
+					{
+						raycast_plain_kernel<<<div_up(r1 - r0, 128), 128, 0, st>>>(S->d_tasks.as<Task>(), q, e - q, r0, r1 - r0, S->d_slots.as<Slot>(),
+							S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(),
+							S->d_bits_f.as<uint32_t>(), ftv, etv, d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), sink,
+							(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
+						U26_TRY(after_launch(ctx, "raycast_plain_kernel"));
+					}
+					q = e;
+				}
+			}
+			else if (total_req)
 			{
 				const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * kSplit;
 				raycast_kernel<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),

@@ -11,6 +11,8 @@ No dataset is read. Each generator takes a seed (numpy PCG64) and returns a Mesh
   the two layers cross each other in figure-eight and boundary-ending contours.
 * layered_sheets(n, layers): stacked n x n sheets 1 mm apart with seeded multi-octave
   value-noise displacement of 2-20 mm so that layers pass through their neighbours.
+* batch_scenes(num): independent two-body scenes (icosphere-derived shells or bumped
+  sheets, 2k-60k triangles each) laid out apart, for the batched-vs-per-scene comparison.
 """
 import numpy as np
 
@@ -111,4 +113,115 @@ def layered_sheets(n=512, layers=5, seed=4):
     m = Mesh(np.concatenate(xs).astype(np.float32), np.concatenate(fs), object_of_vert=np.concatenate(obj),
              rest_x=np.concatenate(rests).astype(np.float32))
     m.meta = {"kind": "layered_sheets", "n": n, "layers": layers, "seed": seed}
+    return m
+
+
+def icosphere(level):
+    """Unit icosphere: the icosahedron with every triangle split in four `level` times (edge
+    midpoints pushed to the sphere); outward winding. 20 * 4^level triangles."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1),
+         (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6), (7, 1, 8),
+         (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = f
+    for _ in range(level):
+        mid = {}
+
+        def m(a, b):
+            k = (min(a, b), max(a, b))
+            if k not in mid:
+                p = verts[a] + verts[b]
+                verts.append(p / np.linalg.norm(p))
+                mid[k] = len(verts) - 1
+            return mid[k]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = m(a, b), m(b, c), m(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(verts), np.array(faces, np.uint32)
+
+
+def _rotation(rng):
+    q = rng.normal(size=4)
+    q /= np.linalg.norm(q)
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def _shell_pair(tris, rng):
+    """Two closed shells derived from icospheres (radius U[0.1, 0.5] m, seeded low-order
+    radial bumps), overlapped by U[5%, 60%] of the smaller radius."""
+    level = int(np.clip(np.round(np.log(max(tris, 80) / 40.0) / np.log(4.0)), 2, 6))
+    unit, f = icosphere(level)
+    parts, rests = [], []
+    radii = rng.uniform(0.1, 0.5, 2)
+    depth = rng.uniform(0.05, 0.6) * radii.min()
+    centers = [np.zeros(3), np.array([radii[0] + radii[1] - depth, 0.0, 0.0])]
+    for k in range(2):
+        R = _rotation(rng)
+        d = unit @ R.T
+        bump = np.zeros(len(d))
+        for _ in range(3):
+            a = _rotation(rng)[0]
+            bump += rng.uniform(0.0, 0.06) * np.cos(rng.integers(2, 6) * np.arccos(np.clip(d @ a, -1.0, 1.0)))
+        rests.append(centers[k] + radii[k] * d)
+        parts.append(centers[k] + radii[k] * (1.0 + bump)[:, None] * d)
+    return parts, rests, [f, f], {"kind": "shells", "level": level, "radii": radii.tolist(), "depth": float(depth)}
+
+
+def _sheet_pair(tris, rng):
+    n = int(np.clip(np.round(np.sqrt(tris / 4.0)) + 1, 8, 256))
+    m = two_sheets(n, seed=int(rng.integers(0, 2 ** 31)))
+    nv = n * n
+    x = m.x.astype(np.float64)
+    rest = m.rest_x.astype(np.float64)
+    f = m.faces[: len(m.faces) // 2]
+    return [x[:nv], x[nv:]], [rest[:nv], rest[nv:]], [f, f], {"kind": "sheets", "n": n, **{k: m.meta[k] for k in ("amplitude", "periods")}}
+
+
+def batch_scenes(num=64, seed=2, tris_lo=2000, tris_hi=60000, spacing=3.0):
+    """The batching workload: `num` independent two-body scenes, each with a seeded triangle
+    count uniform in [tris_lo, tris_hi], made of a pair of icosphere-derived closed shells or
+    a pair of bumped cloth sheets, laid out on a grid `spacing` m apart so that no two
+    scenes touch. meta["scenes"] lists each scene's vertex / face ranges, so every scene can
+    also be evaluated on its own (scene_mesh)."""
+    rng = np.random.default_rng(seed)
+    xs, rests, fs, obj, scenes = [], [], [], [], []
+    nv = nf = 0
+    cols = int(np.ceil(np.sqrt(num)))
+    for s in range(num):
+        tris = int(rng.integers(tris_lo, tris_hi + 1))
+        parts, prest, pf, info = (_shell_pair if rng.uniform() < 0.5 else _sheet_pair)(tris, rng)
+        off = np.array([spacing * (s % cols), spacing * (s // cols), 0.0])
+        v0, f0 = nv, nf
+        for k in range(2):
+            xs.append(parts[k] + off)
+            rests.append(prest[k] + off)
+            fs.append(pf[k] + nv)
+            obj.append(np.full(len(parts[k]), 2 * s + k, np.uint32))
+            nv += len(parts[k])
+            nf += len(pf[k])
+        scenes.append(dict(info, verts=[v0, nv], faces=[f0, nf], tris=nf - f0))
+    m = Mesh(np.concatenate(xs).astype(np.float32), np.concatenate(fs).astype(np.uint32), object_of_vert=np.concatenate(obj),
+             rest_x=np.concatenate(rests).astype(np.float32))
+    m.object_scene = np.repeat(np.arange(num, dtype=np.uint32), 2)
+    m.meta = {"kind": "batch_scenes", "num": num, "seed": seed, "scenes": scenes}
+    return m
+
+
+def scene_mesh(batch, s):
+    """Scene s of a batch_scenes mesh as a mesh of its own (same positions)."""
+    sc = batch.meta["scenes"][s]
+    v0, v1 = sc["verts"]
+    f0, f1 = sc["faces"]
+    x = batch.x[v0:v1]
+    objv = batch.object_of_vert[v0:v1] - batch.object_of_vert[v0]
+    m = Mesh(x, (batch.faces[f0:f1] - v0).astype(np.uint32), object_of_vert=objv.astype(np.uint32), rest_x=batch.rest_x[v0:v1])
+    m.meta = {"kind": "scene_of_batch", "scene": s, **sc}
     return m
