@@ -310,16 +310,20 @@ def main():
     proc = r0.results[(r0.results["flags"] & 16) > 0]
 
     # ---- roofline of the dominant kernel (raycast_kernel, per the ncu launch list):
-    # algorithmic bytes of all its launches in a pass / their CUDA-event time. Bytes: 44 B
-    # per BVH node visited (32 B box + 8 B children + 4 B leaf id), 48 B per triangle leaf
-    # test (12 B indices + 36 B positions), 32 B per edge leaf test (8 B + 24 B), 24 B per
-    # request (source positions) — each counted once, as if caches were ideal.
+    # algorithmic bytes of all its launches in a pass / their CUDA-event time, per ray as
+    # the survey defines them: 44 B per BVH node the ray's own traversal visits (32 B box +
+    # 8 B children + 4 B leaf id), 48 B per triangle leaf test (12 B indices + 36 B
+    # positions), 32 B per edge leaf test (8 B + 24 B), 24 B per request (source positions).
+    # The packet kernel shares each node / leaf record among its 32 rays (packet fetches are
+    # reported beside), so most of these bytes come from L1 / L2 (traffic: ncu).
     peak, peak_kind = _peaks()
-    rc_bytes = 44 * r0.nodes_visited + 48 * (r0.tested - r0.edge_tests) + 32 * r0.edge_tests + 24 * r0.requests
+    rc_bytes = 44 * r0.ray_visits + 48 * (r0.tested - r0.edge_tests) + 32 * r0.edge_tests + 24 * r0.requests
     rc_ms = r0.gpu_ms["raycast"]
     roof = {"bound": "hbm", "achieved": rc_bytes / (rc_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
             "peak_source": peak_kind, "kernel": "raycast_kernel", "kernel_ms_per_pass": rc_ms,
             "launches_per_pass": r0.levels + 1, "algorithmic_bytes_per_pass": rc_bytes, "traffic": None,
+            "ray_node_visits": r0.ray_visits, "packet_node_tests": r0.nodes_visited, "packet_node_fetches": r0.node_fetches,
+            "packet_leaf_fetches": r0.tri_fetches + r0.edge_fetches,
             "note": "achieved uses all raycast launches of one pass; most of the traffic is served by L2"}
     roof["frac"] = roof["achieved"] / peak
     st = sc.stats.cpu().numpy()

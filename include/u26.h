@@ -276,9 +276,13 @@ typedef struct u26_prp_output_view
 	uint32_t levels;				 /* k-ring levels evaluated (max over batches) */
 	uint32_t device_error_flags;
 	double stage_ms[8];				 /* host wall time per stage: preprocess, runtime, candidates, raycast, cull, control, finalize, total */
-	uint64_t ray_nodes;				 /* BVH nodes visited by the ray casts */
+	uint64_t ray_nodes;				 /* ray / node box tests of the ray casts (per ray) */
 	uint64_t ray_edge_tests;		 /* leaf tests of the EE (edge-edge) casts, included in ray_tests */
 	double gpu_ms[6];				 /* GPU time (CUDA events): ray casting, hit sort, union-find, support entries, selection + metrics, download */
+	uint64_t ray_node_fetches;		 /* BVH node records brought in by the ray casts (one per warp packet visit) */
+	uint64_t ray_tri_fetches;		 /* triangle leaf records brought in (one per packet leaf visit) */
+	uint64_t ray_edge_fetches;		 /* edge leaf records brought in */
+	uint64_t ray_visits;			 /* BVH node tests each ray alone would make (the per-ray traversal work) */
 } u26_prp_output_view;
 
 /* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any
@@ -291,5 +295,21 @@ U26_API u26_status u26_prp_resolve(u26_scene* scene, u26_lbvh* face_tree, u26_lb
 	u26_prp_output** out);
 U26_API u26_status u26_prp_output_view_get(const u26_prp_output* out, u26_prp_output_view* view);
 U26_API void u26_prp_output_destroy(u26_prp_output* out);
+
+/* Differentiation over fixed supports (the torch.autograd binding of the objective; the
+ * reference computes dE/dr inside its direction refinement, intersection_resolver2.cpp:
+ * 1268-1320, and has no standalone entry point). For each contour c, with support
+ * hits[hit_offsets[c], hit_offsets[c+1]) and direction dirs[c]: the hit distances are
+ * recomputed from x and r as delta = (w . n) / (r . n); J[c] = (sum of the hits' rest source
+ * areas) * max(delta)^2 and E[c] = sum (delta + 3e-3)^2 / kappa (the displacement cost). With
+ * grad_J / grad_E (upstream gradients, either may be NULL) it also writes grad_dirs[c] =
+ * grad_J dJ/dr + grad_E dE/dr and ADDS grad_J dJ/dx + grad_E dE/dx into grad_x (zero it
+ * first). J's subgradient runs through the first maximal hit in key order. All pointers are
+ * device memory: x [V][3], hits as u26_prp_resolve returns them, hit_offsets [C+1], dirs,
+ * grad_dirs [C][3], the per-vertex / edge / face rest areas and vertex masses of the mesh;
+ * J, E may be NULL. Runs on ctx's stream. */
+U26_API u26_status u26_prp_adjoint(u26_ctx* ctx, const float* x, const u26_prp_hit* hits, const uint32_t* hit_offsets,
+	uint32_t num_contours, const float* dirs, const float* vert_area, const float* edge_area, const float* face_area,
+	const float* vert_mass, float* J, float* E, const float* grad_J, const float* grad_E, float* grad_dirs, float* grad_x);
 
 #endif /* U26_H */

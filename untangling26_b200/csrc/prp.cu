@@ -539,6 +539,48 @@ namespace u26
 			}
 		}
 
+		// ------------------------------------------------------------ request order
+		// Candidate vertices / edges of each slot ordered by the Morton code of their rest
+		// position (edge midpoint), so that the 32 requests of a warp packet start from a
+		// compact patch. Only the request order changes: hits are keyed by primitive ids.
+		__global__ void cand_keys_kernel(const uint32_t* __restrict__ slot_ids, const uint32_t* __restrict__ off, uint32_t nsid,
+			const uint32_t* __restrict__ cand, uint32_t stride, const uint32_t* __restrict__ rank, uint64_t* __restrict__ keys,
+			uint32_t* __restrict__ vals)
+		{
+			const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+			if (g >= off[nsid])
+				return;
+			uint32_t lo = 0, hi = nsid;
+			while (hi - lo > 1)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (off[mid] <= g)
+					lo = mid;
+				else
+					hi = mid;
+			}
+			const uint32_t id = cand[size_t(slot_ids[lo]) * stride + (g - off[lo])];
+			keys[g] = (uint64_t(lo) << 32) | rank[id];
+			vals[g] = id;
+		}
+		__global__ void cand_scatter_kernel(const uint32_t* __restrict__ slot_ids, const uint32_t* __restrict__ off, uint32_t nsid,
+			const uint32_t* __restrict__ vals, uint32_t* __restrict__ cand, uint32_t stride)
+		{
+			const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+			if (g >= off[nsid])
+				return;
+			uint32_t lo = 0, hi = nsid;
+			while (hi - lo > 1)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (off[mid] <= g)
+					lo = mid;
+				else
+					hi = mid;
+			}
+			cand[size_t(slot_ids[lo]) * stride + (g - off[lo])] = vals[g];
+		}
+
 		// ------------------------------------------------------------ ray casting
 		struct Task
 		{
@@ -809,6 +851,8 @@ namespace u26
 				return; // whole warps only
 			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
 			uint32_t tested = 0, visited = 0, etested = 0;
+			uint32_t fetch_nodes = 0, fetch_tris = 0, fetch_edges = 0; // warp-uniform: data each packet brings in
+			uint32_t ray_visits = 0; // the node tests this ray alone would make: its start + 2 per inner node it enters
 
 			// ---- per-lane request
 			int kind = 0; // 1: VF / FV ray on the face tree, 2: EE swept edge on the edge tree
@@ -916,6 +960,7 @@ namespace u26
 			const uint32_t fstart = ffront[part];
 			if (__any_sync(0xFFFFFFFFu, on) && fstart != kInvalid)
 			{
+				ray_visits += on ? 1u : 0u;
 				int sp = 1;
 				if (lane == 0)
 					stack[0] = fstart;
@@ -928,6 +973,7 @@ namespace u26
 					b.mn = __ldg(&fgrow[node].mn);
 					b.mx = __ldg(&fgrow[node].mx);
 					visited += on ? 1u : 0u;
+					fetch_nodes++;
 					const bool hit = on && ray_grown_box(slab, t_lo, t_hi, b);
 					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
 						continue;
@@ -935,6 +981,7 @@ namespace u26
 					if (link_b == kInvalid)
 					{
 						const uint32_t fid = link_a;
+						fetch_tris++;
 						if (hit)
 						{
 							tested++;
@@ -957,6 +1004,7 @@ namespace u26
 						__syncwarp();
 						continue;
 					}
+					ray_visits += hit ? 2u : 0u;
 					if (sp + 2 > kStack)
 					{
 						if (lane == 0)
@@ -986,6 +1034,7 @@ namespace u26
 			const uint32_t estart = efront[part];
 			if (__any_sync(0xFFFFFFFFu, on) && estart != kInvalid)
 			{
+				ray_visits += on ? 1u : 0u;
 				int sp = 1;
 				if (lane == 0)
 					stack[0] = estart;
@@ -998,6 +1047,7 @@ namespace u26
 					g.mn = __ldg(&egrow[node].mn);
 					g.mx = __ldg(&egrow[node].mx);
 					visited += on ? 1u : 0u;
+					fetch_nodes++;
 					const bool hit = on && (smn.x <= g.mx.x) & (smx.x >= g.mn.x) & (smn.y <= g.mx.y) & (smx.y >= g.mn.y) & (smn.z <= g.mx.z) &
 						(smx.z >= g.mn.z);
 					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
@@ -1006,6 +1056,7 @@ namespace u26
 					if (link_b == kInvalid)
 					{
 						const uint32_t e2 = link_a;
+						fetch_edges++;
 						if (hit)
 						{
 							tested++;
@@ -1048,6 +1099,7 @@ namespace u26
 						__syncwarp();
 						continue;
 					}
+					ray_visits += hit ? 2u : 0u;
 					if (sp + 2 > kStack)
 					{
 						if (lane == 0)
@@ -1076,13 +1128,20 @@ namespace u26
 				const uint32_t rsum = __reduce_add_sync(0xFFFFFFFFu, (part == 0 && r < total) ? 1u : 0u);
 				const uint32_t vsum = __reduce_add_sync(0xFFFFFFFFu, visited);
 				const uint32_t esum = __reduce_add_sync(0xFFFFFFFFu, etested);
+				const uint32_t rvsum = __reduce_add_sync(0xFFFFFFFFu, ray_visits);
 				if (lane == 0)
 				{
-					// [0] leaf primitive tests, [1] requests, [2] ray-node tests, [3] edge leaf tests
+					// [0] leaf primitive tests, [1] requests, [2] ray-node tests, [3] edge leaf tests,
+					// [4] node fetches, [5] triangle fetches, [6] edge fetches (per packet),
+					// [7] single-ray node visits
+					atomicAdd(stats + 7, (unsigned long long)rvsum);
 					atomicAdd(stats + 0, (unsigned long long)tsum);
 					atomicAdd(stats + 1, (unsigned long long)rsum);
 					atomicAdd(stats + 2, (unsigned long long)vsum);
 					atomicAdd(stats + 3, (unsigned long long)esum);
+					atomicAdd(stats + 4, (unsigned long long)fetch_nodes);
+					atomicAdd(stats + 5, (unsigned long long)fetch_tris);
+					atomicAdd(stats + 6, (unsigned long long)fetch_edges);
 				}
 			}
 		}
@@ -1292,6 +1351,10 @@ namespace u26
 					atomicAdd(stats + 1, (unsigned long long)rsum);
 					atomicAdd(stats + 2, (unsigned long long)vsum);
 					atomicAdd(stats + 3, (unsigned long long)esum);
+					atomicAdd(stats + 4, (unsigned long long)vsum);
+					atomicAdd(stats + 5, (unsigned long long)(tsum - esum));
+					atomicAdd(stats + 6, (unsigned long long)esum);
+					atomicAdd(stats + 7, (unsigned long long)vsum);
 				}
 			}
 		}
@@ -2484,7 +2547,8 @@ struct u26_scene
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
-	RadixSorter sorter, esorter;
+	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals;
+	RadixSorter sorter, esorter, csorter;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 };
@@ -2500,7 +2564,7 @@ struct u26_prp_output
 	uint64_t ray_tests = 0, ray_requests = 0, ray_pairs = 0;
 	double stage_ms[8] = { 0 };
 	double gpu_ms[6] = { 0 };
-	uint64_t ray_nodes = 0, ray_edge_tests = 0;
+	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0;
 };
 
 template <typename T>
@@ -2598,6 +2662,49 @@ U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* m, u26_sc
 	U26_TRY(upload(ctx, s->d_farea, s->farea));
 	U26_TRY(upload(ctx, s->d_vmass, s->vmass));
 	U26_TRY(upload(ctx, s->d_orient, s->orient));
+	{
+		// 30-bit Morton codes of the rest positions (vertices) and rest edge midpoints over
+		// the rest AABB: the request order of the ray casts
+		float lo[3] = { INFINITY, INFINITY, INFINITY }, hi[3] = { -INFINITY, -INFINITY, -INFINITY };
+		for (uint32_t v = 0; v < s->nv; v++)
+			for (int a = 0; a < 3; a++)
+			{
+				lo[a] = std::fmin(lo[a], s->rest_x[3 * v + a]);
+				hi[a] = std::fmax(hi[a], s->rest_x[3 * v + a]);
+			}
+		auto spread = [](uint32_t q)
+		{
+			q = (q * 0x00010001u) & 0xFF0000FFu;
+			q = (q * 0x00000101u) & 0x0F00F00Fu;
+			q = (q * 0x00000011u) & 0xC30C30C3u;
+			q = (q * 0x00000005u) & 0x49249249u;
+			return q;
+		};
+		auto code = [&](const float* p)
+		{
+			uint32_t c = 0;
+			for (int a = 0; a < 3; a++)
+			{
+				const float ext = hi[a] - lo[a];
+				const float u = ext > 0.0f ? (p[a] - lo[a]) / ext : 0.0f;
+				const uint32_t q = uint32_t(std::fmin(std::fmax(u * 1024.0f, 0.0f), 1023.0f));
+				c |= spread(q) << (2 - a);
+			}
+			return c;
+		};
+		std::vector<uint32_t> vr(std::max(1u, s->nv)), er(std::max(1u, s->ne));
+		for (uint32_t v = 0; v < s->nv; v++)
+			vr[v] = code(&s->rest_x[3 * v]);
+		for (uint32_t e = 0; e < s->ne; e++)
+		{
+			const uint32_t a = s->edges[2 * e], b = s->edges[2 * e + 1];
+			const float mid[3] = { 0.5f * (s->rest_x[3 * a] + s->rest_x[3 * b]), 0.5f * (s->rest_x[3 * a + 1] + s->rest_x[3 * b + 1]),
+				0.5f * (s->rest_x[3 * a + 2] + s->rest_x[3 * b + 2]) };
+			er[e] = code(mid);
+		}
+		U26_TRY(upload(ctx, s->d_vrank, vr));
+		U26_TRY(upload(ctx, s->d_erank, er));
+	}
 	U26_CUDA(ctx, s->d_fn.reserve(sizeof(float) * 3 * std::max(1u, s->nf)));
 	U26_CUDA(ctx, s->d_en.reserve(sizeof(float) * 3 * std::max(1u, s->ne)));
 	U26_CUDA(ctx, s->d_vn.reserve(sizeof(float) * 3 * std::max(1u, s->nv)));
@@ -2619,11 +2726,12 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
 		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
 		&s->d_step_hits, &s->d_step_out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
-		&s->d_cur_opp, &s->d_tab, &s->d_cov };
+		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
 	s->esorter.release();
+	s->csorter.release();
 	delete s;
 }
 
@@ -3152,8 +3260,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 
 	// ---- 3. adaptive k-ring levels, every active (contour, direction) task batched
 	const int b = bits_for(std::max({ S->nv, S->ne, S->nf, 2u }));
-	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 4));
-	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 4, st));
+	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 8));
+	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 8, st));
 	const TreeView ftv = tree_view(face_tree), etv = tree_view(edge_tree);
 	// grown node boxes of this pass's trees and the subtree roots of the split traversal
 	{
@@ -3221,6 +3329,30 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_TRY(after_launch(ctx, "candidates_kernel"));
 		U26_TRY(download(ctx, counts, S->d_counts.ptr, 3 * size_t(nslots)));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
+		// request order: each slot's candidate vertices and edges by rest-space Morton code
+		const uint32_t nsid = uint32_t(sids.size());
+		const int sid_bits = bits_for(nsid + 1);
+		for (int kind = 0; kind < 2; kind++)
+		{
+			std::vector<uint32_t> off(nsid + 1, 0u);
+			for (uint32_t j = 0; j < nsid; j++)
+				off[j + 1] = off[j] + counts[3 * sids[j] + kind];
+			const uint32_t total = off[nsid];
+			if (total < 2)
+				continue;
+			U26_TRY(upload(ctx, S->d_cand_off, off));
+			U26_CUDA(ctx, S->d_ckeys.reserve(sizeof(uint64_t) * total));
+			U26_CUDA(ctx, S->d_cvals.reserve(sizeof(uint32_t) * total));
+			uint32_t* cand = kind == 0 ? S->d_cand_v.as<uint32_t>() : S->d_cand_e.as<uint32_t>();
+			const uint32_t stride = kind == 0 ? vs : es_;
+			cand_keys_kernel<<<div_up(total, 256), 256, 0, st>>>(S->d_slot_ids.as<uint32_t>(), S->d_cand_off.as<uint32_t>(), nsid, cand, stride,
+				kind == 0 ? S->d_vrank.as<uint32_t>() : S->d_erank.as<uint32_t>(), S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>());
+			U26_TRY(after_launch(ctx, "cand_keys_kernel"));
+			U26_TRY(S->csorter.sort(ctx, S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>(), total, 0, 32 + sid_bits));
+			cand_scatter_kernel<<<div_up(total, 256), 256, 0, st>>>(S->d_slot_ids.as<uint32_t>(), S->d_cand_off.as<uint32_t>(), nsid,
+				S->d_cvals.as<uint32_t>(), cand, stride);
+			U26_TRY(after_launch(ctx, "cand_scatter_kernel"));
+		}
 		return U26_OK;
 	};
 
@@ -3979,7 +4111,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->hits.insert(out->hits.end(), cs.hits.begin(), cs.hits.end());
 	}
 	std::vector<unsigned long long> stats;
-	U26_TRY(download(ctx, stats, S->d_stats.ptr, 4));
+	U26_TRY(download(ctx, stats, S->d_stats.ptr, 8));
 	U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, ctx->dev_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
 	U26_CUDA(ctx, cudaStreamSynchronize(st));
 	out->ray_tests = stats[0];
@@ -3987,6 +4119,10 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	out->ray_pairs = alg_tests;
 	out->ray_nodes = stats[2];
 	out->ray_edge_tests = stats[3];
+	out->ray_node_fetches = stats[4];
+	out->ray_tri_fetches = stats[5];
+	out->ray_edge_fetches = stats[6];
+	out->ray_visits = stats[7];
 	out->dev_err = *ctx->host_word;
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
@@ -4040,6 +4176,10 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->ray_pairs = o->ray_pairs;
 	v->ray_nodes = o->ray_nodes;
 	v->ray_edge_tests = o->ray_edge_tests;
+	v->ray_node_fetches = o->ray_node_fetches;
+	v->ray_tri_fetches = o->ray_tri_fetches;
+	v->ray_edge_fetches = o->ray_edge_fetches;
+	v->ray_visits = o->ray_visits;
 	for (int i = 0; i < 6; i++)
 		v->gpu_ms[i] = o->gpu_ms[i];
 	v->levels = o->levels;

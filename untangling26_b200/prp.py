@@ -65,7 +65,8 @@ class PrpOutputView(ctypes.Structure):
         ("contour_offsets", c_vp), ("contour_pairs", c_vp), ("results", c_vp), ("hit_offsets", c_vp), ("hits", c_vp),
         ("directions", c_vp), ("ray_tests", c_u64), ("ray_requests", c_u64), ("ray_pairs", c_u64), ("levels", c_u32),
         ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8), ("ray_nodes", c_u64),
-        ("ray_edge_tests", c_u64), ("gpu_ms", ctypes.c_double * 6),
+        ("ray_edge_tests", c_u64), ("gpu_ms", ctypes.c_double * 6), ("ray_node_fetches", c_u64), ("ray_tri_fetches", c_u64),
+        ("ray_edge_fetches", c_u64), ("ray_visits", c_u64),
     ]
 
 GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
@@ -112,3 +113,7 @@ class PrpResult:
         self.gpu_ms = dict(zip(GPU_PHASES, list(v.gpu_ms)))
         self.nodes_visited = int(v.ray_nodes)
         self.edge_tests = int(v.ray_edge_tests)
+        self.node_fetches = int(v.ray_node_fetches)
+        self.tri_fetches = int(v.ray_tri_fetches)
+        self.edge_fetches = int(v.ray_edge_fetches)
+        self.ray_visits = int(v.ray_visits)
