@@ -123,6 +123,10 @@ def make_workload(name):
         return synthetic.folded_sheet(128, seed=1), {"workload": "folded_sheet_128x128", "triangles": 32258, "seed": 1}
     if name == "two_sheets64":
         return synthetic.two_sheets(64, seed=0), {"workload": "two_sheets_64x64", "triangles": 15876, "seed": 0}
+    if name == "layered5x512":
+        m = synthetic.layered_sheets(512, layers=5, seed=4)
+        return m, {"workload": "layered_sheets_5x512x512", "triangles": int(len(m.faces)), "layers": 5, "seed": 4,
+                   "spacing_mm": 1, "displacement_mm": "U[2, 20] multi-octave"}
     if name == "batch64":
         m = synthetic.batch_scenes(64, seed=2)
         return m, {"workload": "batch_64_two_body_scenes", "triangles": int(len(m.faces)), "scenes": 64, "seed": 2,
@@ -324,7 +328,10 @@ def main():
             "launches_per_pass": r0.levels + 1, "algorithmic_bytes_per_pass": rc_bytes, "traffic": None,
             "ray_node_visits": r0.ray_visits, "packet_node_tests": r0.nodes_visited, "packet_node_fetches": r0.node_fetches,
             "packet_leaf_fetches": r0.tri_fetches + r0.edge_fetches,
-            "note": "achieved uses all raycast launches of one pass; most of the traffic is served by L2"}
+            "packet_bytes_per_pass": 32 * r0.node_fetches + 48 * r0.tri_fetches + 32 * r0.edge_fetches + 24 * r0.requests,
+            "note": ("achieved: the per-ray bytes of all raycast launches of one pass over their time; a warp packet "
+                     "shares each node and leaf record among its 32 rays, so these bytes come mostly from L1 / L2 and "
+                     "the packet's own record traffic (packet_bytes_per_pass) is far below HBM bandwidth")}
     roof["frac"] = roof["achieved"] / peak
     st = sc.stats.cpu().numpy()
     ef_nodes, ef_prims = int(st[0]), int(st[1])
@@ -340,6 +347,25 @@ def main():
             tr = json.load(f)
             roof["traffic"] = tr.get(roof["kernel"])
             roof_ef["traffic"] = tr.get("ef_detect_kernel")
+
+    # ---- LBVH refit: the fused leaf update + bottom-up refit of the face tree alone, L2
+    # flushed before every launch. Algorithmic bytes (each byte once): V x (12 B position +
+    # 4 B thickness) + F x (12 B face + 4 B leaf order + 32 B leaf box write) + (F - 1) x
+    # (8 B children + 4 B parent + 64 B child boxes + 32 B box write).
+    rf_n = 10
+    rf_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(rf_n)]
+    for i in range(rf_n):
+        flush.fill_((i + 7) & 0xFF)
+        rf_ev[i][0].record(stream)
+        sc.refit_face_tree()
+        rf_ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    rf_ms = statistics.median(a.elapsed_time(b) for a, b in rf_ev)
+    nvv, nff = mesh.num_verts, mesh.num_faces
+    rf_bytes = 16 * nvv + 48 * nff + 108 * max(nff - 1, 0)
+    refit = {"kernel": "refit_fused_kernel", "ms": rf_ms, "algorithmic_bytes": rf_bytes,
+             "achieved": rf_bytes / (rf_ms / 1e3) / 1e9, "unit": "GB/s", "peak": peak, "launches": rf_n}
+    refit["frac"] = refit["achieved"] / peak
 
     # ---- the plain form on the same input (same pairs and results): one thread per request
     # from the tree root, per-contour launches; for a batch of scenes, one pass per scene
@@ -420,7 +446,7 @@ def main():
                     "ms_per_step": e2e_ms / args.steps},
             "untangle_passes_per_s": 1e3 * args.steps / total_ms,
             "plain_form": plain,
-            "gpu_launches": int(launches), "roofline": roof, "clocks": clk,
+            "gpu_launches": int(launches), "roofline": roof, "lbvh_refit": refit, "clocks": clk,
             "pass": {"ef_pairs": n_ef, "contours": len(r0.contours), "processed": int(len(proc)),
                      "responses": int((proc["combo_idx"] != 0xFFFFFFFF).sum()), "levels": r0.levels,
                      "ef_leaf_tests": ef_tests_pass, "ray_pair_tests": prp_tests_pass,
