@@ -1458,6 +1458,27 @@ namespace
 		return s[0];
 	}
 
+	// The metrics' canonical sum: the lane sum over lists of up to 8192 terms; a longer list is
+	// cut into chunks of 8192 from its start, each chunk lane-summed, and the chunk sums
+	// lane-summed (the CUDA metrics kernels sum the chunks of a large support in parallel).
+	constexpr uint kSumChunk = 8192;
+	template <typename F>
+	float chunked_sum(uint n, F&& val)
+	{
+		if (n <= kSumChunk)
+			return lane_sum(n, val);
+		const uint nc = (n + kSumChunk - 1) / kSumChunk;
+		std::vector<float> cs(nc);
+		for (uint c = 0; c < nc; c++)
+		{
+			const uint b = c * kSumChunk, m = std::min(kSumChunk, n - b);
+			cs[c] = lane_sum(m, [&](uint i)
+				{ return val(b + i); });
+		}
+		return lane_sum(nc, [&](uint i)
+			{ return cs[i]; });
+	}
+
 	struct PenMetrics
 	{
 		float depth = 0, volume = 0, area = 0, objective = 0, cost = 0;
@@ -1514,11 +1535,11 @@ namespace
 		float depth = 0.0f;
 		for (const Hit& h : c.hits)
 			depth = std::fmax(depth, h.dist);
-		const float area = lane_sum(n, [&](uint i)
+		const float area = chunked_sum(n, [&](uint i)
 			{ float a, al; area_alpha(c.hits[i], a, al); return a; });
-		const float volume = lane_sum(n, [&](uint i)
+		const float volume = chunked_sum(n, [&](uint i)
 			{ float a, al; area_alpha(c.hits[i], a, al); return (a * al) * c.hits[i].dist; });
-		const float kappa = lane_sum(n, [&](uint i)
+		const float kappa = chunked_sum(n, [&](uint i)
 			{
 				const float sd = c.hits[i].dist + 3e-3f;
 				const float e = eff_inv(c.hits[i]);

@@ -10,6 +10,8 @@
 // that the stack-overflow cut-off drops the same pairs.
 #include <algorithm>
 
+#include <cuda/atomic>
+
 #include "lbvh_internal.h"
 
 namespace u26
@@ -358,8 +360,10 @@ namespace u26
 					atomicExch(health, 0u);
 					return;
 				}
-				__threadfence();
-				const uint32_t arrived = atomicAdd(flags + node, 1u);
+				// acq_rel arrival: releases this thread's boxes below the node, and the second
+				// arrival acquires its sibling's (one atom.acq_rel instead of two full fences)
+				const uint32_t arrived = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(flags[node]).fetch_add(1u,
+					cuda::memory_order_acq_rel);
 				if (arrived == 0u)
 					return;
 				if (arrived != 1u)
@@ -367,7 +371,6 @@ namespace u26
 					atomicExch(health, 0u);
 					return;
 				}
-				__threadfence();
 				const uint2 c = __ldg(children + node);
 				const NodeBox l = load_box_cg(boxes + c.x);
 				const NodeBox r = load_box_cg(boxes + c.y);

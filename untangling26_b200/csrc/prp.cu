@@ -40,6 +40,7 @@
 #include <memory>
 #include <numeric>
 #include <set>
+#include <thread>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -2077,20 +2078,14 @@ namespace u26
 		};
 
 		// one warp per task: canonical 32-lane strided sums over its contiguous selected terms
-		__global__ void task_sum_kernel(uint32_t ntasks, const Task* __restrict__ tasks, const uint32_t* __restrict__ seg,
-			const uint32_t* __restrict__ best, const uint32_t* __restrict__ bestcov, const uint32_t* __restrict__ comp_size,
-			const uint32_t* __restrict__ ncand, const uint32_t* __restrict__ sel_begin, const float* __restrict__ terms,
-			const uint32_t* __restrict__ task_max, const uint32_t* __restrict__ anchor_off, TaskOut* __restrict__ out)
+		// The metrics' canonical sum of n interleaved triples (area, volume, kappa terms): each
+		// lane adds its strided terms in order (the loads of 8 steps issued ahead), then an xor
+		// butterfly. Lists longer than kSumChunk are summed per chunk of kSumChunk from their
+		// start (chunk_sum_kernel, in parallel) and the chunk sums summed the same way.
+		constexpr uint32_t kSumChunk = 8192;
+		__device__ __forceinline__ void lane_sum3(const float* __restrict__ terms, uint32_t cnt, int lane, float& sa, float& sv, float& sk)
 		{
-			const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-			const int lane = threadIdx.x & 31;
-			if (t >= ntasks)
-				return;
-			const uint32_t b = best[t];
-			const uint32_t cnt = b != kInf ? comp_size[b] : 0u;
-			const uint32_t p0 = sel_begin[t];
-			float sa = 0.0f, sv = 0.0f, sk = 0.0f;
-			// each lane adds its strided terms in order; the loads of 8 steps are issued ahead
+			sa = sv = sk = 0.0f;
 			uint32_t i = lane;
 			for (; i + 7u * 32u < cnt; i += 8u * 32u)
 			{
@@ -2098,7 +2093,7 @@ namespace u26
 #pragma unroll
 				for (int u = 0; u < 8; u++)
 				{
-					const float* tt = terms + 3 * size_t(p0 + i + 32u * u);
+					const float* tt = terms + 3 * size_t(i + 32u * u);
 					ta[u] = tt[0];
 					tv[u] = tt[1];
 					tk8[u] = tt[2];
@@ -2113,7 +2108,7 @@ namespace u26
 			}
 			for (; i < cnt; i += 32)
 			{
-				const float* tt = terms + 3 * size_t(p0 + i);
+				const float* tt = terms + 3 * size_t(i);
 				sa = sa + tt[0];
 				sv = sv + tt[1];
 				sk = sk + tt[2];
@@ -2124,6 +2119,76 @@ namespace u26
 				sv = sv + __shfl_xor_sync(0xFFFFFFFFu, sv, off);
 				sk = sk + __shfl_xor_sync(0xFFFFFFFFu, sk, off);
 			}
+		}
+
+		// chunks of the supports longer than kSumChunk: nchunk[t], then (after an exclusive
+		// scan) one warp per chunk
+		__global__ void chunk_count_kernel(uint32_t ntasks, const uint32_t* __restrict__ best, const uint32_t* __restrict__ comp_size,
+			uint32_t* __restrict__ nchunk)
+		{
+			const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+			if (t > ntasks)
+				return;
+			uint32_t c = 0;
+			if (t < ntasks)
+			{
+				const uint32_t b = best[t];
+				const uint32_t cnt = b != kInf ? comp_size[b] : 0u;
+				c = cnt > kSumChunk ? (cnt + kSumChunk - 1) / kSumChunk : 0u;
+			}
+			nchunk[t] = c;
+		}
+		__global__ void chunk_sum_kernel(uint32_t ntasks, uint32_t nchunks, const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ best,
+			const uint32_t* __restrict__ comp_size, const uint32_t* __restrict__ sel_begin, const float* __restrict__ terms,
+			float* __restrict__ csum)
+		{
+			const uint32_t g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const int lane = threadIdx.x & 31;
+			if (g >= nchunks)
+				return;
+			uint32_t lo = 0, hi = ntasks;
+			while (hi - lo > 1)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (chunk_off[mid] <= g)
+					lo = mid;
+				else
+					hi = mid;
+			}
+			// lo: the last task whose chunks begin at or before g (tasks without chunks share offsets)
+			const uint32_t t = lo;
+			const uint32_t cnt = comp_size[best[t]];
+			const uint32_t j = g - chunk_off[t];
+			const uint32_t b0 = j * kSumChunk;
+			float sa, sv, sk;
+			lane_sum3(terms + 3 * size_t(sel_begin[t] + b0), min(kSumChunk, cnt - b0), lane, sa, sv, sk);
+			if (lane == 0)
+			{
+				csum[3 * size_t(g)] = sa;
+				csum[3 * size_t(g) + 1] = sv;
+				csum[3 * size_t(g) + 2] = sk;
+			}
+		}
+
+		// one warp per task: the canonical sums of its selected terms and the task's outputs
+		__global__ void task_sum_kernel(uint32_t ntasks, const Task* __restrict__ tasks, const uint32_t* __restrict__ seg,
+			const uint32_t* __restrict__ best, const uint32_t* __restrict__ bestcov, const uint32_t* __restrict__ comp_size,
+			const uint32_t* __restrict__ ncand, const uint32_t* __restrict__ sel_begin, const float* __restrict__ terms,
+			const uint32_t* __restrict__ task_max, const uint32_t* __restrict__ anchor_off, const uint32_t* __restrict__ chunk_off,
+			const float* __restrict__ csum, TaskOut* __restrict__ out)
+		{
+			const uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const int lane = threadIdx.x & 31;
+			if (t >= ntasks)
+				return;
+			const uint32_t b = best[t];
+			const uint32_t cnt = b != kInf ? comp_size[b] : 0u;
+			const uint32_t p0 = sel_begin[t];
+			float sa, sv, sk;
+			if (cnt <= kSumChunk)
+				lane_sum3(terms + 3 * size_t(p0), cnt, lane, sa, sv, sk);
+			else
+				lane_sum3(csum + 3 * size_t(chunk_off[t]), chunk_off[t + 1] - chunk_off[t], lane, sa, sv, sk);
 			if (lane == 0)
 			{
 				const Task tk = tasks[t];
@@ -2357,6 +2422,65 @@ namespace u26
 			out[t] = o;
 		}
 
+		// The selected support of each listed task in canonical (key) order: one CTA per task
+		// compacts the hits of its best component out of the task's sorted segment.
+		__global__ void __launch_bounds__(256) capture_kernel(const uint32_t* __restrict__ list, const uint32_t* __restrict__ out_off,
+			const uint64_t* __restrict__ keys, const uint32_t* __restrict__ root, const uint32_t* __restrict__ best,
+			const uint32_t* __restrict__ seg, const float* __restrict__ pay, HitKeyCodec cd, const uint2* __restrict__ edges,
+			const uint32_t* __restrict__ faces, u26_prp_hit* __restrict__ out)
+		{
+			__shared__ uint32_t wsum[8];
+			__shared__ uint32_t base;
+			const uint32_t t = list[blockIdx.x];
+			const uint32_t b = best[t];
+			const uint32_t lo = seg[t], hi = seg[t + 1];
+			if (threadIdx.x == 0)
+				base = out_off[blockIdx.x];
+			__syncthreads();
+			const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+			for (uint32_t i0 = lo; i0 < hi; i0 += blockDim.x)
+			{
+				const uint32_t i = i0 + threadIdx.x;
+				const bool sel = i < hi && root[i] == b;
+				const uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
+				if (lane == 0)
+					wsum[warp] = __popc(m);
+				__syncthreads();
+				uint32_t off = base;
+				for (int w = 0; w < warp; w++)
+					off += wsum[w];
+				off += __popc(m & ((1u << lane) - 1u));
+				if (sel)
+				{
+					const uint64_t k = keys[i];
+					u26_prp_hit h;
+					h.type = cd.type(k);
+					h.src_id = cd.src(k);
+					h.dst_id = cd.dst(k);
+					uint32_t sv3[3], dv3[3];
+					hit_verts(h.type, h.src_id, h.dst_id, edges, faces, sv3, dv3);
+					for (int q = 0; q < 3; q++)
+					{
+						h.src_verts[q] = sv3[q];
+						h.dst_verts[q] = dv3[q];
+					}
+					h.bary[0] = pay[3 * i];
+					h.bary[1] = pay[3 * i + 1];
+					h.dist = pay[3 * i + 2];
+					out[off] = h;
+				}
+				__syncthreads();
+				if (threadIdx.x == 0)
+				{
+					uint32_t tot = 0;
+					for (int w = 0; w < 8; w++)
+						tot += wsum[w];
+					base += tot;
+				}
+				__syncthreads();
+			}
+		}
+
 		// selected-hit offset of each task: the scanned position of its first hit
 		__global__ void sel_begin_kernel(uint32_t ntasks, const uint32_t* __restrict__ seg, const uint32_t* __restrict__ bsum_scanned,
 			const uint64_t* __restrict__ keys, const uint32_t* __restrict__ root, const uint32_t* __restrict__ best, HitKeyCodec cd,
@@ -2547,7 +2671,7 @@ struct u26_scene
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
-	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals;
+	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp;
 	RadixSorter sorter, esorter, csorter;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
@@ -2726,7 +2850,8 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
 		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
 		&s->d_step_hits, &s->d_step_out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
-		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals };
+		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
+		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
@@ -2753,16 +2878,46 @@ namespace
 		std::vector<uint32_t> vflag_off, vflags;
 	};
 
+	// fn(i) for i in [0, n) over the host cores in static chunks; fn(i) writes only what i owns
+	template <typename F>
+	void host_parallel_for(uint32_t n, F&& fn)
+	{
+		const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+		const uint32_t nt = n < 8192 ? 1u : hw;
+		if (nt == 1)
+		{
+			for (uint32_t i = 0; i < n; i++)
+				fn(i);
+			return;
+		}
+		const uint32_t chunk = (n + nt - 1) / nt;
+		std::vector<std::thread> th;
+		for (uint32_t t = 0; t < nt; t++)
+			th.emplace_back([&, t]()
+				{
+					const uint32_t e = std::min(n, (t + 1) * chunk);
+					for (uint32_t i = t * chunk; i < e; i++)
+						fn(i); });
+		for (auto& h : th)
+			h.join();
+	}
+
 	void build_graph(const u26_scene& S, const std::vector<float>& x, HostGraph& G)
 	{
 		const uint32_t n = uint32_t(G.ef.size());
+		// the canonical EF list is sorted by edge: each edge's pairs form one run
+		std::vector<uint32_t> run(S.ne + 1, 0u);
+		for (uint32_t p = 0; p < n; p++)
+			run[G.ee[p] + 1]++;
+		for (uint32_t e = 0; e < S.ne; e++)
+			run[e + 1] += run[e];
 		auto edge_run = [&](uint32_t e, uint32_t& b, uint32_t& t)
 		{
-			b = uint32_t(std::lower_bound(G.ee.begin(), G.ee.begin() + n, e) - G.ee.begin());
-			t = uint32_t(std::upper_bound(G.ee.begin(), G.ee.begin() + n, e) - G.ee.begin());
+			b = run[e];
+			t = run[e + 1];
 		};
 		G.adj.assign(n, {});
-		for (uint32_t p = 0; p < n; p++)
+		host_parallel_for(n, [&](uint32_t p)
 		{
 			const uint32_t e = G.ee[p], f = G.ff[p];
 			auto& out = G.adj[p];
@@ -2787,14 +2942,14 @@ namespace
 							out.push_back(q);
 				}
 			}
-		}
+		});
 		// loop-vertex pairs
 		struct Loop
 		{
 			uint32_t v, p, e, f;
 		};
-		std::vector<Loop> loops;
-		for (uint32_t p = 0; p < n; p++)
+		std::vector<std::vector<Loop>> loops_of(n);
+		host_parallel_for(n, [&](uint32_t p)
 		{
 			const uint32_t e = G.ee[p], f = G.ff[p];
 			const uint32_t ex = S.edges[2 * e], ey = S.edges[2 * e + 1];
@@ -2814,9 +2969,12 @@ namespace
 					le = has(fa[0], av) ? fa[0] : fa[2];
 				else
 					le = has(fa[0], av) ? fa[0] : fa[1];
-				loops.push_back({ av, p, le, f });
+				loops_of[p].push_back({ av, p, le, f });
 			}
-		}
+		});
+		std::vector<Loop> loops;
+		for (const auto& lv : loops_of)
+			loops.insert(loops.end(), lv.begin(), lv.end());
 		for (const Loop& l : loops)
 		{
 			EfPairH lp{};
@@ -2837,15 +2995,14 @@ namespace
 		{ return mkv(x[3 * v], x[3 * v + 1], x[3 * v + 2]); };
 		G.pos3.resize(na);
 		G.len.resize(na);
-		for (uint32_t p = 0; p < na; p++)
-			G.pos3[p] = X(G.ef[p].idx[0]) * G.ef[p].bary[0] + X(G.ef[p].idx[1]) * (1.0f - G.ef[p].bary[0]);
-		for (uint32_t p = 0; p < na; p++)
-		{
-			float s = 0.0f;
-			for (uint32_t q : G.adj[p])
-				s += hlen(G.pos3[q] - G.pos3[p]);
-			G.len[p] = 0.5f * s;
-		}
+		host_parallel_for(na, [&](uint32_t p)
+			{ G.pos3[p] = X(G.ef[p].idx[0]) * G.ef[p].bary[0] + X(G.ef[p].idx[1]) * (1.0f - G.ef[p].bary[0]); });
+		host_parallel_for(na, [&](uint32_t p)
+			{
+				float s = 0.0f;
+				for (uint32_t q : G.adj[p])
+					s += hlen(G.pos3[q] - G.pos3[p]);
+				G.len[p] = 0.5f * s; });
 		// flood fill with mesh-side parity
 		G.mesh_index.assign(na, kInfH);
 		std::vector<uint8_t> seen(na, 0);
@@ -3582,9 +3739,24 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		else
 			U26_CUDA(ctx, cudaMemsetAsync(S->d_selbegin.ptr, 0, sizeof(uint32_t) * (nt + 1), st));
 		U26_CUDA(ctx, S->d_out.reserve(sizeof(TaskOut) * nt));
+		// chunk sums of the supports longer than kSumChunk
+		U26_CUDA(ctx, S->d_chunk_off.reserve(sizeof(uint32_t) * (nt + 1)));
+		chunk_count_kernel<<<div_up(nt + 1, 256), 256, 0, st>>>(nt, d_best, S->d_csize.as<uint32_t>(), S->d_chunk_off.as<uint32_t>());
+		U26_TRY(after_launch(ctx, "chunk_count_kernel"));
+		U26_TRY(device_exclusive_scan(ctx, S->d_chunk_off.as<uint32_t>(), nt + 1, S->scan_tmp));
+		U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_chunk_off.as<uint32_t>() + nt, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+		U26_CUDA(ctx, cudaStreamSynchronize(st));
+		const uint32_t nchunks = *ctx->host_word;
+		U26_CUDA(ctx, S->d_csum.reserve(sizeof(float) * 3 * size_t(std::max(nchunks, 1u))));
+		if (nchunks)
+		{
+			chunk_sum_kernel<<<div_up(32 * nchunks, 256), 256, 0, st>>>(nt, nchunks, S->d_chunk_off.as<uint32_t>(), d_best,
+				S->d_csize.as<uint32_t>(), S->d_selbegin.as<uint32_t>(), S->d_terms.as<float>(), S->d_csum.as<float>());
+			U26_TRY(after_launch(ctx, "chunk_sum_kernel"));
+		}
 		task_sum_kernel<<<div_up(32 * nt, 256), 256, 0, st>>>(nt, S->d_tasks.as<Task>(), S->d_seg.as<uint32_t>(), d_best, d_bestcov,
 			S->d_csize.as<uint32_t>(), d_ncand, S->d_selbegin.as<uint32_t>(), S->d_terms.as<float>(), S->d_task_max.as<uint32_t>(),
-			S->d_anchor_off.as<uint32_t>(), S->d_out.as<TaskOut>());
+			S->d_anchor_off.as<uint32_t>(), S->d_chunk_off.as<uint32_t>(), S->d_csum.as<float>(), S->d_out.as<TaskOut>());
 		U26_TRY(after_launch(ctx, "task_sum_kernel"));
 		ev.mark(5, st);
 		U26_TRY(download(ctx, tout, S->d_out.ptr, nt));
@@ -3602,6 +3774,19 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		return U26_OK;
 	};
 
+	// prp_select_response over a contour's results
+	auto select_best = [&](const ContourRT& r) -> int
+	{
+		int sel = -1;
+		for (size_t d = 0; d < r.res.size(); d++)
+		{
+			if (!valid_resp(r.res[d]))
+				continue;
+			if (sel < 0 || better_resp(r.res[d], uint32_t(d), r.res[sel], uint32_t(sel)))
+				sel = int(d);
+		}
+		return sel;
+	};
 	// evaluate_current_runtime_directions_template for the listed contours: k from the
 	// initial level, the active directions reset, levels until every active direction has
 	// converged or been pruned
@@ -3695,6 +3880,49 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				r.conv[tk.combo] = (cs.eligible || cs.full_mesh) ? 1 : 0;
 				r.present[tk.combo] = 1;
 				r.res[tk.combo] = std::move(cs);
+			}
+			// the support of each contour's current best response, when this level produced it,
+			// is gathered now while the level's hits are on the device, so that the final
+			// winner needs no re-evaluation (materialize covers whatever is not captured)
+			{
+				constexpr uint64_t kCaptureCap = uint64_t(1) << 24;
+				std::vector<int> task_of(size_t(nact) * 26, -1);
+				for (size_t t = 0; t < tasks.size(); t++)
+					if (tasks[t].combo < 26)
+						task_of[size_t(tasks[t].contour_local) * 26 + tasks[t].combo] = int(t);
+				std::vector<uint32_t> list, off(1, 0u);
+				uint64_t total = 0;
+				for (uint32_t c : remaining)
+				{
+					const int sel = select_best(R[c]);
+					if (sel < 0 || sel >= 26)
+						continue;
+					const int t = task_of[size_t(c) * 26 + sel];
+					const ComboState& cs = R[c].res[sel];
+					if (t < 0 || cs.hits.size() == cs.hit_count || total + cs.hit_count > kCaptureCap)
+						continue;
+					list.push_back(uint32_t(t));
+					total += cs.hit_count;
+					off.push_back(uint32_t(total));
+				}
+				if (!list.empty() && total > 0)
+				{
+					U26_TRY(upload(ctx, S->d_cap_list, list));
+					U26_TRY(upload(ctx, S->d_cap_off, off));
+					U26_CUDA(ctx, S->d_capture.reserve(sizeof(u26_prp_hit) * total));
+					capture_kernel<<<uint32_t(list.size()), 256, 0, st>>>(S->d_cap_list.as<uint32_t>(), S->d_cap_off.as<uint32_t>(),
+						S->d_keys.as<uint64_t>(), S->d_root.as<uint32_t>(), S->d_best.as<uint32_t>(), S->d_seg.as<uint32_t>(), S->d_pay.as<float>(),
+						HitKeyCodec{ b }, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_capture.as<u26_prp_hit>());
+					U26_TRY(after_launch(ctx, "capture_kernel"));
+					std::vector<u26_prp_hit> got;
+					U26_TRY(download(ctx, got, S->d_capture.ptr, total));
+					U26_CUDA(ctx, cudaStreamSynchronize(st));
+					for (size_t q = 0; q < list.size(); q++)
+					{
+						ComboState& cs = R[tasks[list[q]].contour_local].res[tasks[list[q]].combo];
+						cs.hits.assign(got.begin() + off[q], got.begin() + off[q + 1]);
+					}
+				}
 			}
 			std::vector<uint32_t> next;
 			for (uint32_t c : remaining)
@@ -3796,26 +4024,13 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->stage_ms[6] += ms_since(tl);
 		return U26_OK;
 	};
-	// prp_select_response over a contour's results
-	auto select_best = [&](const ContourRT& r) -> int
-	{
-		int sel = -1;
-		for (size_t d = 0; d < r.res.size(); d++)
-		{
-			if (!valid_resp(r.res[d]))
-				continue;
-			if (sel < 0 || better_resp(r.res[d], uint32_t(d), r.res[sel], uint32_t(sel)))
-				sel = int(d);
-		}
-		return sel;
-	};
 	std::vector<int> chosen_idx(nc, -1);
 	{
 		std::vector<std::pair<uint32_t, uint32_t>> cc;
 		for (uint32_t c = 0; c < nact; c++)
 		{
 			chosen_idx[c] = select_best(R[c]);
-			if (chosen_idx[c] >= 0)
+			if (chosen_idx[c] >= 0 && R[c].res[chosen_idx[c]].hits.size() != R[c].res[chosen_idx[c]].hit_count)
 				cc.emplace_back(c, uint32_t(chosen_idx[c]));
 		}
 		U26_TRY(materialize(cc));
@@ -3920,7 +4135,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 					const float actual = resp_obj(acc[c]) - resp_obj(trial);
 					if (pred[c] > 1e-20f && actual / pred[c] > 0.75f)
 						o.trust = std::fmin(1.0f, o.trust * 2.0f);
-					taken.emplace_back(c, d);
+					if (trial.hits.size() != trial.hit_count)
+						taken.emplace_back(c, d);
 				}
 				else
 				{
@@ -3962,8 +4178,16 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			chosen[c] = r.res[sel];
 		pre_area[c] = chosen[c].area;
 		std::set<uint32_t> adjc;
+		auto flagged = [&](uint32_t v)
+		{ return v == kInfH || G.vflag_off[v + 1] > G.vflag_off[v]; };
 		for (const u26_prp_hit& h : chosen[c].hits)
 		{
+			// a hit links contours only through vertices that all carry boundary flags
+			bool any_empty = false;
+			for (int k = 0; k < 3; k++)
+				any_empty = any_empty || !flagged(h.src_verts[k]) || !flagged(h.dst_verts[k]);
+			if (any_empty)
+				continue;
 			std::vector<uint32_t> sv, dv;
 			for (int k = 0; k < 3; k++)
 			{
