@@ -68,13 +68,22 @@ namespace u26
 		const f3 AC = C - A;
 		const f3 N = cross(AB, AC);
 		const f3 neg = -dir;
-		const float nlen = length(N);
 		const float den = dot(neg, N);
+		const f3 to_a = start - A;
+		const float tnum = dot(to_a, N);
+		// misses decided before the square root and the division, only where the exact test
+		// below must also reject: t = tnum / den surely negative (opposite signs, magnitudes far
+		// from underflow), or surely beyond ray_len (1e-5 relative margin)
+		const float aden = fabsf(den), anum = fabsf(tnum);
+		if (aden >= 1e-30f && aden <= 1e20f && anum >= 1e-20f && ((tnum > 0.0f) != (den > 0.0f)))
+			return false;
+		if (aden >= 1e-30f && anum > aden * ray_len * (1.0f + 1e-5f) && ((tnum > 0.0f) == (den > 0.0f)))
+			return false;
+		const float nlen = length(N);
 		if (fabsf(den) < nlen * 1e-6f)
 			return false;
 		const float inv_den = 1.0f / den;
-		const f3 to_a = start - A;
-		const float t = dot(to_a, N) * inv_den;
+		const float t = tnum * inv_den;
 		if (t < 0.0f || t > ray_len)
 			return false;
 		const f3 cx = cross(neg, to_a);
@@ -1520,7 +1529,22 @@ namespace u26
 			return kInf;
 		}
 
-		// find_adjacent_hits rules as exact key lookups inside the task segment
+		__device__ __forceinline__ uint32_t lower_bound_key(const uint64_t* keys, uint32_t lo, uint32_t hi, uint64_t key)
+		{
+			while (lo < hi)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (keys[mid] < key)
+					lo = mid + 1;
+				else
+					hi = mid;
+			}
+			return lo;
+		}
+
+		// find_adjacent_hits rules as exact key lookups inside the task segment. Lookups that
+		// share a (type, source) first find that source's run of hits once, then search the
+		// targets inside the (short) run.
 		__global__ void union_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, const uint32_t* __restrict__ seg,
 			const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const uint32_t* __restrict__ fae,
 			const uint32_t* __restrict__ vav_off, const uint32_t* __restrict__ vav, const uint32_t* __restrict__ vae_off,
@@ -1534,52 +1558,93 @@ namespace u26
 			const uint64_t k = keys[i];
 			const uint32_t t = cd.task(k), ty = cd.type(k), s = cd.src(k), d = cd.dst(k);
 			const uint32_t lo = seg[t], hi = seg[t + 1];
+			// [rb, re): the hits of (t, ty2, src2); the end is found by galloping from rb
+			auto run = [&](uint32_t ty2, uint32_t src2, uint32_t& rb, uint32_t& re)
+			{
+				const uint64_t k0 = cd.make(t, ty2, src2, 0u);
+				const uint64_t k1 = k0 + (uint64_t(1) << cd.b);
+				rb = lower_bound_key(keys, lo, hi, k0);
+				uint32_t a = rb, step = 1;
+				while (a + step <= hi && keys[a + step - 1] < k1)
+				{
+					a += step;
+					step <<= 1;
+				}
+				re = lower_bound_key(keys, a, min(hi, a + step), k1);
+			};
+			auto link_in = [&](uint32_t rb, uint32_t re, uint32_t nty, uint32_t ns, uint32_t nd)
+			{
+				if (rb >= re)
+					return;
+				const uint32_t j = find_key(keys, rb, re, cd.make(t, nty, ns, nd));
+				if (j != kInf && j != i)
+					uf_union(parent, i, j, dev_err);
+			};
 			auto link = [&](uint32_t nty, uint32_t ns, uint32_t nd)
 			{
 				const uint32_t j = find_key(keys, lo, hi, cd.make(t, nty, ns, nd));
 				if (j != kInf && j != i)
 					uf_union(parent, i, j, dev_err);
 			};
+			uint32_t rb, re;
 			if (ty == 0u)
 			{
 				// VF(v, f)
 				for (uint32_t q = vav_off[s]; q < vav_off[s + 1]; q++)
 					link(0u, vav[q], d);
 				for (uint32_t q = vaf_off[s]; q < vaf_off[s + 1]; q++)
+				{
+					run(2u, vaf[q], rb, re);
 					for (int c = 0; c < 3; c++)
-						link(2u, vaf[q], faces[3 * d + c]);
+						link_in(rb, re, 2u, vaf[q], faces[3 * d + c]);
+				}
 				for (uint32_t q = vae_off[s]; q < vae_off[s + 1]; q++)
+				{
+					run(1u, vae[q], rb, re);
 					for (int c = 0; c < 3; c++)
-						link(1u, vae[q], fae[3 * d + c]);
+						link_in(rb, re, 1u, vae[q], fae[3 * d + c]);
+				}
 			}
 			else if (ty == 2u)
 			{
 				// FV(f, w)
 				for (int c = 0; c < 3; c++)
+				{
+					run(0u, faces[3 * s + c], rb, re);
 					for (uint32_t q = vaf_off[d]; q < vaf_off[d + 1]; q++)
-						link(0u, faces[3 * s + c], vaf[q]);
+						link_in(rb, re, 0u, faces[3 * s + c], vaf[q]);
+				}
+				run(2u, s, rb, re);
 				for (uint32_t q = vav_off[d]; q < vav_off[d + 1]; q++)
-					link(2u, s, vav[q]);
+					link_in(rb, re, 2u, s, vav[q]);
 				for (int c = 0; c < 3; c++)
+				{
+					run(1u, fae[3 * s + c], rb, re);
 					for (uint32_t q = vae_off[d]; q < vae_off[d + 1]; q++)
-						link(1u, fae[3 * s + c], vae[q]);
+						link_in(rb, re, 1u, fae[3 * s + c], vae[q]);
+				}
 			}
 			else
 			{
 				// EE(e1, e2)
 				const uint2 a = edges[s], b = edges[d];
+				uint32_t rb2, re2;
+				run(0u, a.x, rb, re);
+				run(0u, a.y, rb2, re2);
 				for (uint32_t q = eaf_off[d]; q < eaf_off[d + 1]; q++)
 				{
-					link(0u, a.x, eaf[q]);
-					link(0u, a.y, eaf[q]);
+					link_in(rb, re, 0u, a.x, eaf[q]);
+					link_in(rb2, re2, 0u, a.y, eaf[q]);
 				}
 				for (uint32_t q = eaf_off[s]; q < eaf_off[s + 1]; q++)
 				{
-					link(2u, eaf[q], b.x);
-					link(2u, eaf[q], b.y);
+					run(2u, eaf[q], rb, re);
+					link_in(rb, re, 2u, eaf[q], b.x);
+					link_in(rb, re, 2u, eaf[q], b.y);
 				}
+				run(1u, s, rb, re);
 				for (uint32_t q = eae_off[d]; q < eae_off[d + 1]; q++)
-					link(1u, s, eae[q]);
+					link_in(rb, re, 1u, s, eae[q]);
 				for (uint32_t q = eae_off[s]; q < eae_off[s + 1]; q++)
 					link(1u, eae[q], d);
 			}
