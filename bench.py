@@ -323,7 +323,7 @@ def main():
     peak, peak_kind = _peaks()
     rc_bytes = 44 * r0.ray_visits + 48 * (r0.tested - r0.edge_tests) + 32 * r0.edge_tests + 24 * r0.requests
     rc_ms = r0.gpu_ms["raycast"]
-    roof = {"bound": "hbm", "achieved": rc_bytes / (rc_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+    roof = {"bound": "hbm", "achieved": rc_bytes / (rc_ms / 1e3) / 1e9 if rc_ms > 0 else 0.0, "peak": peak, "unit": "GB/s",
             "peak_source": peak_kind, "kernel": "raycast_kernel", "kernel_ms_per_pass": rc_ms,
             "launches_per_pass": r0.levels + 1, "algorithmic_bytes_per_pass": rc_bytes, "traffic": None,
             "ray_node_visits": r0.ray_visits, "packet_node_tests": r0.nodes_visited, "packet_node_fetches": r0.node_fetches,

@@ -204,6 +204,8 @@ typedef struct u26_mesh_desc
 	const uint32_t* object_scene;	  /* [objects] independent scene of each object, or NULL (one scene): several
 									   * simulations evaluated in one batch keep their own global centroid
 									   * (the radial seed direction of get_raycasting_direction) */
+	const uint32_t* object_solid;	  /* [objects] 1 for rigid / tetrahedral material (sa_vert_mesh_type), or NULL:
+									   * no solid objects (the solid-interior hit links never apply) */
 } u26_mesh_desc;
 
 typedef struct u26_scene u26_scene;
@@ -227,7 +229,10 @@ typedef struct u26_prp_params
 	uint32_t form;				/* ray casting form: 0 batched packet traversal clipped to the candidate boxes (default),
 								 * 1 the plain form (one thread per request from the root, one launch per contour);
 								 * both decide the same pairs and return the same results */
-	uint32_t reserved;
+	uint32_t solid_interior;	/* PRP_solid_interior_adjacency (1): link hits through solid interiors */
+	uint32_t solid_all;			/* PRP_solid_interior_adjacency_all_meshes (0): treat every mesh as solid */
+	float solid_eps_n;			/* PRP_solid_interior_adjacency_normal_eps (1e-4) */
+	float solid_eps_d;			/* PRP_solid_interior_adjacency_dist_eps (1e-5) */
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:

@@ -211,13 +211,17 @@ class PrpParams(ctypes.Structure):
         ("opt_iterations", ctypes.c_uint32),    # PRP_direction_optimization_iterations
         ("ccr_blend", ctypes.c_uint32),         # PRP_use_blended_intrinsic_coordinates
         ("ccr_blend_weight", ctypes.c_float),   # PRP_intrinsic_blend_weight
+        ("solid_interior", ctypes.c_uint32),    # PRP_solid_interior_adjacency
+        ("solid_all", ctypes.c_uint32),         # PRP_solid_interior_adjacency_all_meshes
+        ("solid_eps_n", ctypes.c_float),        # PRP_solid_interior_adjacency_normal_eps
+        ("solid_eps_d", ctypes.c_float),        # PRP_solid_interior_adjacency_dist_eps
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, brute_force_raycast=0, contour_stride=0, opt_iterations=0, ccr_blend=0,
-                  ccr_blend_weight=0.5)
+                  ccr_blend_weight=0.5, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -70,6 +70,7 @@ namespace
 		const float *rest_vert_area, *rest_edge_area, *rest_face_area, *vert_mass;
 		const uint* mesh_orientation;
 		const uint* object_scene; // [objects] or null: one scene
+		const uint* object_solid; // [objects] 1: rigid / tetrahedral material (sa_vert_mesh_type), or null: none
 	};
 
 	struct Params
@@ -86,6 +87,10 @@ namespace
 		uint opt_iterations; // PRP_direction_optimization_iterations (scene_params.h:65), 0 = off
 		uint ccr_blend;		 // PRP_use_blended_intrinsic_coordinates (scene_params.h:72)
 		float ccr_blend_weight; // PRP_intrinsic_blend_weight (scene_params.h:73)
+		uint solid_interior;	// PRP_solid_interior_adjacency (scene_params.h:77)
+		uint solid_all;			// PRP_solid_interior_adjacency_all_meshes (scene_params.h:78)
+		float solid_eps_n;		// PRP_solid_interior_adjacency_normal_eps (1e-4)
+		float solid_eps_d;		// PRP_solid_interior_adjacency_dist_eps (1e-5)
 	};
 
 	struct EfPair
@@ -1438,6 +1443,63 @@ namespace
 		}
 	}
 
+	// Solid-interior links (intersection_resolver2.cpp:3298-3464): hits that share a source
+	// vertex (VF), a target vertex (FV) or a source edge (EE), ordered by distance, link each
+	// hit to the next one when both targets belong to one solid (rigid / tetrahedral) mesh,
+	// the distance grows by more than eps_d and the ray enters the first target and leaves
+	// through the second (normal signs beyond eps_n). Equal distances are ordered by hit key.
+	void solid_links(const Scene& S, const std::vector<Hit>& H, V3 r, std::vector<std::vector<uint>>& out)
+	{
+		const MeshIn& m = S.m;
+		auto solid_v = [&](uint v)
+		{ return S.p.solid_all || (m.object_solid && m.object_solid[m.vert_object[v]]); };
+		std::map<std::pair<uint, uint>, std::vector<uint>> groups;
+		for (uint i = 0; i < H.size(); i++)
+		{
+			const Hit& h = H[i];
+			groups[{ h.type, h.type == FV ? h.dst_id : h.src_id }].push_back(i);
+		}
+		const float en = S.p.solid_eps_n, ed = S.p.solid_eps_d;
+		for (auto& [g, idx] : groups)
+		{
+			if (idx.size() < 2)
+				continue;
+			std::sort(idx.begin(), idx.end(), [&](uint a, uint b)
+				{
+					if (H[a].dist != H[b].dist) return H[a].dist < H[b].dist;
+					return H[a].key() < H[b].key(); });
+			for (size_t q = 0; q + 1 < idx.size(); q++)
+			{
+				const Hit &A = H[idx[q]], &B = H[idx[q + 1]];
+				bool link = false;
+				if (g.first == EE)
+				{
+					const uint va = edge_of(m, A.dst_id, 0), vb = edge_of(m, B.dst_id, 0);
+					if (m.vert_object[va] == m.vert_object[vb] && solid_v(va) && B.dist - A.dist > ed)
+					{
+						const float da = dot(S.en[A.dst_id], r), db = dot(S.en[B.dst_id], r);
+						link = da < -en && db > en;
+					}
+				}
+				else
+				{
+					const uint fa = A.fid(), fb = B.fid();
+					const uint va = face_of(m, fa, 0), vb = face_of(m, fb, 0);
+					if (m.vert_object[va] == m.vert_object[vb] && solid_v(va) && B.dist - A.dist > ed)
+					{
+						const float da = dot(S.fn[fa], r), db = dot(S.fn[fb], r);
+						link = g.first == VF ? (da < -en && db > en) : (da > en && db < -en);
+					}
+				}
+				if (link)
+				{
+					out[idx[q]].push_back(idx[q + 1]);
+					out[idx[q + 1]].push_back(idx[q]);
+				}
+			}
+		}
+	}
+
 	// Canonical 32-lane strided sum + xor butterfly (the CUDA metrics kernel's order).
 	template <typename F>
 	float lane_sum(uint n, F&& val)
@@ -1738,6 +1800,9 @@ namespace
 		// components
 		HitIndex ix;
 		ix.build(hits);
+		std::vector<std::vector<uint>> solid(hits.size());
+		if (S.p.solid_interior && (S.p.solid_all || m.object_solid))
+			solid_links(S, hits, dir, solid);
 		std::vector<uint8_t> vis(hits.size(), 0);
 		std::vector<uint> nb;
 		uint best_cov = 0, best_n = 0;
@@ -1759,6 +1824,7 @@ namespace
 				att = att || attached[i];
 				nb.clear();
 				hit_neighbours(m, hits, ix, i, nb);
+				nb.insert(nb.end(), solid[i].begin(), solid[i].end());
 				for (uint j : nb)
 					if (!vis[j])
 					{

@@ -65,3 +65,15 @@ def test_batched_scenes_oracle_parity(oracle, u26ctx):
     ef, idx = oracle.detect_ef(b)
     ref = oracle.PrpRun(b, ef, idx, oracle.prp_params(**ALL))
     _compare(res, ref)
+
+
+def test_solid_shells_oracle_parity(oracle, u26ctx):
+    """Closed shells declared solid (object_solid) in a batch with sheets."""
+    from test_prp_gpu import _compare
+    b = synthetic.batch_scenes(num=3, seed=13, tris_lo=2000, tris_hi=5000)
+    kinds = [s["kind"] for s in b.meta["scenes"]]
+    b.object_solid = np.array([1 if kinds[o // 2] == "shells" else 0 for o in range(b.num_objects)], np.uint32)
+    res = _pass(u26ctx, b, **ALL)
+    ef, idx = oracle.detect_ef(b)
+    ref = oracle.PrpRun(b, ef, idx, oracle.prp_params(**ALL))
+    _compare(res, ref)

@@ -125,3 +125,14 @@ def test_prp_plain_form_same_results(u26ctx, mesh_fn):
     sc.close()
     assert plain.device_error_flags == 0 and chosen.device_error_flags == 0
     _compare(plain, chosen)
+
+
+def test_prp_solid_interior_links(oracle, u26ctx):
+    """Solid-interior hit links (rigid / tetrahedral meshes): with every mesh treated as solid,
+    the rays through the folded sheet's two layers link entry and exit hits; the components,
+    supports and metrics change and still match the oracle bit for bit."""
+    m = synthetic.folded_sheet(48, seed=2)
+    res, ref = _run_both(oracle, u26ctx, m, solid_all=1, max_contours=64)
+    base = oracle.PrpRun(m, *oracle.detect_ef(m), oracle.prp_params(max_contours=64))
+    assert any(a["hit_count"] != b["hit_count"] for a, b in zip(ref.results, base.results))
+    _compare(res, ref)

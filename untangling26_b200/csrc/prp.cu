@@ -1529,17 +1529,82 @@ namespace u26
 			return kInf;
 		}
 
-		__device__ __forceinline__ uint32_t lower_bound_key(const uint64_t* keys, uint32_t lo, uint32_t hi, uint64_t key)
+		// ---- run directory: every (task, type, source) run of the sorted hits, in an
+		// open-addressing hash table keyed by that prefix (value: run id; run r spans
+		// [heads[r], heads[r + 1]))
+		struct RunDir
 		{
-			while (lo < hi)
+			const uint64_t* hkeys; // prefix + 1 (0: empty slot)
+			const uint32_t* hvals;
+			const uint32_t* heads;
+			uint32_t mask;
+		};
+		__device__ __forceinline__ uint32_t run_hash(uint64_t p)
+		{
+			p ^= p >> 33;
+			p *= 0xff51afd7ed558ccdull;
+			p ^= p >> 33;
+			p *= 0xc4ceb9fe1a85ec53ull;
+			p ^= p >> 33;
+			return uint32_t(p);
+		}
+		__global__ void run_flags_kernel(const uint64_t* __restrict__ keys, uint32_t n, int b, uint32_t* __restrict__ flag)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i > n)
+				return;
+			flag[i] = (i < n && (i == 0 || (keys[i] >> b) != (keys[i - 1] >> b))) ? 1u : 0u;
+		}
+		// flag[] scanned in place: flag[i] = run id of a head i; flag[n] = number of runs
+		__global__ void run_insert_kernel(const uint64_t* __restrict__ keys, uint32_t n, int b, const uint32_t* __restrict__ scanned,
+			uint32_t* __restrict__ heads, uint64_t* __restrict__ hkeys, uint32_t* __restrict__ hvals, uint32_t mask, uint32_t* __restrict__ dev_err)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i > n)
+				return;
+			if (i == n)
 			{
-				const uint32_t mid = (lo + hi) >> 1;
-				if (keys[mid] < key)
-					lo = mid + 1;
-				else
-					hi = mid;
+				heads[scanned[n]] = n;
+				return;
 			}
-			return lo;
+			if (!(i == 0 || (keys[i] >> b) != (keys[i - 1] >> b)))
+				return;
+			const uint32_t r = scanned[i];
+			heads[r] = i;
+			const uint64_t k = (keys[i] >> b) + 1u;
+			uint32_t h = run_hash(k) & mask;
+			for (uint32_t it = 0; it <= mask; it++)
+			{
+				const unsigned long long old = atomicCAS(reinterpret_cast<unsigned long long*>(hkeys + h), 0ull, (unsigned long long)k);
+				if (old == 0ull)
+				{
+					hvals[h] = r;
+					return;
+				}
+				h = (h + 1u) & mask;
+			}
+			atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
+		}
+		// [rb, re) of the run with this prefix (empty when absent)
+		__device__ __forceinline__ void run_lookup(const RunDir& d, uint64_t prefix, uint32_t& rb, uint32_t& re)
+		{
+			const uint64_t k = prefix + 1u;
+			uint32_t h = run_hash(k) & d.mask;
+			rb = re = 0;
+			for (uint32_t it = 0; it <= d.mask; it++)
+			{
+				const uint64_t v = d.hkeys[h];
+				if (v == k)
+				{
+					const uint32_t r = d.hvals[h];
+					rb = d.heads[r];
+					re = d.heads[r + 1];
+					return;
+				}
+				if (v == 0ull)
+					return;
+				h = (h + 1u) & d.mask;
+			}
 		}
 
 		// find_adjacent_hits rules as exact key lookups inside the task segment. Lookups that
@@ -1550,28 +1615,16 @@ namespace u26
 			const uint32_t* __restrict__ vav_off, const uint32_t* __restrict__ vav, const uint32_t* __restrict__ vae_off,
 			const uint32_t* __restrict__ vae, const uint32_t* __restrict__ vaf_off, const uint32_t* __restrict__ vaf,
 			const uint32_t* __restrict__ eaf_off, const uint32_t* __restrict__ eaf, const uint32_t* __restrict__ eae_off,
-			const uint32_t* __restrict__ eae, uint32_t* __restrict__ parent, uint32_t* __restrict__ dev_err)
+			const uint32_t* __restrict__ eae, RunDir dir, uint32_t* __restrict__ parent, uint32_t* __restrict__ dev_err)
 		{
 			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 			if (i >= n)
 				return;
 			const uint64_t k = keys[i];
 			const uint32_t t = cd.task(k), ty = cd.type(k), s = cd.src(k), d = cd.dst(k);
-			const uint32_t lo = seg[t], hi = seg[t + 1];
-			// [rb, re): the hits of (t, ty2, src2); the end is found by galloping from rb
+			// [rb, re): the hits of (t, ty2, src2), from the run directory
 			auto run = [&](uint32_t ty2, uint32_t src2, uint32_t& rb, uint32_t& re)
-			{
-				const uint64_t k0 = cd.make(t, ty2, src2, 0u);
-				const uint64_t k1 = k0 + (uint64_t(1) << cd.b);
-				rb = lower_bound_key(keys, lo, hi, k0);
-				uint32_t a = rb, step = 1;
-				while (a + step <= hi && keys[a + step - 1] < k1)
-				{
-					a += step;
-					step <<= 1;
-				}
-				re = lower_bound_key(keys, a, min(hi, a + step), k1);
-			};
+			{ run_lookup(dir, cd.make(t, ty2, src2, 0u) >> cd.b, rb, re); };
 			auto link_in = [&](uint32_t rb, uint32_t re, uint32_t nty, uint32_t ns, uint32_t nd)
 			{
 				if (rb >= re)
@@ -1582,9 +1635,9 @@ namespace u26
 			};
 			auto link = [&](uint32_t nty, uint32_t ns, uint32_t nd)
 			{
-				const uint32_t j = find_key(keys, lo, hi, cd.make(t, nty, ns, nd));
-				if (j != kInf && j != i)
-					uf_union(parent, i, j, dev_err);
+				uint32_t rb2, re2;
+				run(nty, ns, rb2, re2);
+				link_in(rb2, re2, nty, ns, nd);
 			};
 			uint32_t rb, re;
 			if (ty == 0u)
@@ -1648,6 +1701,133 @@ namespace u26
 				for (uint32_t q = eae_off[s]; q < eae_off[s + 1]; q++)
 					link(1u, eae[q], d);
 			}
+		}
+
+		// ---- solid-interior links (intersection_resolver2.cpp:3298-3464): hits sharing a
+		// source vertex (VF), target vertex (FV) or source edge (EE), ordered by (distance,
+		// key), link each hit to its successor when both targets lie on one solid mesh, the
+		// distance grows by more than eps_d and the ray enters the first target and leaves
+		// through the second. Each thread finds its hit's successor in its group.
+		struct SolidParams
+		{
+			const float* fn;
+			const float* en;
+			const uint32_t* vobj;
+			const uint8_t* vsolid;
+			uint32_t all;
+			float eps_n, eps_d;
+		};
+		__device__ __forceinline__ bool solid_link_ok(const SolidParams& sp, uint32_t ty, uint32_t ta, uint32_t tb, float da_, float db_, f3 r,
+			const uint2* __restrict__ edges, const uint32_t* __restrict__ faces)
+		{
+			// ta / tb: the targets (faces for VF / FV, second edges for EE) of the hit and its successor
+			const uint32_t va = ty == 1u ? edges[ta].x : faces[3 * ta], vb = ty == 1u ? edges[tb].x : faces[3 * tb];
+			if (sp.vobj[va] != sp.vobj[vb] || !(sp.all || sp.vsolid[va]) || !(db_ - da_ > sp.eps_d))
+				return false;
+			const float* nrm = ty == 1u ? sp.en : sp.fn;
+			const float a = dot(mk3(nrm[3 * ta], nrm[3 * ta + 1], nrm[3 * ta + 2]), r);
+			const float b = dot(mk3(nrm[3 * tb], nrm[3 * tb + 1], nrm[3 * tb + 2]), r);
+			if (ty == 2u)
+				return a > sp.eps_n && b < -sp.eps_n;
+			return a < -sp.eps_n && b > sp.eps_n;
+		}
+
+		// VF and EE groups are runs of the sorted hits (same task, type, source)
+		__global__ void solid_runs_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, const uint32_t* __restrict__ seg,
+			const float* __restrict__ pay, const Task* __restrict__ tasks, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces,
+			SolidParams sp, uint32_t* __restrict__ parent, uint32_t* __restrict__ dev_err)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			const uint64_t k = keys[i];
+			const uint32_t ty = cd.type(k);
+			if (ty == 2u)
+				return;
+			const uint32_t t = cd.task(k), s = cd.src(k);
+			const uint32_t lo = seg[t], hi = seg[t + 1];
+			const uint64_t k0 = cd.make(t, ty, s, 0u), k1 = k0 + (uint64_t(1) << cd.b);
+			// the run around i
+			uint32_t rb = i, re = i + 1;
+			for (int it = 0; it < (1 << 22) && rb > lo && keys[rb - 1] >= k0; it++)
+				rb--;
+			for (int it = 0; it < (1 << 22) && re < hi && keys[re] < k1; it++)
+				re++;
+			const float di = pay[3 * i + 2];
+			uint32_t nxt = kInf;
+			float dn = 0.0f;
+			for (uint32_t j = rb; j < re; j++)
+			{
+				if (j == i)
+					continue;
+				const float dj = pay[3 * j + 2];
+				const bool after = dj > di || (dj == di && j > i);
+				if (after && (nxt == kInf || dj < dn || (dj == dn && j < nxt)))
+				{
+					nxt = j;
+					dn = dj;
+				}
+			}
+			if (nxt == kInf)
+				return;
+			const Task tk = tasks[t];
+			if (solid_link_ok(sp, ty, cd.dst(k), cd.dst(keys[nxt]), di, dn, mk3(tk.dir[0], tk.dir[1], tk.dir[2]), edges, faces))
+				uf_union(parent, i, nxt, dev_err);
+		}
+
+		// FV groups share a target vertex: the FV hits re-keyed by (task, target vertex)
+		__global__ void solid_fv_keys_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, uint64_t* __restrict__ k2,
+			uint32_t* __restrict__ v2, uint32_t* __restrict__ count)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			const uint64_t k = keys[i];
+			if (cd.type(k) != 2u)
+				return;
+			cg::coalesced_group g = cg::coalesced_threads();
+			uint32_t base = 0;
+			if (g.thread_rank() == 0)
+				base = atomicAdd(count, g.size());
+			const uint32_t slot = g.shfl(base, 0) + g.thread_rank();
+			k2[slot] = (uint64_t(cd.task(k)) << cd.b) | cd.dst(k);
+			v2[slot] = i;
+		}
+		__global__ void solid_fv_kernel(const uint64_t* __restrict__ k2, const uint32_t* __restrict__ v2, uint32_t m, const uint64_t* __restrict__ keys,
+			HitKeyCodec cd, const float* __restrict__ pay, const Task* __restrict__ tasks, const uint2* __restrict__ edges,
+			const uint32_t* __restrict__ faces, SolidParams sp, uint32_t* __restrict__ parent, uint32_t* __restrict__ dev_err)
+		{
+			const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+			if (q >= m)
+				return;
+			const uint64_t g = k2[q];
+			uint32_t rb = q, re = q + 1;
+			for (int it = 0; it < (1 << 22) && rb > 0 && k2[rb - 1] == g; it++)
+				rb--;
+			for (int it = 0; it < (1 << 22) && re < m && k2[re] == g; it++)
+				re++;
+			const uint32_t i = v2[q];
+			const float di = pay[3 * i + 2];
+			uint32_t nxt = kInf;
+			float dn = 0.0f;
+			for (uint32_t p = rb; p < re; p++)
+			{
+				const uint32_t j = v2[p];
+				if (j == i)
+					continue;
+				const float dj = pay[3 * j + 2];
+				const bool after = dj > di || (dj == di && j > i);
+				if (after && (nxt == kInf || dj < dn || (dj == dn && j < nxt)))
+				{
+					nxt = j;
+					dn = dj;
+				}
+			}
+			if (nxt == kInf)
+				return;
+			const Task tk = tasks[cd.task(keys[i])];
+			if (solid_link_ok(sp, 2u, cd.src(keys[i]), cd.src(keys[nxt]), di, dn, mk3(tk.dir[0], tk.dir[1], tk.dir[2]), edges, faces))
+				uf_union(parent, i, nxt, dev_err);
 		}
 
 		__global__ void compress_kernel(uint32_t* __restrict__ parent, uint32_t n, const uint8_t* __restrict__ attached,
@@ -2736,8 +2916,10 @@ struct u26_scene
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
-	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp;
-	RadixSorter sorter, esorter, csorter;
+	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals;
+	RadixSorter sorter, esorter, csorter, fvsorter;
+	std::vector<uint8_t> vsolid; // per vertex: its object is rigid / tetrahedral
+	bool any_solid = false;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 };
@@ -2825,6 +3007,13 @@ U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* m, u26_sc
 	cpf(s->earea, m->rest_edge_area, s->ne);
 	cpf(s->farea, m->rest_face_area, s->nf);
 	cpf(s->vmass, m->vert_mass, s->nv);
+	s->vsolid.assign(std::max(1u, s->nv), 0u);
+	if (m->object_solid)
+		for (uint32_t v = 0; v < s->nv; v++)
+		{
+			s->vsolid[v] = m->object_solid[s->vobj[v]] ? 1u : 0u;
+			s->any_solid = s->any_solid || s->vsolid[v];
+		}
 	for (uint32_t o = 0; o < s->nobj; o++)
 	{
 		s->vmax_obj = std::max(s->vmax_obj, s->pv[o + 1] - s->pv[o]);
@@ -2851,6 +3040,7 @@ U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* m, u26_sc
 	U26_TRY(upload(ctx, s->d_farea, s->farea));
 	U26_TRY(upload(ctx, s->d_vmass, s->vmass));
 	U26_TRY(upload(ctx, s->d_orient, s->orient));
+	U26_TRY(upload(ctx, s->d_vsolid, s->vsolid));
 	{
 		// 30-bit Morton codes of the rest positions (vertices) and rest edge midpoints over
 		// the rest AABB: the request order of the ray casts
@@ -2916,12 +3106,14 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
 		&s->d_step_hits, &s->d_step_out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
 		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
-		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp };
+		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp, &s->d_vsolid,
+		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
 	s->esorter.release();
 	s->csorter.release();
+	s->fvsorter.release();
 	delete s;
 }
 
@@ -3693,12 +3885,57 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				S->d_vf_off.as<uint32_t>(), S->d_vf.as<uint32_t>(), S->d_parent.as<uint32_t>(), S->d_att.as<uint8_t>(),
 				S->d_csize.as<uint32_t>(), S->d_catt.as<uint32_t>());
 			U26_TRY(after_launch(ctx, "init_hits_kernel"));
+			// run directory of this level's hits
+			U26_CUDA(ctx, S->d_rflag.reserve(sizeof(uint32_t) * (size_t(nh) + 1)));
+			run_flags_kernel<<<div_up(nh + 1, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, b, S->d_rflag.as<uint32_t>());
+			U26_TRY(after_launch(ctx, "run_flags_kernel"));
+			U26_TRY(device_exclusive_scan(ctx, S->d_rflag.as<uint32_t>(), nh + 1, S->scan_tmp));
+			U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_rflag.as<uint32_t>() + nh, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+			U26_CUDA(ctx, cudaStreamSynchronize(st));
+			const uint32_t nruns = *ctx->host_word;
+			uint32_t hsize = 1024;
+			while (hsize < 2 * nruns)
+				hsize <<= 1;
+			U26_CUDA(ctx, S->d_heads.reserve(sizeof(uint32_t) * (size_t(nruns) + 1)));
+			U26_CUDA(ctx, S->d_hkeys.reserve(sizeof(uint64_t) * hsize));
+			U26_CUDA(ctx, S->d_hvals.reserve(sizeof(uint32_t) * hsize));
+			U26_CUDA(ctx, cudaMemsetAsync(S->d_hkeys.ptr, 0, sizeof(uint64_t) * hsize, st));
+			run_insert_kernel<<<div_up(nh + 1, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, b, S->d_rflag.as<uint32_t>(),
+				S->d_heads.as<uint32_t>(), S->d_hkeys.as<uint64_t>(), S->d_hvals.as<uint32_t>(), hsize - 1, ctx->dev_err);
+			U26_TRY(after_launch(ctx, "run_insert_kernel"));
+			const RunDir rdir{ S->d_hkeys.as<uint64_t>(), S->d_hvals.as<uint32_t>(), S->d_heads.as<uint32_t>(), hsize - 1 };
 			union_kernel<<<div_up(nh, 128), 128, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_edges.as<uint2>(),
 				S->d_faces.as<uint32_t>(), S->d_fae.as<uint32_t>(), S->d_vav_off.as<uint32_t>(), S->d_vav.as<uint32_t>(),
 				S->d_vae_off.as<uint32_t>(), S->d_vae.as<uint32_t>(), S->d_vaf_off.as<uint32_t>(), S->d_vaf.as<uint32_t>(),
 				S->d_eaf_off.as<uint32_t>(), S->d_eaf.as<uint32_t>(), S->d_eae_off.as<uint32_t>(), S->d_eae.as<uint32_t>(),
-				S->d_parent.as<uint32_t>(), ctx->dev_err);
+				rdir, S->d_parent.as<uint32_t>(), ctx->dev_err);
 			U26_TRY(after_launch(ctx, "union_kernel"));
+			if (P->solid_interior && (P->solid_all || S->any_solid))
+			{
+				const SolidParams sp{ S->d_fn.as<float>(), S->d_en.as<float>(), S->d_vobj.as<uint32_t>(), S->d_vsolid.as<uint8_t>(), P->solid_all,
+					P->solid_eps_n, P->solid_eps_d };
+				solid_runs_kernel<<<div_up(nh, 128), 128, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_seg.as<uint32_t>(), S->d_pay.as<float>(),
+					S->d_tasks.as<Task>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), sp, S->d_parent.as<uint32_t>(), ctx->dev_err);
+				U26_TRY(after_launch(ctx, "solid_runs_kernel"));
+				U26_CUDA(ctx, S->d_fvk.reserve(sizeof(uint64_t) * nh));
+				U26_CUDA(ctx, S->d_fvv.reserve(sizeof(uint32_t) * nh));
+				U26_CUDA(ctx, S->d_ecount.reserve(sizeof(uint32_t)));
+				U26_CUDA(ctx, cudaMemsetAsync(S->d_ecount.ptr, 0, sizeof(uint32_t), st));
+				solid_fv_keys_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_keys.as<uint64_t>(), nh, cd, S->d_fvk.as<uint64_t>(),
+					S->d_fvv.as<uint32_t>(), S->d_ecount.as<uint32_t>());
+				U26_TRY(after_launch(ctx, "solid_fv_keys_kernel"));
+				U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_ecount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+				U26_CUDA(ctx, cudaStreamSynchronize(st));
+				const uint32_t nfv = *ctx->host_word;
+				if (nfv > 1)
+				{
+					U26_TRY(S->fvsorter.sort(ctx, S->d_fvk.as<uint64_t>(), S->d_fvv.as<uint32_t>(), nfv, 0, b + tb));
+					solid_fv_kernel<<<div_up(nfv, 128), 128, 0, st>>>(S->d_fvk.as<uint64_t>(), S->d_fvv.as<uint32_t>(), nfv, S->d_keys.as<uint64_t>(), cd,
+						S->d_pay.as<float>(), S->d_tasks.as<Task>(), S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), sp, S->d_parent.as<uint32_t>(),
+						ctx->dev_err);
+					U26_TRY(after_launch(ctx, "solid_fv_kernel"));
+				}
+			}
 			compress_kernel<<<div_up(nh, 256), 256, 0, st>>>(S->d_parent.as<uint32_t>(), nh, S->d_att.as<uint8_t>(), S->d_csize.as<uint32_t>(),
 				S->d_catt.as<uint32_t>(), S->d_root.as<uint32_t>());
 			U26_TRY(after_launch(ctx, "compress_kernel"));

@@ -35,7 +35,7 @@ class MeshDesc(ctypes.Structure):
         ("prefix_verts", _u32p), ("prefix_edges", _u32p), ("prefix_faces", _u32p),
         ("vert_object", _u32p), ("vert_component", _u32p),
         ("rest_vert_area", _f32p), ("rest_edge_area", _f32p), ("rest_face_area", _f32p), ("vert_mass", _f32p),
-        ("mesh_orientation", _u32p), ("object_scene", _u32p),
+        ("mesh_orientation", _u32p), ("object_scene", _u32p), ("object_solid", _u32p),
     ]
 
 
@@ -213,6 +213,8 @@ class Mesh:
         d.mesh_orientation = p(self.mesh_orientation)
         scene = getattr(self, "object_scene", None)
         d.object_scene = p(scene) if scene is not None else None
+        solid = getattr(self, "object_solid", None)
+        d.object_solid = p(np.asarray(solid, np.uint32)) if solid is not None else None
         d._keep = keep
         return d
 

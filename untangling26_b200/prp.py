@@ -26,14 +26,17 @@ class PrpParams(ctypes.Structure):
         ("ccr_blend", c_u32),         # PRP_use_blended_intrinsic_coordinates
         ("ccr_blend_weight", c_f32),  # PRP_intrinsic_blend_weight
         ("form", c_u32),              # 0 batched packet ray casting (default), 1 plain form (baseline)
-        ("reserved", c_u32),
+        ("solid_interior", c_u32),    # PRP_solid_interior_adjacency
+        ("solid_all", c_u32),         # PRP_solid_interior_adjacency_all_meshes
+        ("solid_eps_n", c_f32),       # PRP_solid_interior_adjacency_normal_eps
+        ("solid_eps_d", c_f32),       # PRP_solid_interior_adjacency_dist_eps
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, opt_iterations=0, ccr_blend=0, ccr_blend_weight=0.5,
-                  form=0, reserved=0)
+                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

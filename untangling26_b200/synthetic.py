@@ -100,12 +100,16 @@ def layered_sheets(n=512, layers=5, seed=4):
     rng = np.random.default_rng(seed)
     xg, f = grid(n)
     xs, fs, obj, rests = [], [], [], []
+    h = 1.0 / (n - 1)
     for k in range(layers):
         x = xg.copy()
+        # a seeded sub-cell xy shift per layer keeps the layers' edges off each other's edges
+        # (coincident grids put every crossing on a triangle boundary)
+        x[:, :2] += rng.uniform(0.2, 0.45, 2) * h * (k > 0)
         amp = rng.uniform(0.002, 0.020)
         x[:, 2] = 0.001 * k + amp * _value_noise(rng, x[:, 0], x[:, 1])
         xs.append(x)
-        rest = xg.copy()
+        rest = x.copy()
         rest[:, 2] = 0.001 * k
         rests.append(rest)
         fs.append(f + k * n * n)
