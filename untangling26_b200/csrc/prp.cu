@@ -167,7 +167,7 @@ namespace u26
 			uint32_t bnd_off, bnd_cnt;
 			uint32_t k;
 			uint32_t diam;
-			uint32_t pad[2];
+			uint32_t pad[2]; // [0] contour-side restriction applies, [1] object of the side
 		};
 
 		// ------------------------------------------------------------ distances
@@ -687,8 +687,9 @@ namespace u26
 		// keep the traversal a superset of the exact primitive tests).
 		// The w lanes carry the node's links, so one 32-byte load serves a visit: inner node
 		// (mn.w, mx.w) = (left, right child); leaf (mn.w, mx.w) = (primitive, ~0).
+		// node_off / prim_off place one object's tree in the forest of all objects' trees
 		__global__ void grow_boxes_kernel(const NodeBox* __restrict__ boxes, const uint2* __restrict__ children,
-			const uint32_t* __restrict__ object_idx, uint32_t n, int isotropic, NodeBox* __restrict__ out)
+			const uint32_t* __restrict__ object_idx, uint32_t n, int isotropic, uint32_t node_off, uint32_t prim_off, NodeBox* __restrict__ out)
 		{
 			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 			if (i >= n)
@@ -712,23 +713,23 @@ namespace u26
 			const uint32_t obj = object_idx[i];
 			if (obj != kInvalid)
 			{
-				g.mn.w = __uint_as_float(obj);
+				g.mn.w = __uint_as_float(obj + prim_off);
 				g.mx.w = __uint_as_float(kInvalid);
 			}
 			else
 			{
 				const uint2 ch = children[i];
-				g.mn.w = __uint_as_float(ch.x);
-				g.mx.w = __uint_as_float(ch.y);
+				g.mn.w = __uint_as_float(ch.x + node_off);
+				g.mx.w = __uint_as_float(ch.y + node_off);
 			}
-			out[i] = g;
+			out[node_off + i] = g;
 		}
 
 		// The subtree roots that split one traversal across kSplit threads: the nodes at
 		// depth log2(kSplit) below the root, or shallower leaves; unused entries ~0.
 		constexpr uint32_t kSplit = 8;
 		__global__ void frontier_kernel(const uint2* __restrict__ children, const uint32_t* __restrict__ object_idx, uint32_t n_nodes,
-			uint32_t* __restrict__ out)
+			uint32_t node_off, uint32_t* __restrict__ out)
 		{
 			if (threadIdx.x != 0 || blockIdx.x != 0)
 				return;
@@ -755,7 +756,7 @@ namespace u26
 				nc = nn;
 			}
 			for (uint32_t i = 0; i < kSplit; i++)
-				out[i] = i < nc ? cur[i] : kInvalid;
+				out[i] = i < nc ? cur[i] + node_off : kInvalid;
 		}
 
 		// slab test of a grown box with the ray's reciprocals hoisted (same values as ray_box:
@@ -866,7 +867,7 @@ namespace u26
 
 			// ---- per-lane request
 			int kind = 0; // 1: VF / FV ray on the face tree, 2: EE swept edge on the edge tree
-			uint32_t t = 0, vid = 0, eid = 0;
+			uint32_t t = 0, vid = 0, eid = 0, tobj = 0;
 			bool fv = false;
 			const uint32_t* bits = nullptr;
 			uint32_t tgt_lo = 0, tgt_cnt = 0;
@@ -903,6 +904,7 @@ namespace u26
 					const Slot tgt = slots[fv ? tk.slot0 : tk.slot1];
 					tgt_lo = tgt.f_lo;
 					tgt_cnt = tgt.f_cnt;
+					tobj = tgt.pad[1];
 					bits = bits_f + size_t(fv ? tk.slot0 : tk.slot1) * (f_stride / 32 + 1);
 					const f3 cast = fv ? -dir : dir;
 					orig = ld3(x, vid);
@@ -928,6 +930,7 @@ namespace u26
 					const Slot s1 = slots[tk.slot1];
 					tgt_lo = s1.e_lo;
 					tgt_cnt = s1.e_cnt;
+					tobj = s1.pad[1];
 					ev = edges[eid];
 					p0 = ld3(x, ev.x);
 					const f3 p1 = ld3(x, ev.y);
@@ -966,10 +969,15 @@ namespace u26
 			}
 
 			// ---- face tree: VF / FV rays of the warp
-			bool on = kind == 1;
-			const uint32_t fstart = ffront[part];
-			if (__any_sync(0xFFFFFFFFu, on) && fstart != kInvalid)
+			// each lane starts at its target object's subtree root of this part; lanes with the
+			// same start walk together
+			const uint32_t fstart_l = kind == 1 ? ffront[size_t(tobj) * kSplit + part] : kInvalid;
+			uint32_t fpending = __ballot_sync(0xFFFFFFFFu, fstart_l != kInvalid);
+			while (fpending != 0u)
 			{
+				const uint32_t fstart = __shfl_sync(0xFFFFFFFFu, fstart_l, __ffs(fpending) - 1);
+				const bool on = fstart_l == fstart;
+				fpending &= ~__ballot_sync(0xFFFFFFFFu, on);
 				ray_visits += on ? 1u : 0u;
 				int sp = 1;
 				if (lane == 0)
@@ -1040,10 +1048,13 @@ namespace u26
 			}
 
 			// ---- edge tree: EE swept edges of the warp
-			on = kind == 2;
-			const uint32_t estart = efront[part];
-			if (__any_sync(0xFFFFFFFFu, on) && estart != kInvalid)
+			const uint32_t estart_l = kind == 2 ? efront[size_t(tobj) * kSplit + part] : kInvalid;
+			uint32_t epending = __ballot_sync(0xFFFFFFFFu, estart_l != kInvalid);
+			while (epending != 0u)
 			{
+				const uint32_t estart = __shfl_sync(0xFFFFFFFFu, estart_l, __ffs(epending) - 1);
+				const bool on = estart_l == estart;
+				epending &= ~__ballot_sync(0xFFFFFFFFu, on);
 				ray_visits += on ? 1u : 0u;
 				int sp = 1;
 				if (lane == 0)
@@ -2916,10 +2927,12 @@ struct u26_scene
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
-	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals;
+	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals, d_zero_th;
 	RadixSorter sorter, esorter, csorter, fvsorter;
 	std::vector<uint8_t> vsolid; // per vertex: its object is rigid / tetrahedral
 	bool any_solid = false;
+	std::vector<u26_lbvh*> otree_f, otree_e; // per-object ray-casting trees (built at the first pass)
+	bool otrees_built = false;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 };
@@ -3107,13 +3120,18 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_step_hits, &s->d_step_out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
 		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
 		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp, &s->d_vsolid,
-		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals };
+		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals,
+		&s->d_zero_th };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
 	s->esorter.release();
 	s->csorter.release();
 	s->fvsorter.release();
+	for (u26_lbvh* t : s->otree_f)
+		u26_lbvh_destroy(t);
+	for (u26_lbvh* t : s->otree_e)
+		u26_lbvh_destroy(t);
 	delete s;
 }
 
@@ -3604,7 +3622,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			sl.k = 0;
 			sl.diam = 0;
 			sl.pad[0] = ccr_on ? 1u : 0u;
-			sl.pad[1] = 0u;
+			sl.pad[1] = o; // the side's object: its ray-casting trees
 			bnd.insert(bnd.end(), b[sd].begin(), b[sd].end());
 		}
 		const uint32_t rsc = S->oscene[r.obj[0]];
@@ -3677,26 +3695,64 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 8));
 	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 8, st));
 	const TreeView ftv = tree_view(face_tree), etv = tree_view(edge_tree);
-	// grown node boxes of this pass's trees and the subtree roots of the split traversal
+	// The ray casts traverse one face tree and one edge tree per object (the reference's
+	// per-object CachedBVH): a ray tests only its target object's primitives. The trees are
+	// built at the scene's first pass and refit on every pass; their grown node boxes (with
+	// the child links in the w lanes) form one forest array, and each tree's subtree roots of
+	// the split traversal sit at [object * kSplit, (object + 1) * kSplit).
+	const uint32_t nobj = std::max(1u, S->nobj);
 	{
-		const uint32_t fn_ = ftv.n ? 2 * ftv.n - 1 : 0, en_ = etv.n ? 2 * etv.n - 1 : 0;
-		U26_CUDA(ctx, S->d_fgrow.reserve(sizeof(NodeBox) * std::max(fn_, 1u)));
-		U26_CUDA(ctx, S->d_egrow.reserve(sizeof(NodeBox) * std::max(en_, 1u)));
-		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * kSplit));
-		if (fn_)
+		if (!S->otrees_built)
 		{
-			grow_boxes_kernel<<<div_up(fn_, 256), 256, 0, st>>>(ftv.boxes, ftv.children, ftv.object_idx, fn_, 0, S->d_fgrow.as<NodeBox>());
-			U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
+			U26_CUDA(ctx, S->d_zero_th.reserve(sizeof(float) * std::max(1u, S->nv)));
+			U26_CUDA(ctx, cudaMemsetAsync(S->d_zero_th.ptr, 0, sizeof(float) * std::max(1u, S->nv), st));
+			S->otree_f.assign(nobj, nullptr);
+			S->otree_e.assign(nobj, nullptr);
+			for (uint32_t o = 0; o < S->nobj; o++)
+				for (int kind = 0; kind < 2; kind++)
+				{
+					const uint32_t cnt = kind == 0 ? S->pf[o + 1] - S->pf[o] : S->pe[o + 1] - S->pe[o];
+					if (cnt == 0)
+						continue;
+					const uint32_t* prims = kind == 0 ? S->d_faces.as<uint32_t>() + 3 * size_t(S->pf[o]) : S->d_edges.as<uint32_t>() + 2 * size_t(S->pe[o]);
+					u26_lbvh* t = nullptr;
+					U26_TRY(u26_lbvh_create(ctx, kind == 0 ? U26_TREE_FACE : U26_TREE_EDGE, cnt, &t));
+					(kind == 0 ? S->otree_f : S->otree_e)[o] = t;
+					U26_TRY(u26_lbvh_set_option(t, U26_LBVH_OPT_FULL_GLOBAL_AABB, 1));
+					U26_TRY(u26_lbvh_reduce_aabb(t, d_x, S->nv, prims));
+					U26_TRY(u26_lbvh_construct_tree(t));
+				}
+			S->otrees_built = true;
 		}
-		if (en_)
+		std::vector<uint32_t> foff(nobj + 1, 0u), eoff(nobj + 1, 0u);
+		for (uint32_t o = 0; o < nobj; o++)
 		{
-			grow_boxes_kernel<<<div_up(en_, 256), 256, 0, st>>>(etv.boxes, etv.children, etv.object_idx, en_, 1, S->d_egrow.as<NodeBox>());
-			U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
+			foff[o + 1] = foff[o] + (S->otree_f[o] ? S->otree_f[o]->num_nodes() : 0u);
+			eoff[o + 1] = eoff[o] + (S->otree_e[o] ? S->otree_e[o]->num_nodes() : 0u);
 		}
-		frontier_kernel<<<1, 32, 0, st>>>(ftv.children, ftv.object_idx, fn_, S->d_front.as<uint32_t>());
-		U26_TRY(after_launch(ctx, "frontier_kernel"));
-		frontier_kernel<<<1, 32, 0, st>>>(etv.children, etv.object_idx, en_, S->d_front.as<uint32_t>() + kSplit);
-		U26_TRY(after_launch(ctx, "frontier_kernel"));
+		U26_CUDA(ctx, S->d_fgrow.reserve(sizeof(NodeBox) * std::max(foff[nobj], 1u)));
+		U26_CUDA(ctx, S->d_egrow.reserve(sizeof(NodeBox) * std::max(eoff[nobj], 1u)));
+		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * size_t(nobj) * kSplit));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_front.ptr, 0xFF, sizeof(uint32_t) * 2 * size_t(nobj) * kSplit, st));
+		for (uint32_t o = 0; o < nobj; o++)
+			for (int kind = 0; kind < 2; kind++)
+			{
+				u26_lbvh* t = (kind == 0 ? S->otree_f : S->otree_e)[o];
+				if (!t)
+					continue;
+				const uint32_t* prims = kind == 0 ? S->d_faces.as<uint32_t>() + 3 * size_t(S->pf[o]) : S->d_edges.as<uint32_t>() + 2 * size_t(S->pe[o]);
+				U26_TRY(u26_lbvh_update_and_refit(t, S->d_zero_th.as<float>(), d_x, d_x, prims));
+				const TreeView tv = tree_view(t);
+				const uint32_t nn = t->num_nodes();
+				const uint32_t node_off = kind == 0 ? foff[o] : eoff[o];
+				const uint32_t prim_off = kind == 0 ? S->pf[o] : S->pe[o];
+				grow_boxes_kernel<<<div_up(nn, 256), 256, 0, st>>>(tv.boxes, tv.children, tv.object_idx, nn, kind, node_off, prim_off,
+					(kind == 0 ? S->d_fgrow : S->d_egrow).as<NodeBox>());
+				U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
+				frontier_kernel<<<1, 32, 0, st>>>(tv.children, tv.object_idx, nn, node_off,
+					S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kSplit);
+				U26_TRY(after_launch(ctx, "frontier_kernel"));
+			}
 	}
 	const uint32_t bnd_words = vs / 32 + 1;
 	if (nslots)
@@ -3846,7 +3902,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * kSplit;
 				raycast_kernel<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
 					S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(),
-					ftv, etv, S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(), S->d_front.as<uint32_t>() + kSplit,
+					ftv, etv, S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(),
+					S->d_front.as<uint32_t>() + size_t(nobj) * kSplit,
 					d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
 					(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
 				U26_TRY(after_launch(ctx, "raycast_kernel"));
