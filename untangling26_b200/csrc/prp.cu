@@ -844,7 +844,7 @@ namespace u26
 		// kSplit parts x the requests rounded up to warps; part p starts at frontier node p,
 		// so every (ray, leaf) pair is decided once.
 		constexpr int kStack = 64;
-		__global__ void __launch_bounds__(128, 8) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
+		__global__ void __launch_bounds__(128, 7) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
 			TreeView ftree, TreeView etree, const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow,
@@ -875,10 +875,9 @@ namespace u26
 			float slen = 0.0f, inv_len = 0.0f, t_lo = 0.0f, t_hi = 1.0f;
 			bool seg_ok = false;
 			RaySlab slab{};
-			uint2 ev = make_uint2(0u, 0u);
-			f3 p0 = mk3(0.0f), e1 = mk3(0.0f), pn = mk3(0.0f), smn = mk3(0.0f), smx = mk3(0.0f);
-			float pd = 0.0f, ray_max = 0.0f;
-			bool plane = false;
+			bool ee_req = false; // an EE request: its swept-edge state is set up after the face walk
+			uint32_t ee_slot = 0;
+			float ee_pmax = 0.0f;
 			if (r < total)
 			{
 				// task of this request: last task with req_begin <= r
@@ -931,40 +930,9 @@ namespace u26
 					tgt_lo = s1.e_lo;
 					tgt_cnt = s1.e_cnt;
 					tobj = s1.pad[1];
-					ev = edges[eid];
-					p0 = ld3(x, ev.x);
-					const f3 p1 = ld3(x, ev.y);
-					const float dl2 = dot(dir, dir);
-					ray_max = 1.0f;
-					if (!(dl2 <= 1e-12f))
-					{
-						const float smin = fminf(dot(p0, dir), dot(p1, dir));
-						ray_max = fminf(fmaxf((tk.ee_pmax - smin) / dl2 + 1e-5f, 0.0f), 1.0f);
-					}
-					if (ray_max > 0.0f)
-					{
-						e1 = p1 - p0;
-						pn = cross(e1, dir);
-						const float nl = length(pn);
-						plane = nl >= 1e-10f;
-						if (plane)
-						{
-							pn = pn / nl;
-							pd = dot(pn, p0);
-						}
-						const f3 a_end = p0 + dir * ray_max, b_end = p1 + dir * ray_max;
-						smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
-						smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
-						// intersect the swept box with the grown AABB of the candidate target edges
-						const float* tb = slot_box + 12 * size_t(tk.slot1) + 6;
-						const float g0 = 1e-5f * (1.0f + fmaxf(fabsf(tb[0]), fabsf(tb[3])));
-						const float g1 = 1e-5f * (1.0f + fmaxf(fabsf(tb[1]), fabsf(tb[4])));
-						const float g2 = 1e-5f * (1.0f + fmaxf(fabsf(tb[2]), fabsf(tb[5])));
-						smn = vmax(smn, mk3(tb[0] - g0, tb[1] - g1, tb[2] - g2));
-						smx = vmin(smx, mk3(tb[3] + g0, tb[4] + g1, tb[5] + g2));
-						if (smn.x <= smx.x && smn.y <= smx.y && smn.z <= smx.z)
-							kind = 2;
-					}
+					ee_req = true;
+					ee_slot = tk.slot1;
+					ee_pmax = tk.ee_pmax;
 				}
 			}
 
@@ -1047,7 +1015,49 @@ namespace u26
 				__syncwarp();
 			}
 
-			// ---- edge tree: EE swept edges of the warp
+			// ---- edge tree: EE swept edges of the warp (their state set up here, after the face
+			// rays' state is dead)
+			uint2 ev = make_uint2(0u, 0u);
+			f3 p0 = mk3(0.0f), e1 = mk3(0.0f), pn = mk3(0.0f), smn = mk3(0.0f), smx = mk3(0.0f);
+			float pd = 0.0f, ray_max = 0.0f;
+			bool plane = false;
+			if (ee_req)
+			{
+				ev = edges[eid];
+				p0 = ld3(x, ev.x);
+				const f3 p1 = ld3(x, ev.y);
+				const float dl2 = dot(dir, dir);
+				ray_max = 1.0f;
+				if (!(dl2 <= 1e-12f))
+				{
+					const float smin = fminf(dot(p0, dir), dot(p1, dir));
+					ray_max = fminf(fmaxf((ee_pmax - smin) / dl2 + 1e-5f, 0.0f), 1.0f);
+				}
+				if (ray_max > 0.0f)
+				{
+					e1 = p1 - p0;
+					pn = cross(e1, dir);
+					const float nl = length(pn);
+					plane = nl >= 1e-10f;
+					if (plane)
+					{
+						pn = pn / nl;
+						pd = dot(pn, p0);
+					}
+					const f3 a_end = p0 + dir * ray_max, b_end = p1 + dir * ray_max;
+					smn = vmin(vmin(p0, p1), vmin(a_end, b_end));
+					smx = vmax(vmax(p0, p1), vmax(a_end, b_end));
+					// intersect the swept box with the grown AABB of the candidate target edges
+					const float* tb = slot_box + 12 * size_t(ee_slot) + 6;
+					const float g0 = 1e-5f * (1.0f + fmaxf(fabsf(tb[0]), fabsf(tb[3])));
+					const float g1 = 1e-5f * (1.0f + fmaxf(fabsf(tb[1]), fabsf(tb[4])));
+					const float g2 = 1e-5f * (1.0f + fmaxf(fabsf(tb[2]), fabsf(tb[5])));
+					smn = vmax(smn, mk3(tb[0] - g0, tb[1] - g1, tb[2] - g2));
+					smx = vmin(smx, mk3(tb[3] + g0, tb[4] + g1, tb[5] + g2));
+					if (smn.x <= smx.x && smn.y <= smx.y && smn.z <= smx.z)
+						kind = 2;
+				}
+			}
 			const uint32_t estart_l = kind == 2 ? efront[size_t(tobj) * kSplit + part] : kInvalid;
 			uint32_t epending = __ballot_sync(0xFFFFFFFFu, estart_l != kInvalid);
 			while (epending != 0u)
@@ -1620,7 +1630,12 @@ namespace u26
 
 		// find_adjacent_hits rules as exact key lookups inside the task segment. Lookups that
 		// share a (type, source) first find that source's run of hits once, then search the
-		// targets inside the (short) run.
+		// targets inside the (short) run. Every rule is symmetric (its mirror rule from the
+		// other hit's type gives the same pair, since the adjacency lists are the mesh's
+		// incidence relations), so each unordered pair is looked up from one side only:
+		// same-type pairs from the smaller adjacent id, VF-FV pairs from the FV hit, VF-EE and
+		// FV-EE pairs from the EE hit (the sides with the fewest lookups). The components are
+		// those of the two-sided rules.
 		__global__ void union_kernel(const uint64_t* __restrict__ keys, uint32_t n, HitKeyCodec cd, const uint32_t* __restrict__ seg,
 			const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const uint32_t* __restrict__ fae,
 			const uint32_t* __restrict__ vav_off, const uint32_t* __restrict__ vav, const uint32_t* __restrict__ vae_off,
@@ -1653,21 +1668,10 @@ namespace u26
 			uint32_t rb, re;
 			if (ty == 0u)
 			{
-				// VF(v, f)
+				// VF(v, f) - VF(v', f), v' adjacent to v (VF-FV and VF-EE pairs come from the other side)
 				for (uint32_t q = vav_off[s]; q < vav_off[s + 1]; q++)
-					link(0u, vav[q], d);
-				for (uint32_t q = vaf_off[s]; q < vaf_off[s + 1]; q++)
-				{
-					run(2u, vaf[q], rb, re);
-					for (int c = 0; c < 3; c++)
-						link_in(rb, re, 2u, vaf[q], faces[3 * d + c]);
-				}
-				for (uint32_t q = vae_off[s]; q < vae_off[s + 1]; q++)
-				{
-					run(1u, vae[q], rb, re);
-					for (int c = 0; c < 3; c++)
-						link_in(rb, re, 1u, vae[q], fae[3 * d + c]);
-				}
+					if (vav[q] > s)
+						link(0u, vav[q], d);
 			}
 			else if (ty == 2u)
 			{
@@ -1680,13 +1684,8 @@ namespace u26
 				}
 				run(2u, s, rb, re);
 				for (uint32_t q = vav_off[d]; q < vav_off[d + 1]; q++)
-					link_in(rb, re, 2u, s, vav[q]);
-				for (int c = 0; c < 3; c++)
-				{
-					run(1u, fae[3 * s + c], rb, re);
-					for (uint32_t q = vae_off[d]; q < vae_off[d + 1]; q++)
-						link_in(rb, re, 1u, fae[3 * s + c], vae[q]);
-				}
+					if (vav[q] > d)
+						link_in(rb, re, 2u, s, vav[q]);
 			}
 			else
 			{
@@ -1708,9 +1707,11 @@ namespace u26
 				}
 				run(1u, s, rb, re);
 				for (uint32_t q = eae_off[d]; q < eae_off[d + 1]; q++)
-					link_in(rb, re, 1u, s, eae[q]);
+					if (eae[q] > d)
+						link_in(rb, re, 1u, s, eae[q]);
 				for (uint32_t q = eae_off[s]; q < eae_off[s + 1]; q++)
-					link(1u, eae[q], d);
+					if (eae[q] > s)
+						link(1u, eae[q], d);
 			}
 		}
 
