@@ -152,11 +152,12 @@ def cpu_pass(mesh, max_contours, stride):
     o.lbvh_refit(tree, mesh.x, mesh.x, th, mesh.faces)
     broad, n_broad, _ = o.lbvh_query(tree, o.QUERY_EDGES_UNCULLED, mesh.x, mesh.x, mesh.edges, dh, th)
     ef, idx = o.ef_narrow(broad, mesh.x, mesh.edges, mesh.faces, dh, mesh.vert_property)
-    run = o.PrpRun(mesh, ef, idx, o.prp_params(max_contours=max_contours, contour_stride=stride))
+    run = o.PrpRun(mesh, ef, idx, o.prp_params(max_contours=max_contours, contour_stride=stride), response=RESPONSE)
     return n_broad + run.pairs_tested, time.perf_counter() - t0
 
 
 CPU_BATCH_SCENES = 8  # scenes of the batch workload in the CPU sample
+RESPONSE = (3e-3, 1e8)  # untangling_response_depth, stiffness_untangling (scene_params.h:66, 121-122)
 
 
 def run_cpu_baseline(mesh, max_contours, samples=1):
@@ -242,7 +243,7 @@ def main():
 
     from untangling26_b200 import Context
     from untangling26_b200.intersection_resolver import CollisionScene
-    from untangling26_b200.prp import prp_params
+    from untangling26_b200.prp import prp_params, response_params
 
     if ws > 1:
         import datetime
@@ -256,13 +257,15 @@ def main():
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
     stream = torch.cuda.current_stream(dev)
 
+    rparams = response_params(*RESPONSE)
+
     def device_pass():
         sc.refit_face_tree()
         sc.resolver.reset()
         sc.stats.zero_()
         sc.ef_detect(with_stats=True)
         n = sc.resolver.canonicalize(mesh.num_edges, mesh.num_faces)
-        res = sc.host_resolve(params, num_pairs=n)
+        res = sc.host_resolve(params, num_pairs=n, response=rparams)
         return res
 
     for _ in range(max(args.warmup, 3)):
@@ -290,7 +293,7 @@ def main():
         sc.ef_detect(with_stats=True)
         kev[i][1].record(stream)
         n = sc.resolver.canonicalize(mesh.num_edges, mesh.num_faces)
-        res = sc.host_resolve(params, num_pairs=n)
+        res = sc.host_resolve(params, num_pairs=n, response=rparams)
         ev[i][1].record(stream)
         results.append(res)
         ef_tests.append(sc.stats[1])
@@ -348,6 +351,19 @@ def main():
             roof["traffic"] = tr.get(roof["kernel"])
             roof_ef["traffic"] = tr.get("ef_detect_kernel")
 
+    # ---- response assembly (inside every timed pass): collision pair templates + region CSRs.
+    # Algorithmic bytes: per pair 44 B hit in, 2 x 12 B normals + 2 x 4 B areas, 64 B template +
+    # 16 B info out, 4 vertex-label keys of 8 B written, sorted (4 radix passes of read + write)
+    # and read; per EF pair 5 keys likewise; the three CSR arrays written once.
+    rr = r0.response
+    nkeys = 4 * rr.num_pairs + 5 * len(r0.pairs)
+    rs_bytes = (44 + 32 + 80) * rr.num_pairs + 8 * nkeys * (2 + 2 * 4) + 4 * (
+        int(rr.vert_regions.numel()) + int(rr.edge_regions.numel()) + int(rr.face_regions.numel()))
+    resp = {"pairs": rr.num_pairs, "ms_per_pass": rr.ms, "algorithmic_bytes": rs_bytes,
+            "achieved": rs_bytes / (rr.ms / 1e3) / 1e9 if rr.ms > 0 else 0.0, "unit": "GB/s",
+            "region_words": [int(rr.vert_regions.numel()), int(rr.edge_regions.numel()), int(rr.face_regions.numel())],
+            "note": "host wall time of u26_prp_make_response (hit upload, 12 launches, 3 synchronisations)"}
+
     # ---- LBVH refit: the fused leaf update + bottom-up refit of the face tree alone, L2
     # flushed before every launch. Algorithmic bytes (each byte once): V x (12 B position +
     # 4 B thickness) + F x (12 B face + 4 B leaf order + 32 B leaf box write) + (F - 1) x
@@ -391,7 +407,7 @@ def main():
                 sc_i.stats.zero_()
                 sc_i.ef_detect(with_stats=True)
                 n_i = sc_i.resolver.canonicalize(m_i.num_edges, m_i.num_faces)
-                r_i = sc_i.host_resolve(pparams, num_pairs=n_i)
+                r_i = sc_i.host_resolve(pparams, num_pairs=n_i, response=rparams)
                 tests += int(sc_i.stats[1].item()) + r_i.pairs_tested
             return tests
 
@@ -446,6 +462,7 @@ def main():
                     "ms_per_step": e2e_ms / args.steps},
             "untangle_passes_per_s": 1e3 * args.steps / total_ms,
             "plain_form": plain,
+            "response": resp,
             "gpu_launches": int(launches), "roofline": roof, "lbvh_refit": refit, "clocks": clk,
             "pass": {"ef_pairs": n_ef, "contours": len(r0.contours), "processed": int(len(proc)),
                      "responses": int((proc["combo_idx"] != 0xFFFFFFFF).sum()), "levels": r0.levels,

@@ -301,6 +301,51 @@ U26_API u26_status u26_prp_resolve(u26_scene* scene, u26_lbvh* face_tree, u26_lb
 U26_API u26_status u26_prp_output_view_get(const u26_prp_output* out, u26_prp_output_view* view);
 U26_API void u26_prp_output_destroy(u26_prp_output* out);
 
+/* ---- response assembly ------------------------------------------------------------
+ * The selected supports of a pass as collision pair templates for the Newton system
+ * (make_response_from_min_hitinfo, intersection_resolver2.cpp:2105-2221), optionally
+ * appended to a narrow-phase list after its penalty pairs (upload_response_pairs_to_gpu,
+ * 2223-2294), and the contour-region lists of every vertex, edge and face
+ * (host_apply_untangling_constraint, 2296-2427). */
+typedef struct u26_prp_response_params
+{
+	float depth_threshold; /* untangling_response_depth (3e-3): C = max(-depth - 3e-3, -depth_threshold) */
+	float stiffness;	   /* stiffness_untangling (1e8): k1 = area stiffness C, k2 = area stiffness */
+} u26_prp_response_params;
+
+/* CollisionPair::CollisionPairTemplate (collision_data.h:48-140), 64 B. VF (and FV, which
+ * enters as the VF pair of its target vertex with the normal reversed): indices v f0 f1 f2,
+ * bit 31 of indices[2] set, vec2 = k1 k2 face-bary0 face-bary1. EE: indices a0 a1 b0 b1, bit 31
+ * of indices[3] set, vec2 = k1 k2 edge1-t edge2-t. vec1 = normal xyz, area; vec3 = 0. */
+typedef struct u26_collision_pair
+{
+	uint32_t indices[4];
+	float vec1[4], vec2[4], vec3[4];
+} u26_collision_pair;
+
+/* DEVICE arrays owned by the scene, valid until its next u26_prp_make_response. Region CSRs
+ * use upload_2d_csr_from's layout (buffer_allocator.h:26-59): one array of [n + 1] absolute
+ * offsets followed by the data; region ids 2 contour + mesh role, ascending per row. */
+typedef struct u26_prp_response_view
+{
+	uint32_t num_pairs;
+	const u26_collision_pair* pairs; /* [num_pairs]: contours in order, each contour's hits in order */
+	const uint32_t* pair_info;		 /* [num_pairs][4]: src id, dst id (VF / FV: vertex, face; EE: edge1, edge2),
+									  * packed region 2 (256 contour + solution key) + source role, type (0 VF, 1 FV, 2 EE) */
+	const uint32_t* vert_regions;	 /* [vert_regions_len] */
+	const uint32_t* edge_regions;	 /* [edge_regions_len]: union of the endpoints' regions */
+	const uint32_t* face_regions;	 /* [face_regions_len]: union of the corners' regions */
+	uint32_t vert_regions_len, edge_regions_len, face_regions_len;
+} u26_prp_response_view;
+
+/* out: a finished u26_prp_resolve of this scene (its normals are the scene's current ones).
+ * narrow_list / narrow_indices: optional DEVICE narrow-phase list ([capacity] templates,
+ * [capacity][2] indices) receiving the pairs at [first, first + num_pairs); when
+ * first + num_pairs > capacity nothing is written, view->num_pairs holds the count and
+ * U26_ERR_CAPACITY is returned. Synchronises. */
+U26_API u26_status u26_prp_make_response(u26_scene* scene, const u26_prp_output* out, const u26_prp_response_params* params,
+	u26_collision_pair* narrow_list, uint32_t* narrow_indices, uint32_t first, uint32_t capacity, u26_prp_response_view* view);
+
 /* Differentiation over fixed supports (the torch.autograd binding of the objective; the
  * reference computes dE/dr inside its direction refinement, intersection_resolver2.cpp:
  * 1268-1320, and has no standalone entry point). For each contour c, with support

@@ -167,6 +167,8 @@ def lbvh_query(tree, mode, x0, x1, edges, d_hat, thickness, max_pairs=None):
 
 
 EF_PAIR_DTYPE = np.dtype([("idx", np.uint32, 5), ("bary", np.float32, 3), ("grad", np.float32, 3), ("stiff", np.float32)])
+# CollisionPair::CollisionPairTemplate (collision_data.h:48-140): 64 B
+COLLISION_PAIR_DTYPE = np.dtype([("indices", np.uint32, 4), ("vec1", np.float32, 4), ("vec2", np.float32, 4), ("vec3", np.float32, 4)])
 assert EF_PAIR_DTYPE.itemsize == 48
 
 
@@ -246,7 +248,10 @@ assert RESULT_DTYPE.itemsize == 144 and HIT_DTYPE.itemsize == 48
 class PrpRun:
     """All outputs of one oracle PRP pass."""
 
-    def __init__(self, mesh, ef_pairs, ef_indices, params=None, x=None):
+    def __init__(self, mesh, ef_pairs, ef_indices, params=None, x=None, response=None):
+        """response: (depth_threshold, stiffness) to also assemble the response pairs and the
+        vertex / edge / face region CSRs (attributes response_pairs, response_info,
+        vert_regions, edge_regions, face_regions)."""
         L = lib()
         L.oracle_prp_run.restype = ctypes.c_void_p
         for n in ("oracle_prp_num_pairs", "oracle_prp_num_orig_pairs", "oracle_prp_num_contours", "oracle_prp_contour",
@@ -295,8 +300,40 @@ class PrpRun:
             st = np.zeros(3, np.uint64)
             L.oracle_prp_stats(h, _p(st, _u64p))
             self.tested, self.requests, self.pairs_tested = int(st[0]), int(st[1]), int(st[2])
+            if response is not None:
+                L.oracle_prp_response.restype = ctypes.c_uint32
+                dt, k = ctypes.c_float(response[0]), ctypes.c_float(response[1])
+                lens = np.zeros(3, np.uint32)
+                npairs = L.oracle_prp_response(h, dt, k, None, None, None, None, None, _p(lens, _u32p))
+                self.response_pairs = np.zeros(max(npairs, 1), COLLISION_PAIR_DTYPE)
+                self.response_info = np.zeros((max(npairs, 1), 4), np.uint32)
+                self.vert_regions = np.zeros(lens[0], np.uint32)
+                self.edge_regions = np.zeros(lens[1], np.uint32)
+                self.face_regions = np.zeros(lens[2], np.uint32)
+                L.oracle_prp_response(h, dt, k, self.response_pairs.ctypes.data_as(ctypes.c_void_p), _p(self.response_info, _u32p),
+                                      _p(self.vert_regions, _u32p), _p(self.edge_regions, _u32p), _p(self.face_regions, _u32p), None)
+                self.response_pairs, self.response_info = self.response_pairs[:npairs], self.response_info[:npairs]
         finally:
             L.oracle_prp_free(h)
+
+
+def region_pack(contour, key, mesh):
+    L = lib()
+    L.oracle_region_pack.restype = ctypes.c_uint32
+    return int(L.oracle_region_pack(ctypes.c_uint32(contour), ctypes.c_uint32(key), ctypes.c_uint32(mesh)))
+
+
+def region_semantic(packed):
+    L = lib()
+    L.oracle_region_semantic.restype = ctypes.c_uint32
+    return int(L.oracle_region_semantic(ctypes.c_uint32(packed)))
+
+
+def solution_key(n_src, n_dst, r):
+    L = lib()
+    L.oracle_solution_key.restype = ctypes.c_uint32
+    a, b, c = (np.ascontiguousarray(v, np.float32) for v in (n_src, n_dst, r))
+    return int(L.oracle_solution_key(_p(a, _f32p), _p(b, _f32p), _p(c, _f32p)))
 
 
 def eigen3(S):

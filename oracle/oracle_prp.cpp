@@ -17,6 +17,7 @@
 //   adaptive k-ring       intersection_resolver2.cpp:1058-1230, intersection_resolver2.h:1177-1187
 //   selection             intersection_resolver2.h:807-912, intersection_resolver2.cpp:996-1057
 //   merge / suppression   intersection_resolver2.cpp:413-592, finalize 1956-2103
+//   response + regions    intersection_resolver2.cpp:37-121, 2105-2221, 2296-2427
 //
 // Deviations, all shared with the CUDA path and stated once here:
 //  * The 3x3 symmetric eigen solver (the reference calls Eigen::SelfAdjointEigenSolver::
@@ -2415,6 +2416,182 @@ namespace
 			if (S.suppressed[c])
 				S.selected[c] = ComboInfo{};
 	}
+
+	// ---- response assembly (make_response_from_min_hitinfo, intersection_resolver2.cpp:2105-2221)
+	// and region labels (host_apply_untangling_constraint, intersection_resolver2.cpp:2296-2427)
+	struct PairTemplate // CollisionPair::CollisionPairTemplate, collision_data.h:48-140
+	{
+		uint idx[4];
+		float vec1[4], vec2[4], vec3[4];
+	};
+	struct Response
+	{
+		std::vector<PairTemplate> pairs;
+		std::vector<uint> info; // [pairs][4]: src id, dst id, packed region, type (0 VF, 1 FV, 2 EE)
+		std::vector<uint> vert_csr, edge_csr, face_csr; // upload_2d_csr_from layout, buffer_allocator.h:26-59
+	};
+
+	// prp_classify_hit_solution (intersection_resolver2.cpp:37-107): 3 x sign code of the
+	// source normal's projection on r + the target's; |q| <= 0.1 (or not finite) is 0
+	uint solution_key(V3 n_src, V3 n_dst, V3 r)
+	{
+		const float rl = length(r), sl = length(n_src), dl = length(n_dst);
+		const float sq = rl > 1e-12f && sl > 1e-12f ? dot(n_src / sl, r / rl) : 0.0f;
+		const float dq = rl > 1e-12f && dl > 1e-12f ? dot(n_dst / dl, r / rl) : 0.0f;
+		auto code = [](float q)
+		{
+			if (!std::isfinite(q) || std::fabs(q) <= 0.1f)
+				return 1u;
+			return q > 0.0f ? 2u : 0u;
+		};
+		return 3u * code(sq) + code(dq);
+	}
+
+	// region label of a response pair: 2 (256 contour + solution key) + source mesh role
+	// (prp_pack_response_region_label, intersection_resolver2.cpp:112-121). The ray casts
+	// create every hit with source role 0 (cached_bvh.cpp:271-277, 513).
+	inline uint pack_region(uint contour, uint key, uint mesh) { return 2u * (256u * contour + (key & 255u)) + (mesh & 1u); }
+	inline uint semantic_region(uint packed) { return 2u * ((packed >> 1) / 256u) + (packed & 1u); }
+
+	std::vector<uint> csr_of(const std::vector<std::vector<uint>>& rows)
+	{
+		const uint n = uint(rows.size());
+		std::vector<uint> out(n + 1);
+		uint at = n + 1;
+		for (uint i = 0; i < n; i++)
+		{
+			out[i] = at;
+			at += uint(rows[i].size());
+		}
+		out[n] = at;
+		for (const auto& r : rows)
+			out.insert(out.end(), r.begin(), r.end());
+		return out;
+	}
+
+	Response make_response(const Scene& S, float depth_threshold, float stiffness)
+	{
+		const MeshIn& m = S.m;
+		Response R;
+		for (uint c = 0; c < uint(S.selected.size()); c++)
+		{
+			const ComboInfo& ci = S.selected[c];
+			const float C = std::max(-ci.depth - 3e-3f, -depth_threshold);
+			for (const Hit& h : ci.hits)
+			{
+				PairTemplate t{};
+				V3 n_src, n_dst, normal = ci.dir;
+				float a_src, a_dst;
+				uint type;
+				if (h.type == VF)
+				{
+					n_src = S.vn[h.src_id];
+					n_dst = S.fn[h.dst_id];
+					a_src = m.rest_vert_area[h.src_id];
+					a_dst = m.rest_face_area[h.dst_id];
+					type = 0;
+				}
+				else if (h.type == FV)
+				{
+					n_src = S.fn[h.src_id];
+					n_dst = S.vn[h.dst_id];
+					a_src = m.rest_face_area[h.src_id];
+					a_dst = m.rest_vert_area[h.dst_id];
+					type = 1;
+				}
+				else
+				{
+					n_src = S.en[h.src_id];
+					n_dst = S.en[h.dst_id];
+					a_src = m.rest_edge_area[h.src_id];
+					a_dst = m.rest_edge_area[h.dst_id];
+					type = 2;
+				}
+				const uint region = pack_region(c, solution_key(n_src, n_dst, ci.dir), 0u);
+				const float area = std::max(0.5f * (a_src + a_dst), 3e-6f);
+				const float stiff = area * stiffness;
+				float k1 = stiff * C, k2 = stiff;
+				if (type == 0 && (!std::isfinite(k1) || !std::isfinite(k2)))
+					k1 = k2 = 0.0f;
+				if (type == 0)
+				{
+					t.idx[0] = h.sv[0];
+					t.idx[1] = h.dv[0];
+					t.idx[2] = h.dv[1] | 0x80000000u;
+					t.idx[3] = h.dv[2];
+				}
+				else if (type == 1)
+				{
+					// the FV pair enters as a VF pair of the target vertex, normal reversed
+					t.idx[0] = h.dv[0];
+					t.idx[1] = h.sv[0];
+					t.idx[2] = h.sv[1] | 0x80000000u;
+					t.idx[3] = h.sv[2];
+					normal = -1.0f * normal;
+				}
+				else
+				{
+					t.idx[0] = h.sv[0];
+					t.idx[1] = h.sv[1];
+					t.idx[2] = h.dv[0];
+					t.idx[3] = h.dv[1] | 0x80000000u;
+				}
+				t.vec1[0] = normal.x;
+				t.vec1[1] = normal.y;
+				t.vec1[2] = normal.z;
+				t.vec1[3] = area;
+				t.vec2[0] = k1;
+				t.vec2[1] = k2;
+				t.vec2[2] = h.bary[0];
+				t.vec2[3] = h.bary[1];
+				R.pairs.push_back(t);
+				const uint info[4] = { type == 2 ? h.src_id : h.vid(), type == 2 ? h.dst_id : h.fid(), region, type };
+				R.info.insert(R.info.end(), info, info + 4);
+			}
+		}
+		// vertex regions: each pair's 4 vertices (source side: its semantic region, target
+		// side: the other mesh role) and each EF pair's edge / face vertices
+		std::vector<std::vector<uint>> vr(m.num_verts), er(m.num_edges), fr(m.num_faces);
+		for (size_t i = 0; i < R.pairs.size(); i++)
+		{
+			const uint r = semantic_region(R.info[4 * i + 2]), type = R.info[4 * i + 3];
+			const uint lab[3][4] = { { r, r ^ 1u, r ^ 1u, r ^ 1u }, { r ^ 1u, r, r, r }, { r, r, r ^ 1u, r ^ 1u } };
+			for (int k = 0; k < 4; k++)
+				vr[R.pairs[i].idx[k] & 0x7fffffffu].push_back(lab[type][k]);
+		}
+		for (size_t p = 0; p < S.ef.size(); p++)
+		{
+			const uint er_ = 2u * S.contour_index[p] + S.mesh_index[p], fr_ = er_ ^ 1u;
+			const uint e = S.ef_e[p], f = S.ef_f[p];
+			vr[edge_of(m, e, 0)].push_back(er_);
+			vr[edge_of(m, e, 1)].push_back(er_);
+			for (int k = 0; k < 3; k++)
+				vr[face_of(m, f, k)].push_back(fr_);
+		}
+		for (auto& r : vr)
+		{
+			std::sort(r.begin(), r.end());
+			r.erase(std::unique(r.begin(), r.end()), r.end());
+		}
+		for (uint f = 0; f < m.num_faces; f++)
+		{
+			std::set<uint> u;
+			for (int k = 0; k < 3; k++)
+				u.insert(vr[face_of(m, f, k)].begin(), vr[face_of(m, f, k)].end());
+			fr[f].assign(u.begin(), u.end());
+		}
+		for (uint e = 0; e < m.num_edges; e++)
+		{
+			std::set<uint> u;
+			for (int k = 0; k < 2; k++)
+				u.insert(vr[edge_of(m, e, k)].begin(), vr[edge_of(m, e, k)].end());
+			er[e].assign(u.begin(), u.end());
+		}
+		R.vert_csr = csr_of(vr);
+		R.edge_csr = csr_of(er);
+		R.face_csr = csr_of(fr);
+		return R;
+	}
 } // namespace
 
 // ---- C ABI of the oracle (ctypes) --------------------------------------------------
@@ -2570,6 +2747,37 @@ extern "C"
 		out2[0] = S->tested;
 		out2[1] = S->requests;
 		out2[2] = S->pairs;
+	}
+	// response pairs and region CSRs of a finished run; returns the pair count. Any output
+	// may be null (sizes: pairs 64 B each, info 4 words each, CSRs *_len words).
+	uint oracle_prp_response(void* h, float depth_threshold, float stiffness, void* pairs, uint* info, uint* vert_csr, uint* edge_csr,
+		uint* face_csr, uint* lens3)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		const Response R = make_response(*S, depth_threshold, stiffness);
+		if (pairs)
+			std::memcpy(pairs, R.pairs.data(), R.pairs.size() * sizeof(PairTemplate));
+		if (info)
+			std::copy(R.info.begin(), R.info.end(), info);
+		if (vert_csr)
+			std::copy(R.vert_csr.begin(), R.vert_csr.end(), vert_csr);
+		if (edge_csr)
+			std::copy(R.edge_csr.begin(), R.edge_csr.end(), edge_csr);
+		if (face_csr)
+			std::copy(R.face_csr.begin(), R.face_csr.end(), face_csr);
+		if (lens3)
+		{
+			lens3[0] = uint(R.vert_csr.size());
+			lens3[1] = uint(R.edge_csr.size());
+			lens3[2] = uint(R.face_csr.size());
+		}
+		return uint(R.pairs.size());
+	}
+	uint oracle_region_pack(uint contour, uint key, uint mesh) { return pack_region(contour, key, mesh); }
+	uint oracle_region_semantic(uint packed) { return semantic_region(packed); }
+	uint oracle_solution_key(const float* n_src, const float* n_dst, const float* r)
+	{
+		return solution_key(v3(n_src[0], n_src[1], n_src[2]), v3(n_dst[0], n_dst[1], n_dst[2]), v3(r[0], r[1], r[2]));
 	}
 	void oracle_eigen3(const float* S9, float* out9)
 	{

@@ -72,6 +72,7 @@ _SIGS = {
     "u26_prp_output_destroy": (None, [c_vp]),
     "u26_ef_canonicalize": (c_int, [c_vp, c_u32, c_vp, c_vp, c_u32, c_u32]),
     "u26_prp_adjoint": (c_int, [c_vp, c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
+    "u26_prp_make_response": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_u32, c_vp]),
 }
 
 

@@ -2936,6 +2936,8 @@ struct u26_scene
 	bool otrees_built = false;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
+	uint64_t passes = 0;			  // completed u26_prp_resolve calls (the normals d_fn / d_en / d_vn are the last one's)
+	ResponseState resp;
 };
 
 struct u26_prp_output
@@ -2950,6 +2952,8 @@ struct u26_prp_output
 	double stage_ms[8] = { 0 };
 	double gpu_ms[6] = { 0 };
 	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0;
+	const u26_scene* scene = nullptr; // the pass this output came from
+	uint64_t pass = 0;
 };
 
 template <typename T>
@@ -3129,6 +3133,7 @@ U26_API void u26_scene_destroy(u26_scene* s)
 	s->esorter.release();
 	s->csorter.release();
 	s->fvsorter.release();
+	s->resp.release();
 	for (u26_lbvh* t : s->otree_f)
 		u26_lbvh_destroy(t);
 	for (u26_lbvh* t : s->otree_e)
@@ -4732,7 +4737,59 @@ U26_API u26_status u26_prp_resolve(u26_scene* scene, u26_lbvh* face_tree, u26_lb
 	const u26_status s = prp_run(scene, face_tree, edge_tree, x, ef_pairs, ef_indices, num_pairs, params, o.get());
 	if (s != U26_OK)
 		return s;
+	o->scene = scene;
+	o->pass = ++scene->passes;
 	*out = o.release();
+	return U26_OK;
+}
+
+U26_API u26_status u26_prp_make_response(u26_scene* scene, const u26_prp_output* o, const u26_prp_response_params* params,
+	u26_collision_pair* narrow_list, uint32_t* narrow_indices, uint32_t first, uint32_t capacity, u26_prp_response_view* view)
+{
+	if (!scene || !o || !params || !view)
+		return U26_ERR_INVALID_INPUT;
+	u26_ctx* ctx = scene->ctx;
+	if (o->scene != scene || o->pass != scene->passes)
+		return set_error(ctx, U26_ERR_INVALID_INPUT, "u26_prp_make_response: the output is not this scene's latest pass");
+	if ((narrow_list == nullptr) != (narrow_indices == nullptr))
+		return set_error(ctx, U26_ERR_INVALID_INPUT, "u26_prp_make_response: give both narrow-phase arrays or neither");
+	*view = u26_prp_response_view{};
+	const uint32_t nh = uint32_t(o->hits.size());
+	view->num_pairs = nh;
+	if (narrow_list && (first > capacity || nh > capacity - first))
+		return set_error(ctx, U26_ERR_CAPACITY, "u26_prp_make_response: narrow-phase list holds %u, needs %u", capacity, first + nh);
+	ResponseInputs in{};
+	in.hits = o->hits.data();
+	in.hit_off = o->hit_offsets.data();
+	in.results = o->results.data();
+	in.pair_idx = o->pair_idx.data();
+	in.mesh_index = o->mesh_index.data();
+	in.contour_index = o->contour_index.data();
+	in.nh = nh;
+	in.nc = uint32_t(o->results.size());
+	in.np = uint32_t(o->mesh_index.size());
+	in.nv = scene->nv;
+	in.ne = scene->ne;
+	in.nf = scene->nf;
+	in.fn = scene->d_fn.as<float>();
+	in.en = scene->d_en.as<float>();
+	in.vn = scene->d_vn.as<float>();
+	in.va = scene->d_varea.as<float>();
+	in.ea = scene->d_earea.as<float>();
+	in.fa = scene->d_farea.as<float>();
+	in.edges = scene->d_edges.as<uint2>();
+	in.faces = scene->d_faces.as<uint32_t>();
+	ResponseState& R = scene->resp;
+	U26_TRY(response_run(ctx, in, params->depth_threshold, params->stiffness, R, narrow_list ? narrow_list + first : nullptr,
+		narrow_indices ? narrow_indices + 2 * size_t(first) : nullptr));
+	view->pairs = R.pairs.as<u26_collision_pair>();
+	view->pair_info = R.info.as<uint32_t>();
+	view->vert_regions = R.vcsr.as<uint32_t>();
+	view->edge_regions = R.ecsr.as<uint32_t>();
+	view->face_regions = R.fcsr.as<uint32_t>();
+	view->vert_regions_len = R.vert_len;
+	view->edge_regions_len = R.edge_len;
+	view->face_regions_len = R.face_len;
 	return U26_OK;
 }
 

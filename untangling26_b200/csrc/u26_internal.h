@@ -98,6 +98,36 @@ namespace u26
 			scan_tmp.release();
 		}
 	};
+
+	// Response assembly of one PRP pass (response.cu): host-side results of the pass and the
+	// scene's device tables.
+	struct ResponseInputs
+	{
+		const u26_prp_hit* hits; // host [nh], contour order
+		const uint32_t* hit_off; // host [nc + 1]
+		const u26_prp_result* results; // host [nc]: dir, depth
+		const uint32_t *pair_idx, *mesh_index, *contour_index; // host EF pairs [np]
+		uint32_t nh, nc, np, nv, ne, nf;
+		const float *fn, *en, *vn, *va, *ea, *fa; // device normals and rest areas
+		const uint2* edges;
+		const uint32_t* faces;
+	};
+	struct ResponseState
+	{
+		DevBuf hits, off, cinfo, efp, pairs, info, keys, ukeys, vals, flags, voff, ecnt, fcnt, vcsr, ecsr, fcsr, scan_tmp;
+		RadixSorter sorter;
+		uint32_t num_pairs = 0, vert_len = 0, edge_len = 0, face_len = 0;
+		void release()
+		{
+			DevBuf* b[] = { &hits, &off, &cinfo, &efp, &pairs, &info, &keys, &ukeys, &vals, &flags, &voff, &ecnt, &fcnt, &vcsr, &ecsr, &fcsr, &scan_tmp };
+			for (DevBuf* x : b)
+				x->release();
+			sorter.release();
+		}
+	};
+	// narrow / narrow_idx: optional narrow-phase list slots (already offset to the first free one)
+	u26_status response_run(u26_ctx* ctx, const ResponseInputs& in, float depth_threshold, float stiffness, ResponseState& R,
+		u26_collision_pair* narrow, uint32_t* narrow_idx);
 } // namespace u26
 
 #define U26_TRY(expr)                   \

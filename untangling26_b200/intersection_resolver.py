@@ -12,6 +12,7 @@ EF pairs come back as a structured numpy array with the reference's 48-byte EfPa
 layout (collision_data.h:150-220) and (eid, fid) indices, in canonical (eid, fid) order.
 """
 import ctypes
+import time
 
 import numpy as np
 import torch
@@ -158,10 +159,13 @@ class CollisionScene:
             self.prp_scene = h
             self._desc = desc
 
-    def host_resolve(self, params=None, num_pairs=None):
+    def host_resolve(self, params=None, num_pairs=None, response=None, narrow_list=None, narrow_indices=None, first=0):
         """PRP pass over the canonical EF list of the last detection (call ef_pairs() or
-        canonicalize first). Returns a PrpResult."""
-        from .prp import PrpResult, prp_params
+        canonicalize first). Returns a PrpResult. response: ResponseParams to also assemble
+        the response pairs and region CSRs (result.response, a PrpResponse); narrow_list
+        ([capacity, 16] int32) / narrow_indices ([capacity, 2] int32) receive the pairs at
+        [first, first + n) after the penalty pairs (upload_response_pairs_to_gpu)."""
+        from .prp import PrpResponse, PrpResult, ResponseView, prp_params
         self._ensure_prp_scene()
         params = params or prp_params()
         n = int(self.resolver.ef_count.item()) if num_pairs is None else num_pairs
@@ -172,16 +176,29 @@ class CollisionScene:
             self.prp_scene, self.face_tree.handle, self.edge_tree.handle, ptr(self.x), ptr(self.resolver.ef_list),
             ptr(self.resolver.ef_indices), n, ctypes.byref(params), ctypes.byref(out)), "prp_resolve")
         try:
-            return PrpResult(self.ctx.lib, out)
+            res = PrpResult(self.ctx.lib, out)
+            if response is not None:
+                view = ResponseView()
+                cap = 0 if narrow_list is None else int(narrow_list.shape[0])
+                if narrow_list is not None and (narrow_indices is None or int(narrow_indices.shape[0]) != cap):
+                    raise ValueError("narrow_indices must match narrow_list")
+                t0 = time.perf_counter()
+                self.ctx.check(self.ctx.lib.u26_prp_make_response(
+                    self.prp_scene, out, ctypes.byref(response), ptr(narrow_list) if narrow_list is not None else None,
+                    ptr(narrow_indices) if narrow_indices is not None else None, first, cap, ctypes.byref(view)), "prp_make_response")
+                ms = (time.perf_counter() - t0) * 1e3  # the call synchronises
+                res.response = PrpResponse(view, self.x.device)
+                res.response.ms = ms
+            return res
         finally:
             self.ctx.lib.u26_prp_output_destroy(out)
 
-    def untangle_pass(self, params=None):
+    def untangle_pass(self, params=None, response=None, **narrow):
         """One untangling pass at the current positions: refit, fused EF detection,
-        canonical EF order, PRP contour evaluation."""
+        canonical EF order, PRP contour evaluation (and, with response, its response pairs)."""
         self.detect_ef_fused()
         n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
-        return self.host_resolve(params, num_pairs=n)
+        return self.host_resolve(params, num_pairs=n, response=response, **narrow)
 
     def close(self):
         if getattr(self, "prp_scene", None) is not None:

@@ -74,6 +74,66 @@ class PrpOutputView(ctypes.Structure):
 
 GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
 
+# CollisionPair::CollisionPairTemplate (collision_data.h:48-140), u26_collision_pair: 64 B
+COLLISION_PAIR_DTYPE = np.dtype([("indices", np.uint32, 4), ("vec1", np.float32, 4), ("vec2", np.float32, 4), ("vec3", np.float32, 4)])
+
+
+class ResponseParams(ctypes.Structure):
+    """untangling_response_depth and stiffness_untangling (scene_params.h:66, 121-122)."""
+    _fields_ = [("depth_threshold", ctypes.c_float), ("stiffness", ctypes.c_float)]
+
+
+def response_params(depth_threshold=3e-3, stiffness=1e8):
+    return ResponseParams(depth_threshold, stiffness)
+
+
+class ResponseView(ctypes.Structure):
+    _fields_ = [
+        ("num_pairs", c_u32), ("pairs", c_vp), ("pair_info", c_vp), ("vert_regions", c_vp), ("edge_regions", c_vp),
+        ("face_regions", c_vp), ("vert_regions_len", c_u32), ("edge_regions_len", c_u32), ("face_regions_len", c_u32),
+    ]
+
+
+class _DeviceWords:
+    """__cuda_array_interface__ over words of device memory owned by the library."""
+
+    def __init__(self, p, count):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<i4", "data": (p or 0, False), "version": 3}
+
+
+def _device_words(torch, p, count, device):
+    if count == 0 or not p:
+        return torch.zeros(0, dtype=torch.int32, device=device)
+    return torch.as_tensor(_DeviceWords(p, count), device=device).clone()
+
+
+class PrpResponse:
+    """Response pairs and region CSRs of one pass as device tensors (int32 words):
+    pairs [n, 16] (u26_collision_pair), info [n, 4] (src, dst, packed region, type), and the
+    vertex / edge / face region arrays in upload_2d_csr_from's layout."""
+
+    def __init__(self, view, device):
+        import torch
+        n = view.num_pairs
+        self.num_pairs = n
+        self.pairs = _device_words(torch, view.pairs, 16 * n, device).view(-1, 16)
+        self.info = _device_words(torch, view.pair_info, 4 * n, device).view(-1, 4)
+        self.vert_regions = _device_words(torch, view.vert_regions, view.vert_regions_len, device)
+        self.edge_regions = _device_words(torch, view.edge_regions, view.edge_regions_len, device)
+        self.face_regions = _device_words(torch, view.face_regions, view.face_regions_len, device)
+
+    def host_pairs(self):
+        return self.pairs.cpu().numpy().view(np.uint32).copy().view(COLLISION_PAIR_DTYPE).reshape(-1)
+
+    @staticmethod
+    def csr_rows(arr):
+        """[rows] of a upload_2d_csr_from array (host numpy)."""
+        a = np.asarray(arr, np.uint32)
+        if len(a) == 0:
+            return []
+        n = int(a[0]) - 1
+        return [a[a[i]:a[i + 1]] for i in range(n)]
+
 
 def _host_array(p, count, dtype):
     if count == 0 or not p:
