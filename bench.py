@@ -217,6 +217,64 @@ def reference_arm(args, mesh, config):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def _pair_filter_block(sc, mesh, dev, flush, stream, response, num_ef, peak, steps=5):
+    import torch
+    nv = mesh.num_verts
+    dh = torch.full((nv,), 2e-3, dtype=torch.float32, device=dev)
+    cap = 16 * nv
+    cnt = torch.zeros(1, dtype=torch.int32, device=dev)
+    vfl = torch.zeros((cap, 2), dtype=torch.int32, device=dev)
+    sc.face_tree.broad_phase_query_from_verts(sc.x, sc.x, cnt, vfl, dh, sc.thickness)
+    nvf = min(int(cnt.item()), cap)
+    cnt.zero_()
+    eel = torch.zeros((cap, 2), dtype=torch.int32, device=dev)
+    sc.edge_tree.broad_phase_query_from_edges(sc.x, sc.x, sc.edges, cnt, eel, dh, sc.thickness)
+    nee = min(int(cnt.item()), cap)
+    vf, ee = vfl[:nvf], eel[:nee]
+    bit = torch.tensor(-2 ** 31, dtype=torch.int32, device=dev)
+    fv = sc.faces[vf[:, 1].long()]
+    ea, eb = sc.edges[ee[:, 0].long()], sc.edges[ee[:, 1].long()]
+    idx = torch.cat([torch.stack([vf[:, 0], fv[:, 0], fv[:, 1] | bit, fv[:, 2]], 1),
+                     torch.stack([ea[:, 0], ea[:, 1], eb[:, 0], eb[:, 1] | bit], 1)])
+    n = nvf + nee
+    vec = torch.zeros((n, 12), dtype=torch.float32, device=dev)
+    vec[:, 2] = 1.0
+    vec[:, 4], vec[:, 5] = -1e3, 1e5
+    vec[:nvf, 6], vec[:nvf, 7] = 1.0 / 3.0, 1.0 / 3.0
+    vec[nvf:, 6], vec[nvf:, 7] = 0.5, 0.5
+    pairs0 = torch.cat([idx, vec.view(torch.int32)], 1).contiguous()
+    pidx = torch.cat([vf, ee]).contiguous()
+    offset = torch.full((nv,), 1e-3, dtype=torch.float32, device=dev)
+    vf0, ee0 = vf.clone(), ee.clone()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    pairs = torch.empty_like(pairs0)
+    inv = torch.zeros(nv, dtype=torch.int32, device=dev)
+    for i in range(steps + 1):
+        pairs.copy_(pairs0)
+        vf.copy_(vf0)
+        ee.copy_(ee0)
+        inv.zero_()
+        flush.fill_((i + 3) & 0xFF)
+        if i:
+            evs[i - 1][0].record(stream)
+        sc.filter_invalid_pairs(pairs, pidx, n, offset, inv, response=response, num_ef=num_ef)
+        sc.filter_broad_phase_pairs(vf, nvf, ee, nee, inv, response, num_ef=num_ef)
+        if i:
+            evs[i - 1][1].record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.median(a.elapsed_time(b) for a, b in evs)
+    byts = n * (64 + 48 + 8) + n * (64 + 8 + 16 + 16) + nvf * (8 + 12 + 16 + 16 + 8) + nee * (8 + 16 + 16 + 16 + 8)
+    disabled = int((pairs[:, 5].view(torch.float32) == 0).sum().item())
+    flagged = int(((vf[:, 0] >> 30) != 0).sum().item() + ((ee[:, 0] >> 30) != 0).sum().item())
+    out = {"kernels": ["identify_invalid_kernel", "filter_pairs_kernel", "filter_broad_vf_kernel", "filter_broad_ee_kernel"],
+           "proximity_pairs": n, "broad_vf": nvf, "broad_ee": nee, "disabled": disabled, "flagged_broad": flagged,
+           "invalid_verts": int(inv.sum().item()), "ms": ms, "algorithmic_bytes": byts,
+           "achieved": byts / (ms / 1e3) / 1e9, "unit": "GB/s", "peak": peak,
+           "note": "proximity / CCD pairs within 2 mm from the scene trees, offsets 1 mm; median of 5, L2 flushed"}
+    out["frac"] = out["achieved"] / peak
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -364,6 +422,15 @@ def main():
             "region_words": [int(rr.vert_regions.numel()), int(rr.edge_regions.numel()), int(rr.face_regions.numel())],
             "note": "host wall time of u26_prp_make_response (hit upload, 12 launches, 3 synchronisations)"}
 
+    # ---- region-based pair filtering on this pass's regions: proximity VF / EE pairs within
+    # 2 mm from the scene trees (as narrow-phase templates) through u26_filter_invalid_pairs,
+    # the same pairs as CCD broad-phase lists through u26_filter_broad_phase_pairs; L2 flushed
+    # before each call pair. Algorithmic bytes: per proximity pair 64 B template + 48 B
+    # positions + 8 B offsets (marking), then 64 B template + 8 B indices + 16 B marks +
+    # 16 B region offsets (filter); per broad pair 8 B ids + 12 / 16 B primitive + 16 B marks
+    # + 16 B region offsets + 8 B write.
+    pf = _pair_filter_block(sc, mesh, dev, flush, stream, rr, n_ef, peak)
+
     # ---- LBVH refit: the fused leaf update + bottom-up refit of the face tree alone, L2
     # flushed before every launch. Algorithmic bytes (each byte once): V x (12 B position +
     # 4 B thickness) + F x (12 B face + 4 B leaf order + 32 B leaf box write) + (F - 1) x
@@ -463,6 +530,7 @@ def main():
             "untangle_passes_per_s": 1e3 * args.steps / total_ms,
             "plain_form": plain,
             "response": resp,
+            "pair_filter": pf,
             "gpu_launches": int(launches), "roofline": roof, "lbvh_refit": refit, "clocks": clk,
             "pass": {"ef_pairs": n_ef, "contours": len(r0.contours), "processed": int(len(proc)),
                      "responses": int((proc["combo_idx"] != 0xFFFFFFFF).sum()), "levels": r0.levels,

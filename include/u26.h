@@ -346,6 +346,32 @@ typedef struct u26_prp_response_view
 U26_API u26_status u26_prp_make_response(u26_scene* scene, const u26_prp_output* out, const u26_prp_response_params* params,
 	u26_collision_pair* narrow_list, uint32_t* narrow_indices, uint32_t first, uint32_t capacity, u26_prp_response_view* view);
 
+/* ---- region-based pair filtering ----------------------------------------------------
+ * The contour regions of a pass (u26_prp_response_view's CSRs) applied to the solver's contact
+ * pairs. Region match of two primitives (fn_is_matched_invalid_region, intersection_resolver.cpp:
+ * 2232-2337): 1 when a region of the first is the opposite side (id ^ 1) of a region of the
+ * second; VF pairs compare the vertex row with the face row, EE pairs the two edge rows.
+ *
+ * IntersectionResolver::filter_invalid_pairs (intersection_resolver.cpp:2635-2676): over the
+ * proximity pairs [0, num_proximity_pairs) of the DEVICE narrow-phase list, a pair with
+ * |sum_k w_k x_k|^2 < (vert_offset[i0] + vert_offset[i2])^2 + 1e-10 sets vert_is_invalid on its
+ * vertices; then every pair touching an invalid vertex, or (region arrays given: the reference's
+ * use_untangling with a non-empty region list) whose region match is 1, gets k1 = k2 = 0.
+ * Does nothing when num_ef == 0. vert_is_invalid [num_verts] is the caller's (zeroed at EF
+ * detection, intersection_resolver.cpp:384); template slots with an index >= num_verts (the ~0
+ * placeholder of VV / VE pairs) are skipped. */
+U26_API u26_status u26_filter_invalid_pairs(u26_ctx* ctx, u26_collision_pair* narrow_list, const uint32_t* narrow_indices,
+	uint32_t num_proximity_pairs, uint32_t num_ef, const float* x, const float* vert_offset, uint32_t num_verts, uint32_t* vert_is_invalid,
+	const uint32_t* vert_regions, const uint32_t* edge_regions, const uint32_t* face_regions);
+
+/* IntersectionResolver::filter_broad_phase_pairs (intersection_resolver.cpp:2586-2633): the CCD
+ * broad-phase lists (DEVICE [n][2]: VF (vid, fid), EE (eid1, eid2)) get bit 31 on both ids when
+ * the pair's region match is 1 and bit 30 when one of its four vertices is invalid. Does nothing
+ * when num_ef == 0 or there are no regions (vert_regions NULL). */
+U26_API u26_status u26_filter_broad_phase_pairs(u26_ctx* ctx, uint32_t* vf_list, uint32_t num_vf, uint32_t* ee_list, uint32_t num_ee,
+	uint32_t num_ef, const uint32_t* vert_is_invalid, const uint32_t* vert_regions, const uint32_t* edge_regions,
+	const uint32_t* face_regions, const uint32_t* faces, const uint32_t* edges);
+
 /* Differentiation over fixed supports (the torch.autograd binding of the objective; the
  * reference computes dE/dr inside its direction refinement, intersection_resolver2.cpp:
  * 1268-1320, and has no standalone entry point). For each contour c, with support

@@ -336,6 +336,46 @@ def solution_key(n_src, n_dst, r):
     return int(L.oracle_solution_key(_p(a, _f32p), _p(b, _f32p), _p(c, _f32p)))
 
 
+def region_match(lcsr, l, rcsr, r):
+    """fn_is_matched_invalid_region of rows l (of lcsr) and r (of rcsr): 0 / 1 / 2."""
+    L = lib()
+    L.oracle_region_match.restype = ctypes.c_uint32
+    a = np.ascontiguousarray(lcsr, np.uint32)
+    b = np.ascontiguousarray(rcsr, np.uint32)
+    return int(L.oracle_region_match(_p(a, _u32p), ctypes.c_uint32(l), _p(b, _u32p), ctypes.c_uint32(r)))
+
+
+def filter_invalid_pairs(pairs, pair_indices, num_ef, x, offset, invalid, regions=None):
+    """IntersectionResolver::filter_invalid_pairs over the proximity pairs; returns the
+    filtered (pairs, invalid) copies. regions: (vert, edge, face) CSR arrays or None."""
+    L = lib()
+    pairs = np.ascontiguousarray(pairs).copy()
+    pidx = np.ascontiguousarray(pair_indices, np.uint32)
+    x = np.ascontiguousarray(x, np.float32)
+    off = np.ascontiguousarray(offset, np.float32)
+    inv = np.ascontiguousarray(invalid, np.uint32).copy()
+    rg = [None, None, None] if regions is None else [np.ascontiguousarray(a, np.uint32) for a in regions]
+    L.oracle_filter_invalid_pairs(pairs.ctypes.data_as(ctypes.c_void_p), _p(pidx, _u32p), ctypes.c_uint32(len(pairs)),
+                                  ctypes.c_uint32(num_ef), _p(x, _f32p), _p(off, _f32p), ctypes.c_uint32(len(inv)), _p(inv, _u32p),
+                                  *[(_p(a, _u32p) if a is not None else None) for a in rg])
+    return pairs, inv
+
+
+def filter_broad_phase(vf, ee, num_ef, invalid, regions, faces, edges):
+    """IntersectionResolver::filter_broad_phase_pairs; returns flagged copies of the lists."""
+    L = lib()
+    vf = np.ascontiguousarray(vf, np.uint32).copy()
+    ee = np.ascontiguousarray(ee, np.uint32).copy()
+    inv = np.ascontiguousarray(invalid, np.uint32)
+    rg = [None, None, None] if regions is None else [np.ascontiguousarray(a, np.uint32) for a in regions]
+    f = np.ascontiguousarray(faces, np.uint32)
+    e = np.ascontiguousarray(edges, np.uint32)
+    L.oracle_filter_broad_phase(_p(vf, _u32p), ctypes.c_uint32(len(vf)), _p(ee, _u32p), ctypes.c_uint32(len(ee)),
+                                ctypes.c_uint32(num_ef), _p(inv, _u32p), *[(_p(a, _u32p) if a is not None else None) for a in rg],
+                                _p(f, _u32p), _p(e, _u32p))
+    return vf, ee
+
+
 def eigen3(S):
     S = np.ascontiguousarray(np.asarray(S, np.float32).T)  # columns
     out = np.zeros(9, np.float32)

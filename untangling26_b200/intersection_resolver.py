@@ -200,6 +200,30 @@ class CollisionScene:
         n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
         return self.host_resolve(params, num_pairs=n, response=response, **narrow)
 
+    # ---- region-based pair filtering (IntersectionResolver::filter_invalid_pairs /
+    # filter_broad_phase_pairs, intersection_resolver.cpp:2586-2676): the contour regions of
+    # the last pass's response applied to the solver's contact pairs
+    def _num_ef(self, num_ef):
+        return int(self.resolver.ef_count.item()) if num_ef is None else num_ef
+
+    def filter_invalid_pairs(self, narrow_list, narrow_indices, num_proximity_pairs, vert_offset, vert_is_invalid,
+                             response=None, num_ef=None):
+        """Disable (k1 = k2 = 0) the proximity pairs [0, num_proximity_pairs) of the device
+        narrow-phase list ([n, 16] int32 templates, [n, 2] indices) that touch a vertex made
+        invalid by a too-close proximity pair or, with a PrpResponse, whose region match is 1."""
+        rg = (None, None, None) if response is None else (response.vert_regions, response.edge_regions, response.face_regions)
+        self.ctx.check(self.ctx.lib.u26_filter_invalid_pairs(
+            self.ctx.handle, ptr(narrow_list), ptr(narrow_indices), num_proximity_pairs, self._num_ef(num_ef), ptr(self.x),
+            ptr(vert_offset), self.mesh.num_verts, ptr(vert_is_invalid), *[ptr(t) for t in rg]), "filter_invalid_pairs")
+
+    def filter_broad_phase_pairs(self, vf_list, num_vf, ee_list, num_ee, vert_is_invalid, response, num_ef=None):
+        """Flag the CCD broad-phase VF / EE lists ([n, 2] int32): bit 31 region match,
+        bit 30 an invalid vertex."""
+        rg = (None, None, None) if response is None else (response.vert_regions, response.edge_regions, response.face_regions)
+        self.ctx.check(self.ctx.lib.u26_filter_broad_phase_pairs(
+            self.ctx.handle, ptr(vf_list), num_vf, ptr(ee_list), num_ee, self._num_ef(num_ef), ptr(vert_is_invalid),
+            *[ptr(t) for t in rg], ptr(self.faces), ptr(self.edges)), "filter_broad_phase_pairs")
+
     def close(self):
         if getattr(self, "prp_scene", None) is not None:
             self.ctx.lib.u26_scene_destroy(self.prp_scene)
