@@ -151,9 +151,9 @@ U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint
 	const uint32_t* edge_order, uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices, uint32_t max_ef,
 	uint64_t* stats);
 
-/* Canonical EF order on the device: sort by (eid, fid) — the order
- * host_preprocess_ef_pairs establishes (intersection_resolver.cpp:693-726). count is a
- * host value; num_edges/num_faces bound the key. Pairs and indices are permuted in place. */
+/* Canonical EF order on the device: sort by (eid, fid), equal keys by memcmp of the 48-byte
+ * records — the order host_preprocess_ef_pairs establishes (intersection_resolver.cpp:693-726).
+ * count is a host value; num_edges/num_faces bound the key. Pairs and indices are permuted in place. */
 U26_API u26_status u26_ef_canonicalize(u26_ctx* ctx, uint32_t count, void* ef_pairs, uint32_t* ef_indices,
 	uint32_t num_edges, uint32_t num_faces);
 
@@ -233,6 +233,9 @@ typedef struct u26_prp_params
 	uint32_t solid_all;			/* PRP_solid_interior_adjacency_all_meshes (0): treat every mesh as solid */
 	float solid_eps_n;			/* PRP_solid_interior_adjacency_normal_eps (1e-4) */
 	float solid_eps_d;			/* PRP_solid_interior_adjacency_dist_eps (1e-5) */
+	uint32_t ignore_near_zero_dist_pairs; /* ignore_near_zero_dist_pairs (1, scene_params.h:55; the CLI sets 0):
+										   * 0 drops degenerate EF pairs (a barycentric coordinate < 1e-4) that
+										   * have no non-degenerate adjacent pair (intersection_resolver.cpp:841-896) */
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:
@@ -345,6 +348,20 @@ typedef struct u26_prp_response_view
  * U26_ERR_CAPACITY is returned. Synchronises. */
 U26_API u26_status u26_prp_make_response(u26_scene* scene, const u26_prp_output* out, const u26_prp_response_params* params,
 	u26_collision_pair* narrow_list, uint32_t* narrow_indices, uint32_t first, uint32_t capacity, u26_prp_response_view* view);
+
+/* Near-zero-distance proximity pairs as EF pairs (fn_add_ef_from_proximity_pairs,
+ * intersection_resolver.cpp:199-363; run by ef_dcd_intersection_query when
+ * ignore_near_zero_dist_pairs is off, 404-422). Over the proximity pairs [0, min(*narrow_count,
+ * max_proximity)) of the DEVICE narrow-phase list (count read on the device), a VF or EE pair
+ * with |sum_k w_k x_k|^2 < 1e-10 appends zero-stiffness EF pairs through *ef_count: VF (v, f)
+ * gives (e, f) for every edge e at v; EE (e1, e2) gives (e1, g) for each face g at e2 holding
+ * e2 and no vertex of e1, and (e2, g) for each face at e1 likewise. vert_adj_edges_csr /
+ * edge_adj_faces_csr: DEVICE adjacency in upload_2d_csr_from's one-array layout
+ * (sa_vert_adj_edges_csr, edge_adj_faces_csr). Canonicalise the EF list afterwards. */
+U26_API u26_status u26_ef_add_from_proximity(u26_ctx* ctx, const u26_collision_pair* narrow_list, const uint32_t* narrow_indices,
+	const uint32_t* narrow_count, uint32_t max_proximity, const float* x, const uint32_t* edges, const uint32_t* faces,
+	const uint32_t* vert_adj_edges_csr, const uint32_t* edge_adj_faces_csr, uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices,
+	uint32_t max_ef);
 
 /* ---- region-based pair filtering ----------------------------------------------------
  * The contour regions of a pass (u26_prp_response_view's CSRs) applied to the solver's contact

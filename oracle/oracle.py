@@ -217,13 +217,15 @@ class PrpParams(ctypes.Structure):
         ("solid_all", ctypes.c_uint32),         # PRP_solid_interior_adjacency_all_meshes
         ("solid_eps_n", ctypes.c_float),        # PRP_solid_interior_adjacency_normal_eps
         ("solid_eps_d", ctypes.c_float),        # PRP_solid_interior_adjacency_dist_eps
+        ("ignore_near_zero_dist_pairs", ctypes.c_uint32),  # scene_params.h:55
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, brute_force_raycast=0, contour_stride=0, opt_iterations=0, ccr_blend=0,
-                  ccr_blend_weight=0.5, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5)
+                  ccr_blend_weight=0.5, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5,
+                  ignore_near_zero_dist_pairs=1)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -359,6 +361,41 @@ def filter_invalid_pairs(pairs, pair_indices, num_ef, x, offset, invalid, region
                                   ctypes.c_uint32(num_ef), _p(x, _f32p), _p(off, _f32p), ctypes.c_uint32(len(inv)), _p(inv, _u32p),
                                   *[(_p(a, _u32p) if a is not None else None) for a in rg])
     return pairs, inv
+
+
+def csr_one_array(offsets, data):
+    """upload_2d_csr_from's layout (buffer_allocator.h:26-59): [n + 1] absolute offsets, then the data."""
+    off = np.asarray(offsets, np.int64)
+    n = len(off) - 1
+    return np.concatenate([off - off[0] + n + 1, np.asarray(data, np.int64)]).astype(np.uint32)
+
+
+def ef_from_proximity(pairs, pair_indices, x, edges, faces, vae_csr, eaf_csr):
+    """fn_add_ef_from_proximity_pairs over all given proximity pairs, in pair order."""
+    L = lib()
+    L.oracle_ef_from_proximity.restype = ctypes.c_uint32
+    pairs = np.ascontiguousarray(pairs)
+    pidx = np.ascontiguousarray(pair_indices, np.uint32)
+    arrs = [np.ascontiguousarray(a, t) for a, t in ((x, np.float32), (edges, np.uint32), (faces, np.uint32), (vae_csr, np.uint32),
+                                                    (eaf_csr, np.uint32))]
+    args = lambda out, idx, cap: (pairs.ctypes.data_as(ctypes.c_void_p), _p(pidx, _u32p), ctypes.c_uint32(len(pairs)),
+                                  _p(arrs[0], _f32p), _p(arrs[1], _u32p), _p(arrs[2], _u32p), _p(arrs[3], _u32p), _p(arrs[4], _u32p),
+                                  out, idx, ctypes.c_uint32(cap))
+    n = L.oracle_ef_from_proximity(*args(None, None, 0))
+    out = np.zeros(max(n, 1), EF_PAIR_DTYPE)
+    idx = np.zeros((max(n, 1), 2), np.uint32)
+    L.oracle_ef_from_proximity(*args(out.ctypes.data_as(ctypes.c_void_p), _p(idx, _u32p), n))
+    return out[:n], idx[:n]
+
+
+def canonical_ef(pairs, indices):
+    """host_preprocess_ef_pairs' canonical order (intersection_resolver.cpp:693-726): (eid, fid),
+    then memcmp of the 48-byte records."""
+    pairs = np.ascontiguousarray(pairs)
+    indices = np.ascontiguousarray(indices, np.uint32).reshape(-1, 2)
+    raw = pairs.view(np.uint8).reshape(len(pairs), -1)
+    order = sorted(range(len(pairs)), key=lambda i: (int(indices[i, 0]), int(indices[i, 1]), raw[i].tobytes()))
+    return pairs[order], indices[order]
 
 
 def filter_broad_phase(vf, ee, num_ef, invalid, regions, faces, edges):

@@ -92,6 +92,7 @@ namespace
 		uint solid_all;			// PRP_solid_interior_adjacency_all_meshes (scene_params.h:78)
 		float solid_eps_n;		// PRP_solid_interior_adjacency_normal_eps (1e-4)
 		float solid_eps_d;		// PRP_solid_interior_adjacency_dist_eps (1e-5)
+		uint ignore_near_zero_dist_pairs; // scene_params.h:55 (1; the CLI sets 0)
 	};
 
 	struct EfPair
@@ -744,7 +745,7 @@ namespace
 	void preprocess(Scene& S)
 	{
 		const MeshIn& m = S.m;
-		const uint n = uint(S.ef.size());
+		uint n = uint(S.ef.size());
 		S.num_orig_pairs = n;
 		auto build_adj = [&](uint count)
 		{
@@ -775,6 +776,51 @@ namespace
 			return adj;
 		};
 		S.adj = build_adj(n);
+		// degenerate filter (intersection_resolver.cpp:841-896): with near-zero-distance pairs in
+		// play, a pair with a barycentric coordinate below 1e-4 stays only when one of its
+		// adjacent pairs is not degenerate; if that would remove every pair, all stay
+		if (!S.p.ignore_near_zero_dist_pairs && n > 0)
+		{
+			auto degenerate = [](const EfPair& e)
+			{
+				const float eb0 = e.bary[0], eb1 = 1.0f - e.bary[0];
+				const float f0 = e.bary[1], f1 = e.bary[2], f2 = 1.0f - e.bary[1] - e.bary[2];
+				return std::min(eb0, eb1) < 1e-4f || std::min(std::min(f0, f1), f2) < 1e-4f;
+			};
+			std::vector<uint8_t> deg(n);
+			uint ndeg = 0;
+			for (uint p = 0; p < n; p++)
+				ndeg += (deg[p] = degenerate(S.ef[p]) ? 1 : 0);
+			if (ndeg)
+			{
+				std::vector<uint> keep;
+				for (uint p = 0; p < n; p++)
+				{
+					bool k = !deg[p];
+					for (uint q : S.adj[p])
+						k = k || !deg[q];
+					if (k)
+						keep.push_back(p);
+				}
+				if (!keep.empty() && keep.size() < n)
+				{
+					std::vector<EfPair> ef;
+					std::vector<uint> ee, ff;
+					for (uint p : keep)
+					{
+						ef.push_back(S.ef[p]);
+						ee.push_back(S.ef_e[p]);
+						ff.push_back(S.ef_f[p]);
+					}
+					S.ef = std::move(ef);
+					S.ef_e = std::move(ee);
+					S.ef_f = std::move(ff);
+					n = uint(keep.size());
+					S.num_orig_pairs = n;
+					S.adj = build_adj(n);
+				}
+			}
+		}
 		// loop vertices (find_loop_vertex, non-GIA path)
 		std::vector<uint> loop_vid, loop_pair, loop_e, loop_f;
 		for (uint p = 0; p < n; p++)

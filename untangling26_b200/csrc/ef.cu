@@ -248,6 +248,45 @@ namespace u26
 			vals[i] = i;
 		}
 
+		// 48-byte record a < b in memcmp order (bytes in memory order, unsigned)
+		__device__ __forceinline__ bool rec_less(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b)
+		{
+#pragma unroll
+			for (int w = 0; w < 12; w++)
+			{
+				const uint32_t x = __byte_perm(a[w], 0u, 0x0123u), y = __byte_perm(b[w], 0u, 0x0123u);
+				if (x != y)
+					return x < y;
+			}
+			return false;
+		}
+
+		// Equal (eid, fid) keys (duplicate pairs, e.g. from the proximity conversion) are put in
+		// payload memcmp order, the tie-break of host_preprocess_ef_pairs' canonical sort
+		// (intersection_resolver.cpp:700-716): each run head insertion-sorts its run of the
+		// sorted permutation.
+		__global__ void __launch_bounds__(256) ef_tiebreak_kernel(const uint64_t* __restrict__ keys, uint32_t* __restrict__ perm, uint32_t n,
+			const uint32_t* __restrict__ recs)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i + 1 >= n || (i > 0 && keys[i] == keys[i - 1]) || keys[i + 1] != keys[i])
+				return;
+			uint32_t j = i + 1;
+			while (j < n && keys[j] == keys[i])
+				j++;
+			for (uint32_t a = i + 1; a < j; a++)
+			{
+				const uint32_t v = perm[a];
+				uint32_t b = a;
+				while (b > i && rec_less(recs + 12 * size_t(v), recs + 12 * size_t(perm[b - 1])))
+				{
+					perm[b] = perm[b - 1];
+					b--;
+				}
+				perm[b] = v;
+			}
+		}
+
 		__global__ void __launch_bounds__(256) ef_gather_kernel(const uint32_t* __restrict__ perm, uint32_t count,
 			const EfPairDev* __restrict__ src, const uint2* __restrict__ src_idx, EfPairDev* __restrict__ dst,
 			uint2* __restrict__ dst_idx)
@@ -261,6 +300,131 @@ namespace u26
 		}
 	} // namespace
 } // namespace u26
+
+namespace u26
+{
+	namespace
+	{
+		// fn_add_ef_from_proximity_pairs (intersection_resolver.cpp:199-363): a VF or EE proximity
+		// pair at near-zero distance (|sum_k w_k x_k|^2 < 1e-10) becomes EF pairs of zero
+		// stiffness. VF (v, f): (e, f) for every edge e at v, edge barycentre 1 at v, face
+		// barycentres |w1|, |w2|. EE (e1, e2): (e1, g) for the faces g at e2 that share no vertex
+		// with e1 and hold e2 (two matched corners), and (e2, g) for the faces at e1 likewise;
+		// the corners of g on the shared edge take e1's barycentres in both (as the reference
+		// writes them, intersection_resolver.cpp:289-300). Pairs are appended through *ef_count (order: the canonical sort's).
+		__device__ __forceinline__ void emit_ef(uint32_t* __restrict__ ef_count, EfPairDev* __restrict__ out, uint32_t* __restrict__ out_idx,
+			uint32_t max_ef, uint2 edge, uint3 face, float eb0, float fb0, float fb1, uint32_t eid, uint32_t fid)
+		{
+			const uint32_t slot = atomicAdd(ef_count, 1u);
+			if (slot >= max_ef)
+				return;
+			EfPairDev r;
+			r.idx[0] = edge.x;
+			r.idx[1] = edge.y;
+			r.idx[2] = face.x;
+			r.idx[3] = face.y;
+			r.idx[4] = face.z;
+			r.bary[0] = eb0;
+			r.bary[1] = fb0;
+			r.bary[2] = fb1;
+			r.grad[0] = r.grad[1] = r.grad[2] = 0.0f;
+			r.stiff = 0.0f;
+			out[slot] = r;
+			reinterpret_cast<uint2*>(out_idx)[slot] = make_uint2(eid, fid);
+		}
+
+		__global__ void __launch_bounds__(256) ef_from_proximity_kernel(const u26_collision_pair* __restrict__ pairs,
+			const uint2* __restrict__ pidx, const uint32_t* __restrict__ pair_count, uint32_t max_proximity, const float* __restrict__ x,
+			const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const uint32_t* __restrict__ vae_csr,
+			const uint32_t* __restrict__ eaf_csr, uint32_t* __restrict__ ef_count, EfPairDev* __restrict__ out, uint32_t* __restrict__ out_idx,
+			uint32_t max_ef)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= min(*pair_count, max_proximity))
+				return;
+			const uint4 raw = *reinterpret_cast<const uint4*>(pairs[i].indices);
+			const uint32_t type = (raw.x >> 31) + ((raw.y & 0x80000000u) >> 30) + ((raw.z & 0x80000000u) >> 29) + ((raw.w & 0x80000000u) >> 28);
+			if (type != 4u && type != 8u)
+				return;
+			const float b2 = pairs[i].vec2[2], b3 = pairs[i].vec2[3];
+			float w[4];
+			if (type == 4u)
+			{
+				w[0] = 1.0f, w[1] = -b2, w[2] = -b3, w[3] = (b2 + b3) - 1.0f;
+			}
+			else
+			{
+				w[0] = b2, w[1] = 1.0f - b2, w[2] = -b3, w[3] = b3 - 1.0f;
+			}
+			const uint32_t id[4] = { raw.x & 0x7FFFFFFFu, raw.y & 0x7FFFFFFFu, raw.z & 0x7FFFFFFFu, raw.w & 0x7FFFFFFFu };
+			const f3 d = ((w[0] * ld3(x, id[0]) + w[1] * ld3(x, id[1])) + w[2] * ld3(x, id[2])) + w[3] * ld3(x, id[3]);
+			if (dot(d, d) >= 1e-10f)
+				return;
+			const uint2 q = pidx[i];
+			if (type == 4u)
+			{
+				const uint32_t vid = id[0], fid = q.y;
+				const uint3 face = make_uint3(faces[3 * fid], faces[3 * fid + 1], faces[3 * fid + 2]);
+				const float fb0 = fabsf(w[1]), fb1 = fabsf(w[2]);
+				for (uint32_t k = vae_csr[vid]; k < vae_csr[vid + 1]; k++)
+				{
+					const uint32_t ae = vae_csr[k];
+					const uint2 e = edges[ae];
+					emit_ef(ef_count, out, out_idx, max_ef, e, face, e.x == vid ? 1.0f : 0.0f, fb0, fb1, ae, fid);
+				}
+				return;
+			}
+			const uint32_t eid1 = q.x, eid2 = q.y;
+			const uint2 e1 = edges[eid1], e2 = edges[eid2];
+			const float e1b0 = fabsf(w[0]), e1b1 = fabsf(w[1]), e2b0 = fabsf(w[2]);
+			// faces at e2 against e1, then faces at e1 against e2
+			for (int side = 0; side < 2; side++)
+			{
+				const uint32_t at = side == 0 ? eid2 : eid1;
+				const uint2 other = side == 0 ? e1 : e2; // the edge that must not touch the face
+				const uint2 on = side == 0 ? e2 : e1;	  // the edge whose corners the face holds
+				for (uint32_t k = eaf_csr[at]; k < eaf_csr[at + 1]; k++)
+				{
+					const uint32_t af = eaf_csr[k];
+					const uint32_t fv[3] = { faces[3 * af], faces[3 * af + 1], faces[3 * af + 2] };
+					bool shares = false;
+					for (int c = 0; c < 3; c++)
+						shares = shares || fv[c] == other.x || fv[c] == other.y;
+					if (shares)
+						continue;
+					float fb[3] = { 0.0f, 0.0f, 0.0f };
+					uint32_t matched = 0;
+					for (int c = 0; c < 3; c++)
+					{
+						if (fv[c] == on.x)
+						{
+							fb[c] = e1b0;
+							matched++;
+						}
+						else if (fv[c] == on.y)
+						{
+							fb[c] = e1b1;
+							matched++;
+						}
+					}
+					if (matched != 2u)
+						continue;
+					const uint3 face = make_uint3(fv[0], fv[1], fv[2]);
+					if (side == 0)
+						emit_ef(ef_count, out, out_idx, max_ef, e1, face, e1b0, fb[0], fb[1], eid1, af);
+					else
+						emit_ef(ef_count, out, out_idx, max_ef, e2, face, e2b0, fb[0], fb[1], eid2, af);
+				}
+			}
+		}
+	} // namespace
+} // namespace u26
+
+u26_status u26::ef_tiebreak(u26_ctx* ctx, const uint64_t* sorted_keys, uint32_t* perm, uint32_t count, const void* recs)
+{
+	ef_tiebreak_kernel<<<div_up(count, 256), 256, 0, ctx->stream>>>(sorted_keys, perm, count, static_cast<const uint32_t*>(recs));
+	return after_launch(ctx, "ef_tiebreak_kernel");
+}
 
 using namespace u26;
 
@@ -341,6 +505,24 @@ U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint
 	return after_launch(ctx, "ef_detect_kernel");
 }
 
+U26_API u26_status u26_ef_add_from_proximity(u26_ctx* ctx, const u26_collision_pair* narrow_list, const uint32_t* narrow_indices,
+	const uint32_t* narrow_count, uint32_t max_proximity, const float* x, const uint32_t* edges, const uint32_t* faces,
+	const uint32_t* vert_adj_edges_csr, const uint32_t* edge_adj_faces_csr, uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices,
+	uint32_t max_ef)
+{
+	if (!ctx)
+		return U26_ERR_INVALID_INPUT;
+	if (max_proximity == 0)
+		return U26_OK;
+	if (!narrow_list || !narrow_indices || !narrow_count || !x || !edges || !faces || !vert_adj_edges_csr || !edge_adj_faces_csr ||
+		!ef_count || (max_ef && (!ef_pairs || !ef_indices)))
+		return set_error(ctx, U26_ERR_INVALID_INPUT, "u26_ef_add_from_proximity: null input");
+	ef_from_proximity_kernel<<<div_up(max_proximity, 256), 256, 0, ctx->stream>>>(narrow_list, reinterpret_cast<const uint2*>(narrow_indices),
+		narrow_count, max_proximity, x, reinterpret_cast<const uint2*>(edges), faces, vert_adj_edges_csr, edge_adj_faces_csr, ef_count,
+		static_cast<EfPairDev*>(ef_pairs), ef_indices, max_ef);
+	return after_launch(ctx, "ef_from_proximity_kernel");
+}
+
 U26_API u26_status u26_ef_canonicalize(u26_ctx* ctx, uint32_t count, void* ef_pairs, uint32_t* ef_indices, uint32_t num_edges,
 	uint32_t num_faces)
 {
@@ -363,6 +545,7 @@ U26_API u26_status u26_ef_canonicalize(u26_ctx* ctx, uint32_t count, void* ef_pa
 	while (bits < 64 && (uint64_t(1) << bits) < key_max)
 		bits++;
 	U26_TRY(s->sorter.sort(ctx, s->keys.as<uint64_t>(), s->vals.as<uint32_t>(), count, 0, bits));
+	U26_TRY(ef_tiebreak(ctx, s->keys.as<uint64_t>(), s->vals.as<uint32_t>(), count, ef_pairs));
 	U26_CUDA(ctx, cudaMemcpyAsync(s->pairs.ptr, ef_pairs, sizeof(EfPairDev) * count, cudaMemcpyDeviceToDevice, ctx->stream));
 	U26_CUDA(ctx, cudaMemcpyAsync(s->idx.ptr, ef_indices, sizeof(uint2) * count, cudaMemcpyDeviceToDevice, ctx->stream));
 	ef_gather_kernel<<<div_up(count, 256), 256, 0, ctx->stream>>>(s->vals.as<uint32_t>(), count, s->pairs.as<EfPairDev>(),

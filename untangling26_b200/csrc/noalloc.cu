@@ -125,6 +125,7 @@ U26_API u26_status u26_ef_canonicalize_noalloc(u26_ctx* ctx, uint32_t count, voi
 	while (bits < 64 && (uint64_t(1) << bits) < key_max)
 		bits++;
 	U26_TRY(RadixSorter::sort_into(ctx, keys, vals, count, 0, bits, keys_alt, vals_alt, counts));
+	U26_TRY(ef_tiebreak(ctx, keys, vals, count, pairs_copy));
 	noalloc_gather_kernel<<<div_up(count, 256), 256, 0, ctx->stream>>>(vals, count, pairs_copy, idx_copy, static_cast<EfRec*>(ef_pairs),
 		reinterpret_cast<uint2*>(ef_indices));
 	return after_launch(ctx, "noalloc_gather_kernel");

@@ -3183,20 +3183,24 @@ namespace
 			h.join();
 	}
 
-	void build_graph(const u26_scene& S, const std::vector<float>& x, HostGraph& G)
+	// returns the EF pair count after the degenerate filter (before loop-vertex pairs)
+	uint32_t build_graph(const u26_scene& S, const std::vector<float>& x, HostGraph& G, bool ignore_near_zero)
 	{
-		const uint32_t n = uint32_t(G.ef.size());
+		uint32_t n = uint32_t(G.ef.size());
 		// the canonical EF list is sorted by edge: each edge's pairs form one run
 		std::vector<uint32_t> run(S.ne + 1, 0u);
-		for (uint32_t p = 0; p < n; p++)
-			run[G.ee[p] + 1]++;
-		for (uint32_t e = 0; e < S.ne; e++)
-			run[e + 1] += run[e];
 		auto edge_run = [&](uint32_t e, uint32_t& b, uint32_t& t)
 		{
 			b = run[e];
 			t = run[e + 1];
 		};
+		auto build_adj = [&]()
+		{
+		std::fill(run.begin(), run.end(), 0u);
+		for (uint32_t p = 0; p < n; p++)
+			run[G.ee[p] + 1]++;
+		for (uint32_t e = 0; e < S.ne; e++)
+			run[e + 1] += run[e];
 		G.adj.assign(n, {});
 		host_parallel_for(n, [&](uint32_t p)
 		{
@@ -3224,6 +3228,53 @@ namespace
 				}
 			}
 		});
+		};
+		build_adj();
+		// degenerate filter (intersection_resolver.cpp:841-896): with near-zero-distance pairs in
+		// play, a pair with a barycentric coordinate below 1e-4 stays only when one of its
+		// adjacent pairs is not degenerate; if that would remove every pair, all stay
+		if (!ignore_near_zero && n > 0)
+		{
+			std::vector<uint8_t> deg(n);
+			uint32_t ndeg = 0;
+			for (uint32_t p = 0; p < n; p++)
+			{
+				const EfPairH& e = G.ef[p];
+				const float eb0 = e.bary[0], eb1 = 1.0f - e.bary[0];
+				const float f0 = e.bary[1], f1 = e.bary[2], f2 = 1.0f - e.bary[1] - e.bary[2];
+				deg[p] = (std::min(eb0, eb1) < 1e-4f || std::min(std::min(f0, f1), f2) < 1e-4f) ? 1 : 0;
+				ndeg += deg[p];
+			}
+			if (ndeg)
+			{
+				std::vector<uint32_t> keep;
+				for (uint32_t p = 0; p < n; p++)
+				{
+					bool k = !deg[p];
+					for (uint32_t q : G.adj[p])
+						k = k || !deg[q];
+					if (k)
+						keep.push_back(p);
+				}
+				if (!keep.empty() && keep.size() < n)
+				{
+					std::vector<EfPairH> ef;
+					std::vector<uint32_t> ee, ff;
+					for (uint32_t p : keep)
+					{
+						ef.push_back(G.ef[p]);
+						ee.push_back(G.ee[p]);
+						ff.push_back(G.ff[p]);
+					}
+					G.ef = std::move(ef);
+					G.ee = std::move(ee);
+					G.ff = std::move(ff);
+					n = uint32_t(keep.size());
+					build_adj();
+				}
+			}
+		}
+		const uint32_t n_kept = n;
 		// loop-vertex pairs
 		struct Loop
 		{
@@ -3370,6 +3421,7 @@ namespace
 		}
 		for (uint32_t v = 0; v < S.nv; v++)
 			G.vflag_off[v + 1] += G.vflag_off[v];
+		return n_kept;
 	}
 
 	std::vector<V3h> directions(const u26_scene& S, const std::vector<float>& x, const HostGraph& G, const ContourRT& r, uint32_t mode,
@@ -3555,8 +3607,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		G.ee[i] = idx[2 * i];
 		G.ff[i] = idx[2 * i + 1];
 	}
-	build_graph(*S, x, G);
-	out->num_orig_pairs = num_pairs;
+	out->num_orig_pairs = build_graph(*S, x, G, P->ignore_near_zero_dist_pairs != 0);
 	out->stage_ms[0] = ms_since(t0);
 	const uint32_t na = uint32_t(G.ef.size());
 	const uint32_t nc = uint32_t(G.contours.size());

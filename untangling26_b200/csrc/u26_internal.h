@@ -99,6 +99,10 @@ namespace u26
 		}
 	};
 
+	// Canonical EF order, ties: equal sorted keys put their permutation entries in memcmp order
+	// of the 48-byte records recs[perm[i]] (ef.cu).
+	u26_status ef_tiebreak(u26_ctx* ctx, const uint64_t* sorted_keys, uint32_t* perm, uint32_t count, const void* recs);
+
 	// Response assembly of one PRP pass (response.cu): host-side results of the pass and the
 	// scene's device tables.
 	struct ResponseInputs

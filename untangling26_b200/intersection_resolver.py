@@ -48,6 +48,17 @@ class IntersectionResolver:
             ptr(vert_property), ptr(d_hat), ptr(self.ef_count), ptr(self.ef_list), ptr(self.ef_indices), self.max_ef),
             "ef_narrow_phase")
 
+    def add_ef_from_proximity_pairs(self, narrow_list, narrow_indices, narrow_count, x, edges, faces, vae_csr, eaf_csr,
+                                    max_proximity=None):
+        """fn_add_ef_from_proximity_pairs (intersection_resolver.cpp:199-363): near-zero-distance
+        VF / EE pairs of the device narrow-phase list ([n, 16] templates, [n, 2] indices, count
+        on the device) appended to the EF list as zero-stiffness EF pairs."""
+        cap = int(narrow_list.shape[0]) if max_proximity is None else max_proximity
+        self.ctx.check(self.ctx.lib.u26_ef_add_from_proximity(
+            self.ctx.handle, ptr(narrow_list), ptr(narrow_indices), ptr(narrow_count), cap, ptr(x), ptr(edges), ptr(faces),
+            ptr(vae_csr), ptr(eaf_csr), ptr(self.ef_count), ptr(self.ef_list), ptr(self.ef_indices), self.max_ef),
+            "ef_add_from_proximity")
+
     def canonicalize(self, num_edges, num_faces):
         """Sort the EF list by (eid, fid) on the device (synchronises for the count)."""
         n = int(self.ef_count.item())
@@ -193,10 +204,29 @@ class CollisionScene:
         finally:
             self.ctx.lib.u26_prp_output_destroy(out)
 
-    def untangle_pass(self, params=None, response=None, **narrow):
-        """One untangling pass at the current positions: refit, fused EF detection,
-        canonical EF order, PRP contour evaluation (and, with response, its response pairs)."""
+    def _adjacency_csrs(self):
+        """sa_vert_adj_edges_csr / edge_adj_faces_csr in upload_2d_csr_from's one-array layout."""
+        if getattr(self, "_vae_csr", None) is None:
+            dev = self.x.device
+            self._vae_csr = torch.from_numpy(self.mesh.vert_adj_edges.one_array().view(np.int32)).to(dev)
+            self._eaf_csr = torch.from_numpy(self.mesh.edge_adj_faces_ext.one_array().view(np.int32)).to(dev)
+        return self._vae_csr, self._eaf_csr
+
+    def add_ef_from_proximity_pairs(self, narrow_list, narrow_indices, narrow_count, max_proximity=None):
+        """Near-zero-distance proximity pairs as EF pairs (the reference's
+        ignore_near_zero_dist_pairs = false, intersection_resolver.cpp:404-422)."""
+        vae, eaf = self._adjacency_csrs()
+        self.resolver.add_ef_from_proximity_pairs(narrow_list, narrow_indices, narrow_count, self.x, self.edges, self.faces, vae, eaf,
+                                                  max_proximity)
+
+    def untangle_pass(self, params=None, response=None, proximity=None, **narrow):
+        """One untangling pass at the current positions: refit, fused EF detection (plus, with
+        proximity = (narrow_list, narrow_indices, narrow_count), the near-zero-distance proximity
+        pairs as EF pairs), canonical EF order, PRP contour evaluation (and, with response, its
+        response pairs)."""
         self.detect_ef_fused()
+        if proximity is not None:
+            self.add_ef_from_proximity_pairs(*proximity)
         n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
         return self.host_resolve(params, num_pairs=n, response=response, **narrow)
 

@@ -55,6 +55,13 @@ class CSR:
     def counts(self):
         return np.diff(self.offsets.astype(np.int64))
 
+    def one_array(self):
+        """upload_2d_csr_from's layout (buffer_allocator.h:26-59): [n + 1] absolute offsets
+        into the same array, then the data."""
+        n = len(self)
+        off = self.offsets.astype(np.int64) - int(self.offsets[0]) + n + 1
+        return np.concatenate([off, self.data.astype(np.int64)]).astype(np.uint32)
+
 
 def _group(keys, values, n):
     """CSR of `values` grouped by `keys` (stable: original order kept inside a group)."""

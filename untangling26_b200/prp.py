@@ -30,13 +30,14 @@ class PrpParams(ctypes.Structure):
         ("solid_all", c_u32),         # PRP_solid_interior_adjacency_all_meshes
         ("solid_eps_n", c_f32),       # PRP_solid_interior_adjacency_normal_eps
         ("solid_eps_d", c_f32),       # PRP_solid_interior_adjacency_dist_eps
+        ("ignore_near_zero_dist_pairs", c_u32),  # 0: drop isolated degenerate EF pairs (the CLI's setting)
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, opt_iterations=0, ccr_blend=0, ccr_blend_weight=0.5,
-                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5)
+                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

@@ -9,6 +9,8 @@ No dataset is read. Each generator takes a seed (numpy PCG64) and returns a Mesh
 * folded_sheet(n): one n x n sheet (n = 256: 130,050 triangles) folded flat about a
   seeded line, then Gaussian vertex noise of 0.3 x edge length on every axis, so that
   the two layers cross each other in figure-eight and boundary-ending contours.
+* sheets_in_contact(n): two_sheets(n) with a third sheet lying exactly on sheet A (zero-distance
+  proximity pairs, for the near-zero-distance EF conversion).
 * layered_sheets(n, layers): stacked n x n sheets 1 mm apart with seeded multi-octave
   value-noise displacement of 2-20 mm so that layers pass through their neighbours.
 * batch_scenes(num): independent two-body scenes (icosphere-derived shells or bumped
@@ -53,6 +55,23 @@ def two_sheets(n=64, seed=0):
     obj = np.concatenate([np.zeros(n * n, np.uint32), np.ones(n * n, np.uint32)])
     m = Mesh(x.astype(np.float32), faces, object_of_vert=obj, rest_x=np.concatenate([xa, xb * [1, 1, 0] + [0, 0, 0.002]], 0))
     m.meta = {"kind": "two_sheets", "n": n, "seed": seed, "amplitude": amp, "periods": periods}
+    return m
+
+
+def sheets_in_contact(n=32, seed=0):
+    """two_sheets(n) plus a third sheet lying exactly on sheet A (the same vertex positions,
+    its own object): every vertex and edge of it is at zero distance from A, the
+    near-zero-distance proximity pairs that the reference turns into EF pairs when
+    ignore_near_zero_dist_pairs is off."""
+    m2 = two_sheets(n, seed)
+    nn = n * n
+    xa = m2.x[:nn]
+    x = np.concatenate([m2.x, xa], 0)
+    faces = np.concatenate([m2.faces, m2.faces[: len(m2.faces) // 2] + 2 * nn], 0)
+    obj = np.concatenate([np.zeros(nn, np.uint32), np.ones(nn, np.uint32), np.full(nn, 2, np.uint32)])
+    rest = np.concatenate([m2.rest_x, m2.rest_x[:nn]], 0)
+    m = Mesh(x.astype(np.float32), faces, object_of_vert=obj, rest_x=rest)
+    m.meta = dict(m2.meta, kind="sheets_in_contact")
     return m
 
 
