@@ -75,10 +75,24 @@ namespace u26
 		// below must also reject: t = tnum / den surely negative (opposite signs, magnitudes far
 		// from underflow), or surely beyond ray_len (1e-5 relative margin)
 		const float aden = fabsf(den), anum = fabsf(tnum);
-		if (aden >= 1e-30f && aden <= 1e20f && anum >= 1e-20f && ((tnum > 0.0f) != (den > 0.0f)))
+		const bool den_ok = aden >= 1e-30f && aden <= 1e20f; // 1 / den neither overflows nor underflows
+		if (den_ok && anum >= 1e-20f && ((tnum > 0.0f) != (den > 0.0f)))
 			return false;
 		if (aden >= 1e-30f && anum > aden * ray_len * (1.0f + 1e-5f) && ((tnum > 0.0f) == (den > 0.0f)))
 			return false;
+		// the barycentric numerators (uu = nu / den, vv = nv / den): a numerator of the other sign
+		// than den makes its coordinate negative, and nu + nv beyond den (1e-5 relative margin,
+		// both of den's sign by then) puts uu + vv above 1 - 1e-6; both rejections the exact test
+		// below makes too, here without its square root and division
+		const f3 cx = cross(neg, to_a);
+		const float nu = dot(AC, cx), nv = -dot(AB, cx);
+		if (den_ok)
+		{
+			if ((nu > 0.0f && den < 0.0f) || (nu < 0.0f && den > 0.0f) || (nv > 0.0f && den < 0.0f) || (nv < 0.0f && den > 0.0f))
+				return false;
+			if (fabsf(nu + nv) > aden * (1.0f + 1e-5f))
+				return false;
+		}
 		const float nlen = length(N);
 		if (fabsf(den) < nlen * 1e-6f)
 			return false;
@@ -86,11 +100,10 @@ namespace u26
 		const float t = tnum * inv_den;
 		if (t < 0.0f || t > ray_len)
 			return false;
-		const f3 cx = cross(neg, to_a);
-		const float uu = dot(AC, cx) * inv_den;
+		const float uu = nu * inv_den;
 		if (uu < 1e-6f || uu > (1.0f - 1e-6f))
 			return false;
-		const float vv = -dot(AB, cx) * inv_den;
+		const float vv = nv * inv_den;
 		if (vv < 1e-6f || (vv + uu) > (1.0f - 1e-6f))
 			return false;
 		out_t = t;
@@ -761,48 +774,34 @@ namespace u26
 
 		// slab test of a grown box with the ray's reciprocals hoisted (same values as ray_box:
 		// t0 <= t1 follows from the reciprocal's sign)
+		// Slab test against the grown node boxes: t = box * inv - o * inv, one explicit fma per
+		// plane. The boxes carry the conservative margin 1e-5 (1 + |c|), far above the rounding of
+		// this form (a few ulp of o * inv), so no box the ray meets is rejected; a slab the ray
+		// runs parallel to (|d| < 1e-30) gets inv = +-1e30, which turns the same arithmetic into
+		// the inside-the-slab test. Node tests only prune: the leaf tests decide the hits.
 		struct RaySlab
 		{
-			float o[3], inv[3];
-			uint32_t par; // bit a: |d_a| < 1e-30 (the ray is parallel to slab a)
+			float inv[3], oinv[3];
 		};
 		__device__ __forceinline__ RaySlab make_slab(f3 o, f3 d)
 		{
 			RaySlab r;
 			const float oo[3] = { o.x, o.y, o.z }, dd[3] = { d.x, d.y, d.z };
-			r.par = 0;
 #pragma unroll
 			for (int a = 0; a < 3; a++)
 			{
-				r.o[a] = oo[a];
-				if (fabsf(dd[a]) < 1e-30f)
-				{
-					r.par |= 1u << a;
-					r.inv[a] = 0.0f;
-				}
-				else
-					r.inv[a] = 1.0f / dd[a];
+				r.inv[a] = fabsf(dd[a]) < 1e-30f ? copysignf(1e30f, dd[a]) : 1.0f / dd[a];
+				r.oinv[a] = oo[a] * r.inv[a];
 			}
 			return r;
 		}
 		__device__ __forceinline__ bool ray_grown_box(const RaySlab& r, float t_lo, float t_hi, const NodeBox& g)
 		{
-			float tmin = t_lo, tmax = t_hi;
-			const float lo[3] = { g.mn.x, g.mn.y, g.mn.z }, hi[3] = { g.mx.x, g.mx.y, g.mx.z };
-#pragma unroll
-			for (int a = 0; a < 3; a++)
-			{
-				if (r.par & (1u << a))
-				{
-					if (r.o[a] < lo[a] || r.o[a] > hi[a])
-						return false;
-					continue;
-				}
-				const float ta = (lo[a] - r.o[a]) * r.inv[a], tb = (hi[a] - r.o[a]) * r.inv[a];
-				const bool pos = r.inv[a] >= 0.0f;
-				tmin = fmaxf(tmin, pos ? ta : tb);
-				tmax = fminf(tmax, pos ? tb : ta);
-			}
+			const float ax = __fmaf_rn(g.mn.x, r.inv[0], -r.oinv[0]), bx = __fmaf_rn(g.mx.x, r.inv[0], -r.oinv[0]);
+			const float ay = __fmaf_rn(g.mn.y, r.inv[1], -r.oinv[1]), by = __fmaf_rn(g.mx.y, r.inv[1], -r.oinv[1]);
+			const float az = __fmaf_rn(g.mn.z, r.inv[2], -r.oinv[2]), bz = __fmaf_rn(g.mx.z, r.inv[2], -r.oinv[2]);
+			const float tmin = fmaxf(fmaxf(t_lo, fminf(ax, bx)), fmaxf(fminf(ay, by), fminf(az, bz)));
+			const float tmax = fminf(fminf(t_hi, fmaxf(ax, bx)), fminf(fmaxf(ay, by), fmaxf(az, bz)));
 			return tmin <= tmax;
 		}
 
@@ -852,9 +851,10 @@ namespace u26
 			const uint32_t* __restrict__ faces, const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats,
 			uint32_t* __restrict__ dev_err)
 		{
-			__shared__ uint32_t s_stack[4][kStack];
 			const int lane = threadIdx.x & 31;
-			uint32_t* stack = s_stack[threadIdx.x >> 5];
+			// the packet's traversal stack lives in registers across the warp: entry k in lane k & 31
+			// of s_lo (k < 32) or s_hi (k >= 32); every lane holds the same stack pointer
+			uint32_t s_lo = 0u, s_hi = 0u;
 			const uint32_t warps_per_part = (total + 31u) >> 5;
 			const uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 			const uint32_t part = wi / warps_per_part; // warp-uniform
@@ -947,24 +947,24 @@ namespace u26
 				const bool on = fstart_l == fstart;
 				fpending &= ~__ballot_sync(0xFFFFFFFFu, on);
 				ray_visits += on ? 1u : 0u;
-				int sp = 1;
-				if (lane == 0)
-					stack[0] = fstart;
-				__syncwarp();
+				// depth first: a hit inner node continues with its first child and stacks the second
+				uint32_t node = fstart;
+				int sp = 0;
 				uint32_t loop = 0;
-				while (sp > 0)
+				for (;;)
 				{
-					const uint32_t node = stack[--sp];
 					NodeBox b;
 					b.mn = __ldg(&fgrow[node].mn);
 					b.mx = __ldg(&fgrow[node].mx);
 					visited += on ? 1u : 0u;
 					fetch_nodes++;
 					const bool hit = on && ray_grown_box(slab, t_lo, t_hi, b);
-					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
-						continue;
 					const uint32_t link_a = __float_as_uint(b.mn.w), link_b = __float_as_uint(b.mx.w);
-					if (link_b == kInvalid)
+					bool descend = false;
+					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
+					{
+					}
+					else if (link_b == kInvalid)
 					{
 						const uint32_t fid = link_a;
 						fetch_tris++;
@@ -988,29 +988,39 @@ namespace u26
 							}
 						}
 						__syncwarp();
-						continue;
 					}
-					ray_visits += hit ? 2u : 0u;
-					if (sp + 2 > kStack)
+					else
 					{
-						if (lane == 0)
-							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
-						break;
+						ray_visits += hit ? 2u : 0u;
+						if (sp + 1 > kStack)
+						{
+							if (lane == 0)
+								atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
+							break;
+						}
+						if (lane == (sp & 31))
+						{
+							if (sp < 32)
+								s_lo = link_b;
+							else
+								s_hi = link_b;
+						}
+						sp++;
+						node = link_a;
+						descend = true;
 					}
-					__syncwarp();
-					if (lane == 0)
-					{
-						stack[sp] = link_b;
-						stack[sp + 1] = link_a;
-					}
-					sp += 2;
-					__syncwarp();
 					if (++loop > 4000000u)
 					{
 						if (lane == 0)
 							atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
 						break;
 					}
+					if (descend)
+						continue;
+					if (sp == 0)
+						break;
+					sp--;
+					node = __shfl_sync(0xFFFFFFFFu, sp < 32 ? s_lo : s_hi, sp & 31);
 				}
 				__syncwarp();
 			}
@@ -1066,14 +1076,11 @@ namespace u26
 				const bool on = estart_l == estart;
 				epending &= ~__ballot_sync(0xFFFFFFFFu, on);
 				ray_visits += on ? 1u : 0u;
-				int sp = 1;
-				if (lane == 0)
-					stack[0] = estart;
-				__syncwarp();
+				uint32_t node = estart;
+				int sp = 0;
 				uint32_t loop = 0;
-				while (sp > 0)
+				for (;;)
 				{
-					const uint32_t node = stack[--sp];
 					NodeBox g;
 					g.mn = __ldg(&egrow[node].mn);
 					g.mx = __ldg(&egrow[node].mx);
@@ -1081,10 +1088,12 @@ namespace u26
 					fetch_nodes++;
 					const bool hit = on && (smn.x <= g.mx.x) & (smx.x >= g.mn.x) & (smn.y <= g.mx.y) & (smx.y >= g.mn.y) & (smn.z <= g.mx.z) &
 						(smx.z >= g.mn.z);
-					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
-						continue;
 					const uint32_t link_a = __float_as_uint(g.mn.w), link_b = __float_as_uint(g.mx.w);
-					if (link_b == kInvalid)
+					bool descend = false;
+					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
+					{
+					}
+					else if (link_b == kInvalid)
 					{
 						const uint32_t e2 = link_a;
 						fetch_edges++;
@@ -1113,45 +1122,73 @@ namespace u26
 										const float det = -dot(dir, n);
 										if (!(fabsf(det) < 1e-10f))
 										{
-											const float inv = 1.0f / det;
 											const float d_r_e1_e2 = dot(rr, cross(e1, e2v));
 											const float d_dir_r_e2 = dot(dir, cross(rr, e2v));
 											const float d_dir_e1_r = dot(dir, cross(e1, rr));
-											const float sv = -d_r_e1_e2 * inv;
-											const float t1 = -d_dir_r_e2 * inv;
-											const float t2 = d_dir_e1_r * inv;
-											if (sv >= 0.0f && sv <= ray_max && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f)
-												emit(sink, t, 1u, eid, e2, 1.0f - t1, 1.0f - t2, sv);
+											const float n_sv = -d_r_e1_e2, n_t1 = -d_dir_r_e2, n_t2 = d_dir_e1_r; // x = n_x / det
+											// misses decided before the division, only where the test below rejects too:
+											// a numerator (|n| >= 1e-20, so n / det stays nonzero) of the other sign than
+											// det, or t1, t2 beyond 1 / sv beyond ray_max by a 1e-5 relative margin
+											const float adet = fabsf(det);
+											bool maybe = true;
+											if (adet <= 1e20f)
+											{
+												auto neg = [&](float v)
+												{ return fabsf(v) >= 1e-20f && ((v > 0.0f) != (det > 0.0f)); };
+												const float lim = adet * (1.0f + 1e-5f);
+												maybe = !(neg(n_sv) || neg(n_t1) || neg(n_t2) || fabsf(n_t1) > lim || fabsf(n_t2) > lim ||
+													(ray_max >= 1e-20f && fabsf(n_sv) > lim * ray_max));
+											}
+											if (maybe)
+											{
+												const float inv = 1.0f / det;
+												const float sv = n_sv * inv;
+												const float t1 = n_t1 * inv;
+												const float t2 = n_t2 * inv;
+												if (sv >= 0.0f && sv <= ray_max && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f)
+													emit(sink, t, 1u, eid, e2, 1.0f - t1, 1.0f - t2, sv);
+											}
 										}
 									}
 								}
 							}
 						}
 						__syncwarp();
-						continue;
 					}
-					ray_visits += hit ? 2u : 0u;
-					if (sp + 2 > kStack)
+					else
 					{
-						if (lane == 0)
-							atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
-						break;
+						ray_visits += hit ? 2u : 0u;
+						if (sp + 1 > kStack)
+						{
+							if (lane == 0)
+								atomicOr(dev_err, U26_DEVERR_STACK_OVERFLOW);
+							break;
+						}
+						if (lane == (sp & 31))
+						{
+							if (sp < 32)
+								s_lo = link_b;
+							else
+								s_hi = link_b;
+						}
+						sp++;
+						node = link_a;
+						descend = true;
 					}
-					__syncwarp();
-					if (lane == 0)
-					{
-						stack[sp] = link_b;
-						stack[sp + 1] = link_a;
-					}
-					sp += 2;
-					__syncwarp();
 					if (++loop > 4000000u)
 					{
 						if (lane == 0)
 							atomicOr(dev_err, U26_DEVERR_ITERATION_CAP);
 						break;
 					}
+					if (descend)
+						continue;
+					if (sp == 0)
+						break;
+					sp--;
+					node = __shfl_sync(0xFFFFFFFFu, sp < 32 ? s_lo : s_hi, sp & 31);
 				}
+				__syncwarp();
 			}
 			if (stats)
 			{
