@@ -740,7 +740,7 @@ namespace u26
 
 		// The subtree roots that split one traversal across kSplit threads: the nodes at
 		// depth log2(kSplit) below the root, or shallower leaves; unused entries ~0.
-		constexpr uint32_t kSplit = 8;
+		constexpr uint32_t kSplit = 16;
 		__global__ void frontier_kernel(const uint2* __restrict__ children, const uint32_t* __restrict__ object_idx, uint32_t n_nodes,
 			uint32_t node_off, uint32_t* __restrict__ out)
 		{
