@@ -270,7 +270,7 @@ def _pair_filter_block(sc, mesh, dev, flush, stream, response, num_ef, peak, ste
     torch.cuda.synchronize()
     ms = statistics.median(a.elapsed_time(b) for a, b in evs)
     byts = n * (64 + 48 + 8) + n * (64 + 8 + 16 + 16) + nvf * (8 + 12 + 16 + 16 + 8) + nee * (8 + 16 + 16 + 16 + 8)
-    disabled = int((pairs[:, 5].view(torch.float32) == 0).sum().item())
+    disabled = int((pairs[:, 9].view(torch.float32) == 0).sum().item())  # k2 (vec2[1])
     flagged = int(((vf[:, 0] >> 30) != 0).sum().item() + ((ee[:, 0] >> 30) != 0).sum().item())
     out = {"kernels": ["identify_invalid_kernel", "filter_pairs_kernel", "filter_broad_vf_kernel", "filter_broad_ee_kernel"],
            "proximity_pairs": n, "broad_vf": nvf, "broad_ee": nee, "disabled": disabled, "flagged_broad": flagged,

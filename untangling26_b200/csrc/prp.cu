@@ -40,6 +40,7 @@
 #include <memory>
 #include <numeric>
 #include <set>
+#include <atomic>
 #include <thread>
 #include <vector>
 
@@ -3220,6 +3221,29 @@ namespace
 			h.join();
 	}
 
+	// fn(i) for i in [0, n) over the host cores, items handed out one at a time (for few,
+	// uneven items such as contours); fn(i) writes only what i owns
+	template <typename F>
+	void host_parallel_dynamic(uint32_t n, F&& fn)
+	{
+		const uint32_t nt = std::min(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+		if (nt <= 1)
+		{
+			for (uint32_t i = 0; i < n; i++)
+				fn(i);
+			return;
+		}
+		std::atomic<uint32_t> next{ 0u };
+		std::vector<std::thread> th;
+		for (uint32_t t = 0; t < nt; t++)
+			th.emplace_back([&]()
+				{
+					for (uint32_t i = next.fetch_add(1u); i < n; i = next.fetch_add(1u))
+						fn(i); });
+		for (auto& h : th)
+			h.join();
+	}
+
 	// returns the EF pair count after the degenerate filter (before loop-vertex pairs)
 	uint32_t build_graph(const u26_scene& S, const std::vector<float>& x, HostGraph& G, bool ignore_near_zero)
 	{
@@ -3435,29 +3459,35 @@ namespace
 				t = nb == 1 ? 4u : nb == 2 ? 5u : 0u;
 			G.type[c] = t;
 		}
-		// vertex boundary flags 2c + side (CSR, sorted unique)
-		std::vector<std::pair<uint32_t, uint32_t>> vf;
+		// vertex boundary flags 2c + side (CSR, sorted unique per vertex): bucketed by vertex
+		// (counting sort), then each short row sorted and deduplicated
+		std::vector<uint32_t> row(S.nv + 1, 0u);
+		for (uint32_t p = 0; p < na; p++)
+			if (!G.ef[p].is_loop())
+				for (int k = 0; k < 5; k++)
+					row[G.ef[p].idx[k] + 1]++;
+		for (uint32_t v = 0; v < S.nv; v++)
+			row[v + 1] += row[v];
+		std::vector<uint32_t> fill(row.begin(), row.end() - 1), flat(row[S.nv]);
 		for (uint32_t p = 0; p < na; p++)
 		{
 			if (G.ef[p].is_loop())
 				continue;
 			const uint32_t fe = 2 * G.contour_index[p] + G.mesh_index[p];
-			for (int k = 0; k < 2; k++)
-				vf.push_back({ G.ef[p].idx[k], fe });
-			for (int k = 2; k < 5; k++)
-				vf.push_back({ G.ef[p].idx[k], fe ^ 1u });
+			for (int k = 0; k < 5; k++)
+				flat[fill[G.ef[p].idx[k]]++] = k < 2 ? fe : (fe ^ 1u);
 		}
-		std::sort(vf.begin(), vf.end());
-		vf.erase(std::unique(vf.begin(), vf.end()), vf.end());
 		G.vflag_off.assign(S.nv + 1, 0u);
-		G.vflags.resize(vf.size());
-		for (size_t i = 0; i < vf.size(); i++)
-		{
-			G.vflag_off[vf[i].first + 1]++;
-			G.vflags[i] = vf[i].second;
-		}
+		host_parallel_for(S.nv, [&](uint32_t v)
+			{
+				std::sort(flat.begin() + row[v], flat.begin() + row[v + 1]);
+				G.vflag_off[v + 1] = uint32_t(std::unique(flat.begin() + row[v], flat.begin() + row[v + 1]) - (flat.begin() + row[v]));
+			});
 		for (uint32_t v = 0; v < S.nv; v++)
 			G.vflag_off[v + 1] += G.vflag_off[v];
+		G.vflags.resize(G.vflag_off[S.nv]);
+		host_parallel_for(S.nv, [&](uint32_t v)
+			{ std::copy(flat.begin() + row[v], flat.begin() + row[v] + (G.vflag_off[v + 1] - G.vflag_off[v]), G.vflags.begin() + G.vflag_off[v]); });
 		return n_kept;
 	}
 
@@ -4623,9 +4653,10 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	std::vector<float> pre_area(nc, 0.0f);
 	auto flags_of = [&](uint32_t v)
 	{ return std::vector<uint32_t>(G.vflags.begin() + G.vflag_off[v], G.vflags.begin() + G.vflag_off[v + 1]); };
-	for (uint32_t c = 0; c < nact; c++)
+	// per contour (independent: each writes its own chosen / pre_area / merge entry)
+	host_parallel_dynamic(nact, [&](uint32_t c)
 	{
-		ContourRT& r = R[c];
+		const ContourRT& r = R[c];
 		const int sel = chosen_idx[c];
 		if (sel >= 0)
 			chosen[c] = r.res[sel];
@@ -4679,7 +4710,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 					}
 		}
 		merge[c].assign(adjc.begin(), adjc.end());
-	}
+	});
 	// the reference evaluates contours in batches: a contour only sees merge partners from
 	// its own or earlier batches (later ones have no object ids yet)
 	const uint32_t bsz = std::max(1u, P->batch_size);
