@@ -741,7 +741,7 @@ namespace u26
 
 		// The subtree roots that split one traversal across kSplit threads: the nodes at
 		// depth log2(kSplit) below the root, or shallower leaves; unused entries ~0.
-		constexpr uint32_t kSplit = 16;
+		constexpr uint32_t kSplit = 8;
 		__global__ void frontier_kernel(const uint2* __restrict__ children, const uint32_t* __restrict__ object_idx, uint32_t n_nodes,
 			uint32_t node_off, uint32_t* __restrict__ out)
 		{
@@ -2975,6 +2975,8 @@ struct u26_scene
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 	uint64_t passes = 0;			  // completed u26_prp_resolve calls (the normals d_fn / d_en / d_vn are the last one's)
+	void* cap_host = nullptr;		  // pinned staging of the captured supports (grow-only)
+	size_t cap_host_bytes = 0;
 	ResponseState resp;
 };
 
@@ -3172,6 +3174,8 @@ U26_API void u26_scene_destroy(u26_scene* s)
 	s->csorter.release();
 	s->fvsorter.release();
 	s->resp.release();
+	if (s->cap_host)
+		cudaFreeHost(s->cap_host);
 	for (u26_lbvh* t : s->otree_f)
 		u26_lbvh_destroy(t);
 	for (u26_lbvh* t : s->otree_e)
@@ -4397,14 +4401,25 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 						S->d_keys.as<uint64_t>(), S->d_root.as<uint32_t>(), S->d_best.as<uint32_t>(), S->d_seg.as<uint32_t>(), S->d_pay.as<float>(),
 						HitKeyCodec{ b }, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_capture.as<u26_prp_hit>());
 					U26_TRY(after_launch(ctx, "capture_kernel"));
-					std::vector<u26_prp_hit> got;
-					U26_TRY(download(ctx, got, S->d_capture.ptr, total));
-					U26_CUDA(ctx, cudaStreamSynchronize(st));
-					for (size_t q = 0; q < list.size(); q++)
+					// through pinned staging: the captured supports can be tens of MB per level
+					const size_t bytes = sizeof(u26_prp_hit) * total;
+					if (S->cap_host_bytes < bytes)
 					{
-						ComboState& cs = R[tasks[list[q]].contour_local].res[tasks[list[q]].combo];
-						cs.hits.assign(got.begin() + off[q], got.begin() + off[q + 1]);
+						if (S->cap_host)
+							cudaFreeHost(S->cap_host);
+						S->cap_host = nullptr;
+						S->cap_host_bytes = 0;
+						U26_CUDA(ctx, cudaMallocHost(&S->cap_host, bytes + bytes / 2));
+						S->cap_host_bytes = bytes + bytes / 2;
 					}
+					U26_CUDA(ctx, cudaMemcpyAsync(S->cap_host, S->d_capture.ptr, bytes, cudaMemcpyDeviceToHost, st));
+					U26_CUDA(ctx, cudaStreamSynchronize(st));
+					const u26_prp_hit* got = static_cast<const u26_prp_hit*>(S->cap_host);
+					host_parallel_dynamic(uint32_t(list.size()), [&](uint32_t q)
+						{
+							ComboState& cs = R[tasks[list[q]].contour_local].res[tasks[list[q]].combo];
+							cs.hits.assign(got + off[q], got + off[q + 1]);
+						});
 				}
 			}
 			std::vector<uint32_t> next;
