@@ -135,10 +135,8 @@ def make_workload(name):
 
 
 def _dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from untangling26_b200.multirank import dist_env
+    return dist_env()
 
 
 def cpu_pass(mesh, max_contours, stride):
@@ -372,12 +370,9 @@ def main():
     ef_tests_pass = int(ef_tests[-1].item())
     prp_tests_pass = results[-1].pairs_tested
     tests_pass = ef_tests_pass + prp_tests_pass
-    total_ms = sum(step_ms)
-    if ws > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = tests_pass * args.steps * ws / (total_ms / 1e3)
+    from untangling26_b200.multirank import job_throughput, job_time_ms
+    total_ms = job_time_ms(sum(step_ms), device=dev)  # max over ranks (each rank runs its own scene replica)
+    value = job_throughput(tests_pass * args.steps, ws, total_ms)
     r0 = results[-1]
     proc = r0.results[(r0.results["flags"] & 16) > 0]
 
