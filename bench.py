@@ -422,7 +422,7 @@ def main():
     resp = {"pairs": rr.num_pairs, "ms_per_pass": rr.ms, "algorithmic_bytes": rs_bytes,
             "achieved": rs_bytes / (rr.ms / 1e3) / 1e9 if rr.ms > 0 else 0.0, "unit": "GB/s",
             "region_words": [int(rr.vert_regions.numel()), int(rr.edge_regions.numel()), int(rr.face_regions.numel())],
-            "note": "host wall time of u26_prp_make_response (hit upload, 12 launches, 3 synchronisations)"}
+            "note": "host wall time of u26_prp_make_response (hit upload, 12 launches, 2 synchronisations)"}
 
     # ---- region-based pair filtering on this pass's regions: proximity VF / EE pairs within
     # 1 mm (no shared vertex) from the scene trees (as narrow-phase templates) through u26_filter_invalid_pairs,

@@ -847,8 +847,8 @@ namespace u26
 		__global__ void __launch_bounds__(128, 7) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
-			TreeView ftree, TreeView etree, const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow,
-			const uint32_t* __restrict__ ffront, const uint32_t* __restrict__ efront, const float* __restrict__ x, const uint2* __restrict__ edges,
+			const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow, const uint32_t* __restrict__ ffront,
+			const uint32_t* __restrict__ efront, const float* __restrict__ x, const uint2* __restrict__ edges,
 			const uint32_t* __restrict__ faces, const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats,
 			uint32_t* __restrict__ dev_err)
 		{
@@ -4030,7 +4030,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * kSplit;
 				raycast_kernel<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
 					S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(),
-					ftv, etv, S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(),
+					S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(),
 					S->d_front.as<uint32_t>() + size_t(nobj) * kSplit,
 					d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
 					(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);

@@ -368,13 +368,13 @@ namespace u26
 		U26_TRY(after_launch(ctx, "prim_count_kernel<3>"));
 		U26_TRY(device_exclusive_scan(ctx, R.ecnt.as<uint32_t>(), in.ne + 1, R.scan_tmp));
 		U26_TRY(device_exclusive_scan(ctx, R.fcnt.as<uint32_t>(), in.nf + 1, R.scan_tmp));
+		// both totals in one round trip (the context's pinned staging holds 16 words)
 		uint32_t tot[2];
 		U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, R.ecnt.as<uint32_t>() + in.ne, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+		U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word + 1, R.fcnt.as<uint32_t>() + in.nf, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
-		tot[0] = *ctx->host_word;
-		U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, R.fcnt.as<uint32_t>() + in.nf, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-		U26_CUDA(ctx, cudaStreamSynchronize(st));
-		tot[1] = *ctx->host_word;
+		tot[0] = ctx->host_word[0];
+		tot[1] = ctx->host_word[1];
 		R.edge_len = in.ne + 1 + tot[0];
 		R.face_len = in.nf + 1 + tot[1];
 		U26_CUDA(ctx, R.ecsr.reserve(sizeof(uint32_t) * R.edge_len));
