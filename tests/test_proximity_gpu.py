@@ -92,3 +92,28 @@ def test_degenerate_filter_pass(oracle, u26ctx):
     res = sc.host_resolve(prp_params(**kw), num_pairs=len(mod))
     _compare(res, ref)
     sc.close()
+
+
+def test_proximity_conversion_overflow(oracle, u26ctx):
+    """An EF list too small for the converted pairs: the count still reaches the full total (so the
+    caller can grow the list), every slot below the capacity is written and none past it."""
+    from untangling26_b200._native import ptr
+    m = synthetic.sheets_in_contact(16, seed=0)
+    pairs, pidx = contact_pairs(m, 16)
+    vae, eaf = m.vert_adj_edges.one_array(), m.edge_adj_faces_ext.one_array()
+    efp, _ = oracle.ef_from_proximity(pairs, pidx, m.x, m.edges, m.faces, vae, eaf)
+    cap = 8
+    assert len(efp) > cap
+    dev = torch.device("cuda", u26ctx.device)
+    nl, ni, cnt = _device_lists(u26ctx, pairs, pidx)
+    up = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int32).copy()).to(dev)
+    x, edges, faces, d_vae, d_eaf = up(m.x), up(m.edges), up(m.faces), up(vae), up(eaf)
+    ef_list = torch.full((2 * cap, 12), -7, dtype=torch.int32, device=dev)
+    ef_idx = torch.full((2 * cap, 2), -7, dtype=torch.int32, device=dev)
+    ef_count = torch.zeros(1, dtype=torch.int32, device=dev)
+    u26ctx.check(u26ctx.lib.u26_ef_add_from_proximity(u26ctx.handle, ptr(nl), ptr(ni), ptr(cnt), len(pairs), ptr(x), ptr(edges),
+                                                      ptr(faces), ptr(d_vae), ptr(d_eaf), ptr(ef_count), ptr(ef_list), ptr(ef_idx), cap),
+                 "ef_add_from_proximity")
+    assert int(ef_count.item()) == len(efp)
+    assert bool((ef_list[:cap] != -7).any(1).all()) and bool((ef_idx[:cap] != -7).any(1).all())
+    assert bool((ef_list[cap:] == -7).all()) and bool((ef_idx[cap:] == -7).all())

@@ -98,3 +98,18 @@ def test_response_narrow_list_capacity(oracle, u26ctx):
         _run(oracle, u26ctx, m, narrow=(nl, ni), first=2)
     assert e.value.status == 1
     assert torch.all(nl == -5) and torch.all(ni == -9)
+
+
+def test_response_without_intersections(oracle, u26ctx):
+    """No EF pairs: no response pairs, every region row empty, a narrow list left untouched."""
+    m = synthetic.two_sheets(16, seed=0)
+    m.x[m.num_verts // 2:, 2] += 3.0
+    dev = torch.device("cuda", u26ctx.device)
+    nl = torch.full((16, 16), -5, dtype=torch.int32, device=dev)
+    ni = torch.full((16, 2), -9, dtype=torch.int32, device=dev)
+    res, ref = _run(oracle, u26ctx, m, narrow=(nl, ni), first=3)
+    assert res.response.num_pairs == 0 and len(ref.response_pairs) == 0
+    _compare(res, ref)
+    vr = res.response.vert_regions.cpu().numpy().view(np.uint32)
+    assert len(vr) == m.num_verts + 1 and np.all(vr == m.num_verts + 1)
+    assert torch.all(nl == -5) and torch.all(ni == -9)
