@@ -291,6 +291,7 @@ typedef struct u26_prp_output_view
 	uint64_t ray_tri_fetches;		 /* triangle leaf records brought in (one per packet leaf visit) */
 	uint64_t ray_edge_fetches;		 /* edge leaf records brought in */
 	uint64_t ray_visits;			 /* BVH node tests each ray alone would make (the per-ray traversal work) */
+	uint64_t ray_candidate_tests;	 /* leaf tests whose primitive is a candidate target of the request's task */
 } u26_prp_output_view;
 
 /* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any

@@ -218,6 +218,7 @@ class PrpParams(ctypes.Structure):
         ("solid_eps_n", ctypes.c_float),        # PRP_solid_interior_adjacency_normal_eps
         ("solid_eps_d", ctypes.c_float),        # PRP_solid_interior_adjacency_dist_eps
         ("ignore_near_zero_dist_pairs", ctypes.c_uint32),  # scene_params.h:55
+        ("contour_offset", ctypes.c_uint32),    # with contour_stride: contours c with c % stride == offset % stride
     ]
 
 
@@ -225,7 +226,7 @@ def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, brute_force_raycast=0, contour_stride=0, opt_iterations=0, ccr_blend=0,
                   ccr_blend_weight=0.5, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5,
-                  ignore_near_zero_dist_pairs=1)
+                  ignore_near_zero_dist_pairs=1, contour_offset=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p

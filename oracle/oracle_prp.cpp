@@ -93,6 +93,7 @@ namespace
 		float solid_eps_n;		// PRP_solid_interior_adjacency_normal_eps (1e-4)
 		float solid_eps_d;		// PRP_solid_interior_adjacency_dist_eps (1e-5)
 		uint ignore_near_zero_dist_pairs; // scene_params.h:55 (1; the CLI sets 0)
+		uint contour_offset; // with contour_stride: evaluate contours c with c % stride == offset % stride
 	};
 
 	struct EfPair
@@ -2395,7 +2396,7 @@ namespace
 		std::vector<uint> active;
 		const uint stride = std::max(1u, S.p.contour_stride);
 		for (uint c = 0; c < nc && c < S.p.max_contours; c++)
-			if (c % stride == 0)
+			if (c % stride == S.p.contour_offset % stride)
 				active.push_back(c);
 		const uint bs = std::max(1u, S.p.batch_size);
 		for (size_t b0 = 0; b0 < active.size(); b0 += bs)

@@ -60,4 +60,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_lbvh_goldens.py /path/to/reference-checkout")
+    main(sys.argv[1])

@@ -862,7 +862,7 @@ namespace u26
 			if (part >= kSplit)
 				return; // whole warps only
 			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
-			uint32_t tested = 0, visited = 0, etested = 0;
+			uint32_t tested = 0, visited = 0, etested = 0, ctested = 0;
 			uint32_t fetch_nodes = 0, fetch_tris = 0, fetch_edges = 0; // warp-uniform: data each packet brings in
 			uint32_t ray_visits = 0; // the node tests this ray alone would make: its start + 2 per inner node it enters
 
@@ -974,6 +974,7 @@ namespace u26
 							tested++;
 							if (bit_test(bits, tgt_lo, tgt_cnt, fid))
 							{
+								ctested++;
 								const uint32_t f0 = faces[3 * fid], f1 = faces[3 * fid + 1], f2 = faces[3 * fid + 2];
 								if (vid != f0 && vid != f1 && vid != f2)
 								{
@@ -1104,6 +1105,7 @@ namespace u26
 							etested++;
 							if (bit_test(bits, tgt_lo, tgt_cnt, e2))
 							{
+								ctested++;
 								const uint2 qv = edges[e2];
 								if (!(ev.x == qv.x || ev.x == qv.y || ev.y == qv.x || ev.y == qv.y))
 								{
@@ -1198,12 +1200,14 @@ namespace u26
 				const uint32_t vsum = __reduce_add_sync(0xFFFFFFFFu, visited);
 				const uint32_t esum = __reduce_add_sync(0xFFFFFFFFu, etested);
 				const uint32_t rvsum = __reduce_add_sync(0xFFFFFFFFu, ray_visits);
+				const uint32_t csum = __reduce_add_sync(0xFFFFFFFFu, ctested);
 				if (lane == 0)
 				{
 					// [0] leaf primitive tests, [1] requests, [2] ray-node tests, [3] edge leaf tests,
 					// [4] node fetches, [5] triangle fetches, [6] edge fetches (per packet),
-					// [7] single-ray node visits
+					// [7] single-ray node visits, [8] leaf tests of candidate targets
 					atomicAdd(stats + 7, (unsigned long long)rvsum);
+					atomicAdd(stats + 8, (unsigned long long)csum);
 					atomicAdd(stats + 0, (unsigned long long)tsum);
 					atomicAdd(stats + 1, (unsigned long long)rsum);
 					atomicAdd(stats + 2, (unsigned long long)vsum);
@@ -2991,7 +2995,7 @@ struct u26_prp_output
 	uint64_t ray_tests = 0, ray_requests = 0, ray_pairs = 0;
 	double stage_ms[8] = { 0 };
 	double gpu_ms[6] = { 0 };
-	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0;
+	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0, ray_candidate_tests = 0;
 	const u26_scene* scene = nullptr; // the pass this output came from
 	uint64_t pass = 0;
 };
@@ -3820,8 +3824,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 
 	// ---- 3. adaptive k-ring levels, every active (contour, direction) task batched
 	const int b = bits_for(std::max({ S->nv, S->ne, S->nf, 2u }));
-	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 8));
-	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 8, st));
+	U26_CUDA(ctx, S->d_stats.reserve(sizeof(unsigned long long) * 16));
+	U26_CUDA(ctx, cudaMemsetAsync(S->d_stats.ptr, 0, sizeof(unsigned long long) * 16, st));
 	const TreeView ftv = tree_view(face_tree), etv = tree_view(edge_tree);
 	// The ray casts traverse one face tree and one edge tree per object (the reference's
 	// per-object CachedBVH): a ray tests only its target object's primitives. The trees are
@@ -4834,7 +4838,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->hits.insert(out->hits.end(), cs.hits.begin(), cs.hits.end());
 	}
 	std::vector<unsigned long long> stats;
-	U26_TRY(download(ctx, stats, S->d_stats.ptr, 8));
+	U26_TRY(download(ctx, stats, S->d_stats.ptr, 16));
 	U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, ctx->dev_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
 	U26_CUDA(ctx, cudaStreamSynchronize(st));
 	out->ray_tests = stats[0];
@@ -4846,6 +4850,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	out->ray_tri_fetches = stats[5];
 	out->ray_edge_fetches = stats[6];
 	out->ray_visits = stats[7];
+	out->ray_candidate_tests = stats[8];
 	out->dev_err = *ctx->host_word;
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
@@ -4955,6 +4960,7 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->ray_tri_fetches = o->ray_tri_fetches;
 	v->ray_edge_fetches = o->ray_edge_fetches;
 	v->ray_visits = o->ray_visits;
+	v->ray_candidate_tests = o->ray_candidate_tests;
 	for (int i = 0; i < 6; i++)
 		v->gpu_ms[i] = o->gpu_ms[i];
 	v->levels = o->levels;

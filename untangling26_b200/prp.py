@@ -70,7 +70,7 @@ class PrpOutputView(ctypes.Structure):
         ("directions", c_vp), ("ray_tests", c_u64), ("ray_requests", c_u64), ("ray_pairs", c_u64), ("levels", c_u32),
         ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8), ("ray_nodes", c_u64),
         ("ray_edge_tests", c_u64), ("gpu_ms", ctypes.c_double * 6), ("ray_node_fetches", c_u64), ("ray_tri_fetches", c_u64),
-        ("ray_edge_fetches", c_u64), ("ray_visits", c_u64),
+        ("ray_edge_fetches", c_u64), ("ray_visits", c_u64), ("ray_candidate_tests", c_u64),
     ]
 
 GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
@@ -181,3 +181,4 @@ class PrpResult:
         self.tri_fetches = int(v.ray_tri_fetches)
         self.edge_fetches = int(v.ray_edge_fetches)
         self.ray_visits = int(v.ray_visits)
+        self.candidate_tests = int(v.ray_candidate_tests)

@@ -238,6 +238,30 @@ def batch_scenes(num=64, seed=2, tris_lo=2000, tris_hi=60000, spacing=3.0):
     return m
 
 
+def sub_batch(batch, scene_ids):
+    """The listed scenes of a batch_scenes mesh as a batch of their own (same positions, in
+    the listed order); meta["scenes"][j]["batch_scene"] names scene j's index in `batch`."""
+    xs, rests, fs, obj, scenes = [], [], [], [], []
+    nv = nf = 0
+    for j, s in enumerate(scene_ids):
+        sc = batch.meta["scenes"][s]
+        v0, v1 = sc["verts"]
+        f0, f1 = sc["faces"]
+        xs.append(batch.x[v0:v1])
+        rests.append(batch.rest_x[v0:v1])
+        fs.append(batch.faces[f0:f1] - v0 + nv)
+        obj.append(batch.object_of_vert[v0:v1] - batch.object_of_vert[v0] + 2 * j)
+        scenes.append(dict(sc, verts=[nv, nv + v1 - v0], faces=[nf, nf + f1 - f0], batch_scene=int(s)))
+        nv += v1 - v0
+        nf += f1 - f0
+    m = Mesh(np.concatenate(xs), np.concatenate(fs).astype(np.uint32), object_of_vert=np.concatenate(obj).astype(np.uint32),
+             rest_x=np.concatenate(rests))
+    m.object_scene = np.repeat(np.arange(len(scene_ids), dtype=np.uint32), 2)
+    m.meta = {"kind": "batch_scenes", "num": len(scene_ids), "seed": batch.meta["seed"], "scenes": scenes,
+              "of_batch": batch.meta["num"]}
+    return m
+
+
 def scene_mesh(batch, s):
     """Scene s of a batch_scenes mesh as a mesh of its own (same positions)."""
     sc = batch.meta["scenes"][s]
