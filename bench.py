@@ -325,6 +325,27 @@ def _timed_passes(runner, steps, flush, stream):
     return [a.elapsed_time(b) for a, b in ev], out
 
 
+def refit_rate(sc, mesh, flush, stream, peak, n=10):
+    """Median time of the fused leaf update + refit of the scene's face tree over n launches
+    (L2 flushed before each). Algorithmic bytes, each once: V x (12 B position + 4 B
+    thickness) + F x (12 B face + 4 B leaf order + 32 B leaf box written) + (F - 1) x
+    (8 B children + 4 B parent + 4 B range + 64 B child boxes read + 32 B box written)."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n + 2)]
+    for i, (a, b) in enumerate(ev):
+        flush.fill_((i + 7) & 0xFF)
+        a.record(stream)
+        sc.refit_face_tree()
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.median(a.elapsed_time(b) for a, b in ev[2:])
+    byts = 16 * mesh.num_verts + 48 * mesh.num_faces + 112 * max(mesh.num_faces - 1, 0)
+    out = {"kernel": "refit_block_kernel", "triangles": int(mesh.num_faces), "ms": ms, "algorithmic_bytes": byts,
+           "achieved": byts / (ms / 1e3) / 1e9, "unit": "GB/s", "peak": peak}
+    out["frac"] = out["achieved"] / peak
+    return out
+
+
 def _traffic(kernel, workload):
     prof = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if not os.path.exists(prof):
@@ -430,19 +451,18 @@ def main():
         roof["traffic_source"] = tr.get("source")
     roof["packet_record_bytes_per_pass"] = 32 * r0.node_fetches + 48 * r0.tri_fetches + 32 * r0.edge_fetches + 24 * r0.requests
 
-    # ---- LBVH refit alone (fused leaf update + bottom-up refit of the face tree), L2 flushed
-    rf_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(10)]
-    for i, (a, b) in enumerate(rf_ev):
-        flush.fill_((i + 7) & 0xFF)
-        a.record(stream)
-        runner.sc.refit_face_tree()
-        b.record(stream)
-    torch.cuda.synchronize()
-    rf_ms = statistics.median(a.elapsed_time(b) for a, b in rf_ev)
-    rf_bytes = 16 * tmesh.num_verts + 48 * tmesh.num_faces + 108 * max(tmesh.num_faces - 1, 0)
-    refit = {"kernel": "refit_fused_kernel", "triangles": int(tmesh.num_faces), "ms": rf_ms, "algorithmic_bytes": rf_bytes,
-             "achieved": rf_bytes / (rf_ms / 1e3) / 1e9, "unit": "GB/s", "peak": peak}
-    refit["frac"] = refit["achieved"] / peak
+    # ---- LBVH refit alone (fused leaf update + bottom-up refit of a face tree), L2 flushed
+    # before each launch: the timed batch's scene tree and the scale form's mesh (five stacked
+    # 512 x 512 sheets, 2.6 M triangles), where the refit is long enough to be bandwidth-bound
+    refit = {"timed_batch": refit_rate(runner.sc, tmesh, flush, stream, peak)}
+    if ws == 1:
+        from untangling26_b200 import synthetic
+        from untangling26_b200.intersection_resolver import CollisionScene
+        lm = synthetic.layered_sheets(512, layers=5, seed=4)
+        lsc = CollisionScene(ctx, lm, d_hat=1e-3, thickness=0.0, max_broad_pairs=1, max_ef_pairs=1)
+        lsc.construct_lbvh()
+        refit["layered_5x512"] = refit_rate(lsc, lm, flush, stream, peak)
+        lsc.close()
     runner.close()
 
     # ---- the whole batch: chosen form and the plain form (per-scene passes, one thread per

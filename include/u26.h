@@ -145,7 +145,10 @@ U26_API u26_status u26_ef_narrow_phase(u26_ctx* ctx, const uint32_t* broad_pairs
  * list would not have overflowed. edge_order (optional, uint32[num_edges]) is the order
  * in which threads take the edges, e.g. an edge tree's sorted_get_original so that a
  * warp walks spatially close edges; NULL means edge id order. stats (optional,
- * uint64[2]) accumulates node boxes tested and leaf triangles tested. */
+ * uint64[4]) accumulates node boxes tested, leaf triangles tested, and (given stats) the
+ * FP64 recheck of every EF test whose FP32 decision lies inside its static error band:
+ * [2] the tests rechecked, [3] those whose FP64 decision differs. The EF set keeps the
+ * FP32 decisions either way. */
 U26_API u26_status u26_ef_detect(u26_lbvh* face_tree, const float* x, const uint32_t* edges, uint32_t num_edges,
 	const uint32_t* faces, const uint32_t* vert_property, const float* d_hat, const float* thickness,
 	const uint32_t* edge_order, uint32_t* ef_count, void* ef_pairs, uint32_t* ef_indices, uint32_t max_ef,
@@ -236,6 +239,10 @@ typedef struct u26_prp_params
 	uint32_t ignore_near_zero_dist_pairs; /* ignore_near_zero_dist_pairs (1, scene_params.h:55; the CLI sets 0):
 										   * 0 drops degenerate EF pairs (a barycentric coordinate < 1e-4) that
 										   * have no non-degenerate adjacent pair (intersection_resolver.cpp:841-896) */
+	uint32_t fp64_recheck;		/* 1 (default): every VF / FV / EE leaf test of the batched form whose FP32 decision lies
+								 * inside its static forward-error band is re-evaluated in FP64 and counted
+								 * (u26_prp_output_view.fp64_rechecks / fp64_flips); the hit sets keep the FP32
+								 * decisions. Also evaluates the selected supports' metrics in FP64 (fp64_*_rel_err). */
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:
@@ -292,6 +299,14 @@ typedef struct u26_prp_output_view
 	uint64_t ray_edge_fetches;		 /* edge leaf records brought in */
 	uint64_t ray_visits;			 /* BVH node tests each ray alone would make (the per-ray traversal work) */
 	uint64_t ray_candidate_tests;	 /* leaf tests whose primitive is a candidate target of the request's task */
+	uint64_t fp64_rechecks;			 /* with fp64_recheck: leaf tests inside their FP32 error band, re-evaluated in FP64 */
+	uint64_t fp64_flips;			 /* ... of which the FP64 decision differs from the FP32 one (the hit sets keep FP32) */
+	uint64_t dc_tie_rechecks;		 /* selected supports whose largest and second largest depth lie within the depth's
+									  * error band (the argmax that sets D_C is uncertain), re-evaluated in FP64 */
+	uint64_t dc_tie_flips;			 /* ... of which the FP64 argmax is another hit */
+	double fp64_delta_rel_err;		 /* max over the selected hits of |delta_32 - delta_64| / delta_64 */
+	double fp64_dc_rel_err;			 /* max over processed contours of |D_C,32 - D_C,64| / D_C,64 (depth) */
+	double fp64_j_rel_err;			 /* max over processed contours of |J_32 - J_64| / J_64 (objective) */
 } u26_prp_output_view;
 
 /* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any

@@ -189,6 +189,17 @@ def ef_narrow(broad_pairs, x, edges, faces, d_hat, vprop=None):
     return out[:cnt], idx[:cnt]
 
 
+def ef_recheck(broad_pairs, x, edges, faces, d_hat, vprop=None):
+    """FP64 recheck counts of the EF tests over broad-phase pairs: (rechecked, flipped)."""
+    broad_pairs = np.ascontiguousarray(broad_pairs, dtype=np.uint32).reshape(-1, 2)
+    arrs = [np.ascontiguousarray(a, t) for a, t in ((x, np.float32), (edges, np.uint32), (faces, np.uint32), (d_hat, np.float32))]
+    vp = None if vprop is None else np.ascontiguousarray(vprop, dtype=np.uint32)
+    out = np.zeros(2, np.uint64)
+    lib().oracle_ef_recheck(_p(broad_pairs, _u32p), ctypes.c_uint32(len(broad_pairs)), _p(arrs[0], _f32p), _p(arrs[1], _u32p),
+                            _p(arrs[2], _u32p), _pn(vp, _u32p), _p(arrs[3], _f32p), _p(out, _u64p))
+    return int(out[0]), int(out[1])
+
+
 def line_intersection(p0, p1, a, b, c):
     arrs = [np.ascontiguousarray(v, dtype=np.float32) for v in (p0, p1, a, b, c)]
     bary = np.zeros(3, np.float32)
@@ -219,6 +230,7 @@ class PrpParams(ctypes.Structure):
         ("solid_eps_d", ctypes.c_float),        # PRP_solid_interior_adjacency_dist_eps
         ("ignore_near_zero_dist_pairs", ctypes.c_uint32),  # scene_params.h:55
         ("contour_offset", ctypes.c_uint32),    # with contour_stride: contours c with c % stride == offset % stride
+        ("fp64_recheck", ctypes.c_uint32),      # count the FP64 rechecks of the leaf tests inside their FP32 error band
     ]
 
 
@@ -226,7 +238,7 @@ def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, brute_force_raycast=0, contour_stride=0, opt_iterations=0, ccr_blend=0,
                   ccr_blend_weight=0.5, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5,
-                  ignore_near_zero_dist_pairs=1, contour_offset=0)
+                  ignore_near_zero_dist_pairs=1, contour_offset=0, fp64_recheck=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -303,6 +315,23 @@ class PrpRun:
             st = np.zeros(3, np.uint64)
             L.oracle_prp_stats(h, _p(st, _u64p))
             self.tested, self.requests, self.pairs_tested = int(st[0]), int(st[1]), int(st[2])
+            rc = np.zeros(2, np.uint64)
+            L.oracle_prp_recheck(h, _p(rc, _u64p))
+            # FP64: per contour (J, D_C, max relative depth error, D_C tie, tie flip)
+            f64 = np.zeros((max(nc, 1), 5), np.float64)
+            L.oracle_prp_fp64(h, f64.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+            self.fp64_contours = f64[:nc]
+            with np.errstate(divide="ignore", invalid="ignore"):
+                has = f64[:nc, 1] > 0
+                j32 = self.results["objective"].astype(np.float64)
+                d32 = self.results["depth"].astype(np.float64)
+                jerr = np.abs(j32 - f64[:nc, 0]) / f64[:nc, 0]
+                derr = np.abs(d32 - f64[:nc, 1]) / f64[:nc, 1]
+            self.fp64 = {"rechecks": int(rc[0]), "flips": int(rc[1]), "dc_tie_rechecks": int(f64[:nc, 3].sum()),
+                         "dc_tie_flips": int(f64[:nc, 4].sum()),
+                         "delta_rel_err": float(f64[:nc, 2].max()) if nc else 0.0,
+                         "dc_rel_err": float(derr[has].max()) if has.any() else 0.0,
+                         "j_rel_err": float(jerr[(f64[:nc, 0] > 0)].max()) if (f64[:nc, 0] > 0).any() else 0.0}
             if response is not None:
                 L.oracle_prp_response.restype = ctypes.c_uint32
                 dt, k = ctypes.c_float(response[0]), ctypes.c_float(response[1])

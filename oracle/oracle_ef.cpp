@@ -6,6 +6,7 @@
 //   Solver/SimulationCore/collision_data.h:150-220  EfPair layout (48 bytes)
 // Loaded only by tests/ and bench.py's cpu_baseline leg.
 #include "oracle_common.h"
+#include "oracle_fp64.h"
 
 using namespace u26o;
 
@@ -175,5 +176,40 @@ extern "C"
 			out_indices[2 * k + 1] = broad_pairs[2 * order[k] + 1];
 		}
 		return count;
+	}
+
+	// The FP64 recheck of the EF tests over broad-phase pairs (u26_ef_detect's stats[2..3]):
+	// out[0] tests rechecked (FP32 decision inside its error band), out[1] FP32 / FP64 flips.
+	void oracle_ef_recheck(const uint* broad_pairs, uint num_broad, const float* x, const uint* edges, const uint* faces,
+		const uint* vprop, const float* d_hat, uint64_t* out)
+	{
+		std::vector<uint8_t> rc(num_broad, 0);
+		parallel_for(num_broad, [&](uint i)
+			{
+				const uint eid = broad_pairs[2 * i], fid = broad_pairs[2 * i + 1];
+				const uint e0 = edges[2 * eid], e1 = edges[2 * eid + 1];
+				const uint f0 = faces[3 * fid], f1 = faces[3 * fid + 1], f2 = faces[3 * fid + 2];
+				if (e0 == f0 || e0 == f1 || e0 == f2 || e1 == f0 || e1 == f1 || e1 == f2)
+					return;
+				const uint lp = vprop ? vprop[e0] : 0u;
+				const uint rp = vprop ? vprop[f0] : 0u;
+				if ((vprop_fixed(lp) && vprop_fixed(rp)) || (vprop_rigid(lp) && vprop_rigid(rp) && vprop_object(lp) == vprop_object(rp)))
+					return;
+				if (d_hat[e0] + d_hat[f0] == 0.0f)
+					return;
+				EfPairRec rec;
+				const bool pass32 = ef_test(eid, fid, x, edges, faces, vprop, d_hat, rec);
+				const V3 pe0 = load3(x, e0), pe1 = load3(x, e1), A = load3(x, f0), B = load3(x, f1), C = load3(x, f2);
+				V3 fb = v3(0.0f);
+				float t = 0.0f;
+				const bool seg32 = line_intersection(pe0, pe1, A, B, C, fb, t);
+				rc[i] = uint8_t(recheck_ef(pe0, pe1, A, B, C, seg32, t, fb, pass32));
+			});
+		out[0] = out[1] = 0;
+		for (uint i = 0; i < num_broad; i++)
+		{
+			out[0] += rc[i] & 1u;
+			out[1] += rc[i] >> 1;
+		}
 	}
 }

@@ -39,6 +39,7 @@
 #include <string>
 
 #include "oracle_common.h"
+#include "oracle_fp64.h"
 
 namespace u26o
 {
@@ -94,6 +95,7 @@ namespace
 		float solid_eps_d;		// PRP_solid_interior_adjacency_dist_eps (1e-5)
 		uint ignore_near_zero_dist_pairs; // scene_params.h:55 (1; the CLI sets 0)
 		uint contour_offset; // with contour_stride: evaluate contours c with c % stride == offset % stride
+		uint fp64_recheck;	 // count the FP64 rechecks of the leaf tests inside their FP32 error band
 	};
 
 	struct EfPair
@@ -548,8 +550,52 @@ namespace
 		return true;
 	}
 
+	// FP64 recheck counts of the ray casts: leaf tests rechecked, FP32 / FP64 flips. Counted
+	// over the leaf tests the CUDA path's batched form makes: those whose primitive box, grown
+	// by its conservative margin 1e-5 (1 + |coordinate|) per axis, the ray (swept edge) meets.
+	struct Recheck
+	{
+		uint64_t n = 0, flips = 0;
+		void add(uint rc)
+		{
+			n += rc & 1u;
+			flips += rc >> 1;
+		}
+	};
+
+	// the ray [0, 1] of orig + t cast against the face's grown box (the slab test with one
+	// fused multiply-add per plane, as the batched ray casts evaluate it)
+	inline bool face_gate(V3 orig, V3 cast, V3 A, V3 B, V3 C)
+	{
+		const V3 mn = vmin(vmin(A, vmin(B, C)), vmin(A, vmin(B, C))), mx = vmax(vmax(A, vmax(B, C)), vmax(A, vmax(B, C)));
+		const float lo[3] = { mn.x, mn.y, mn.z }, hi[3] = { mx.x, mx.y, mx.z };
+		const float o[3] = { orig.x, orig.y, orig.z }, d[3] = { cast.x, cast.y, cast.z };
+		float tmin = 0.0f, tmax = 1.0f;
+		float a[3], b[3];
+		for (int k = 0; k < 3; k++)
+		{
+			const float e = 1e-5f * (1.0f + std::fmax(std::fabs(lo[k]), std::fabs(hi[k])));
+			const float inv = std::fabs(d[k]) < 1e-30f ? std::copysign(1e30f, d[k]) : 1.0f / d[k];
+			const float oinv = o[k] * inv;
+			a[k] = std::fma(lo[k] - e, inv, -oinv);
+			b[k] = std::fma(hi[k] + e, inv, -oinv);
+		}
+		tmin = std::fmax(std::fmax(tmin, std::fmin(a[0], b[0])), std::fmax(std::fmin(a[1], b[1]), std::fmin(a[2], b[2])));
+		tmax = std::fmin(std::fmin(tmax, std::fmax(a[0], b[0])), std::fmin(std::fmax(a[1], b[1]), std::fmax(a[2], b[2])));
+		return tmin <= tmax;
+	}
+	// the swept edge's box against the target edge's grown box (one margin for all axes)
+	inline bool edge_gate(V3 smin, V3 smax, V3 q0, V3 q1)
+	{
+		const V3 mn = vmin(q0, q1), mx = vmax(q0, q1);
+		const float e = 1e-5f * (1.0f + std::fmax(std::fmax(std::fmax(std::fabs(mn.x), std::fabs(mx.x)), std::fmax(std::fabs(mn.y), std::fabs(mx.y))),
+			std::fmax(std::fabs(mn.z), std::fabs(mx.z))));
+		return smin.x <= mx.x + e && smax.x >= mn.x - e && smin.y <= mx.y + e && smax.y >= mn.y - e && smin.z <= mx.z + e &&
+			smax.z >= mn.z - e;
+	}
+
 	// ray_cast_from_verts_batched for one request (BVH or brute force over the targets)
-	void cast_vert(const MeshIn& m, const CachedBVH* bvh, const VertRequest& q, std::vector<Hit>& out, uint64_t& tested)
+	void cast_vert(const MeshIn& m, const CachedBVH* bvh, const VertRequest& q, std::vector<Hit>& out, uint64_t& tested, Recheck* rc)
 	{
 		const float ray_max = 1.0f;
 		if (q.target_cnt == 0)
@@ -567,8 +613,16 @@ namespace
 			if (!hop_ok(q.hop, q.max_hop, { m.faces[3 * fid], m.faces[3 * fid + 1], m.faces[3 * fid + 2] }))
 				return;
 			Hit h;
-			if (vert_face_test(m, q.vid, orig, end, fid, h, q.fv, ray_max))
+			const bool hit = vert_face_test(m, q.vid, orig, end, fid, h, q.fv, ray_max);
+			if (hit)
 				out.push_back(h);
+			const uint f0 = m.faces[3 * fid], f1 = m.faces[3 * fid + 1], f2 = m.faces[3 * fid + 2];
+			if (rc && q.vid != f0 && q.vid != f1 && q.vid != f2)
+			{
+				const V3 A = load3(m.x, f0), B = load3(m.x, f1), C = load3(m.x, f2);
+				if (face_gate(orig, cast, A, B, C))
+					rc->add(recheck_vert_face(orig, end, A, B, C, hit));
+			}
 		};
 		if (bvh == nullptr)
 		{
@@ -616,12 +670,14 @@ namespace
 		}
 	}
 
-	void cast_edge(const MeshIn& m, const CachedBVH* bvh, const EdgeRequest& q, std::vector<Hit>& out, uint64_t& tested)
+	void cast_edge(const MeshIn& m, const CachedBVH* bvh, const EdgeRequest& q, std::vector<Hit>& out, uint64_t& tested, Recheck* rc)
 	{
 		const float ray_max = std::fmin(std::fmax(q.max_dist, 0.0f), 1.0f);
 		if (ray_max <= 0.0f || q.target_cnt == 0)
 			return;
 		const EdgeRay r = make_edge_ray(m, q.eid, q.dir, ray_max);
+		const V3 sw_lo = vmin(vmin(r.p0, r.p1), vmin(r.p0 + q.dir * ray_max, r.p1 + q.dir * ray_max));
+		const V3 sw_hi = vmax(vmax(r.p0, r.p1), vmax(r.p0 + q.dir * ray_max, r.p1 + q.dir * ray_max));
 		auto leaf = [&](uint eid2)
 		{
 			tested++;
@@ -632,8 +688,16 @@ namespace
 			if (!hop_ok(q.hop, q.max_hop, { m.edges[2 * eid2], m.edges[2 * eid2 + 1] }))
 				return;
 			Hit h;
-			if (edge_edge_test(m, r, q.eid, eid2, h))
+			const bool hit = edge_edge_test(m, r, q.eid, eid2, h);
+			if (hit)
 				out.push_back(h);
+			const uint a0 = m.edges[2 * q.eid], a1 = m.edges[2 * q.eid + 1], b0 = m.edges[2 * eid2], b1 = m.edges[2 * eid2 + 1];
+			if (rc && !(a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1))
+			{
+				const V3 q0 = load3(m.x, b0), q1 = load3(m.x, b1);
+				if (edge_gate(sw_lo, sw_hi, q0, q1))
+					rc->add(recheck_edge_edge(r.p0, r.p1, q.dir, ray_max, r.plane, r.pn, r.pd, q0, q1, hit));
+			}
 		};
 		if (bvh == nullptr)
 		{
@@ -732,7 +796,7 @@ namespace
 		std::vector<uint8_t> processed, suppressed;
 		std::vector<float> pre_area;
 		std::vector<std::vector<uint>> merge_adj;
-		uint64_t tested = 0, requests = 0, pairs = 0;
+		uint64_t tested = 0, requests = 0, pairs = 0, rechecks = 0, flips = 0;
 		// per-object BVHs (faces, edges)
 		std::vector<std::unique_ptr<CachedBVH>> face_bvh, edge_bvh;
 		std::mutex mtx;
@@ -1744,6 +1808,8 @@ namespace
 		};
 		std::vector<Hit> hits;
 		uint64_t tested = 0, requests = 0, pairs = 0;
+		Recheck rcl;
+		Recheck* rc = S.p.fp64_recheck ? &rcl : nullptr;
 		const bool brute = S.p.brute_force_raycast != 0;
 		const CachedBVH* fb_dst = brute ? nullptr : S.face_bvh[r.object_ids[1]].get();
 		const CachedBVH* eb_dst = brute ? nullptr : S.edge_bvh[r.object_ids[1]].get();
@@ -1761,7 +1827,7 @@ namespace
 			for (uint v : r.cand_v[0])
 			{
 				q.vid = v;
-				cast_vert(m, fb_dst, q, hits, tested);
+				cast_vert(m, fb_dst, q, hits, tested, rc);
 				requests++;
 				pairs += r.cand_f[1].size();
 			}
@@ -1793,7 +1859,7 @@ namespace
 					const float smin = std::fmin(dot(load3(m.x, edge_of(m, e, 0)), dir), dot(load3(m.x, edge_of(m, e, 1)), dir));
 					q.max_dist = std::fmin(std::fmax((pmax - smin) / dl2 + 1e-5f, 0.0f), 1.0f);
 				}
-				cast_edge(m, eb_dst, q, hits, tested);
+				cast_edge(m, eb_dst, q, hits, tested, rc);
 				requests++;
 				pairs += r.cand_e[1].size();
 			}
@@ -1811,7 +1877,7 @@ namespace
 			for (uint v : r.cand_v[1])
 			{
 				q.vid = v;
-				cast_vert(m, fb_src, q, hits, tested);
+				cast_vert(m, fb_src, q, hits, tested, rc);
 				requests++;
 				pairs += r.cand_f[0].size();
 			}
@@ -1821,6 +1887,8 @@ namespace
 			S.tested += tested;
 			S.requests += requests;
 			S.pairs += pairs;
+			S.rechecks += rcl.n;
+			S.flips += rcl.flips;
 		}
 		info.unculled = uint(hits.size());
 		if (hits.empty())
@@ -2794,6 +2862,85 @@ extern "C"
 		out2[0] = S->tested;
 		out2[1] = S->requests;
 		out2[2] = S->pairs;
+	}
+	// FP64 recheck counts of the ray casts (fp64_recheck set): rechecked, flipped
+	void oracle_prp_recheck(void* h, uint64_t* out2)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		out2[0] = S->rechecks;
+		out2[1] = S->flips;
+	}
+	// The selected supports in FP64 (the double instantiation of prp_eval_penetration_v2's
+	// depth, D_C and J, intersection_resolver2.cpp:1883-1954): per contour with a response,
+	// out[c] = {J_64, D_C_64, max relative depth error, tie, flip} (tie: the two largest FP32
+	// depths lie within 4 g D_C of each other; flip: the FP64 argmax is another hit), and
+	// zeros elsewhere. Hits in canonical order; sums and maxima sequential in double.
+	void oracle_prp_fp64(void* h, double* out5)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		const MeshIn& m = S->m;
+		for (uint c = 0; c < uint(S->selected.size()); c++)
+		{
+			double* o = out5 + 5 * size_t(c);
+			o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
+			const ComboInfo& ci = S->selected[c];
+			if (!ci.present || ci.hits.empty())
+				continue;
+			std::vector<Hit> hs = ci.hits;
+			std::sort(hs.begin(), hs.end(), [](const Hit& a, const Hit& b)
+				{ return a.type != b.type ? a.type < b.type : (a.src_id != b.src_id ? a.src_id < b.src_id : a.dst_id < b.dst_id); });
+			double area = 0.0, dc64 = -1.0, derr = 0.0;
+			float m32 = -1.0f, s32 = -1.0f;
+			size_t arg32 = 0, arg64 = 0;
+			for (size_t i = 0; i < hs.size(); i++)
+			{
+				const Hit& hh = hs[i];
+				double d64;
+				if (hh.type == EE)
+				{
+					const D3 p0 = d3(load3(m.x, m.edges[2 * hh.src_id])), p1 = d3(load3(m.x, m.edges[2 * hh.src_id + 1]));
+					const D3 q0 = d3(load3(m.x, m.edges[2 * hh.dst_id])), q1 = d3(load3(m.x, m.edges[2 * hh.dst_id + 1]));
+					const D3 n = crossd(p1 - p0, q1 - q0);
+					const double det = -dotd(d3(ci.dir), n);
+					d64 = det != 0.0 ? -dotd(q0 - p0, n) / det : double(hh.dist);
+				}
+				else
+				{
+					const bool fv = hh.type == FV;
+					const uint v = fv ? hh.dst_id : hh.src_id, f = fv ? hh.src_id : hh.dst_id;
+					const V3 orig = load3(m.x, v);
+					const V3 end = orig + (fv ? -ci.dir : ci.dir) * 1.0f;
+					D3 b64;
+					double t64;
+					d64 = seg_tri_f64(d3(orig), d3(end), d3(load3(m.x, m.faces[3 * f])), d3(load3(m.x, m.faces[3 * f + 1])),
+							  d3(load3(m.x, m.faces[3 * f + 2])), b64, t64)
+						? t64 * 1.0
+						: double(hh.dist);
+				}
+				area += double(hh.type == VF ? m.rest_vert_area[hh.src_id] : hh.type == EE ? m.rest_edge_area[hh.src_id] : m.rest_face_area[hh.src_id]);
+				if (d64 > dc64)
+				{
+					dc64 = d64;
+					arg64 = i;
+				}
+				if (hh.dist > m32)
+				{
+					s32 = m32;
+					m32 = hh.dist;
+					arg32 = i;
+				}
+				else if (hh.dist > s32)
+					s32 = hh.dist;
+				if (d64 > 0.0)
+					derr = std::fmax(derr, std::fabs(double(hh.dist) - d64) / d64);
+			}
+			const bool tie = hs.size() > 1 && m32 - s32 <= 4.0f * kGamma * m32;
+			o[0] = area * dc64 * dc64;
+			o[1] = dc64;
+			o[2] = derr;
+			o[3] = tie ? 1.0 : 0.0;
+			o[4] = (tie && arg64 != arg32) ? 1.0 : 0.0;
+		}
 	}
 	// response pairs and region CSRs of a finished run; returns the pair count. Any output
 	// may be null (sizes: pairs 64 B each, info 4 words each, CSRs *_len words).

@@ -151,3 +151,27 @@ def test_capacity_truncation_reports_count(oracle, u26ctx):
     t.broad_phase_query_from_edges_unculled(dx0, dx0, _dev(m.edges), count, pairs, _dev(d_hat), dth)
     assert int(count.item()) == total > 8
     assert (pairs.cpu().numpy() != -7).all()
+
+
+@pytest.mark.parametrize("n_leaves", [511, 512, 513, 1025, 70000])
+def test_repeated_refits(oracle, u26ctx, n_leaves):
+    """Refit after refit at moving positions, fused and leaf-only: the block-local climb's
+    device arrival counters carry over between refits (2 per refit, never reset), every
+    refit's boxes equal the oracle's."""
+    rng = np.random.default_rng(n_leaves)
+    x = rng.uniform(-1, 1, (n_leaves * 3, 3)).astype(np.float32)
+    f = np.arange(n_leaves * 3, dtype=np.uint32).reshape(-1, 3)
+    m = Mesh(x, f)
+    th = np.zeros(m.num_verts, np.float32)
+    ot, t, (dx0, dx1, dth, dprims) = _build_both(oracle, u26ctx, TREE_FACE, m)
+    for k in range(4):
+        xk = (x + np.float32(0.05 * (k + 1)) * np.sin(x * (k + 2))).astype(np.float32)
+        oracle.lbvh_refit(ot, xk, xk, th, m.faces)
+        dxk = _dev(xk)
+        if k % 2:
+            t.update_face_tree_leave_aabb(dth, dxk, dxk, dprims)
+            t.refit()
+        else:
+            t.update_and_refit(dth, dxk, dxk, dprims)
+        assert t.check_health()
+        _assert_tree_equal(ot, t.arrays())

@@ -12,6 +12,7 @@
 //    walks the face tree in the reference's visit order and tests the triangle as soon
 //    as a leaf overlaps, so no broad-phase list is written or re-read.
 #include "lbvh_internal.h"
+#include "predicates.cuh"
 
 namespace u26
 {
@@ -70,9 +71,10 @@ namespace u26
 		return false;
 	}
 
-	// The per-pair body of fn_narrow_phase_ef_dcd_query.
-	__device__ __forceinline__ bool ef_pair_test(uint32_t e0, uint32_t e1, uint32_t f0, uint32_t f1, uint32_t f2,
-		const float* __restrict__ x, const uint32_t* __restrict__ vprop, const float* __restrict__ d_hat, EfPairDev& rec)
+	// The pair filters of fn_narrow_phase_ef_dcd_query ahead of the geometric test: shared
+	// vertices, vertex properties, zero contact distance (exact, no rounding involved).
+	__device__ __forceinline__ bool ef_pair_eligible(uint32_t e0, uint32_t e1, uint32_t f0, uint32_t f1, uint32_t f2,
+		const uint32_t* __restrict__ vprop, const float* __restrict__ d_hat)
 	{
 		if (e0 == f0 || e0 == f1 || e0 == f2 || e1 == f0 || e1 == f1 || e1 == f2)
 			return false;
@@ -82,7 +84,30 @@ namespace u26
 			return false;
 		if ((lp & 2u) && (rp & 2u) && ((lp >> 16) & 0x7FFFu) == ((rp >> 16) & 0x7FFFu))
 			return false;
-		if (__ldg(d_hat + e0) + __ldg(d_hat + f0) == 0.0f)
+		return __ldg(d_hat + e0) + __ldg(d_hat + f0) != 0.0f;
+	}
+
+	// The FP64 recheck of one EF test (predicates.cuh): 0 when its FP32 decision (pass32) lies
+	// outside the error band, else 1, plus 2 when the FP64 decision differs. Out of line: it
+	// runs once per eligible leaf test and keeps its registers off the traversal loop.
+	__device__ __noinline__ uint32_t ef_recheck(f3 pe0, f3 pe1, f3 A, f3 B, f3 C, bool pass32)
+	{
+		f3 fb = mk3(0.0f);
+		float t = 0.0f;
+		const bool seg32 = line_intersection(pe0, pe1, A, B, C, fb, t);
+		Band bd;
+		ef_pair_band(pe0, pe1, A, B, C, seg32, t, fb, bd);
+		if (!bd.recheck())
+			return 0u;
+		const bool pass64 = ef_pair_f64(dd(pe0), dd(pe1), dd(A), dd(B), dd(C));
+		return 1u | (pass64 != pass32 ? 2u : 0u);
+	}
+
+	// The per-pair body of fn_narrow_phase_ef_dcd_query.
+	__device__ __forceinline__ bool ef_pair_test(uint32_t e0, uint32_t e1, uint32_t f0, uint32_t f1, uint32_t f2,
+		const float* __restrict__ x, const uint32_t* __restrict__ vprop, const float* __restrict__ d_hat, EfPairDev& rec)
+	{
+		if (!ef_pair_eligible(e0, e1, f0, f1, f2, vprop, d_hat))
 			return false;
 		const f3 pe0 = ld3(x, e0), pe1 = ld3(x, e1);
 		const f3 A = ld3(x, f0), B = ld3(x, f1), C = ld3(x, f2);
@@ -175,7 +200,7 @@ namespace u26
 			uint32_t stack[32];
 			int sp = 0;
 			stack[sp++] = 0u;
-			uint32_t loop = 0, visited = 0, tested = 0;
+			uint32_t loop = 0, visited = 0, tested = 0, rechecks = 0, flips = 0;
 			while (sp > 0)
 			{
 				const uint32_t node = stack[--sp];
@@ -199,11 +224,18 @@ namespace u26
 							tested++;
 							const uint32_t f0 = __ldg(faces + 3 * fid), f1 = __ldg(faces + 3 * fid + 1), f2 = __ldg(faces + 3 * fid + 2);
 							EfPairDev rec;
-							if (ef_pair_test(e.x, e.y, f0, f1, f2, x, vprop, d_hat, rec))
+							const bool pass32 = ef_pair_test(e.x, e.y, f0, f1, f2, x, vprop, d_hat, rec);
+							if (pass32)
 							{
 								const uint32_t slot = atomicAdd(ef_count, 1u);
 								if (slot < max_ef)
 									store_ef(out, out_idx, slot, rec, eid, fid);
+							}
+							if (stats && ef_pair_eligible(e.x, e.y, f0, f1, f2, vprop, d_hat))
+							{
+								const uint32_t rc = ef_recheck(pa, pb, ld3(x, f0), ld3(x, f1), ld3(x, f2), pass32);
+								rechecks += rc & 1u;
+								flips += rc >> 1;
 							}
 						}
 						else if (sp < 32)
@@ -225,14 +257,21 @@ namespace u26
 			}
 			if (stats)
 			{
-				// warp-aggregated counters: [0] node boxes tested, [1] leaf primitives tested
+				// warp-aggregated counters: [0] node boxes tested, [1] leaf primitives tested,
+				// [2] EF tests rechecked in FP64 (inside their FP32 error band), [3] FP32 / FP64 flips
 				const uint32_t mask = __activemask();
 				const uint32_t v = __reduce_add_sync(mask, visited);
 				const uint32_t t = __reduce_add_sync(mask, tested);
+				const uint32_t rc = __reduce_add_sync(mask, rechecks);
+				const uint32_t fl = __reduce_add_sync(mask, flips);
 				if ((threadIdx.x & 31) == uint32_t(__ffs(mask) - 1))
 				{
 					atomicAdd(stats + 0, (unsigned long long)v);
 					atomicAdd(stats + 1, (unsigned long long)t);
+					if (rc)
+						atomicAdd(stats + 2, (unsigned long long)rc);
+					if (fl)
+						atomicAdd(stats + 3, (unsigned long long)fl);
 				}
 			}
 		}

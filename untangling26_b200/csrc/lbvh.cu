@@ -194,7 +194,7 @@ namespace u26
 
 		// fn_build_inner_nodes: determineRange + findSplit (Karras 2012) over unique keys.
 		__global__ void __launch_bounds__(256) karras_kernel(const uint64_t* __restrict__ keys, uint32_t n, uint2* __restrict__ children,
-			uint32_t* __restrict__ parent)
+			uint32_t* __restrict__ parent, uint32_t* __restrict__ node_range)
 		{
 			const int nid = blockIdx.x * blockDim.x + threadIdx.x;
 			const int num_inner = int(n) - 1;
@@ -254,6 +254,7 @@ namespace u26
 			parent[c_left] = uint32_t(nid);
 			parent[c_right] = uint32_t(nid);
 			children[nid] = make_uint2(uint32_t(c_left), uint32_t(c_right));
+			node_range[nid] = uint32_t(j);
 		}
 
 		// fn_check_construction.
@@ -319,85 +320,118 @@ namespace u26
 			boxes[n - 1 + lid] = b;
 		}
 
-		__device__ __forceinline__ NodeBox load_box_cg(const NodeBox* p)
+		// Bottom-up union (fn_refit_tree_aabb, lbvh.cpp:694-758) without spin-waits. One thread
+		// per leaf climbs; at each inner node the first arrival stops and the second owns the
+		// union. The climb stays inside its block while it can: block b owns the leaves
+		// [b * kRefitBlock, (b + 1) * kRefitBlock), and an inner node's leaves form a contiguous
+		// range with the node's own index at one end (Karras 2012), so a node whose range lies
+		// inside the block is reached by the block's threads only. Its arrival counter and its
+		// box live in shared memory (the box is written out as well). A node whose range
+		// crosses a block boundary, and every ancestor of it, joins through a device counter
+		// that gains 2 per refit: an even value before the increment marks the first arrival,
+		// so the counters need no reset between refits. The leaf update runs in the same
+		// thread when FUSED. Every climb is bounded by kMaxClimb steps.
+		constexpr uint32_t kRefitBlock = 512;
+		struct Box6
 		{
-			NodeBox b;
-			b.mn = __ldcg(&p->mn);
-			b.mx = __ldcg(&p->mx);
-			return b;
+			float v[6];
+		};
+		__device__ __forceinline__ void load_box6_cg(const NodeBox* p, f3& mn, f3& mx)
+		{
+			const float4 a = __ldcg(&p->mn), b = __ldcg(&p->mx);
+			mn = mk3(a.x, a.y, a.z);
+			mx = mk3(b.x, b.y, b.z);
 		}
-
-		// Bottom-up union. One thread per leaf climbs; at each inner node the first arrival
-		// (atomicAdd returns 0) stops and the second owns the union. The leaf update runs
-		// in the same thread when FUSED. Every climb is bounded by kMaxClimb steps.
 		template <int TYPE, bool FUSED>
-		__device__ __forceinline__ void refit_body(const uint32_t* __restrict__ sorted_get_original, NodeBox* __restrict__ boxes,
-			const float* __restrict__ x0, const float* __restrict__ x1, const float* __restrict__ thickness,
+		__global__ void __launch_bounds__(kRefitBlock) refit_block_kernel(const uint32_t* __restrict__ sorted_get_original,
+			NodeBox* __restrict__ boxes, const float* __restrict__ x0, const float* __restrict__ x1, const float* __restrict__ thickness,
 			const uint32_t* __restrict__ prims, const uint32_t* __restrict__ parent, const uint2* __restrict__ children,
-			uint32_t* __restrict__ flags, uint32_t n, uint32_t* __restrict__ health)
+			const uint32_t* __restrict__ node_range, uint32_t* __restrict__ flags, uint32_t n, uint32_t* __restrict__ health)
 		{
-			const uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x;
-			if (lid >= n)
+			__shared__ uint32_t s_cnt[kRefitBlock];
+			__shared__ Box6 s_leaf[kRefitBlock];
+			__shared__ Box6 s_inner[kRefitBlock];
+			const uint32_t base = blockIdx.x * kRefitBlock;
+			const uint32_t cnt = min(kRefitBlock, n - base);
+			s_cnt[threadIdx.x] = 0u;
+			__syncthreads();
+			if (threadIdx.x >= cnt)
 				return;
 			const uint32_t ni = n - 1;
+			const uint32_t lid = base + threadIdx.x;
+			f3 mn, mx;
 			if constexpr (FUSED)
 			{
-				f3 mn, mx;
 				leaf_box<TYPE>(x0, x1, thickness, prims, __ldg(sorted_get_original + lid), mn, mx);
-				NodeBox b;
-				b.mn = make_float4(mn.x, mn.y, mn.z, 0.0f);
-				b.mx = make_float4(mx.x, mx.y, mx.z, 1.0f);
-				__stcg(&boxes[ni + lid].mn, b.mn);
-				__stcg(&boxes[ni + lid].mx, b.mx);
+				__stcg(&boxes[ni + lid].mn, make_float4(mn.x, mn.y, mn.z, 0.0f));
+				__stcg(&boxes[ni + lid].mx, make_float4(mx.x, mx.y, mx.z, 1.0f));
 			}
+			else
+				load_box6_cg(boxes + ni + lid, mn, mx);
+			s_leaf[threadIdx.x] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
 			constexpr uint32_t kMaxClimb = 100000u;
 			uint32_t node = __ldg(parent + ni + lid);
 			uint32_t steps = 0;
+			bool local = true;
 			while (node != kInvalid)
 			{
-				if (++steps > kMaxClimb)
+				if (++steps > kMaxClimb || node >= ni)
 				{
 					atomicExch(health, 0u);
 					return;
 				}
-				// acq_rel arrival: releases this thread's boxes below the node, and the second
-				// arrival acquires its sibling's (one atom.acq_rel instead of two full fences)
-				const uint32_t arrived = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(flags[node]).fetch_add(1u,
-					cuda::memory_order_acq_rel);
-				if (arrived == 0u)
-					return;
-				if (arrived != 1u)
+				if (local)
 				{
-					atomicExch(health, 0u);
-					return;
+					const uint32_t r = __ldg(node_range + node);
+					local = min(node, r) >= base && max(node, r) < base + cnt;
+				}
+				if (local)
+				{
+					__threadfence_block(); // this thread's box writes before its arrival
+					if (atomicAdd(&s_cnt[node - base], 1u) == 0u)
+						return;
+					__threadfence_block();
+				}
+				else
+				{
+					// acq_rel arrival: releases this thread's boxes below the node, and the second
+					// arrival acquires its sibling's
+					const uint32_t arrived = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(flags[node]).fetch_add(1u,
+						cuda::memory_order_acq_rel);
+					if ((arrived & 1u) == 0u)
+						return;
 				}
 				const uint2 c = __ldg(children + node);
-				const NodeBox l = load_box_cg(boxes + c.x);
-				const NodeBox r = load_box_cg(boxes + c.y);
-				NodeBox o;
-				o.mn = make_float4(fminf(l.mn.x, r.mn.x), fminf(l.mn.y, r.mn.y), fminf(l.mn.z, r.mn.z), 0.0f);
-				o.mx = make_float4(fmaxf(l.mx.x, r.mx.x), fmaxf(l.mx.y, r.mx.y), fmaxf(l.mx.z, r.mx.z), 1.0f);
-				__stcg(&boxes[node].mn, o.mn);
-				__stcg(&boxes[node].mx, o.mx);
+				f3 amn, amx, bmn, bmx;
+				if (local)
+				{
+					// children of a node inside the block are inside it too (checked, not assumed)
+					const uint32_t ia = c.x >= ni ? c.x - ni - base : c.x - base, ib = c.y >= ni ? c.y - ni - base : c.y - base;
+					if (ia >= cnt || ib >= cnt)
+					{
+						atomicExch(health, 0u);
+						return;
+					}
+					const Box6 a = c.x >= ni ? s_leaf[ia] : s_inner[ia];
+					const Box6 b = c.y >= ni ? s_leaf[ib] : s_inner[ib];
+					amn = mk3(a.v[0], a.v[1], a.v[2]);
+					amx = mk3(a.v[3], a.v[4], a.v[5]);
+					bmn = mk3(b.v[0], b.v[1], b.v[2]);
+					bmx = mk3(b.v[3], b.v[4], b.v[5]);
+				}
+				else
+				{
+					load_box6_cg(boxes + c.x, amn, amx);
+					load_box6_cg(boxes + c.y, bmn, bmx);
+				}
+				mn = vmin(amn, bmn);
+				mx = vmax(amx, bmx);
+				__stcg(&boxes[node].mn, make_float4(mn.x, mn.y, mn.z, 0.0f));
+				__stcg(&boxes[node].mx, make_float4(mx.x, mx.y, mx.z, 1.0f));
+				if (local)
+					s_inner[node - base] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
 				node = __ldg(parent + node);
 			}
-		}
-
-		template <int TYPE>
-		__global__ void __launch_bounds__(256) refit_plain_kernel(const uint32_t* __restrict__ sgo, NodeBox* __restrict__ boxes,
-			const float* __restrict__ x0, const float* __restrict__ x1, const float* __restrict__ th, const uint32_t* __restrict__ prims,
-			const uint32_t* __restrict__ parent, const uint2* __restrict__ children, uint32_t* __restrict__ flags, uint32_t n,
-			uint32_t* __restrict__ health)
-		{
-			refit_body<TYPE, false>(sgo, boxes, x0, x1, th, prims, parent, children, flags, n, health);
-		}
-		template <int TYPE>
-		__global__ void __launch_bounds__(256) refit_fused_kernel(const uint32_t* __restrict__ sgo, NodeBox* __restrict__ boxes,
-			const float* __restrict__ x0, const float* __restrict__ x1, const float* __restrict__ th, const uint32_t* __restrict__ prims,
-			const uint32_t* __restrict__ parent, const uint2* __restrict__ children, uint32_t* __restrict__ flags, uint32_t n,
-			uint32_t* __restrict__ health)
-		{
-			refit_body<TYPE, true>(sgo, boxes, x0, x1, th, prims, parent, children, flags, n, health);
 		}
 
 		// query_template2 with the reference's visit order: pop, test child 0 then child 1,
@@ -505,6 +539,8 @@ namespace u26
 		U26_CUDA(ctx, t->block_aabb.reserve(sizeof(float) * 6 * div_up(n, 256)));
 		U26_CUDA(ctx, t->global_aabb.reserve(sizeof(float) * 6));
 		U26_CUDA(ctx, t->refit_flags.reserve(sizeof(uint32_t) * std::max<uint32_t>(n - 1, 1)));
+		U26_CUDA(ctx, cudaMemsetAsync(t->refit_flags.ptr, 0, sizeof(uint32_t) * std::max<uint32_t>(n - 1, 1), ctx->stream));
+		U26_CUDA(ctx, t->node_range.reserve(sizeof(uint32_t) * std::max<uint32_t>(n - 1, 1)));
 		U26_CUDA(ctx, t->health.reserve(sizeof(uint32_t)));
 		U26_CUDA(ctx, cudaMemsetAsync(t->health.ptr, 0, sizeof(uint32_t), ctx->stream));
 		U26_CUDA(ctx, cudaMemsetAsync(t->node_aabb.ptr, 0, sizeof(NodeBox) * nn, ctx->stream));
@@ -563,6 +599,7 @@ U26_API void u26_lbvh_destroy(u26_lbvh* t)
 	t->block_aabb.release();
 	t->global_aabb.release();
 	t->refit_flags.release();
+	t->node_range.release();
 	t->health.release();
 	t->sorter.release();
 	delete t;
@@ -609,12 +646,14 @@ U26_API u26_status u26_lbvh_construct_tree(u26_lbvh* t)
 	U26_TRY(after_launch(ctx, "apply_sorted_kernel"));
 	if (n > 1)
 	{
-		karras_kernel<<<div_up(n - 1, 256), 256, 0, ctx->stream>>>(keys, n, t->children.as<uint2>(), t->parent.as<uint32_t>());
+		karras_kernel<<<div_up(n - 1, 256), 256, 0, ctx->stream>>>(keys, n, t->children.as<uint2>(), t->parent.as<uint32_t>(),
+			t->node_range.as<uint32_t>());
 		U26_TRY(after_launch(ctx, "karras_kernel"));
 		check_kernel<<<div_up(n - 1, 256), 256, 0, ctx->stream>>>(t->children.as<uint2>(), t->parent.as<uint32_t>(), n - 1,
 			t->health.as<uint32_t>());
 		U26_TRY(after_launch(ctx, "check_kernel"));
 	}
+	t->built = true;
 	return U26_OK;
 }
 
@@ -639,17 +678,33 @@ static u26_status refit_impl(u26_lbvh* t, bool fused, const float* thickness, co
 			return u26_lbvh_update_leaves(t, thickness, x0, x1, prims);
 		return U26_OK;
 	}
-	U26_CUDA(ctx, cudaMemsetAsync(t->refit_flags.ptr, 0, sizeof(uint32_t) * (t->n - 1), ctx->stream));
-	const uint32_t grid = div_up(t->n, 256);
-	if (fused)
-		U26_DISPATCH_TYPE(t->type, refit_fused_kernel, grid, 256, ctx->stream, t->sorted_get_original.as<uint32_t>(),
-			t->node_aabb.as<NodeBox>(), x0, x1, thickness, prims, t->parent.as<uint32_t>(), t->children.as<uint2>(),
-			t->refit_flags.as<uint32_t>(), t->n, t->health.as<uint32_t>());
+	if (!t->built)
+		return set_error(ctx, U26_ERR_INVALID_INPUT, "refit: call u26_lbvh_construct_tree first");
+	const uint32_t grid = div_up(t->n, kRefitBlock);
+#define U26_REFIT(T, F)                                                                                                          \
+	refit_block_kernel<T, F><<<grid, kRefitBlock, 0, ctx->stream>>>(t->sorted_get_original.as<uint32_t>(), t->node_aabb.as<NodeBox>(), \
+		x0, x1, thickness, prims, t->parent.as<uint32_t>(), t->children.as<uint2>(), t->node_range.as<uint32_t>(),                   \
+		t->refit_flags.as<uint32_t>(), t->n, t->health.as<uint32_t>())
+	if (t->type == U26_TREE_FACE)
+	{
+		if (fused)
+			U26_REFIT(U26_TREE_FACE, true);
+		else
+			U26_REFIT(U26_TREE_FACE, false);
+	}
+	else if (t->type == U26_TREE_EDGE)
+	{
+		if (fused)
+			U26_REFIT(U26_TREE_EDGE, true);
+		else
+			U26_REFIT(U26_TREE_EDGE, false);
+	}
+	else if (fused)
+		U26_REFIT(U26_TREE_VERT, true);
 	else
-		U26_DISPATCH_TYPE(t->type, refit_plain_kernel, grid, 256, ctx->stream, t->sorted_get_original.as<uint32_t>(),
-			t->node_aabb.as<NodeBox>(), x0, x1, thickness, prims, t->parent.as<uint32_t>(), t->children.as<uint2>(),
-			t->refit_flags.as<uint32_t>(), t->n, t->health.as<uint32_t>());
-	return after_launch(ctx, "refit_kernel");
+		U26_REFIT(U26_TREE_VERT, false);
+#undef U26_REFIT
+	return after_launch(ctx, "refit_block_kernel");
 }
 
 U26_API u26_status u26_lbvh_refit(u26_lbvh* t)

@@ -16,7 +16,8 @@ struct u26_lbvh
 	u26::DevBuf node_aabb;			 // NodeBox[2n-1]
 	u26::DevBuf block_aabb;			 // float[ceil(n/256)][6]
 	u26::DevBuf global_aabb;		 // float[6]
-	u26::DevBuf refit_flags;		 // uint32[max(n-1,1)]
+	u26::DevBuf refit_flags;		 // uint32[max(n-1,1)]: arrival counters, even between refits
+	u26::DevBuf node_range;			 // uint32[max(n-1,1)]: inner node i covers leaves [min(i, r), max(i, r)], r = node_range[i]
 	u26::DevBuf health;				 // uint32[1]: 1 healthy
 	u26::RadixSorter sorter;
 	// inputs of the last reduce_aabb (construct_tree reads them, as the reference
@@ -27,6 +28,7 @@ struct u26_lbvh
 	// 1: all leaf blocks (the true global AABB, better Morton spread)
 	int full_global_aabb = 0;
 	uint32_t last_num_verts = 0;
+	bool built = false; // construct_tree has run (parent / children / node_range are valid)
 
 	uint32_t num_inner() const { return n > 0 ? n - 1 : 0; }
 	uint32_t num_nodes() const { return n > 0 ? 2 * n - 1 : 0; }

@@ -47,6 +47,7 @@
 #include <cooperative_groups.h>
 
 #include "lbvh_internal.h"
+#include "predicates.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -836,6 +837,25 @@ namespace u26
 			hs.payload[3 * slot + 2] = dist;
 		}
 
+		// FP64 rechecks (predicates.cuh) of one VF / FV ray - triangle test and one swept edge -
+		// edge test whose FP32 decision lies inside its error band: bit 0 set, bit 1 when the FP64
+		// decision differs from hit32 (the FP32 decision, which the hit sets keep). Out of line:
+		// they run for a small fraction of the leaf tests, and keep their registers off the
+		// traversal loop (the band test itself is inline).
+		__device__ __noinline__ uint32_t recheck_vf(f3 orig, f3 cast, f3 A, f3 B, f3 C, bool hit32)
+		{
+			const f3 end = orig + cast * 1.0f;
+			d3 b64;
+			double t64;
+			const bool h64 = line_intersection_f64(dd(orig), dd(end), dd(A), dd(B), dd(C), b64, t64) && t64 >= 0.0 && t64 <= 1.0;
+			return 1u | (h64 != hit32 ? 2u : 0u);
+		}
+		__device__ __noinline__ uint32_t recheck_ee(f3 p0, f3 e1, f3 dir, float ray_max, f3 q0, f3 q1, bool hit32)
+		{
+			const bool h64 = edge_edge_f64(dd(p0), dd(p0 + e1), dd(dir), double(ray_max), dd(q0), dd(q1));
+			return 1u | (h64 != hit32 ? 2u : 0u);
+		}
+
 		// Packet traversal: a warp takes 32 consecutive requests (one task's candidate vertices
 		// or edges in BFS order: one direction, nearby origins) and walks the union of their
 		// paths with one shared stack, every lane testing its own ray against each popped node
@@ -844,6 +864,7 @@ namespace u26
 		// kSplit parts x the requests rounded up to warps; part p starts at frontier node p,
 		// so every (ray, leaf) pair is decided once.
 		constexpr int kStack = 64;
+		template <bool RECHECK>
 		__global__ void __launch_bounds__(128, 7) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
@@ -862,7 +883,7 @@ namespace u26
 			if (part >= kSplit)
 				return; // whole warps only
 			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
-			uint32_t tested = 0, visited = 0, etested = 0, ctested = 0;
+			uint32_t tested = 0, visited = 0, etested = 0, ctested = 0, rechecks = 0, flips = 0;
 			uint32_t fetch_nodes = 0, fetch_tris = 0, fetch_edges = 0; // warp-uniform: data each packet brings in
 			uint32_t ray_visits = 0; // the node tests this ray alone would make: its start + 2 per inner node it enters
 
@@ -976,15 +997,24 @@ namespace u26
 							{
 								ctested++;
 								const uint32_t f0 = faces[3 * fid], f1 = faces[3 * fid + 1], f2 = faces[3 * fid + 2];
-								if (vid != f0 && vid != f1 && vid != f2)
+								if (vid != f0 && vid != f1 && vid != f2 && seg_ok)
 								{
 									f3 bary;
 									float tt;
-									if (seg_ok && ray_tri(orig, sray, slen, ld3(x, f0), ld3(x, f1), ld3(x, f2), tt, bary))
+									const f3 A = ld3(x, f0), B = ld3(x, f1), C = ld3(x, f2);
+									bool hit32 = false;
+									if (ray_tri(orig, sray, slen, A, B, C, tt, bary))
 									{
 										tt = tt * inv_len;
-										if (tt >= 0.0f && tt <= 1.0f)
+										hit32 = tt >= 0.0f && tt <= 1.0f;
+										if (hit32)
 											emit(sink, t, fv ? 2u : 0u, fv ? fid : vid, fv ? vid : fid, bary.x, bary.y, tt * 1.0f);
+									}
+									if (RECHECK && tri_needs_recheck(orig, sray, slen, A, B, C))
+									{
+										const uint32_t rc = recheck_vf(orig, fv ? -dir : dir, A, B, C, hit32);
+										rechecks += rc & 1u;
+										flips += rc >> 1;
 									}
 								}
 							}
@@ -1110,7 +1140,7 @@ namespace u26
 								if (!(ev.x == qv.x || ev.x == qv.y || ev.y == qv.x || ev.y == qv.y))
 								{
 									const f3 q0 = ld3(x, qv.x), q1 = ld3(x, qv.y);
-									bool sep = false;
+									bool sep = false, ee_hit = false;
 									if (plane)
 									{
 										const float d0 = dot(pn, q0) - pd;
@@ -1149,9 +1179,21 @@ namespace u26
 												const float t1 = n_t1 * inv;
 												const float t2 = n_t2 * inv;
 												if (sv >= 0.0f && sv <= ray_max && t1 >= 0.0f && t1 <= 1.0f && t2 >= 0.0f && t2 <= 1.0f)
+												{
+													ee_hit = true;
 													emit(sink, t, 1u, eid, e2, 1.0f - t1, 1.0f - t2, sv);
+												}
 											}
 										}
+									}
+									Band bd;
+									if (RECHECK)
+										edge_edge_band(p0, e1, dir, ray_max, plane, pn, pd, q0, q1, bd);
+									if (RECHECK && bd.recheck())
+									{
+										const uint32_t rc = recheck_ee(p0, e1, dir, ray_max, q0, q1, ee_hit);
+										rechecks += rc & 1u;
+										flips += rc >> 1;
 									}
 								}
 							}
@@ -1201,6 +1243,8 @@ namespace u26
 				const uint32_t esum = __reduce_add_sync(0xFFFFFFFFu, etested);
 				const uint32_t rvsum = __reduce_add_sync(0xFFFFFFFFu, ray_visits);
 				const uint32_t csum = __reduce_add_sync(0xFFFFFFFFu, ctested);
+				const uint32_t rcsum = __reduce_add_sync(0xFFFFFFFFu, rechecks);
+				const uint32_t flsum = __reduce_add_sync(0xFFFFFFFFu, flips);
 				if (lane == 0)
 				{
 					// [0] leaf primitive tests, [1] requests, [2] ray-node tests, [3] edge leaf tests,
@@ -1208,6 +1252,11 @@ namespace u26
 					// [7] single-ray node visits, [8] leaf tests of candidate targets
 					atomicAdd(stats + 7, (unsigned long long)rvsum);
 					atomicAdd(stats + 8, (unsigned long long)csum);
+					// [9] FP64 rechecks of leaf tests inside their error band, [10] FP32 / FP64 flips
+					if (rcsum)
+						atomicAdd(stats + 9, (unsigned long long)rcsum);
+					if (flsum)
+						atomicAdd(stats + 10, (unsigned long long)flsum);
 					atomicAdd(stats + 0, (unsigned long long)tsum);
 					atomicAdd(stats + 1, (unsigned long long)rsum);
 					atomicAdd(stats + 2, (unsigned long long)vsum);
@@ -2796,6 +2845,93 @@ namespace u26
 				p += selected_flag(keys, root, best, cd, i, n);
 			sel_begin[t] = p;
 		}
+
+		// ---- FP64 evaluation of the selected supports (prp_eval_penetration_v2's terms,
+		// intersection_resolver2.cpp:1883-1954): every hit's depth delta recomputed in FP64 from
+		// the float positions (the ray / swept-edge test of its kind along the contour's
+		// direction), D_C = max delta, J = (sum of the source rest areas) D_C^2, all in double
+		// and in the hits' canonical order; and the D_C tie check: when the largest and second
+		// largest FP32 depths lie within the depth's error band, the argmax is re-decided in FP64.
+		struct Fp64In
+		{
+			uint32_t hit_begin, hit_end;
+			float dir[3];
+			float j32, dc32;
+		};
+		struct Fp64Out
+		{
+			double j64, dc64, delta_err;
+			uint32_t tie, flip;
+		};
+		__device__ __forceinline__ double hit_delta_f64(const u26_prp_hit& h, f3 dir, const float* __restrict__ x, const uint2* __restrict__ edges,
+			const uint32_t* __restrict__ faces)
+		{
+			if (h.type == 1u)
+			{
+				const uint2 a = edges[h.src_id], b = edges[h.dst_id];
+				const d3 p0 = dd(ld3(x, a.x)), p1 = dd(ld3(x, a.y)), q0 = dd(ld3(x, b.x)), q1 = dd(ld3(x, b.y));
+				const d3 n = cross(p1 - p0, q1 - q0);
+				const double det = -dot(dd(dir), n);
+				return det != 0.0 ? -dot(q0 - p0, n) / det : double(h.dist);
+			}
+			const bool fv = h.type == 2u;
+			const uint32_t v = fv ? h.dst_id : h.src_id, f = fv ? h.src_id : h.dst_id;
+			const f3 orig = ld3(x, v);
+			const f3 end = orig + (fv ? -dir : dir) * 1.0f;
+			d3 b64;
+			double t64;
+			if (!line_intersection_f64(dd(orig), dd(end), dd(ld3(x, faces[3 * f])), dd(ld3(x, faces[3 * f + 1])), dd(ld3(x, faces[3 * f + 2])),
+					b64, t64))
+				return double(h.dist); // FP64 misses the hit (an FP32 / FP64 flip): keep its FP32 depth
+			return t64 * 1.0;
+		}
+		__global__ void fp64_metrics_kernel(uint32_t nc, const Fp64In* __restrict__ in, const u26_prp_hit* __restrict__ hits,
+			const float* __restrict__ x, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const float* __restrict__ varea,
+			const float* __restrict__ earea, const float* __restrict__ farea, double* __restrict__ delta64, Fp64Out* __restrict__ out)
+		{
+			const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			const uint32_t lane = threadIdx.x & 31u;
+			if (c >= nc)
+				return;
+			const Fp64In ci = in[c];
+			const f3 dir = mk3(ci.dir[0], ci.dir[1], ci.dir[2]);
+			for (uint32_t h = ci.hit_begin + lane; h < ci.hit_end; h += 32u)
+				delta64[h] = hit_delta_f64(hits[h], dir, x, edges, faces);
+			__syncwarp();
+			if (lane != 0u)
+				return;
+			double area = 0.0, dc64 = -1.0, derr = 0.0;
+			float m32 = -1.0f, s32 = -1.0f;
+			uint32_t arg32 = ci.hit_begin, arg64 = ci.hit_begin;
+			for (uint32_t h = ci.hit_begin; h < ci.hit_end; h++)
+			{
+				const u26_prp_hit hh = hits[h];
+				area += double(hh.type == 0u ? varea[hh.src_id] : hh.type == 1u ? earea[hh.src_id] : farea[hh.src_id]);
+				const double d64 = delta64[h];
+				if (d64 > dc64)
+				{
+					dc64 = d64;
+					arg64 = h;
+				}
+				if (hh.dist > m32)
+				{
+					s32 = m32;
+					m32 = hh.dist;
+					arg32 = h;
+				}
+				else if (hh.dist > s32)
+					s32 = hh.dist;
+				if (d64 > 0.0)
+					derr = fmax(derr, fabs(double(hh.dist) - d64) / d64);
+			}
+			Fp64Out o;
+			o.j64 = area * dc64 * dc64;
+			o.dc64 = dc64;
+			o.delta_err = derr;
+			o.tie = (ci.hit_end - ci.hit_begin > 1u && m32 - s32 <= 4.0f * kBandGamma * m32) ? 1u : 0u;
+			o.flip = (o.tie && arg64 != arg32) ? 1u : 0u;
+			out[c] = o;
+		}
 	} // namespace
 } // namespace u26
 
@@ -2969,6 +3105,7 @@ struct u26_scene
 	DevBuf d_ekeys, d_evals, d_ecount, d_cand_roots, d_vf_off, d_vf, d_anchor_off, d_anchors, d_out, d_sel;
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
+	DevBuf d_f64in, d_f64hits, d_f64delta, d_f64out; // FP64 evaluation of the selected supports
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
 	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals, d_zero_th;
 	RadixSorter sorter, esorter, csorter, fvsorter;
@@ -2996,6 +3133,8 @@ struct u26_prp_output
 	double stage_ms[8] = { 0 };
 	double gpu_ms[6] = { 0 };
 	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0, ray_candidate_tests = 0;
+	uint64_t fp64_rechecks = 0, fp64_flips = 0, dc_tie_rechecks = 0, dc_tie_flips = 0;
+	double fp64_delta_rel_err = 0.0, fp64_dc_rel_err = 0.0, fp64_j_rel_err = 0.0;
 	const u26_scene* scene = nullptr; // the pass this output came from
 	uint64_t pass = 0;
 };
@@ -3166,7 +3305,7 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_stats, &s->d_seg, &s->d_parent, &s->d_root, &s->d_att, &s->d_csize, &s->d_catt, &s->d_ekeys, &s->d_evals,
 		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
 		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
-		&s->d_step_hits, &s->d_step_out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
+		&s->d_step_hits, &s->d_step_out, &s->d_f64in, &s->d_f64hits, &s->d_f64delta, &s->d_f64out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
 		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
 		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp, &s->d_vsolid,
 		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals,
@@ -3647,6 +3786,49 @@ struct LevelEvents
 	}
 };
 
+// The selected supports' depths, D_C and J in FP64 against their FP32 values (max relative
+// errors over the pass) and the D_C tie rechecks.
+static u26_status fp64_metrics(u26_scene* S, const float* d_x, u26_prp_output* out)
+{
+	u26_ctx* ctx = S->ctx;
+	cudaStream_t st = ctx->stream;
+	std::vector<Fp64In> in;
+	for (size_t c = 0; c < out->results.size(); c++)
+	{
+		const u26_prp_result& r = out->results[c];
+		if (r.combo_idx == kInf || r.hit_count == 0)
+			continue;
+		in.push_back(Fp64In{ out->hit_offsets[c], out->hit_offsets[c + 1], { r.dir[0], r.dir[1], r.dir[2] }, r.objective, r.depth });
+	}
+	if (in.empty())
+		return U26_OK;
+	DevBuf &d_in = S->d_f64in, &d_hits = S->d_f64hits, &d_delta = S->d_f64delta, &d_out = S->d_f64out;
+	U26_TRY(upload(ctx, d_in, in));
+	U26_TRY(upload(ctx, d_hits, out->hits));
+	U26_CUDA(ctx, d_delta.reserve(sizeof(double) * out->hits.size()));
+	U26_CUDA(ctx, d_out.reserve(sizeof(Fp64Out) * in.size()));
+	const uint32_t nc = uint32_t(in.size());
+	fp64_metrics_kernel<<<div_up(nc * 32u, 128u), 128, 0, st>>>(nc, d_in.as<Fp64In>(), d_hits.as<u26_prp_hit>(), d_x, S->d_edges.as<uint2>(),
+		S->d_faces.as<uint32_t>(), S->d_varea.as<float>(), S->d_earea.as<float>(), S->d_farea.as<float>(), d_delta.as<double>(),
+		d_out.as<Fp64Out>());
+	U26_TRY(after_launch(ctx, "fp64_metrics_kernel"));
+	std::vector<Fp64Out> res;
+	U26_TRY(download(ctx, res, d_out.ptr, in.size()));
+	U26_CUDA(ctx, cudaStreamSynchronize(st));
+	for (size_t i = 0; i < res.size(); i++)
+	{
+		const Fp64Out& o = res[i];
+		out->fp64_delta_rel_err = std::max(out->fp64_delta_rel_err, o.delta_err);
+		if (o.dc64 > 0.0)
+			out->fp64_dc_rel_err = std::max(out->fp64_dc_rel_err, std::fabs(double(in[i].dc32) - o.dc64) / o.dc64);
+		if (o.j64 > 0.0)
+			out->fp64_j_rel_err = std::max(out->fp64_j_rel_err, std::fabs(double(in[i].j32) - o.j64) / o.j64);
+		out->dc_tie_rechecks += o.tie;
+		out->dc_tie_flips += o.flip;
+	}
+	return U26_OK;
+}
+
 static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree, const float* d_x, const void* d_pairs,
 	const uint32_t* d_idx, uint32_t num_pairs, const u26_prp_params* P, u26_prp_output* out)
 {
@@ -4032,11 +4214,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			else if (total_req)
 			{
 				const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * kSplit;
-				raycast_kernel<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
-					S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(),
-					S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(),
-					S->d_front.as<uint32_t>() + size_t(nobj) * kSplit,
-					d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
+				const bool rc = attempt == 0 && !hits_out && P->fp64_recheck;
+				(rc ? raycast_kernel<true> : raycast_kernel<false>)<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt,
+					total_req, S->d_slots.as<Slot>(), S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs,
+					S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(), S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(),
+					S->d_front.as<uint32_t>(), S->d_front.as<uint32_t>() + size_t(nobj) * kSplit, d_x, S->d_edges.as<uint2>(),
+					S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
 					(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
 				U26_TRY(after_launch(ctx, "raycast_kernel"));
 			}
@@ -4851,7 +5034,11 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	out->ray_edge_fetches = stats[6];
 	out->ray_visits = stats[7];
 	out->ray_candidate_tests = stats[8];
+	out->fp64_rechecks = stats[9];
+	out->fp64_flips = stats[10];
 	out->dev_err = *ctx->host_word;
+	if (P->fp64_recheck && P->form == 0 && !out->hits.empty())
+		U26_TRY(fp64_metrics(S, d_x, out));
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
 	if (out->dev_err & (U26_DEVERR_STACK_OVERFLOW | U26_DEVERR_ITERATION_CAP))
@@ -4961,6 +5148,13 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->ray_edge_fetches = o->ray_edge_fetches;
 	v->ray_visits = o->ray_visits;
 	v->ray_candidate_tests = o->ray_candidate_tests;
+	v->fp64_rechecks = o->fp64_rechecks;
+	v->fp64_flips = o->fp64_flips;
+	v->dc_tie_rechecks = o->dc_tie_rechecks;
+	v->dc_tie_flips = o->dc_tie_flips;
+	v->fp64_delta_rel_err = o->fp64_delta_rel_err;
+	v->fp64_dc_rel_err = o->fp64_dc_rel_err;
+	v->fp64_j_rel_err = o->fp64_j_rel_err;
 	for (int i = 0; i < 6; i++)
 		v->gpu_ms[i] = o->gpu_ms[i];
 	v->levels = o->levels;

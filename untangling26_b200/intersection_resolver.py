@@ -223,8 +223,9 @@ class CollisionScene:
         """One untangling pass at the current positions: refit, fused EF detection (plus, with
         proximity = (narrow_list, narrow_indices, narrow_count), the near-zero-distance proximity
         pairs as EF pairs), canonical EF order, PRP contour evaluation (and, with response, its
-        response pairs)."""
-        self.detect_ef_fused()
+        response pairs). The EF detection counts its node / leaf tests and FP64 rechecks into
+        self.stats ([nodes, leaf tests, rechecked, flipped])."""
+        self.detect_ef_fused(with_stats=True)
         if proximity is not None:
             self.add_ef_from_proximity_pairs(*proximity)
         n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)

@@ -31,13 +31,14 @@ class PrpParams(ctypes.Structure):
         ("solid_eps_n", c_f32),       # PRP_solid_interior_adjacency_normal_eps
         ("solid_eps_d", c_f32),       # PRP_solid_interior_adjacency_dist_eps
         ("ignore_near_zero_dist_pairs", c_u32),  # 0: drop isolated degenerate EF pairs (the CLI's setting)
+        ("fp64_recheck", c_u32),  # 1: FP64 recheck of the leaf tests inside their FP32 error band, FP64 metrics
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, opt_iterations=0, ccr_blend=0, ccr_blend_weight=0.5,
-                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1)
+                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1, fp64_recheck=1)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -71,6 +72,8 @@ class PrpOutputView(ctypes.Structure):
         ("device_error_flags", c_u32), ("stage_ms", ctypes.c_double * 8), ("ray_nodes", c_u64),
         ("ray_edge_tests", c_u64), ("gpu_ms", ctypes.c_double * 6), ("ray_node_fetches", c_u64), ("ray_tri_fetches", c_u64),
         ("ray_edge_fetches", c_u64), ("ray_visits", c_u64), ("ray_candidate_tests", c_u64),
+        ("fp64_rechecks", c_u64), ("fp64_flips", c_u64), ("dc_tie_rechecks", c_u64), ("dc_tie_flips", c_u64),
+        ("fp64_delta_rel_err", ctypes.c_double), ("fp64_dc_rel_err", ctypes.c_double), ("fp64_j_rel_err", ctypes.c_double),
     ]
 
 GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
@@ -182,3 +185,6 @@ class PrpResult:
         self.edge_fetches = int(v.ray_edge_fetches)
         self.ray_visits = int(v.ray_visits)
         self.candidate_tests = int(v.ray_candidate_tests)
+        self.fp64 = {"rechecks": int(v.fp64_rechecks), "flips": int(v.fp64_flips), "dc_tie_rechecks": int(v.dc_tie_rechecks),
+                     "dc_tie_flips": int(v.dc_tie_flips), "delta_rel_err": float(v.fp64_delta_rel_err),
+                     "dc_rel_err": float(v.fp64_dc_rel_err), "j_rel_err": float(v.fp64_j_rel_err)}
