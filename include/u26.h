@@ -365,6 +365,19 @@ typedef struct u26_prp_response_view
 U26_API u26_status u26_prp_make_response(u26_scene* scene, const u26_prp_output* out, const u26_prp_response_params* params,
 	u26_collision_pair* narrow_list, uint32_t* narrow_indices, uint32_t first, uint32_t capacity, u26_prp_response_view* view);
 
+/* A fixed step along an assembled response (the position update of the scale form's passes and
+ * of the untangling26 repair loop, in place of the Newton solve that consumes the same pairs,
+ * newton_solver.cpp:2254-2326). Each DEVICE response pair asks its sides apart along its normal
+ * by Delta = -k1 / k2 (= min(depth + 3e-3, depth_threshold)): the pair's first primitive (the
+ * VF template's vertex, the EE template's first edge) by +Delta / 2, the second by -Delta / 2,
+ * split among its vertices by the template's barycentric weights. Every vertex that a pair
+ * touches moves by scale x the weighted mean of its requests. DEVICE x [num_verts][3] is
+ * updated in place; scratch: DEVICE int64[4 * num_verts], all zero before the first call (each
+ * call leaves it zero again); moved (optional, DEVICE uint64) receives the count of moved
+ * vertices. Deterministic: the sums are taken in fixed point. No reference counterpart. */
+U26_API u26_status u26_response_step(u26_ctx* ctx, const u26_collision_pair* pairs, uint32_t num_pairs, float* x, uint32_t num_verts,
+	float scale, long long* scratch, unsigned long long* moved);
+
 /* Near-zero-distance proximity pairs as EF pairs (fn_add_ef_from_proximity_pairs,
  * intersection_resolver.cpp:199-363; run by ef_dcd_intersection_query when
  * ignore_near_zero_dist_pairs is off, 404-422). Over the proximity pairs [0, min(*narrow_count,

@@ -73,6 +73,7 @@ _SIGS = {
     "u26_ef_canonicalize": (c_int, [c_vp, c_u32, c_vp, c_vp, c_u32, c_u32]),
     "u26_prp_adjoint": (c_int, [c_vp, c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "u26_prp_make_response": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_u32, c_vp]),
+    "u26_response_step": (c_int, [c_vp, c_vp, c_u32, c_vp, c_u32, ctypes.c_float, c_vp, c_vp]),
     "u26_ef_add_from_proximity": (c_int, [c_vp, c_vp, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32]),
     "u26_filter_invalid_pairs": (c_int, [c_vp, c_vp, c_vp, c_u32, c_u32, c_vp, c_vp, c_u32, c_vp, c_vp, c_vp, c_vp]),
     "u26_filter_broad_phase_pairs": (c_int, [c_vp, c_vp, c_u32, c_vp, c_u32, c_u32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp]),

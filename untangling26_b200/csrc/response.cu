@@ -389,3 +389,101 @@ namespace u26
 		return U26_OK;
 	}
 } // namespace u26
+
+// ---- a fixed step along the assembled response -----------------------------------------
+// Each response pair asks its two sides apart along its normal n by Delta = -k1 / k2 = -C =
+// min(depth + 3e-3, depth_threshold): the pair's first primitive (the VF template's vertex, the
+// EE template's first edge) moves +Delta / 2 n, the second -Delta / 2 n, shared among the
+// primitive's vertices by its barycentric weights. A vertex moves by the weighted mean of the
+// displacements its pairs ask for, times `scale`. The sums are accumulated in 2^-40 m and 2^-32
+// fixed point (integer atomics), so the step does not depend on the order in which pairs land.
+namespace u26
+{
+	namespace
+	{
+		constexpr double kStepScale = 1099511627776.0; // 2^40
+		constexpr double kWeightScale = 4294967296.0;  // 2^32
+
+		__device__ __forceinline__ void step_add(long long* __restrict__ acc, uint32_t v, uint32_t nv, f3 d, float w)
+		{
+			if (v >= nv || !(w > 0.0f))
+				return;
+			long long* a = acc + 4 * size_t(v);
+			atomicAdd(reinterpret_cast<unsigned long long*>(a + 0), (unsigned long long)llrint(double(d.x * w) * kStepScale));
+			atomicAdd(reinterpret_cast<unsigned long long*>(a + 1), (unsigned long long)llrint(double(d.y * w) * kStepScale));
+			atomicAdd(reinterpret_cast<unsigned long long*>(a + 2), (unsigned long long)llrint(double(d.z * w) * kStepScale));
+			atomicAdd(reinterpret_cast<unsigned long long*>(a + 3), (unsigned long long)llrint(double(w) * kWeightScale));
+		}
+
+		__global__ void __launch_bounds__(256) step_pairs_kernel(const u26_collision_pair* __restrict__ pairs, uint32_t n, uint32_t nv,
+			long long* __restrict__ acc)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			const u26_collision_pair p = pairs[i];
+			const float k1 = p.vec2[0], k2 = p.vec2[1];
+			if (!(k2 > 0.0f) || !isfinite(k1))
+				return;
+			const float delta = -k1 / k2;
+			const f3 half = mk3(p.vec1[0], p.vec1[1], p.vec1[2]) * (0.5f * delta);
+			if (p.indices[2] & kTypeBit)
+			{
+				// VF template: vertex, face (f0 f1 f2), face barycentres b0 b1
+				const float b0 = p.vec2[2], b1 = p.vec2[3], b2 = 1.0f - b0 - b1;
+				step_add(acc, p.indices[0], nv, half, 1.0f);
+				step_add(acc, p.indices[1], nv, -half, b0);
+				step_add(acc, p.indices[2] & ~kTypeBit, nv, -half, b1);
+				step_add(acc, p.indices[3], nv, -half, b2);
+			}
+			else if (p.indices[3] & kTypeBit)
+			{
+				// EE template: edge a0 a1, edge b0 b1, edge parameters
+				const float ta = p.vec2[2], tb = p.vec2[3];
+				step_add(acc, p.indices[0], nv, half, ta);
+				step_add(acc, p.indices[1], nv, half, 1.0f - ta);
+				step_add(acc, p.indices[2], nv, -half, tb);
+				step_add(acc, p.indices[3] & ~kTypeBit, nv, -half, 1.0f - tb);
+			}
+		}
+
+		__global__ void __launch_bounds__(256) step_apply_kernel(float* __restrict__ x, uint32_t nv, long long* __restrict__ acc, float scale,
+			unsigned long long* __restrict__ moved)
+		{
+			const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+			if (v >= nv)
+				return;
+			long long* a = acc + 4 * size_t(v);
+			const long long w = a[3];
+			if (w > 0)
+			{
+				const double inv = kWeightScale / double(w) / kStepScale;
+				for (int c = 0; c < 3; c++)
+					x[3 * v + c] = float(double(x[3 * v + c]) + double(scale) * (double(a[c]) * inv));
+				if (moved)
+					atomicAdd(moved, 1ull);
+			}
+			a[0] = a[1] = a[2] = a[3] = 0; // ready for the next call
+		}
+	} // namespace
+} // namespace u26
+
+U26_API u26_status u26_response_step(u26_ctx* ctx, const u26_collision_pair* pairs, uint32_t num_pairs, float* x, uint32_t num_verts,
+	float scale, long long* scratch, unsigned long long* moved)
+{
+	if (!ctx)
+		return U26_ERR_INVALID_INPUT;
+	if (!x || !scratch || (num_pairs && !pairs))
+		return set_error(ctx, U26_ERR_INVALID_INPUT, "u26_response_step: null input");
+	if (num_verts == 0)
+		return U26_OK;
+	if (moved)
+		U26_CUDA(ctx, cudaMemsetAsync(moved, 0, sizeof(unsigned long long), ctx->stream));
+	if (num_pairs)
+	{
+		step_pairs_kernel<<<div_up(num_pairs, 256), 256, 0, ctx->stream>>>(pairs, num_pairs, num_verts, scratch);
+		U26_TRY(after_launch(ctx, "step_pairs_kernel"));
+	}
+	step_apply_kernel<<<div_up(num_verts, 256), 256, 0, ctx->stream>>>(x, num_verts, scratch, scale, moved);
+	return after_launch(ctx, "step_apply_kernel");
+}

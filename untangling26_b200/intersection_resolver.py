@@ -231,6 +231,19 @@ class CollisionScene:
         n = self.resolver.canonicalize(self.mesh.num_edges, self.mesh.num_faces)
         return self.host_resolve(params, num_pairs=n, response=response, **narrow)
 
+    def response_step(self, response, scale=1.0):
+        """x <- x + a fixed step along the pass's assembled response (u26_response_step): every
+        pair asks its sides apart by -k1 / k2 along its normal, each vertex moves by scale x the
+        weighted mean of its requests. Returns the number of vertices moved."""
+        nv = self.mesh.num_verts
+        if getattr(self, "_step_scratch", None) is None:
+            self._step_scratch = torch.zeros(4 * nv, dtype=torch.int64, device=self.dev)
+            self._step_moved = torch.zeros(1, dtype=torch.int64, device=self.dev)
+        self.ctx.check(self.ctx.lib.u26_response_step(
+            self.ctx.handle, ptr(response.pairs), response.num_pairs, ptr(self.x), nv, float(scale), ptr(self._step_scratch),
+            ptr(self._step_moved)), "response_step")
+        return int(self._step_moved.item())
+
     # ---- region-based pair filtering (IntersectionResolver::filter_invalid_pairs /
     # filter_broad_phase_pairs, intersection_resolver.cpp:2586-2676): the contour regions of
     # the last pass's response applied to the solver's contact pairs
