@@ -468,6 +468,8 @@ namespace u26
 	} // namespace
 } // namespace u26
 
+using namespace u26;
+
 U26_API u26_status u26_response_step(u26_ctx* ctx, const u26_collision_pair* pairs, uint32_t num_pairs, float* x, uint32_t num_verts,
 	float scale, long long* scratch, unsigned long long* moved)
 {
