@@ -295,7 +295,9 @@ class PassRunner:
         self.mesh = mesh
         self.sc = CollisionScene(ctx, mesh, d_hat=1e-3, thickness=0.0, max_ef_pairs=max(1 << 16, mesh.num_edges))
         self.sc.construct_lbvh()
-        self.params = prp_params(**params)
+        # the chosen form: FP64 recheck of the in-band predicates, traversal configuration
+        # autotuned on the scene's first (warm-up) pass
+        self.params = prp_params(**dict(dict(fp64_recheck=1, autotune=1), **params))
         self.rparams = response_params(*RESPONSE)
 
     def run(self, with_stats=True):
@@ -387,8 +389,11 @@ def main():
 
     tmesh = wl.timed_mesh(rank, ws)
     runner = PassRunner(ctx, tmesh, wl.params)
+    tuned = None
     for _ in range(max(args.warmup, 3)):
-        runner.run()
+        r = runner.run()
+        if r.raycast_config.get("tuned_this_pass"):
+            tuned = r.raycast_config
     torch.cuda.synchronize()
 
     # ---- device-resident timed region: K passes over the timed scenes
@@ -404,6 +409,7 @@ def main():
     clk = clocks.stop()
     launches = ctx.launch_count() - launches0
     r0 = results[-1]
+    ef_rc = (int(runner.sc.stats[2].item()), int(runner.sc.stats[3].item()))
     tests_pass = r0.tested
     for r in results:
         if r.tested != tests_pass or r.device_error_flags:
@@ -525,6 +531,12 @@ def main():
                      "gpu_ms": {k: round(v, 2) for k, v in r0.gpu_ms.items()},
                      "stage_ms": {k: round(v, 2) for k, v in r0.stage_ms.items()}},
             "parity": parity,
+            "fp64": dict(r0.fp64, ef_rechecks=ef_rc[0], ef_flips=ef_rc[1],
+                         note="rechecks / flips: leaf tests of the timed pass inside their FP32 error band, re-decided in FP64 "
+                              "(sets keep FP32); *_rel_err: the selected supports' FP32 depth, D_C and J against FP64"),
+            "raycast_config": {"parts": r0.raycast_config["parts"], "blocks_per_sm": r0.raycast_config["blocks_per_sm"],
+                               "autotune_ms": tuned.get("tune_ms") if tuned else None,
+                               "note": "chosen by the autotuner on the first warm-up pass: ray-casting ms of each parts x blocks/SM"},
             "untangle_passes_per_s": 1e3 / pass_ms, "pass_seconds": pass_ms / 1e3,
             "speedup_vs_cpu_pass": (cpu["pass_seconds"] / (pass_ms / 1e3)) if cpu and cpu.get("pass_seconds") else None,
             "full_batch": full,

@@ -243,6 +243,8 @@ typedef struct u26_prp_params
 								 * inside its static forward-error band is re-evaluated in FP64 and counted
 								 * (u26_prp_output_view.fp64_rechecks / fp64_flips); the hit sets keep the FP32
 								 * decisions. Also evaluates the selected supports' metrics in FP64 (fp64_*_rel_err). */
+	uint32_t autotune;			/* 1: the scene's first pass times every ray-casting configuration (subtree parts x blocks
+								 * per SM) on each of its launches and the scene keeps the fastest; 0: 8 parts, 7 blocks */
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:
@@ -307,6 +309,12 @@ typedef struct u26_prp_output_view
 	double fp64_delta_rel_err;		 /* max over the selected hits of |delta_32 - delta_64| / delta_64 */
 	double fp64_dc_rel_err;			 /* max over processed contours of |D_C,32 - D_C,64| / D_C,64 (depth) */
 	double fp64_j_rel_err;			 /* max over processed contours of |J_32 - J_64| / J_64 (objective) */
+	double tune_ms[9];				 /* autotune pass: ray-casting time (ms, summed over the pass's launches) of each
+									  * configuration (subtree parts, blocks per SM): (4,6) (4,7) (4,8) (8,6) (8,7)
+									  * (8,8) (16,6) (16,7) (16,8) */
+	uint32_t raycast_parts;			 /* configuration the scene's ray casts use from now on: subtree parts per request */
+	uint32_t raycast_blocks_per_sm;	 /* ... and resident 128-thread blocks per SM */
+	uint32_t tuned;					 /* 1 when this pass ran the autotuner (its choice holds for the scene's later passes) */
 } u26_prp_output_view;
 
 /* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any

@@ -740,19 +740,22 @@ namespace u26
 			out[node_off + i] = g;
 		}
 
-		// The subtree roots that split one traversal across kSplit threads: the nodes at
-		// depth log2(kSplit) below the root, or shallower leaves; unused entries ~0.
-		constexpr uint32_t kSplit = 8;
+		// The subtree roots that split one traversal across `split` parts (4, 8 or 16): the nodes
+		// at depth log2(split) below the root, or shallower leaves; unused entries ~0. One object's
+		// frontiers for the three splits sit at [0, 4), [4, 12) and [12, 28) of its kFrontStride
+		// words.
+		constexpr uint32_t kMaxSplit = 16, kFrontStride = 28;
+		__host__ __device__ constexpr uint32_t front_offset(uint32_t split) { return split == 4u ? 0u : split == 8u ? 4u : 12u; }
 		__global__ void frontier_kernel(const uint2* __restrict__ children, const uint32_t* __restrict__ object_idx, uint32_t n_nodes,
 			uint32_t node_off, uint32_t* __restrict__ out)
 		{
 			if (threadIdx.x != 0 || blockIdx.x != 0)
 				return;
-			uint32_t cur[kSplit], nxt[kSplit];
+			uint32_t cur[kMaxSplit], nxt[kMaxSplit];
 			uint32_t nc = 0;
 			if (n_nodes > 0)
 				cur[nc++] = 0u;
-			for (uint32_t d = 1; d < kSplit; d <<= 1)
+			for (uint32_t d = 1; d < kMaxSplit; d <<= 1)
 			{
 				uint32_t nn = 0;
 				for (uint32_t i = 0; i < nc; i++)
@@ -769,9 +772,10 @@ namespace u26
 				for (uint32_t i = 0; i < nn; i++)
 					cur[i] = nxt[i];
 				nc = nn;
+				if (2u * d >= 4u)
+					for (uint32_t i = 0; i < 2u * d; i++)
+						out[front_offset(2u * d) + i] = i < nc ? cur[i] + node_off : kInvalid;
 			}
-			for (uint32_t i = 0; i < kSplit; i++)
-				out[i] = i < nc ? cur[i] + node_off : kInvalid;
 		}
 
 		// slab test of a grown box with the ray's reciprocals hoisted (same values as ray_box:
@@ -861,17 +865,18 @@ namespace u26
 		// paths with one shared stack, every lane testing its own ray against each popped node
 		// (one broadcast load per node) and its own leaf primitives. Face-tree requests (VF,
 		// FV) and edge-tree requests (EE) of a warp take one packet walk each. The grid is
-		// kSplit parts x the requests rounded up to warps; part p starts at frontier node p,
-		// so every (ray, leaf) pair is decided once.
+		// `split` parts x the requests rounded up to warps; part p starts at the p-th node of the
+		// target tree's frontier for that split, so every (ray, leaf) pair is decided once.
+		// MINB: resident 128-thread blocks per SM the registers are sized for.
 		constexpr int kStack = 64;
-		template <bool RECHECK>
-		__global__ void __launch_bounds__(128, 7) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
+		template <bool RECHECK, int MINB>
+		__global__ void __launch_bounds__(128, MINB) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
 			const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow, const uint32_t* __restrict__ ffront,
 			const uint32_t* __restrict__ efront, const float* __restrict__ x, const uint2* __restrict__ edges,
 			const uint32_t* __restrict__ faces, const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats,
-			uint32_t* __restrict__ dev_err)
+			uint32_t split, uint32_t* __restrict__ dev_err)
 		{
 			const int lane = threadIdx.x & 31;
 			// the packet's traversal stack lives in registers across the warp: entry k in lane k & 31
@@ -880,7 +885,7 @@ namespace u26
 			const uint32_t warps_per_part = (total + 31u) >> 5;
 			const uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 			const uint32_t part = wi / warps_per_part; // warp-uniform
-			if (part >= kSplit)
+			if (part >= split)
 				return; // whole warps only
 			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
 			uint32_t tested = 0, visited = 0, etested = 0, ctested = 0, rechecks = 0, flips = 0;
@@ -961,7 +966,8 @@ namespace u26
 			// ---- face tree: VF / FV rays of the warp
 			// each lane starts at its target object's subtree root of this part; lanes with the
 			// same start walk together
-			const uint32_t fstart_l = kind == 1 ? ffront[size_t(tobj) * kSplit + part] : kInvalid;
+			const uint32_t foff = front_offset(split);
+			const uint32_t fstart_l = kind == 1 ? ffront[size_t(tobj) * kFrontStride + foff + part] : kInvalid;
 			uint32_t fpending = __ballot_sync(0xFFFFFFFFu, fstart_l != kInvalid);
 			while (fpending != 0u)
 			{
@@ -1100,7 +1106,7 @@ namespace u26
 						kind = 2;
 				}
 			}
-			const uint32_t estart_l = kind == 2 ? efront[size_t(tobj) * kSplit + part] : kInvalid;
+			const uint32_t estart_l = kind == 2 ? efront[size_t(tobj) * kFrontStride + foff + part] : kInvalid;
 			uint32_t epending = __ballot_sync(0xFFFFFFFFu, estart_l != kInvalid);
 			while (epending != 0u)
 			{
@@ -1266,6 +1272,25 @@ namespace u26
 					atomicAdd(stats + 6, (unsigned long long)fetch_edges);
 				}
 			}
+		}
+
+		// The traversal configurations the autotuner chooses from: subtree parts per request
+		// (4, 8, 16) x resident blocks of 128 threads per SM the registers are sized for (6, 7, 8:
+		// at most 80, 72 or 64 registers per thread). The packet is the warp (32 requests).
+		struct RaycastConfig
+		{
+			uint32_t split;
+			int min_blocks;
+		};
+		constexpr RaycastConfig kRaycastConfigs[] = { { 4, 6 }, { 4, 7 }, { 4, 8 }, { 8, 6 }, { 8, 7 }, { 8, 8 }, { 16, 6 }, { 16, 7 },
+			{ 16, 8 } };
+		constexpr int kNumRaycastConfigs = 9, kDefaultRaycastConfig = 4; // 8 parts, 7 blocks per SM
+		using RaycastFn = decltype(&raycast_kernel<false, 7>);
+		inline RaycastFn raycast_variant(bool recheck, int min_blocks)
+		{
+			if (recheck)
+				return min_blocks == 6 ? &raycast_kernel<true, 6> : min_blocks == 8 ? &raycast_kernel<true, 8> : &raycast_kernel<true, 7>;
+			return min_blocks == 6 ? &raycast_kernel<false, 6> : min_blocks == 8 ? &raycast_kernel<false, 8> : &raycast_kernel<false, 7>;
 		}
 
 		// ---- the plain form (the comparison baseline of the batched, filtered form above):
@@ -3115,6 +3140,7 @@ struct u26_scene
 	bool otrees_built = false;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
+	int tuned_cfg = -1;				  // autotuned ray-casting configuration (-1: not tuned yet)
 	uint64_t passes = 0;			  // completed u26_prp_resolve calls (the normals d_fn / d_en / d_vn are the last one's)
 	void* cap_host = nullptr;		  // pinned staging of the captured supports (grow-only)
 	size_t cap_host_bytes = 0;
@@ -3134,6 +3160,9 @@ struct u26_prp_output
 	double gpu_ms[6] = { 0 };
 	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0, ray_candidate_tests = 0;
 	uint64_t fp64_rechecks = 0, fp64_flips = 0, dc_tie_rechecks = 0, dc_tie_flips = 0;
+	double tune_ms[9] = { 0 }; // autotuner: ray-casting time of each configuration over the tuning pass
+	int raycast_cfg = -1;	   // configuration the scene's launches use from now on (index of the table)
+	uint32_t tuned = 0;		   // this pass ran the autotuner
 	double fp64_delta_rel_err = 0.0, fp64_dc_rel_err = 0.0, fp64_j_rel_err = 0.0;
 	const u26_scene* scene = nullptr; // the pass this output came from
 	uint64_t pass = 0;
@@ -4013,7 +4042,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	// per-object CachedBVH): a ray tests only its target object's primitives. The trees are
 	// built at the scene's first pass and refit on every pass; their grown node boxes (with
 	// the child links in the w lanes) form one forest array, and each tree's subtree roots of
-	// the split traversal sit at [object * kSplit, (object + 1) * kSplit).
+	// the split traversals sit at [object * kFrontStride, (object + 1) * kFrontStride).
 	const uint32_t nobj = std::max(1u, S->nobj);
 	{
 		if (!S->otrees_built)
@@ -4046,8 +4075,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		}
 		U26_CUDA(ctx, S->d_fgrow.reserve(sizeof(NodeBox) * std::max(foff[nobj], 1u)));
 		U26_CUDA(ctx, S->d_egrow.reserve(sizeof(NodeBox) * std::max(eoff[nobj], 1u)));
-		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * size_t(nobj) * kSplit));
-		U26_CUDA(ctx, cudaMemsetAsync(S->d_front.ptr, 0xFF, sizeof(uint32_t) * 2 * size_t(nobj) * kSplit, st));
+		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride));
+		U26_CUDA(ctx, cudaMemsetAsync(S->d_front.ptr, 0xFF, sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride, st));
 		for (uint32_t o = 0; o < nobj; o++)
 			for (int kind = 0; kind < 2; kind++)
 			{
@@ -4064,7 +4093,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 					(kind == 0 ? S->d_fgrow : S->d_egrow).as<NodeBox>());
 				U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
 				frontier_kernel<<<1, 32, 0, st>>>(tv.children, tv.object_idx, nn, node_off,
-					S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kSplit);
+					S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kFrontStride);
 				U26_TRY(after_launch(ctx, "frontier_kernel"));
 			}
 	}
@@ -4086,6 +4115,28 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	// hit capacity kept by the scene across passes; grows by 1.5x the count that overflowed
 	uint32_t hit_cap = std::max<uint32_t>(S->hit_cap, 1u << 22);
 	const bool trace = std::getenv("U26_PRP_TRACE") != nullptr;
+	// traversal configuration: with autotune, the scene's first pass times every configuration
+	// on each of its ray-casting launches and the scene keeps the fastest (summed over that
+	// pass) for its later passes
+	const bool tuning = P->autotune && P->form == 0 && S->tuned_cfg < 0;
+	const int cfg_now = S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig;
+	std::vector<cudaEvent_t> tune_ev;
+	struct EventsGuard
+	{
+		std::vector<cudaEvent_t>& v;
+		~EventsGuard()
+		{
+			for (cudaEvent_t e : v)
+				cudaEventDestroy(e);
+		}
+	} tune_guard{ tune_ev };
+	if (tuning)
+		for (int i = 0; i < 2 * kNumRaycastConfigs; i++)
+		{
+			cudaEvent_t e;
+			U26_CUDA(ctx, cudaEventCreate(&e));
+			tune_ev.push_back(e);
+		}
 	LevelEvents ev(true);
 	uint64_t alg_tests = 0;
 
@@ -4213,15 +4264,41 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			}
 			else if (total_req)
 			{
-				const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * kSplit;
 				const bool rc = attempt == 0 && !hits_out && P->fp64_recheck;
-				(rc ? raycast_kernel<true> : raycast_kernel<false>)<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt,
-					total_req, S->d_slots.as<Slot>(), S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs,
-					S->d_bits_e.as<uint32_t>(), S->d_bits_f.as<uint32_t>(), S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(),
-					S->d_front.as<uint32_t>(), S->d_front.as<uint32_t>() + size_t(nobj) * kSplit, d_x, S->d_edges.as<uint2>(),
-					S->d_faces.as<uint32_t>(), S->d_slot_box.as<float>(), sink,
-					(attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr, ctx->dev_err);
-				U26_TRY(after_launch(ctx, "raycast_kernel"));
+				auto launch = [&](int cfg, unsigned long long* stats) -> u26_status
+				{
+					const RaycastConfig c = kRaycastConfigs[cfg];
+					const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * c.split;
+					const RaycastFn kern = raycast_variant(rc, c.min_blocks);
+					kern<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
+						S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(),
+						S->d_bits_f.as<uint32_t>(), S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(),
+						S->d_front.as<uint32_t>() + size_t(nobj) * kFrontStride, d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(),
+						S->d_slot_box.as<float>(), sink, stats, c.split, ctx->dev_err);
+					return after_launch(ctx, "raycast_kernel");
+				};
+				if (tuning && attempt == 0 && !hits_out)
+				{
+					// autotuner: every configuration on this level's launch, timed with CUDA events;
+					// each trial's hits are discarded (the counter is reset) and the launch below
+					// produces the level's hits and statistics
+					for (int cfg = 0; cfg < kNumRaycastConfigs; cfg++)
+					{
+						U26_CUDA(ctx, cudaMemsetAsync(S->d_hitcount.ptr, 0, sizeof(uint32_t), st));
+						U26_CUDA(ctx, cudaEventRecord(tune_ev[2 * cfg], st));
+						U26_TRY(launch(cfg, nullptr));
+						U26_CUDA(ctx, cudaEventRecord(tune_ev[2 * cfg + 1], st));
+					}
+					U26_CUDA(ctx, cudaStreamSynchronize(st));
+					for (int cfg = 0; cfg < kNumRaycastConfigs; cfg++)
+					{
+						float ms = 0.0f;
+						U26_CUDA(ctx, cudaEventElapsedTime(&ms, tune_ev[2 * cfg], tune_ev[2 * cfg + 1]));
+						out->tune_ms[cfg] += ms;
+					}
+					U26_CUDA(ctx, cudaMemsetAsync(S->d_hitcount.ptr, 0, sizeof(uint32_t), st));
+				}
+				U26_TRY(launch(cfg_now, (attempt == 0 && !hits_out) ? S->d_stats.as<unsigned long long>() : nullptr));
 			}
 			U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, S->d_hitcount.ptr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
 			U26_CUDA(ctx, cudaStreamSynchronize(st));
@@ -5039,6 +5116,10 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	out->dev_err = *ctx->host_word;
 	if (P->fp64_recheck && P->form == 0 && !out->hits.empty())
 		U26_TRY(fp64_metrics(S, d_x, out));
+	if (tuning && out->tune_ms[0] > 0.0)
+		S->tuned_cfg = int(std::min_element(out->tune_ms, out->tune_ms + kNumRaycastConfigs) - out->tune_ms);
+	out->raycast_cfg = P->form == 0 ? (S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig) : -1;
+	out->tuned = tuning ? 1u : 0u;
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
 	if (out->dev_err & (U26_DEVERR_STACK_OVERFLOW | U26_DEVERR_ITERATION_CAP))
@@ -5155,6 +5236,11 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->fp64_delta_rel_err = o->fp64_delta_rel_err;
 	v->fp64_dc_rel_err = o->fp64_dc_rel_err;
 	v->fp64_j_rel_err = o->fp64_j_rel_err;
+	for (int i = 0; i < 9; i++)
+		v->tune_ms[i] = o->tune_ms[i];
+	v->raycast_parts = o->raycast_cfg >= 0 ? kRaycastConfigs[o->raycast_cfg].split : 0u;
+	v->raycast_blocks_per_sm = o->raycast_cfg >= 0 ? uint32_t(kRaycastConfigs[o->raycast_cfg].min_blocks) : 0u;
+	v->tuned = o->tuned;
 	for (int i = 0; i < 6; i++)
 		v->gpu_ms[i] = o->gpu_ms[i];
 	v->levels = o->levels;

@@ -32,13 +32,14 @@ class PrpParams(ctypes.Structure):
         ("solid_eps_d", c_f32),       # PRP_solid_interior_adjacency_dist_eps
         ("ignore_near_zero_dist_pairs", c_u32),  # 0: drop isolated degenerate EF pairs (the CLI's setting)
         ("fp64_recheck", c_u32),  # 1: FP64 recheck of the leaf tests inside their FP32 error band, FP64 metrics
+        ("autotune", c_u32),      # 1: the scene's first pass picks the fastest ray-casting configuration
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, opt_iterations=0, ccr_blend=0, ccr_blend_weight=0.5,
-                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1, fp64_recheck=1)
+                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1, fp64_recheck=1, autotune=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
@@ -74,8 +75,10 @@ class PrpOutputView(ctypes.Structure):
         ("ray_edge_fetches", c_u64), ("ray_visits", c_u64), ("ray_candidate_tests", c_u64),
         ("fp64_rechecks", c_u64), ("fp64_flips", c_u64), ("dc_tie_rechecks", c_u64), ("dc_tie_flips", c_u64),
         ("fp64_delta_rel_err", ctypes.c_double), ("fp64_dc_rel_err", ctypes.c_double), ("fp64_j_rel_err", ctypes.c_double),
+        ("tune_ms", ctypes.c_double * 9), ("raycast_parts", c_u32), ("raycast_blocks_per_sm", c_u32), ("tuned", c_u32),
     ]
 
+RAYCAST_CONFIGS = ((4, 6), (4, 7), (4, 8), (8, 6), (8, 7), (8, 8), (16, 6), (16, 7), (16, 8))  # (subtree parts, blocks / SM)
 GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
 
 # CollisionPair::CollisionPairTemplate (collision_data.h:48-140), u26_collision_pair: 64 B
@@ -185,6 +188,10 @@ class PrpResult:
         self.edge_fetches = int(v.ray_edge_fetches)
         self.ray_visits = int(v.ray_visits)
         self.candidate_tests = int(v.ray_candidate_tests)
+        self.raycast_config = {"parts": int(v.raycast_parts), "blocks_per_sm": int(v.raycast_blocks_per_sm),
+                               "tuned_this_pass": bool(v.tuned)}
+        if v.tuned:
+            self.raycast_config["tune_ms"] = {f"{p}x{b}": round(float(ms), 3) for (p, b), ms in zip(RAYCAST_CONFIGS, v.tune_ms)}
         self.fp64 = {"rechecks": int(v.fp64_rechecks), "flips": int(v.fp64_flips), "dc_tie_rechecks": int(v.dc_tie_rechecks),
                      "dc_tie_flips": int(v.dc_tie_flips), "delta_rel_err": float(v.fp64_delta_rel_err),
                      "dc_rel_err": float(v.fp64_dc_rel_err), "j_rel_err": float(v.fp64_j_rel_err)}
