@@ -245,6 +245,8 @@ typedef struct u26_prp_params
 								 * decisions. Also evaluates the selected supports' metrics in FP64 (fp64_*_rel_err). */
 	uint32_t autotune;			/* 1: the scene's first pass times every ray-casting configuration (subtree parts x blocks
 								 * per SM) on each of its launches and the scene keeps the fastest; 0: 8 parts, 7 blocks */
+	uint32_t raycast_config;	/* 0: the default or autotuned configuration; k in 1..9: use configuration k - 1 of the
+								 * table in u26_prp_output_view.tune_ms (every configuration returns the same results) */
 } u26_prp_params;
 
 /* Per-contour result (PRPMinContourHitInfo, intersection_resolver2.h:508-550). flags:

@@ -4118,8 +4118,9 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	// traversal configuration: with autotune, the scene's first pass times every configuration
 	// on each of its ray-casting launches and the scene keeps the fastest (summed over that
 	// pass) for its later passes
-	const bool tuning = P->autotune && P->form == 0 && S->tuned_cfg < 0;
-	const int cfg_now = S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig;
+	const bool forced = P->raycast_config >= 1 && P->raycast_config <= uint32_t(kNumRaycastConfigs);
+	const bool tuning = !forced && P->autotune && P->form == 0 && S->tuned_cfg < 0;
+	const int cfg_now = forced ? int(P->raycast_config) - 1 : S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig;
 	std::vector<cudaEvent_t> tune_ev;
 	struct EventsGuard
 	{
@@ -5118,7 +5119,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_TRY(fp64_metrics(S, d_x, out));
 	if (tuning && out->tune_ms[0] > 0.0)
 		S->tuned_cfg = int(std::min_element(out->tune_ms, out->tune_ms + kNumRaycastConfigs) - out->tune_ms);
-	out->raycast_cfg = P->form == 0 ? (S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig) : -1;
+	out->raycast_cfg = P->form != 0 ? -1 : forced ? cfg_now : S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig;
 	out->tuned = tuning ? 1u : 0u;
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);

@@ -33,13 +33,14 @@ class PrpParams(ctypes.Structure):
         ("ignore_near_zero_dist_pairs", c_u32),  # 0: drop isolated degenerate EF pairs (the CLI's setting)
         ("fp64_recheck", c_u32),  # 1: FP64 recheck of the leaf tests inside their FP32 error band, FP64 metrics
         ("autotune", c_u32),      # 1: the scene's first pass picks the fastest ray-casting configuration
+        ("raycast_config", c_u32),  # 0: default / autotuned; k: configuration k - 1 of RAYCAST_CONFIGS
     ]
 
 
 def prp_params(**kw):
     p = PrpParams(max_contours=256, direction_mode=0, use_ccr=1, ccr_tau=0.25, ccr_use_rest=1, ccr_use_current=1,
                   batch_size=32, opt_iterations=0, ccr_blend=0, ccr_blend_weight=0.5,
-                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1, fp64_recheck=1, autotune=0)
+                  form=0, solid_interior=1, solid_all=0, solid_eps_n=1e-4, solid_eps_d=1e-5, ignore_near_zero_dist_pairs=1, fp64_recheck=1, autotune=0, raycast_config=0)
     for k, v in kw.items():
         setattr(p, k, v)
     return p
