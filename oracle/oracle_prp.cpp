@@ -613,25 +613,82 @@ namespace
 			if (!hop_ok(q.hop, q.max_hop, { m.faces[3 * fid], m.faces[3 * fid + 1], m.faces[3 * fid + 2] }))
 				return;
 			Hit h;
-			const bool hit = vert_face_test(m, q.vid, orig, end, fid, h, q.fv, ray_max);
-			if (hit)
+			if (vert_face_test(m, q.vid, orig, end, fid, h, q.fv, ray_max))
 				out.push_back(h);
+		};
+		// the FP64 recheck count: the candidate faces (not incident to the ray's vertex) whose
+		// grown box the ray meets, found by a second walk over node boxes grown by twice that
+		// margin (so that rounding in the node test never drops one)
+		auto count_leaf = [&](uint fid)
+		{
+			if (!in_span(fid, q.target_lo, q.target_cnt) || (q.targets && !std::binary_search(q.targets->begin(), q.targets->end(), fid)))
+				return;
 			const uint f0 = m.faces[3 * fid], f1 = m.faces[3 * fid + 1], f2 = m.faces[3 * fid + 2];
-			if (rc && q.vid != f0 && q.vid != f1 && q.vid != f2)
-			{
-				const V3 A = load3(m.x, f0), B = load3(m.x, f1), C = load3(m.x, f2);
-				if (face_gate(orig, cast, A, B, C))
-					rc->add(recheck_vert_face(orig, end, A, B, C, hit));
-			}
+			if (!hop_ok(q.hop, q.max_hop, { f0, f1, f2 }) || q.vid == f0 || q.vid == f1 || q.vid == f2)
+				return;
+			const V3 A = load3(m.x, f0), B = load3(m.x, f1), C = load3(m.x, f2);
+			if (!face_gate(orig, cast, A, B, C))
+				return;
+			Hit h;
+			rc->add(recheck_vert_face(orig, end, A, B, C, vert_face_test(m, q.vid, orig, end, fid, h, q.fv, ray_max)));
 		};
 		if (bvh == nullptr)
 		{
 			for (uint fid : *q.targets)
+			{
 				leaf(fid);
+				if (rc)
+					count_leaf(fid);
+			}
 			return;
 		}
 		if (bvh->nodes.empty())
 			return;
+		if (rc)
+		{
+			auto grown = [&](const BvhNode& n)
+			{
+				const float lo[3] = { n.bmin.x, n.bmin.y, n.bmin.z }, hi[3] = { n.bmax.x, n.bmax.y, n.bmax.z };
+				const float o[3] = { orig.x, orig.y, orig.z }, d[3] = { cast.x, cast.y, cast.z };
+				float tmin = 0.0f, tmax = ray_max;
+				for (int k = 0; k < 3; k++)
+				{
+					const float e = 2e-5f * (1.0f + std::fmax(std::fabs(lo[k]), std::fabs(hi[k])));
+					const float l = lo[k] - e, hh = hi[k] + e;
+					if (std::fabs(d[k]) < 1e-30f)
+					{
+						if (o[k] < l || o[k] > hh)
+							return false;
+						continue;
+					}
+					float t0 = (l - o[k]) / d[k], t1 = (hh - o[k]) / d[k];
+					if (t0 > t1)
+						std::swap(t0, t1);
+					tmin = std::fmax(tmin, t0);
+					tmax = std::fmin(tmax, t1);
+				}
+				return tmin <= tmax;
+			};
+			std::vector<int> st2{ 0 };
+			while (!st2.empty())
+			{
+				const int nid = st2.back();
+				st2.pop_back();
+				const BvhNode& n = bvh->nodes[nid];
+				if (!grown(n))
+					continue;
+				if (n.left == -1 && n.right == -1)
+					for (int i = n.start; i < n.start + n.count; i++)
+						count_leaf(bvh->order[i]);
+				else
+				{
+					if (n.left != -1)
+						st2.push_back(n.left);
+					if (n.right != -1)
+						st2.push_back(n.right);
+				}
+			}
+		}
 		const V3 inv = v3(1.0f / cast.x, 1.0f / cast.y, 1.0f / cast.z);
 		auto slab = [&](const BvhNode& n)
 		{
@@ -688,21 +745,59 @@ namespace
 			if (!hop_ok(q.hop, q.max_hop, { m.edges[2 * eid2], m.edges[2 * eid2 + 1] }))
 				return;
 			Hit h;
-			const bool hit = edge_edge_test(m, r, q.eid, eid2, h);
-			if (hit)
+			if (edge_edge_test(m, r, q.eid, eid2, h))
 				out.push_back(h);
-			const uint a0 = m.edges[2 * q.eid], a1 = m.edges[2 * q.eid + 1], b0 = m.edges[2 * eid2], b1 = m.edges[2 * eid2 + 1];
-			if (rc && !(a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1))
-			{
-				const V3 q0 = load3(m.x, b0), q1 = load3(m.x, b1);
-				if (edge_gate(sw_lo, sw_hi, q0, q1))
-					rc->add(recheck_edge_edge(r.p0, r.p1, q.dir, ray_max, r.plane, r.pn, r.pd, q0, q1, hit));
-			}
 		};
+		// the FP64 recheck count: the candidate edges (sharing no vertex with the swept edge)
+		// whose grown box the swept edge's box meets, found by a second walk over node boxes
+		// grown by twice that margin
+		auto count_leaf = [&](uint eid2)
+		{
+			if (!in_span(eid2, q.target_lo, q.target_cnt) || (q.targets && !std::binary_search(q.targets->begin(), q.targets->end(), eid2)))
+				return;
+			const uint a0 = m.edges[2 * q.eid], a1 = m.edges[2 * q.eid + 1], b0 = m.edges[2 * eid2], b1 = m.edges[2 * eid2 + 1];
+			if (!hop_ok(q.hop, q.max_hop, { b0, b1 }) || a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1)
+				return;
+			const V3 q0 = load3(m.x, b0), q1 = load3(m.x, b1);
+			if (!edge_gate(sw_lo, sw_hi, q0, q1))
+				return;
+			Hit h;
+			rc->add(recheck_edge_edge(r.p0, r.p1, q.dir, ray_max, r.plane, r.pn, r.pd, q0, q1, edge_edge_test(m, r, q.eid, eid2, h)));
+		};
+		if (rc && bvh != nullptr && !bvh->nodes.empty())
+		{
+			std::vector<int> st2{ 0 };
+			while (!st2.empty())
+			{
+				const int nid = st2.back();
+				st2.pop_back();
+				const BvhNode& n = bvh->nodes[nid];
+				const float e = 2e-5f * (1.0f + std::fmax(std::fmax(std::fmax(std::fabs(n.bmin.x), std::fabs(n.bmax.x)),
+														std::fmax(std::fabs(n.bmin.y), std::fabs(n.bmax.y))),
+												  std::fmax(std::fabs(n.bmin.z), std::fabs(n.bmax.z))));
+				if (!(sw_lo.x <= n.bmax.x + e && sw_hi.x >= n.bmin.x - e && sw_lo.y <= n.bmax.y + e && sw_hi.y >= n.bmin.y - e &&
+						sw_lo.z <= n.bmax.z + e && sw_hi.z >= n.bmin.z - e))
+					continue;
+				if (n.left == -1 && n.right == -1)
+					for (int i = n.start; i < n.start + n.count; i++)
+						count_leaf(bvh->order[i]);
+				else
+				{
+					if (n.left != -1)
+						st2.push_back(n.left);
+					if (n.right != -1)
+						st2.push_back(n.right);
+				}
+			}
+		}
 		if (bvh == nullptr)
 		{
 			for (uint e : *q.targets)
+			{
 				leaf(e);
+				if (rc)
+					count_leaf(e);
+			}
 			return;
 		}
 		if (bvh->nodes.empty())

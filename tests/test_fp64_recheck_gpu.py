@@ -19,9 +19,9 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("mesh_fn,kw", [
     (lambda: synthetic.folded_sheet(64, seed=2), dict(max_contours=64)),
-    (lambda: synthetic.two_sheets(64, seed=3), {}),
+    (lambda: synthetic.two_sheets(48, seed=3), {}),
     (lambda: synthetic.folded_sheet(48, seed=2), dict(max_contours=64, direction_mode=1, opt_iterations=4)),
-], ids=["folded64", "two_sheets64", "folded48_26dirs_4steps"])
+], ids=["folded64", "two_sheets48", "folded48_26dirs_4steps"])
 def test_recheck_counts_and_fp64_metrics(oracle, u26ctx, mesh_fn, kw):
     from test_prp_gpu import _compare
     m = mesh_fn()

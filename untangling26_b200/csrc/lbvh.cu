@@ -351,13 +351,23 @@ namespace u26
 			__shared__ uint32_t s_cnt[kRefitBlock];
 			__shared__ Box6 s_leaf[kRefitBlock];
 			__shared__ Box6 s_inner[kRefitBlock];
+			// topology of the inner nodes [base, base + cnt), read once with coalesced loads, so
+			// that the climb's dependent lookups inside the block hit shared memory
+			__shared__ uint2 s_child[kRefitBlock];
+			__shared__ uint32_t s_parent[kRefitBlock], s_range[kRefitBlock];
 			const uint32_t base = blockIdx.x * kRefitBlock;
 			const uint32_t cnt = min(kRefitBlock, n - base);
+			const uint32_t ni = n - 1;
 			s_cnt[threadIdx.x] = 0u;
+			if (base + threadIdx.x < ni)
+			{
+				s_child[threadIdx.x] = __ldg(children + base + threadIdx.x);
+				s_parent[threadIdx.x] = __ldg(parent + base + threadIdx.x);
+				s_range[threadIdx.x] = __ldg(node_range + base + threadIdx.x);
+			}
 			__syncthreads();
 			if (threadIdx.x >= cnt)
 				return;
-			const uint32_t ni = n - 1;
 			const uint32_t lid = base + threadIdx.x;
 			f3 mn, mx;
 			if constexpr (FUSED)
@@ -380,9 +390,11 @@ namespace u26
 					atomicExch(health, 0u);
 					return;
 				}
+				// node in this block's id range (its topology is in shared memory)
+				const bool here = node - base < cnt;
 				if (local)
 				{
-					const uint32_t r = __ldg(node_range + node);
+					const uint32_t r = here ? s_range[node - base] : __ldg(node_range + node);
 					local = min(node, r) >= base && max(node, r) < base + cnt;
 				}
 				if (local)
@@ -401,7 +413,7 @@ namespace u26
 					if ((arrived & 1u) == 0u)
 						return;
 				}
-				const uint2 c = __ldg(children + node);
+				const uint2 c = here ? s_child[node - base] : __ldg(children + node);
 				f3 amn, amx, bmn, bmx;
 				if (local)
 				{
@@ -430,7 +442,7 @@ namespace u26
 				__stcg(&boxes[node].mx, make_float4(mx.x, mx.y, mx.z, 1.0f));
 				if (local)
 					s_inner[node - base] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
-				node = __ldg(parent + node);
+				node = here ? s_parent[node - base] : __ldg(parent + node);
 			}
 		}
 

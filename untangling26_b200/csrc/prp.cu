@@ -1124,8 +1124,20 @@ namespace u26
 					g.mx = __ldg(&egrow[node].mx);
 					visited += on ? 1u : 0u;
 					fetch_nodes++;
-					const bool hit = on && (smn.x <= g.mx.x) & (smx.x >= g.mn.x) & (smn.y <= g.mx.y) & (smx.y >= g.mn.y) & (smn.z <= g.mx.z) &
+					bool hit = on && (smn.x <= g.mx.x) & (smx.x >= g.mn.x) & (smn.y <= g.mx.y) & (smx.y >= g.mn.y) & (smn.z <= g.mx.z) &
 						(smx.z >= g.mn.z);
+					// the swept edge lies in the plane (pn, pd): a box that keeps clear of the slab
+					// |dot(pn, q) - pd| <= 1e-6 holds only edges the leaf's separating-plane test
+					// rejects (cached_bvh.cpp:433-473 prunes its nodes the same way). The boxes carry
+					// the 1e-5 (1 + |c|) margin, far above the rounding of this test, so no edge the
+					// leaf test keeps is pruned.
+					if (hit && plane)
+					{
+						const f3 c = mk3(0.5f * (g.mn.x + g.mx.x), 0.5f * (g.mn.y + g.mx.y), 0.5f * (g.mn.z + g.mx.z));
+						const f3 h = mk3(0.5f * (g.mx.x - g.mn.x), 0.5f * (g.mx.y - g.mn.y), 0.5f * (g.mx.z - g.mn.z));
+						const float rad = (h.x * fabsf(pn.x) + h.y * fabsf(pn.y)) + h.z * fabsf(pn.z);
+						hit = fabsf(dot(pn, c) - pd) <= rad + 1e-6f;
+					}
 					const uint32_t link_a = __float_as_uint(g.mn.w), link_b = __float_as_uint(g.mx.w);
 					bool descend = false;
 					if (__ballot_sync(0xFFFFFFFFu, hit) == 0u)
