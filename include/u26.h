@@ -72,6 +72,10 @@ U26_API const char* u26_ctx_last_error(const u26_ctx* ctx);
 U26_API u26_status u26_ctx_device_errors(u26_ctx* ctx, uint32_t* flags, int reset);
 /* Number of kernels this context has launched since creation (instrumentation). */
 U26_API uint64_t u26_ctx_launch_count(const u26_ctx* ctx);
+/* Device and pinned host allocations the library has made in this process so far (every
+ * context); a diagnostic: entry points documented as allocation-free leave it unchanged. No
+ * reference counterpart. */
+U26_API uint64_t u26_alloc_count(void);
 U26_API const char* u26_version(void);
 
 /* ---- LBVH (replaces lcs::LBVH, lbvh.h:164-325) -----------------------------------
@@ -167,9 +171,11 @@ U26_API u26_status u26_ef_canonicalize(u26_ctx* ctx, uint32_t count, void* ef_pa
  * u26_ef_canonicalize. Its scratch is a fixed array of U26_NOALLOC_SCRATCH_BYTES in
  * the library's static device memory, held on every GPU that loads the library until the
  * process exits; count above U26_NOALLOC_MAX_EF_PAIRS returns U26_ERR_CAPACITY. The
- * first call on each device looks up the array's device address (make that first call
- * before any stream capture). All calls share the one array: calls that overlap on the
- * GPU (other streams or contexts) race and must be ordered by the caller. */
+ * first call on each context looks up the array's device address on the context's device
+ * and keeps it on the context (make that first call before any stream capture; a context
+ * created after a device reset looks the address up again). All calls share the one array:
+ * calls that overlap on the GPU (other streams or contexts) race and must be ordered by
+ * the caller. */
 #define U26_NOALLOC_MAX_EF_PAIRS 32768u
 #define U26_NOALLOC_SCRATCH_BYTES 2637824u
 U26_API u26_status u26_ef_canonicalize_noalloc(u26_ctx* ctx, uint32_t count, void* ef_pairs, uint32_t* ef_indices,

@@ -56,6 +56,25 @@ def test_noalloc_matches_allocating_sort_twice(u26ctx):
         assert np.all(np.diff(keys) >= 0), "not in canonical (eid, fid) order"
 
 
+def test_noalloc_allocates_nothing():
+    """On a context that has never sorted, the no-alloc sort (its first call included, which
+    looks up the scratch address) leaves the library's allocation count unchanged."""
+    from untangling26_b200 import Context
+    ctx = Context(0)
+    try:
+        mesh = synthetic.two_sheets(40, seed=4)
+        pairs, idx, n = _unsorted_ef(ctx, mesh)
+        torch.cuda.synchronize()
+        before = ctx.lib.u26_alloc_count()
+        for _ in range(2):
+            ctx.check(ctx.lib.u26_ef_canonicalize_noalloc(ctx.handle, n, ptr(pairs), ptr(idx), mesh.num_edges, mesh.num_faces),
+                      "canonicalize_noalloc")
+        torch.cuda.synchronize()
+        assert ctx.lib.u26_alloc_count() == before
+    finally:
+        ctx.close()
+
+
 def test_noalloc_rejects_oversize(u26ctx):
     st = u26ctx.lib.u26_ef_canonicalize_noalloc(u26ctx.handle, 32769, ctypes.c_void_p(16), ctypes.c_void_p(16), 10, 10)
     assert st == 1  # U26_ERR_CAPACITY, nothing launched

@@ -51,6 +51,7 @@ _SIGS = {
     "u26_ctx_last_error": (ctypes.c_char_p, [c_vp]),
     "u26_ctx_device_errors": (c_int, [c_vp, c_u32p, c_int]),
     "u26_ctx_launch_count": (c_u64, [c_vp]),
+    "u26_alloc_count": (c_u64, []),
     "u26_lbvh_create": (c_int, [c_vp, c_int, c_u32, ctypes.POINTER(c_vp)]),
     "u26_lbvh_destroy": (None, [c_vp]),
     "u26_lbvh_reduce_aabb": (c_int, [c_vp, c_vp, c_u32, c_vp]),

@@ -4,7 +4,14 @@
 void u26_ef_release_ctx(const u26_ctx* ctx);
 void u26_prp_release_ctx(const u26_ctx* ctx);
 
+namespace u26
+{
+	std::atomic<uint64_t> g_alloc_count{ 0 };
+}
+
 using namespace u26;
+
+U26_API uint64_t u26_alloc_count(void) { return g_alloc_count.load(std::memory_order_relaxed); }
 
 U26_API const char* u26_version(void) { return "u26-b200 0.1 (sm_100a)"; }
 
@@ -32,6 +39,7 @@ U26_API u26_status u26_ctx_create(int device, void* cuda_stream, u26_ctx** out)
 		u26_ctx_destroy(ctx);
 		return U26_ERR_CUDA;
 	}
+	g_alloc_count.fetch_add(2, std::memory_order_relaxed);
 	*out = ctx;
 	return U26_OK;
 }

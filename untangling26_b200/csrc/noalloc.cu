@@ -8,8 +8,6 @@
 // array (U26_NOALLOC_SCRATCH_BYTES, about 2.6 MB) until the process exits.
 //
 // The caller still passes the EF pairs and indices, which are sorted in place.
-#include <mutex>
-
 #include "u26_internal.h"
 
 namespace
@@ -31,7 +29,7 @@ namespace
 		"scratch regions must stay 256-byte aligned");
 
 	// The scratch array. Host code must not use its name as an address: the device
-	// address comes from cudaGetSymbolAddress, once per device, in scratch_for_device.
+	// address comes from cudaGetSymbolAddress, once per context, in scratch_for_context.
 	static __device__ __align__(256) unsigned char g_ef_sort_scratch[U26_NOALLOC_SCRATCH_BYTES];
 
 	struct EfRec
@@ -63,30 +61,24 @@ namespace
 		dst_idx[i] = src_idx[j];
 	}
 
-	std::mutex g_scratch_mutex;
-	unsigned char* g_scratch_ptr[64] = {};
-
-	// Device address of the scratch array on `device`, looked up once with that device
-	// current. The first call on each device does the lookup.
-	u26_status scratch_for_device(u26_ctx* ctx, unsigned char** out)
+	// Device address of the scratch array for the context's device, looked up with that device
+	// current by the first call on the context and kept on it. A context made after a device
+	// reset looks it up anew.
+	u26_status scratch_for_context(u26_ctx* ctx, unsigned char** out)
 	{
-		const int dev = ctx->device;
-		if (dev < 0 || dev >= 64)
-			return u26::set_error(ctx, U26_ERR_INVALID_INPUT, "u26_ef_canonicalize_noalloc: device %d out of range", dev);
-		std::lock_guard<std::mutex> lock(g_scratch_mutex);
-		if (g_scratch_ptr[dev] == nullptr)
+		if (ctx->noalloc_scratch == nullptr)
 		{
 			int prev = 0;
 			U26_CUDA(ctx, cudaGetDevice(&prev));
-			U26_CUDA(ctx, cudaSetDevice(dev));
+			U26_CUDA(ctx, cudaSetDevice(ctx->device));
 			void* p = nullptr;
 			const cudaError_t e = cudaGetSymbolAddress(&p, g_ef_sort_scratch);
 			cudaSetDevice(prev);
 			if (e != cudaSuccess || p == nullptr)
 				return u26::set_error(ctx, U26_ERR_CUDA, "cudaGetSymbolAddress(scratch): %s", cudaGetErrorString(e));
-			g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+			ctx->noalloc_scratch = static_cast<unsigned char*>(p);
 		}
-		*out = g_scratch_ptr[dev];
+		*out = ctx->noalloc_scratch;
 		return U26_OK;
 	}
 } // namespace
@@ -106,7 +98,7 @@ U26_API u26_status u26_ef_canonicalize_noalloc(u26_ctx* ctx, uint32_t count, voi
 	if (!ef_pairs || !ef_indices || num_faces == 0 || num_edges == 0)
 		return set_error(ctx, U26_ERR_INVALID_INPUT, "u26_ef_canonicalize_noalloc: bad input");
 	unsigned char* base = nullptr;
-	U26_TRY(scratch_for_device(ctx, &base));
+	U26_TRY(scratch_for_context(ctx, &base));
 	uint64_t* keys = reinterpret_cast<uint64_t*>(base + kKeys);
 	uint64_t* keys_alt = reinterpret_cast<uint64_t*>(base + kKeysAlt);
 	uint32_t* vals = reinterpret_cast<uint32_t*>(base + kVals);

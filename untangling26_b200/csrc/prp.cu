@@ -4687,6 +4687,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 						S->cap_host = nullptr;
 						S->cap_host_bytes = 0;
 						U26_CUDA(ctx, cudaMallocHost(&S->cap_host, bytes + bytes / 2));
+						g_alloc_count.fetch_add(1, std::memory_order_relaxed);
 						S->cap_host_bytes = bytes + bytes / 2;
 					}
 					U26_CUDA(ctx, cudaMemcpyAsync(S->cap_host, S->d_capture.ptr, bytes, cudaMemcpyDeviceToHost, st));

@@ -1,6 +1,7 @@
 // Host-side internals of libu26: the context object, grow-only device buffers and
 // error plumbing shared by the .cu translation units.
 #pragma once
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -18,10 +19,16 @@ struct u26_ctx
 	uint32_t* dev_err = nullptr;
 	// pinned host staging word for small readbacks
 	uint32_t* host_word = nullptr;
+	// device address of the allocation-free EF sort's static scratch, looked up by the first
+	// u26_ef_canonicalize_noalloc call on this context
+	unsigned char* noalloc_scratch = nullptr;
 };
 
 namespace u26
 {
+	// device and pinned-host allocations the library has made (u26_alloc_count)
+	extern std::atomic<uint64_t> g_alloc_count;
+
 	// Grow-only device allocation owned by a context-side object.
 	struct DevBuf
 	{
@@ -37,7 +44,10 @@ namespace u26
 			bytes = 0;
 			cudaError_t e = cudaMalloc(&ptr, want);
 			if (e == cudaSuccess)
+			{
 				bytes = want;
+				g_alloc_count.fetch_add(1, std::memory_order_relaxed);
+			}
 			return e;
 		}
 		void release()
