@@ -147,6 +147,7 @@ class Workload:
         from untangling26_b200 import synthetic
         self.name = name
         self.batch = name.startswith("batch")
+        self.repair = False
         self.params = dict(max_contours=ALL_CONTOURS, batch_size=ALL_CONTOURS)
         if name == "batch64":
             self.full = synthetic.batch_scenes(64, seed=2)
@@ -174,6 +175,17 @@ class Workload:
             self.params = dict(max_contours=256, batch_size=32)
             self.config = {"workload": "two_sheets_64x64", "seed": 0, "triangles": 15876, "directions": "reference seeds (<=10)",
                            "opt_iterations": 0, "contours": "first 256"}
+        elif name == "layered5x512":
+            # the scale form: five stacked 512 x 512 sheets 1 mm apart with multi-octave
+            # displacement of 2-20 mm; every step is one untangling pass followed by a fixed step
+            # along its assembled response (the repair loop), so the K steps are K passes of it
+            self.full = synthetic.layered_sheets(512, layers=5, seed=4)
+            self.timed_ids = None
+            self.params = dict(max_contours=256, batch_size=32)
+            self.repair = True
+            self.config = {"workload": "layered_sheets_5x512x512", "seed": 4, "layers": 5, "triangles": int(self.full.num_faces),
+                           "spacing_mm": 1, "displacement_mm": "U[2, 20] multi-octave", "directions": "reference seeds (<=10)",
+                           "opt_iterations": 0, "contours": "first 256 of each pass", "update": "response step, scale 1"}
         else:
             raise SystemExit(f"unknown workload {name}")
         self.config["l2"] = "flushed between steps (256 MB write)"
@@ -314,14 +326,19 @@ class PassRunner:
         self.sc.close()
 
 
-def _timed_passes(runner, steps, flush, stream):
+def _timed_passes(runner, steps, flush, stream, repair=False):
+    """K timed passes; with repair, each pass is followed (inside its timed step) by the fixed
+    step along its assembled response, so the passes form the repair sequence."""
     import torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     out = []
     for i in range(steps):
         flush.fill_(i & 0xFF)
         ev[i][0].record(stream)
-        out.append(runner.run())
+        res = runner.run()
+        if repair:
+            runner.sc.response_step(res.response, 1.0)
+        out.append(res)
         ev[i][1].record(stream)
     torch.cuda.synchronize()
     return [a.elapsed_time(b) for a, b in ev], out
@@ -403,17 +420,23 @@ def main():
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    step_ms, results = _timed_passes(runner, args.steps, flush, stream)
+    step_ms, results = _timed_passes(runner, args.steps, flush, stream, repair=wl.repair)
     if ws > 1:
         dist.barrier()
     clk = clocks.stop()
     launches = ctx.launch_count() - launches0
-    r0 = results[-1]
+    # the pass compared with the oracle: the last one, or with repair the first (the input's positions)
+    r0 = results[0] if wl.repair else results[-1]
     ef_rc = (int(runner.sc.stats[2].item()), int(runner.sc.stats[3].item()))
-    tests_pass = r0.tested
+    tests_pass = sum(r.tested for r in results) / len(results)
     for r in results:
-        if r.tested != tests_pass or r.device_error_flags:
-            raise SystemExit(f"passes differ between steps ({r.tested} vs {tests_pass} leaf tests) or device errors")
+        if r.device_error_flags or (not wl.repair and r.tested != r0.tested):
+            raise SystemExit(f"passes differ between steps ({r.tested} vs {r0.tested} leaf tests) or device errors")
+    repair = None
+    if wl.repair:
+        repair = {"ef_pairs_per_pass": [int(r.num_orig_pairs) for r in results], "contours_per_pass": [len(r.contours) for r in results],
+                  "response_pairs_per_pass": [int(r.response.num_pairs) for r in results], "pass_ms": [round(t, 2) for t in step_ms],
+                  "passes_per_s": 1e3 * len(step_ms) / sum(step_ms)}
     total_ms = job_time_ms(sum(step_ms), device=dev)  # max over ranks
     tests_all = tests_pass
     if ws > 1:
@@ -425,7 +448,7 @@ def main():
 
     # ---- e2e through the public API with host buffers (positions in, results out)
     x_host = torch.from_numpy(tmesh.x).pin_memory()
-    e_ms, d2h = [], 0
+    e_ms, d2h, e_tests = [], 0, 0
     for i in range(args.steps):
         flush.fill_(i & 0xFF)
         torch.cuda.synchronize()
@@ -434,9 +457,14 @@ def main():
         res = runner.run()  # the per-contour results and supports come back to the host inside u26_prp_resolve
         torch.cuda.synchronize()
         e_ms.append(1e3 * (time.perf_counter() - t0))
+        e_tests += res.tested
         d2h = int(sum(h.nbytes for h in res.hits) + res.results.nbytes + res.pairs.nbytes)
     e2e_ms = job_time_ms(sum(e_ms), device=dev)
-    e2e_value = tests_all * args.steps / (e2e_ms / 1e3)
+    if ws > 1:
+        t = torch.tensor([float(e_tests)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        e_tests = t.item()
+    e2e_value = e_tests / (e2e_ms / 1e3)
 
     # ---- roofline of the dominant kernel: raycast_kernel. Its CUDA-event time per pass is
     # measured here; the DRAM bytes and warp instructions per pass come from one ncu capture
@@ -531,6 +559,7 @@ def main():
                      "gpu_ms": {k: round(v, 2) for k, v in r0.gpu_ms.items()},
                      "stage_ms": {k: round(v, 2) for k, v in r0.stage_ms.items()}},
             "parity": parity,
+            "repair": repair,
             "fp64": dict(r0.fp64, ef_rechecks=ef_rc[0], ef_flips=ef_rc[1],
                          note="rechecks / flips: leaf tests of the timed pass inside their FP32 error band, re-decided in FP64 "
                               "(sets keep FP32); *_rel_err: the selected supports' FP32 depth, D_C and J against FP64"),
