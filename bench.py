@@ -430,8 +430,12 @@ def main():
     ef_rc = (int(runner.sc.stats[2].item()), int(runner.sc.stats[3].item()))
     tests_pass = sum(r.tested for r in results) / len(results)
     for r in results:
-        if r.device_error_flags or (not wl.repair and r.tested != r0.tested):
-            raise SystemExit(f"passes differ between steps ({r.tested} vs {r0.tested} leaf tests) or device errors")
+        if r.device_error_flags:
+            raise SystemExit(f"device error flags 0x{r.device_error_flags:x}")
+        # every timed pass returns the same results (the leaf-test count may differ by a few between
+        # passes: see the packet walk's node tests)
+        if not wl.repair and (r.results.tobytes() != r0.results.tobytes() or any(a.tobytes() != b.tobytes() for a, b in zip(r.hits, r0.hits))):
+            raise SystemExit("timed passes returned different results")
     repair = None
     if wl.repair:
         repair = {"ef_pairs_per_pass": [int(r.num_orig_pairs) for r in results], "contours_per_pass": [len(r.contours) for r in results],
@@ -552,6 +556,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(tmesh.x.nbytes), "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": int(launches), "clocks": clk, "roofline": roof, "cpu_baseline": cpu, "lbvh_refit": refit,
+            "leaf_tests_per_step": [int(r.tested) for r in results],
             "pass": {"scenes": len(tmesh.meta.get("scenes", [0])), "triangles": int(tmesh.num_faces), "ef_pairs": int(len(r0.pairs)),
                      "contours": len(r0.contours), "levels": r0.levels, "requests": r0.requests, "leaf_tests": r0.tested,
                      "candidate_leaf_tests": r0.candidate_tests, "ray_node_visits": r0.ray_visits,
