@@ -169,6 +169,12 @@ class Workload:
             self.params = dict(max_contours=256, batch_size=32, direction_mode=1, opt_iterations=8)
             self.config = {"workload": "folded_sheet_256x256", "seed": 1, "triangles": 130050, "fold_noise_sigma_edge_lengths": 0.3,
                            "directions": "26 lattice", "opt_iterations": 8, "contours": "first 256"}
+        elif name == "folded128":  # a small case of the folded sheet (profiling)
+            self.full = synthetic.folded_sheet(128, seed=1)
+            self.timed_ids = None
+            self.params = dict(max_contours=256, batch_size=32)
+            self.config = {"workload": "folded_sheet_128x128", "seed": 1, "triangles": int(self.full.num_faces),
+                           "directions": "reference seeds (<=10)", "opt_iterations": 0, "contours": "first 256"}
         elif name == "two_sheets64":
             self.full = synthetic.two_sheets(64, seed=0)
             self.timed_ids = None
@@ -569,8 +575,10 @@ def main():
                          note="rechecks / flips: leaf tests of the timed pass inside their FP32 error band, re-decided in FP64 "
                               "(sets keep FP32); *_rel_err: the selected supports' FP32 depth, D_C and J against FP64"),
             "raycast_config": {"parts": r0.raycast_config["parts"], "blocks_per_sm": r0.raycast_config["blocks_per_sm"],
+                               "queue": r0.raycast_config["queue"],
                                "autotune_ms": tuned.get("tune_ms") if tuned else None,
-                               "note": "chosen by the autotuner on the first warm-up pass: ray-casting ms of each parts x blocks/SM"},
+                               "note": "chosen by the autotuner on the first warm-up pass: ray-casting ms of each parts x blocks/SM "
+                                       "(q: persistent work-queue grid)"},
             "untangle_passes_per_s": 1e3 / pass_ms, "pass_seconds": pass_ms / 1e3,
             "speedup_vs_cpu_pass": (cpu["pass_seconds"] / (pass_ms / 1e3)) if cpu and cpu.get("pass_seconds") else None,
             "full_batch": full,

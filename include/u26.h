@@ -250,8 +250,9 @@ typedef struct u26_prp_params
 								 * (u26_prp_output_view.fp64_rechecks / fp64_flips); the hit sets keep the FP32
 								 * decisions. Also evaluates the selected supports' metrics in FP64 (fp64_*_rel_err). */
 	uint32_t autotune;			/* 1: the scene's first pass times every ray-casting configuration (subtree parts x blocks
-								 * per SM) on each of its launches and the scene keeps the fastest; 0: 8 parts, 7 blocks */
-	uint32_t raycast_config;	/* 0: the default or autotuned configuration; k in 1..9: use configuration k - 1 of the
+								 * per SM x grid form) on each of its launches and the scene keeps the fastest;
+								 * 0: 8 parts, 7 blocks, a warp per work item */
+	uint32_t raycast_config;	/* 0: the default or autotuned configuration; k in 1..18: use configuration k - 1 of the
 								 * table in u26_prp_output_view.tune_ms (every configuration returns the same results) */
 } u26_prp_params;
 
@@ -317,12 +318,14 @@ typedef struct u26_prp_output_view
 	double fp64_delta_rel_err;		 /* max over the selected hits of |delta_32 - delta_64| / delta_64 */
 	double fp64_dc_rel_err;			 /* max over processed contours of |D_C,32 - D_C,64| / D_C,64 (depth) */
 	double fp64_j_rel_err;			 /* max over processed contours of |J_32 - J_64| / J_64 (objective) */
-	double tune_ms[9];				 /* autotune pass: ray-casting time (ms, summed over the pass's launches) of each
-									  * configuration (subtree parts, blocks per SM): (4,6) (4,7) (4,8) (8,6) (8,7)
-									  * (8,8) (16,6) (16,7) (16,8) */
+	double tune_ms[18];				 /* autotune pass: ray-casting time (ms, summed over the pass's launches) of each
+									  * configuration (subtree parts, blocks per SM, grid form): (4,6) (4,7) (4,8) (8,6)
+									  * (8,7) (8,8) (16,6) (16,7) (16,8) with a warp per work item, then the same nine
+									  * with a persistent grid whose warps take work items from a queue */
 	uint32_t raycast_parts;			 /* configuration the scene's ray casts use from now on: subtree parts per request */
-	uint32_t raycast_blocks_per_sm;	 /* ... and resident 128-thread blocks per SM */
+	uint32_t raycast_blocks_per_sm;	 /* ... resident 128-thread blocks per SM */
 	uint32_t tuned;					 /* 1 when this pass ran the autotuner (its choice holds for the scene's later passes) */
+	uint32_t raycast_queue;			 /* ... and 1 for the persistent work-queue grid */
 } u26_prp_output_view;
 
 /* One PRP pass. face_tree / edge_tree: the scene's face and edge LBVHs refit at x (any

@@ -869,28 +869,42 @@ namespace u26
 		// target tree's frontier for that split, so every (ray, leaf) pair is decided once.
 		// MINB: resident 128-thread blocks per SM the registers are sized for.
 		constexpr int kStack = 64;
-		template <bool RECHECK, int MINB>
+		template <bool RECHECK, int MINB, bool QUEUE>
 		__global__ void __launch_bounds__(128, MINB) raycast_kernel(const Task* __restrict__ tasks, uint32_t ntasks, uint32_t total,
 			const Slot* __restrict__ slots, const uint32_t* __restrict__ cand_v, const uint32_t* __restrict__ cand_e, uint32_t v_stride,
 			uint32_t e_stride, uint32_t f_stride, const uint32_t* __restrict__ bits_e, const uint32_t* __restrict__ bits_f,
 			const NodeBox* __restrict__ fgrow, const NodeBox* __restrict__ egrow, const uint32_t* __restrict__ ffront,
 			const uint32_t* __restrict__ efront, const float* __restrict__ x, const uint2* __restrict__ edges,
 			const uint32_t* __restrict__ faces, const float* __restrict__ slot_box, HitSink sink, unsigned long long* __restrict__ stats,
-			uint32_t split, uint32_t* __restrict__ dev_err)
+			uint32_t split, uint32_t* __restrict__ queue, uint32_t* __restrict__ dev_err)
 		{
 			const int lane = threadIdx.x & 31;
 			// the packet's traversal stack lives in registers across the warp: entry k in lane k & 31
 			// of s_lo (k < 32) or s_hi (k >= 32); every lane holds the same stack pointer
 			uint32_t s_lo = 0u, s_hi = 0u;
 			const uint32_t warps_per_part = (total + 31u) >> 5;
-			const uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-			const uint32_t part = wi / warps_per_part; // warp-uniform
-			if (part >= split)
-				return; // whole warps only
-			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
-			uint32_t tested = 0, visited = 0, etested = 0, ctested = 0, rechecks = 0, flips = 0;
+			const uint32_t items = split * warps_per_part; // (part, packet) work items
+			uint32_t tested = 0, visited = 0, etested = 0, ctested = 0, rechecks = 0, flips = 0, reqs = 0;
 			uint32_t fetch_nodes = 0, fetch_tris = 0, fetch_edges = 0; // warp-uniform: data each packet brings in
 			uint32_t ray_visits = 0; // the node tests this ray alone would make: its start + 2 per inner node it enters
+			// QUEUE (persistent form): every warp takes work items from a device counter until none is
+			// left, so no warp idles while the other warps of its block finish; otherwise the grid
+			// has one warp per item
+			uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			for (;;)
+			{
+			if constexpr (QUEUE)
+			{
+				uint32_t it = 0;
+				if (lane == 0)
+					it = atomicAdd(queue, 1u);
+				wi = __shfl_sync(0xFFFFFFFFu, it, 0);
+			}
+			if (wi >= items)
+				break; // whole warps only
+			const uint32_t part = wi / warps_per_part; // warp-uniform
+			const uint32_t r = (wi - part * warps_per_part) * 32u + uint32_t(lane);
+			reqs += (part == 0 && r < total) ? 1u : 0u;
 
 			// ---- per-lane request
 			int kind = 0; // 1: VF / FV ray on the face tree, 2: EE swept edge on the edge tree
@@ -1253,10 +1267,13 @@ namespace u26
 				}
 				__syncwarp();
 			}
+			if constexpr (!QUEUE)
+				break;
+			}
 			if (stats)
 			{
 				const uint32_t tsum = __reduce_add_sync(0xFFFFFFFFu, tested);
-				const uint32_t rsum = __reduce_add_sync(0xFFFFFFFFu, (part == 0 && r < total) ? 1u : 0u);
+				const uint32_t rsum = __reduce_add_sync(0xFFFFFFFFu, reqs);
 				const uint32_t vsum = __reduce_add_sync(0xFFFFFFFFu, visited);
 				const uint32_t esum = __reduce_add_sync(0xFFFFFFFFu, etested);
 				const uint32_t rvsum = __reduce_add_sync(0xFFFFFFFFu, ray_visits);
@@ -1288,21 +1305,29 @@ namespace u26
 
 		// The traversal configurations the autotuner chooses from: subtree parts per request
 		// (4, 8, 16) x resident blocks of 128 threads per SM the registers are sized for (6, 7, 8:
-		// at most 80, 72 or 64 registers per thread). The packet is the warp (32 requests).
+		// at most 80, 72 or 64 registers per thread) x the grid form (one warp per work item, or a
+		// persistent grid of warps taking items from a queue). The packet is the warp (32 requests).
 		struct RaycastConfig
 		{
 			uint32_t split;
 			int min_blocks;
+			bool queue;
 		};
-		constexpr RaycastConfig kRaycastConfigs[] = { { 4, 6 }, { 4, 7 }, { 4, 8 }, { 8, 6 }, { 8, 7 }, { 8, 8 }, { 16, 6 }, { 16, 7 },
-			{ 16, 8 } };
-		constexpr int kNumRaycastConfigs = 9, kDefaultRaycastConfig = 4; // 8 parts, 7 blocks per SM
-		using RaycastFn = decltype(&raycast_kernel<false, 7>);
-		inline RaycastFn raycast_variant(bool recheck, int min_blocks)
+		constexpr RaycastConfig kRaycastConfigs[] = { { 4, 6, false }, { 4, 7, false }, { 4, 8, false }, { 8, 6, false }, { 8, 7, false },
+			{ 8, 8, false }, { 16, 6, false }, { 16, 7, false }, { 16, 8, false }, { 4, 6, true }, { 4, 7, true }, { 4, 8, true }, { 8, 6, true },
+			{ 8, 7, true }, { 8, 8, true }, { 16, 6, true }, { 16, 7, true }, { 16, 8, true } };
+		constexpr int kNumRaycastConfigs = 18, kDefaultRaycastConfig = 4; // 8 parts, 7 blocks per SM, a warp per item
+		using RaycastFn = decltype(&raycast_kernel<false, 7, false>);
+		template <bool R, bool Q>
+		inline RaycastFn raycast_variant_q(int min_blocks)
+		{
+			return min_blocks == 6 ? &raycast_kernel<R, 6, Q> : min_blocks == 8 ? &raycast_kernel<R, 8, Q> : &raycast_kernel<R, 7, Q>;
+		}
+		inline RaycastFn raycast_variant(bool recheck, int min_blocks, bool queue)
 		{
 			if (recheck)
-				return min_blocks == 6 ? &raycast_kernel<true, 6> : min_blocks == 8 ? &raycast_kernel<true, 8> : &raycast_kernel<true, 7>;
-			return min_blocks == 6 ? &raycast_kernel<false, 6> : min_blocks == 8 ? &raycast_kernel<false, 8> : &raycast_kernel<false, 7>;
+				return queue ? raycast_variant_q<true, true>(min_blocks) : raycast_variant_q<true, false>(min_blocks);
+			return queue ? raycast_variant_q<false, true>(min_blocks) : raycast_variant_q<false, false>(min_blocks);
 		}
 
 		// ---- the plain form (the comparison baseline of the batched, filtered form above):
@@ -3143,6 +3168,7 @@ struct u26_scene
 	DevBuf d_bnd_bits, d_slot_box, d_ncand, d_best, d_bsum, d_task_max, d_selbegin, d_pos, d_terms;
 	DevBuf d_step_in, d_step_hits, d_step_out;
 	DevBuf d_f64in, d_f64hits, d_f64delta, d_f64out; // FP64 evaluation of the selected supports
+	DevBuf d_queue;									  // work-item counter of the persistent ray casts
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
 	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals, d_zero_th;
 	RadixSorter sorter, esorter, csorter, fvsorter;
@@ -3153,6 +3179,7 @@ struct u26_scene
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 	int tuned_cfg = -1;				  // autotuned ray-casting configuration (-1: not tuned yet)
+	uint32_t num_sms = 148;			  // the device's SM count (the persistent grid's size)
 	uint64_t passes = 0;			  // completed u26_prp_resolve calls (the normals d_fn / d_en / d_vn are the last one's)
 	void* cap_host = nullptr;		  // pinned staging of the captured supports (grow-only)
 	size_t cap_host_bytes = 0;
@@ -3172,7 +3199,7 @@ struct u26_prp_output
 	double gpu_ms[6] = { 0 };
 	uint64_t ray_nodes = 0, ray_edge_tests = 0, ray_node_fetches = 0, ray_tri_fetches = 0, ray_edge_fetches = 0, ray_visits = 0, ray_candidate_tests = 0;
 	uint64_t fp64_rechecks = 0, fp64_flips = 0, dc_tie_rechecks = 0, dc_tie_flips = 0;
-	double tune_ms[9] = { 0 }; // autotuner: ray-casting time of each configuration over the tuning pass
+	double tune_ms[18] = { 0 }; // autotuner: ray-casting time of each configuration over the tuning pass
 	int raycast_cfg = -1;	   // configuration the scene's launches use from now on (index of the table)
 	uint32_t tuned = 0;		   // this pass ran the autotuner
 	double fp64_delta_rel_err = 0.0, fp64_dc_rel_err = 0.0, fp64_j_rel_err = 0.0;
@@ -3207,6 +3234,10 @@ U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* m, u26_sc
 		return set_error(ctx, U26_ERR_INVALID_INPUT, "u26_scene_create: missing mesh table");
 	std::unique_ptr<u26_scene> s(new u26_scene());
 	s->ctx = ctx;
+	int sms = 0;
+	if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device) == cudaSuccess && sms > 0)
+		s->num_sms = uint32_t(sms);
+	U26_CUDA(ctx, s->d_queue.reserve(sizeof(uint32_t)));
 	s->nv = m->num_verts;
 	s->ne = m->num_edges;
 	s->nf = m->num_faces;
@@ -3346,7 +3377,7 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_stats, &s->d_seg, &s->d_parent, &s->d_root, &s->d_att, &s->d_csize, &s->d_catt, &s->d_ekeys, &s->d_evals,
 		&s->d_ecount, &s->d_cand_roots, &s->d_vf_off, &s->d_vf, &s->d_anchor_off, &s->d_anchors, &s->d_out, &s->d_sel, &s->d_bnd_bits,
 		&s->d_slot_box, &s->d_ncand, &s->d_best, &s->d_bsum, &s->d_task_max, &s->d_selbegin, &s->d_pos, &s->d_terms, &s->d_step_in,
-		&s->d_step_hits, &s->d_step_out, &s->d_f64in, &s->d_f64hits, &s->d_f64delta, &s->d_f64out, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
+		&s->d_step_hits, &s->d_step_out, &s->d_f64in, &s->d_f64hits, &s->d_f64delta, &s->d_f64out, &s->d_queue, &s->d_fgrow, &s->d_egrow, &s->d_front, &s->d_cur_own,
 		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
 		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp, &s->d_vsolid,
 		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals,
@@ -4282,12 +4313,19 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				{
 					const RaycastConfig c = kRaycastConfigs[cfg];
 					const uint64_t nthreads = uint64_t(div_up(total_req, 32u)) * 32u * c.split;
-					const RaycastFn kern = raycast_variant(rc, c.min_blocks);
-					kern<<<uint32_t(div_up64(nthreads, 128)), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
+					uint64_t blocks = div_up64(nthreads, 128);
+					if (c.queue)
+					{
+						// persistent grid: the blocks that fit on the GPU at once, items from a counter
+						blocks = std::min<uint64_t>(blocks, uint64_t(S->num_sms) * uint64_t(c.min_blocks));
+						U26_CUDA(ctx, cudaMemsetAsync(S->d_queue.ptr, 0, sizeof(uint32_t), st));
+					}
+					const RaycastFn kern = raycast_variant(rc, c.min_blocks, c.queue);
+					kern<<<uint32_t(blocks), 128, 0, st>>>(S->d_tasks.as<Task>(), nt, total_req, S->d_slots.as<Slot>(),
 						S->d_cand_v.as<uint32_t>(), S->d_cand_e.as<uint32_t>(), vs, es_, fs, S->d_bits_e.as<uint32_t>(),
 						S->d_bits_f.as<uint32_t>(), S->d_fgrow.as<NodeBox>(), S->d_egrow.as<NodeBox>(), S->d_front.as<uint32_t>(),
 						S->d_front.as<uint32_t>() + size_t(nobj) * kFrontStride, d_x, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(),
-						S->d_slot_box.as<float>(), sink, stats, c.split, ctx->dev_err);
+						S->d_slot_box.as<float>(), sink, stats, c.split, S->d_queue.as<uint32_t>(), ctx->dev_err);
 					return after_launch(ctx, "raycast_kernel");
 				};
 				if (tuning && attempt == 0 && !hits_out)
@@ -5250,8 +5288,9 @@ U26_API u26_status u26_prp_output_view_get(const u26_prp_output* o, u26_prp_outp
 	v->fp64_delta_rel_err = o->fp64_delta_rel_err;
 	v->fp64_dc_rel_err = o->fp64_dc_rel_err;
 	v->fp64_j_rel_err = o->fp64_j_rel_err;
-	for (int i = 0; i < 9; i++)
+	for (int i = 0; i < kNumRaycastConfigs; i++)
 		v->tune_ms[i] = o->tune_ms[i];
+	v->raycast_queue = o->raycast_cfg >= 0 && kRaycastConfigs[o->raycast_cfg].queue ? 1u : 0u;
 	v->raycast_parts = o->raycast_cfg >= 0 ? kRaycastConfigs[o->raycast_cfg].split : 0u;
 	v->raycast_blocks_per_sm = o->raycast_cfg >= 0 ? uint32_t(kRaycastConfigs[o->raycast_cfg].min_blocks) : 0u;
 	v->tuned = o->tuned;

@@ -76,10 +76,17 @@ class PrpOutputView(ctypes.Structure):
         ("ray_edge_fetches", c_u64), ("ray_visits", c_u64), ("ray_candidate_tests", c_u64),
         ("fp64_rechecks", c_u64), ("fp64_flips", c_u64), ("dc_tie_rechecks", c_u64), ("dc_tie_flips", c_u64),
         ("fp64_delta_rel_err", ctypes.c_double), ("fp64_dc_rel_err", ctypes.c_double), ("fp64_j_rel_err", ctypes.c_double),
-        ("tune_ms", ctypes.c_double * 9), ("raycast_parts", c_u32), ("raycast_blocks_per_sm", c_u32), ("tuned", c_u32),
+        ("tune_ms", ctypes.c_double * 18), ("raycast_parts", c_u32), ("raycast_blocks_per_sm", c_u32), ("tuned", c_u32),
+        ("raycast_queue", c_u32),
     ]
 
-RAYCAST_CONFIGS = ((4, 6), (4, 7), (4, 8), (8, 6), (8, 7), (8, 8), (16, 6), (16, 7), (16, 8))  # (subtree parts, blocks / SM)
+# (subtree parts, blocks / SM, persistent work-queue grid)
+RAYCAST_CONFIGS = tuple((p, b, q) for q in (False, True) for p in (4, 8, 16) for b in (6, 7, 8))
+def config_name(c):
+    """'8x7' (parts x blocks per SM, a warp per item) or '8x7q' (persistent work-queue grid)."""
+    return f"{c[0]}x{c[1]}" + ("q" if c[2] else "")
+
+
 GPU_PHASES = ("raycast", "sort", "union", "entries", "select", "download")
 
 # CollisionPair::CollisionPairTemplate (collision_data.h:48-140), u26_collision_pair: 64 B
@@ -190,9 +197,9 @@ class PrpResult:
         self.ray_visits = int(v.ray_visits)
         self.candidate_tests = int(v.ray_candidate_tests)
         self.raycast_config = {"parts": int(v.raycast_parts), "blocks_per_sm": int(v.raycast_blocks_per_sm),
-                               "tuned_this_pass": bool(v.tuned)}
+                               "queue": bool(v.raycast_queue), "tuned_this_pass": bool(v.tuned)}
         if v.tuned:
-            self.raycast_config["tune_ms"] = {f"{p}x{b}": round(float(ms), 3) for (p, b), ms in zip(RAYCAST_CONFIGS, v.tune_ms)}
+            self.raycast_config["tune_ms"] = {config_name(c): round(float(ms), 3) for c, ms in zip(RAYCAST_CONFIGS, v.tune_ms)}
         self.fp64 = {"rechecks": int(v.fp64_rechecks), "flips": int(v.fp64_flips), "dc_tie_rechecks": int(v.dc_tie_rechecks),
                      "dc_tie_flips": int(v.dc_tie_flips), "delta_rel_err": float(v.fp64_delta_rel_err),
                      "dc_rel_err": float(v.fp64_dc_rel_err), "j_rel_err": float(v.fp64_j_rel_err)}
