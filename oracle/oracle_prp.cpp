@@ -2984,7 +2984,10 @@ extern "C"
 			std::vector<Hit> hs = ci.hits;
 			std::sort(hs.begin(), hs.end(), [](const Hit& a, const Hit& b)
 				{ return a.type != b.type ? a.type < b.type : (a.src_id != b.src_id ? a.src_id < b.src_id : a.dst_id < b.dst_id); });
-			double area = 0.0, dc64 = -1.0, derr = 0.0;
+			// source areas summed as the kernel's warp does: 32 strided partial sums (hit i into
+			// lane i % 32, in hit order), then the xor butterfly (lane l adds lane l ^ 16, ^ 8, ..., ^ 1)
+			double lane_area[32] = { 0.0 };
+			double dc64 = -1.0, derr = 0.0;
 			float m32 = -1.0f, s32 = -1.0f;
 			size_t arg32 = 0, arg64 = 0;
 			for (size_t i = 0; i < hs.size(); i++)
@@ -3012,7 +3015,7 @@ extern "C"
 						? t64 * 1.0
 						: double(hh.dist);
 				}
-				area += double(hh.type == VF ? m.rest_vert_area[hh.src_id] : hh.type == EE ? m.rest_edge_area[hh.src_id] : m.rest_face_area[hh.src_id]);
+				lane_area[i % 32] += double(hh.type == VF ? m.rest_vert_area[hh.src_id] : hh.type == EE ? m.rest_edge_area[hh.src_id] : m.rest_face_area[hh.src_id]);
 				if (d64 > dc64)
 				{
 					dc64 = d64;
@@ -3029,6 +3032,14 @@ extern "C"
 				if (d64 > 0.0)
 					derr = std::fmax(derr, std::fabs(double(hh.dist) - d64) / d64);
 			}
+			for (int off = 16; off > 0; off >>= 1)
+			{
+				double nv[32];
+				for (int l = 0; l < 32; l++)
+					nv[l] = lane_area[l] + lane_area[l ^ off];
+				std::copy(nv, nv + 32, lane_area);
+			}
+			const double area = lane_area[0];
 			const bool tie = hs.size() > 1 && m32 - s32 <= 4.0f * kGamma * m32;
 			o[0] = area * dc64 * dc64;
 			o[1] = dc64;

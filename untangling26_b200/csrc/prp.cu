@@ -2947,9 +2947,13 @@ namespace u26
 				return double(h.dist); // FP64 misses the hit (an FP32 / FP64 flip): keep its FP32 depth
 			return t64 * 1.0;
 		}
+		// Warp per contour. Each lane takes the hits h = begin + lane, begin + lane + 32, ...: their
+		// FP64 depths, its partial source-area sum (in that order), the maxima; the partial sums
+		// then combine by the xor butterfly (lane l adds lane l ^ 16, ^ 8, ^ 4, ^ 2, ^ 1), a fixed
+		// order the oracle restates. Ties of a maximum keep the smallest hit index.
 		__global__ void fp64_metrics_kernel(uint32_t nc, const Fp64In* __restrict__ in, const u26_prp_hit* __restrict__ hits,
 			const float* __restrict__ x, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const float* __restrict__ varea,
-			const float* __restrict__ earea, const float* __restrict__ farea, double* __restrict__ delta64, Fp64Out* __restrict__ out)
+			const float* __restrict__ earea, const float* __restrict__ farea, Fp64Out* __restrict__ out)
 		{
 			const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 			const uint32_t lane = threadIdx.x & 31u;
@@ -2957,19 +2961,14 @@ namespace u26
 				return;
 			const Fp64In ci = in[c];
 			const f3 dir = mk3(ci.dir[0], ci.dir[1], ci.dir[2]);
-			for (uint32_t h = ci.hit_begin + lane; h < ci.hit_end; h += 32u)
-				delta64[h] = hit_delta_f64(hits[h], dir, x, edges, faces);
-			__syncwarp();
-			if (lane != 0u)
-				return;
 			double area = 0.0, dc64 = -1.0, derr = 0.0;
 			float m32 = -1.0f, s32 = -1.0f;
-			uint32_t arg32 = ci.hit_begin, arg64 = ci.hit_begin;
-			for (uint32_t h = ci.hit_begin; h < ci.hit_end; h++)
+			uint32_t arg32 = kInvalid, arg64 = kInvalid;
+			for (uint32_t h = ci.hit_begin + lane; h < ci.hit_end; h += 32u)
 			{
 				const u26_prp_hit hh = hits[h];
+				const double d64 = hit_delta_f64(hh, dir, x, edges, faces);
 				area += double(hh.type == 0u ? varea[hh.src_id] : hh.type == 1u ? earea[hh.src_id] : farea[hh.src_id]);
-				const double d64 = delta64[h];
 				if (d64 > dc64)
 				{
 					dc64 = d64;
@@ -2986,6 +2985,31 @@ namespace u26
 				if (d64 > 0.0)
 					derr = fmax(derr, fabs(double(hh.dist) - d64) / d64);
 			}
+			for (int off = 16; off > 0; off >>= 1)
+			{
+				area += __shfl_xor_sync(0xFFFFFFFFu, area, off);
+				derr = fmax(derr, __shfl_xor_sync(0xFFFFFFFFu, derr, off));
+				const double od = __shfl_xor_sync(0xFFFFFFFFu, dc64, off);
+				const uint32_t oa = __shfl_xor_sync(0xFFFFFFFFu, arg64, off);
+				if (od > dc64 || (od == dc64 && oa < arg64))
+				{
+					dc64 = od;
+					arg64 = oa;
+				}
+				// the two largest FP32 depths of both lanes (a multiset: equal values both count)
+				const float om = __shfl_xor_sync(0xFFFFFFFFu, m32, off), os = __shfl_xor_sync(0xFFFFFFFFu, s32, off);
+				const uint32_t oa32 = __shfl_xor_sync(0xFFFFFFFFu, arg32, off);
+				if (om > m32 || (om == m32 && oa32 < arg32))
+				{
+					s32 = fmaxf(m32, os);
+					m32 = om;
+					arg32 = oa32;
+				}
+				else
+					s32 = fmaxf(s32, om);
+			}
+			if (lane != 0u)
+				return;
 			Fp64Out o;
 			o.j64 = area * dc64 * dc64;
 			o.dc64 = dc64;
@@ -3874,15 +3898,13 @@ static u26_status fp64_metrics(u26_scene* S, const float* d_x, u26_prp_output* o
 	}
 	if (in.empty())
 		return U26_OK;
-	DevBuf &d_in = S->d_f64in, &d_hits = S->d_f64hits, &d_delta = S->d_f64delta, &d_out = S->d_f64out;
+	DevBuf &d_in = S->d_f64in, &d_hits = S->d_f64hits, &d_out = S->d_f64out;
 	U26_TRY(upload(ctx, d_in, in));
 	U26_TRY(upload(ctx, d_hits, out->hits));
-	U26_CUDA(ctx, d_delta.reserve(sizeof(double) * out->hits.size()));
 	U26_CUDA(ctx, d_out.reserve(sizeof(Fp64Out) * in.size()));
 	const uint32_t nc = uint32_t(in.size());
 	fp64_metrics_kernel<<<div_up(nc * 32u, 128u), 128, 0, st>>>(nc, d_in.as<Fp64In>(), d_hits.as<u26_prp_hit>(), d_x, S->d_edges.as<uint2>(),
-		S->d_faces.as<uint32_t>(), S->d_varea.as<float>(), S->d_earea.as<float>(), S->d_farea.as<float>(), d_delta.as<double>(),
-		d_out.as<Fp64Out>());
+		S->d_faces.as<uint32_t>(), S->d_varea.as<float>(), S->d_earea.as<float>(), S->d_farea.as<float>(), d_out.as<Fp64Out>());
 	U26_TRY(after_launch(ctx, "fp64_metrics_kernel"));
 	std::vector<Fp64Out> res;
 	U26_TRY(download(ctx, res, d_out.ptr, in.size()));
