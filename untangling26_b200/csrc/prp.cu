@@ -918,7 +918,7 @@ namespace u26
 			RaySlab slab{};
 			bool ee_req = false; // an EE request: its swept-edge state is set up after the face walk
 			uint32_t ee_slot = 0;
-			float ee_pmax = 0.0f;
+			float ee_pmax = 0.0f, ee_pmin = 0.0f;
 			if (r < total)
 			{
 				// task of this request: last task with req_begin <= r
@@ -974,6 +974,7 @@ namespace u26
 					ee_req = true;
 					ee_slot = tk.slot1;
 					ee_pmax = tk.ee_pmax;
+					ee_pmin = tk.ee_pmin;
 				}
 			}
 
@@ -1081,7 +1082,7 @@ namespace u26
 			// rays' state is dead)
 			uint2 ev = make_uint2(0u, 0u);
 			f3 p0 = mk3(0.0f), e1 = mk3(0.0f), pn = mk3(0.0f), smn = mk3(0.0f), smx = mk3(0.0f);
-			float pd = 0.0f, ray_max = 0.0f;
+			float pd = 0.0f, ray_max = 0.0f, proj_lo = 0.0f, proj_hi = 0.0f;
 			bool plane = false;
 			if (ee_req)
 			{
@@ -1097,6 +1098,11 @@ namespace u26
 				}
 				if (ray_max > 0.0f)
 				{
+					// the swept edge's extent along dir (prp_compute_edge_projection_bounds with the
+					// target edges' lower bound, cached_bvh.cpp:377-473), widened by 1e-6
+					const float ep0 = dot(p0, dir), ep1 = dot(p1, dir);
+					proj_lo = fmaxf(fminf(ep0, ep1), ee_pmin - 1e-5f) - 1e-6f;
+					proj_hi = (fmaxf(ep0, ep1) + ray_max * dl2) + 1e-6f;
 					e1 = p1 - p0;
 					pn = cross(e1, dir);
 					const float nl = length(pn);
@@ -1145,12 +1151,19 @@ namespace u26
 					// rejects (cached_bvh.cpp:433-473 prunes its nodes the same way). The boxes carry
 					// the 1e-5 (1 + |c|) margin, far above the rounding of this test, so no edge the
 					// leaf test keeps is pruned.
-					if (hit && plane)
+					// and a box whose extent along dir misses the swept edge's holds no edge it reaches
+					if (hit)
 					{
 						const f3 c = mk3(0.5f * (g.mn.x + g.mx.x), 0.5f * (g.mn.y + g.mx.y), 0.5f * (g.mn.z + g.mx.z));
 						const f3 h = mk3(0.5f * (g.mx.x - g.mn.x), 0.5f * (g.mx.y - g.mn.y), 0.5f * (g.mx.z - g.mn.z));
-						const float rad = (h.x * fabsf(pn.x) + h.y * fabsf(pn.y)) + h.z * fabsf(pn.z);
-						hit = fabsf(dot(pn, c) - pd) <= rad + 1e-6f;
+						const float cp = dot(c, dir);
+						const float pr = (h.x * fabsf(dir.x) + h.y * fabsf(dir.y)) + h.z * fabsf(dir.z);
+						hit = !(cp + pr < proj_lo || cp - pr > proj_hi);
+						if (hit && plane)
+						{
+							const float rad = (h.x * fabsf(pn.x) + h.y * fabsf(pn.y)) + h.z * fabsf(pn.z);
+							hit = fabsf(dot(pn, c) - pd) <= rad + 1e-6f;
+						}
 					}
 					const uint32_t link_a = __float_as_uint(g.mn.w), link_b = __float_as_uint(g.mx.w);
 					bool descend = false;
