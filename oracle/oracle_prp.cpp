@@ -584,14 +584,27 @@ namespace
 		tmax = std::fmin(std::fmin(tmax, std::fmax(a[0], b[0])), std::fmin(std::fmax(a[1], b[1]), std::fmax(a[2], b[2])));
 		return tmin <= tmax;
 	}
-	// the swept edge's box against the target edge's grown box (one margin for all axes)
-	inline bool edge_gate(V3 smin, V3 smax, V3 q0, V3 q1)
+	// the batched form's leaf test of a target edge against a swept edge: the edge's grown box
+	// (one margin for all axes) against the swept box, the swept edge's extent along dir
+	// [proj_lo, proj_hi] and, with a plane, the slab |dot(pn, q) - pd| <= 1e-6
+	inline bool edge_gate(V3 smin, V3 smax, float proj_lo, float proj_hi, V3 dir, bool plane, V3 pn, float pd, V3 q0, V3 q1)
 	{
 		const V3 mn = vmin(q0, q1), mx = vmax(q0, q1);
 		const float e = 1e-5f * (1.0f + std::fmax(std::fmax(std::fmax(std::fabs(mn.x), std::fabs(mx.x)), std::fmax(std::fabs(mn.y), std::fabs(mx.y))),
 			std::fmax(std::fabs(mn.z), std::fabs(mx.z))));
-		return smin.x <= mx.x + e && smax.x >= mn.x - e && smin.y <= mx.y + e && smax.y >= mn.y - e && smin.z <= mx.z + e &&
-			smax.z >= mn.z - e;
+		const V3 gl = v3(mn.x - e, mn.y - e, mn.z - e), gh = v3(mx.x + e, mx.y + e, mx.z + e);
+		if (!(smin.x <= gh.x && smax.x >= gl.x && smin.y <= gh.y && smax.y >= gl.y && smin.z <= gh.z && smax.z >= gl.z))
+			return false;
+		const V3 c = v3(0.5f * (gl.x + gh.x), 0.5f * (gl.y + gh.y), 0.5f * (gl.z + gh.z));
+		const V3 h = v3(0.5f * (gh.x - gl.x), 0.5f * (gh.y - gl.y), 0.5f * (gh.z - gl.z));
+		const float cp = dot(c, dir);
+		const float pr = (h.x * std::fabs(dir.x) + h.y * std::fabs(dir.y)) + h.z * std::fabs(dir.z);
+		if (cp + pr < proj_lo || cp - pr > proj_hi)
+			return false;
+		if (!plane)
+			return true;
+		const float rad = (h.x * std::fabs(pn.x) + h.y * std::fabs(pn.y)) + h.z * std::fabs(pn.z);
+		return std::fabs(dot(pn, c) - pd) <= rad + 1e-6f;
 	}
 
 	// ray_cast_from_verts_batched for one request (BVH or brute force over the targets)
@@ -735,6 +748,9 @@ namespace
 		const EdgeRay r = make_edge_ray(m, q.eid, q.dir, ray_max);
 		const V3 sw_lo = vmin(vmin(r.p0, r.p1), vmin(r.p0 + q.dir * ray_max, r.p1 + q.dir * ray_max));
 		const V3 sw_hi = vmax(vmax(r.p0, r.p1), vmax(r.p0 + q.dir * ray_max, r.p1 + q.dir * ray_max));
+		const float g_ep0 = dot(r.p0, q.dir), g_ep1 = dot(r.p1, q.dir);
+		const float g_lo = std::fmax(std::fmin(g_ep0, g_ep1), q.target_proj_min - 1e-5f) - 1e-6f;
+		const float g_hi = (std::fmax(g_ep0, g_ep1) + ray_max * dot(q.dir, q.dir)) + 1e-6f;
 		auto leaf = [&](uint eid2)
 		{
 			tested++;
@@ -759,7 +775,7 @@ namespace
 			if (!hop_ok(q.hop, q.max_hop, { b0, b1 }) || a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1)
 				return;
 			const V3 q0 = load3(m.x, b0), q1 = load3(m.x, b1);
-			if (!edge_gate(sw_lo, sw_hi, q0, q1))
+			if (!edge_gate(sw_lo, sw_hi, g_lo, g_hi, q.dir, r.plane, r.pn, r.pd, q0, q1))
 				return;
 			Hit h;
 			rc->add(recheck_edge_edge(r.p0, r.p1, q.dir, ray_max, r.plane, r.pn, r.pd, q0, q1, edge_edge_test(m, r, q.eid, eid2, h)));
