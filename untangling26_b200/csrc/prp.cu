@@ -569,8 +569,8 @@ namespace u26
 		// position (edge midpoint), so that the 32 requests of a warp packet start from a
 		// compact patch. Only the request order changes: hits are keyed by primitive ids.
 		__global__ void cand_keys_kernel(const uint32_t* __restrict__ slot_ids, const uint32_t* __restrict__ off, uint32_t nsid,
-			const uint32_t* __restrict__ cand, uint32_t stride, const uint32_t* __restrict__ rank, uint64_t* __restrict__ keys,
-			uint32_t* __restrict__ vals)
+			const uint32_t* __restrict__ cand, uint32_t stride, const uint32_t* __restrict__ rank, int code_bits, int id_bits,
+			uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
 		{
 			const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
 			if (g >= off[nsid])
@@ -585,7 +585,9 @@ namespace u26
 					hi = mid;
 			}
 			const uint32_t id = cand[size_t(slot_ids[lo]) * stride + (g - off[lo])];
-			keys[g] = (uint64_t(lo) << 32) | rank[id];
+			// (slot, Morton code, id): unique keys, so the request order (and the packets) do not
+			// depend on the order the candidates were found in
+			keys[g] = (uint64_t(lo) << (code_bits + id_bits)) | (uint64_t(rank[id] >> (30 - code_bits)) << id_bits) | id;
 			vals[g] = id;
 		}
 		__global__ void cand_scatter_kernel(const uint32_t* __restrict__ slot_ids, const uint32_t* __restrict__ off, uint32_t nsid,
@@ -4259,10 +4261,14 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			U26_CUDA(ctx, S->d_cvals.reserve(sizeof(uint32_t) * total));
 			uint32_t* cand = kind == 0 ? S->d_cand_v.as<uint32_t>() : S->d_cand_e.as<uint32_t>();
 			const uint32_t stride = kind == 0 ? vs : es_;
+			const int id_bits = bits_for(kind == 0 ? S->nv : S->ne);
+			const int code_bits = std::max(0, std::min(30, 64 - sid_bits - id_bits));
 			cand_keys_kernel<<<div_up(total, 256), 256, 0, st>>>(S->d_slot_ids.as<uint32_t>(), S->d_cand_off.as<uint32_t>(), nsid, cand, stride,
-				kind == 0 ? S->d_vrank.as<uint32_t>() : S->d_erank.as<uint32_t>(), S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>());
+				kind == 0 ? S->d_vrank.as<uint32_t>() : S->d_erank.as<uint32_t>(), code_bits, id_bits, S->d_ckeys.as<uint64_t>(),
+				S->d_cvals.as<uint32_t>());
 			U26_TRY(after_launch(ctx, "cand_keys_kernel"));
-			U26_TRY(S->csorter.sort(ctx, S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>(), total, 0, 32 + sid_bits));
+			U26_TRY(S->csorter.sort(ctx, S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>(), total, 0,
+				std::min(64, sid_bits + code_bits + id_bits)));
 			cand_scatter_kernel<<<div_up(total, 256), 256, 0, st>>>(S->d_slot_ids.as<uint32_t>(), S->d_cand_off.as<uint32_t>(), nsid,
 				S->d_cvals.as<uint32_t>(), cand, stride);
 			U26_TRY(after_launch(ctx, "cand_scatter_kernel"));
