@@ -358,31 +358,95 @@ namespace u26
 			const uint32_t base = blockIdx.x * kRefitBlock;
 			const uint32_t cnt = min(kRefitBlock, n - base);
 			const uint32_t ni = n - 1;
-			s_cnt[threadIdx.x] = 0u;
-			if (base + threadIdx.x < ni)
+			const uint32_t t = threadIdx.x;
+			s_cnt[t] = 0u;
+			bool inner_local = false; // inner node base + t lies inside the block (its box is written below)
+			if (base + t < ni)
 			{
-				s_child[threadIdx.x] = __ldg(children + base + threadIdx.x);
-				s_parent[threadIdx.x] = __ldg(parent + base + threadIdx.x);
-				s_range[threadIdx.x] = __ldg(node_range + base + threadIdx.x);
+				s_child[t] = __ldg(children + base + t);
+				s_parent[t] = __ldg(parent + base + t);
+				const uint32_t r = __ldg(node_range + base + t);
+				s_range[t] = r;
+				inner_local = min(base + t, r) >= base && max(base + t, r) < base + cnt;
+			}
+			// phase 1: leaf boxes (into shared memory; written out in phase 3)
+			const uint32_t lid = base + t;
+			if (t < cnt)
+			{
+				f3 mn, mx;
+				if constexpr (FUSED)
+					leaf_box<TYPE>(x0, x1, thickness, prims, __ldg(sorted_get_original + lid), mn, mx);
+				else
+					load_box6_cg(boxes + ni + lid, mn, mx);
+				s_leaf[t] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
 			}
 			__syncthreads();
-			if (threadIdx.x >= cnt)
-				return;
-			const uint32_t lid = base + threadIdx.x;
-			f3 mn, mx;
-			if constexpr (FUSED)
-			{
-				leaf_box<TYPE>(x0, x1, thickness, prims, __ldg(sorted_get_original + lid), mn, mx);
-				__stcg(&boxes[ni + lid].mn, make_float4(mn.x, mn.y, mn.z, 0.0f));
-				__stcg(&boxes[ni + lid].mx, make_float4(mx.x, mx.y, mx.z, 1.0f));
-			}
-			else
-				load_box6_cg(boxes + ni + lid, mn, mx);
-			s_leaf[threadIdx.x] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
+			// phase 2: the climb through the nodes inside the block, in shared memory only (no device
+			// stores in flight, so the block-scope fences stay cheap). A thread that reaches a node
+			// crossing the block boundary keeps it as `pending` for phase 4.
 			constexpr uint32_t kMaxClimb = 100000u;
-			uint32_t node = __ldg(parent + ni + lid);
+			uint32_t pending = kInvalid;
+			if (t < cnt)
+			{
+				uint32_t node = __ldg(parent + ni + lid);
+				uint32_t steps = 0;
+				while (node != kInvalid)
+				{
+					if (++steps > kMaxClimb || node >= ni)
+					{
+						atomicExch(health, 0u);
+						node = kInvalid;
+						break;
+					}
+					const uint32_t k = node - base;
+					if (!(k < cnt && min(node, s_range[k]) >= base && max(node, s_range[k]) < base + cnt))
+					{
+						pending = node; // crosses the block boundary
+						break;
+					}
+					__threadfence_block(); // this thread's shared boxes before its arrival
+					if (atomicAdd(&s_cnt[k], 1u) == 0u)
+						break;
+					__threadfence_block();
+					const uint2 c = s_child[k];
+					// children of a node inside the block are inside it too (checked, not assumed)
+					const uint32_t ia = c.x >= ni ? c.x - ni - base : c.x - base, ib = c.y >= ni ? c.y - ni - base : c.y - base;
+					if (ia >= cnt || ib >= cnt)
+					{
+						atomicExch(health, 0u);
+						break;
+					}
+					const Box6 ba = c.x >= ni ? s_leaf[ia] : s_inner[ia];
+					const Box6 bb = c.y >= ni ? s_leaf[ib] : s_inner[ib];
+					s_inner[k] = Box6{ { fminf(ba.v[0], bb.v[0]), fminf(ba.v[1], bb.v[1]), fminf(ba.v[2], bb.v[2]), fmaxf(ba.v[3], bb.v[3]),
+						fmaxf(ba.v[4], bb.v[4]), fmaxf(ba.v[5], bb.v[5]) } };
+					node = s_parent[k];
+				}
+			}
+			__syncthreads();
+			// phase 3: the block's leaf boxes and local inner boxes, written out coalesced
+			if (t < cnt)
+			{
+				const Box6 l = s_leaf[t];
+				__stcg(&boxes[ni + lid].mn, make_float4(l.v[0], l.v[1], l.v[2], 0.0f));
+				__stcg(&boxes[ni + lid].mx, make_float4(l.v[3], l.v[4], l.v[5], 1.0f));
+			}
+			if (inner_local)
+			{
+				const Box6 b = s_inner[t];
+				__stcg(&boxes[base + t].mn, make_float4(b.v[0], b.v[1], b.v[2], 0.0f));
+				__stcg(&boxes[base + t].mx, make_float4(b.v[3], b.v[4], b.v[5], 1.0f));
+			}
+			__syncthreads();
+			if (pending == kInvalid)
+				return;
+			// phase 4: nodes crossing block boundaries, through device counters that gain 2 per refit
+			// (an even value before the increment marks the first arrival). The acq_rel arrival
+			// releases the block's boxes written above (ordered before it by the barrier) and the
+			// second arrival acquires the sibling's.
+			__threadfence(); // the block's phase 3 stores, ordered by the barrier, before the release below
+			uint32_t node = pending;
 			uint32_t steps = 0;
-			bool local = true;
 			while (node != kInvalid)
 			{
 				if (++steps > kMaxClimb || node >= ni)
@@ -390,59 +454,18 @@ namespace u26
 					atomicExch(health, 0u);
 					return;
 				}
-				// node in this block's id range (its topology is in shared memory)
-				const bool here = node - base < cnt;
-				if (local)
-				{
-					const uint32_t r = here ? s_range[node - base] : __ldg(node_range + node);
-					local = min(node, r) >= base && max(node, r) < base + cnt;
-				}
-				if (local)
-				{
-					__threadfence_block(); // this thread's box writes before its arrival
-					if (atomicAdd(&s_cnt[node - base], 1u) == 0u)
-						return;
-					__threadfence_block();
-				}
-				else
-				{
-					// acq_rel arrival: releases this thread's boxes below the node, and the second
-					// arrival acquires its sibling's
-					const uint32_t arrived = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(flags[node]).fetch_add(1u,
-						cuda::memory_order_acq_rel);
-					if ((arrived & 1u) == 0u)
-						return;
-				}
-				const uint2 c = here ? s_child[node - base] : __ldg(children + node);
+				const uint32_t arrived = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(flags[node]).fetch_add(1u,
+					cuda::memory_order_acq_rel);
+				if ((arrived & 1u) == 0u)
+					return;
+				const uint2 c = __ldg(children + node);
 				f3 amn, amx, bmn, bmx;
-				if (local)
-				{
-					// children of a node inside the block are inside it too (checked, not assumed)
-					const uint32_t ia = c.x >= ni ? c.x - ni - base : c.x - base, ib = c.y >= ni ? c.y - ni - base : c.y - base;
-					if (ia >= cnt || ib >= cnt)
-					{
-						atomicExch(health, 0u);
-						return;
-					}
-					const Box6 a = c.x >= ni ? s_leaf[ia] : s_inner[ia];
-					const Box6 b = c.y >= ni ? s_leaf[ib] : s_inner[ib];
-					amn = mk3(a.v[0], a.v[1], a.v[2]);
-					amx = mk3(a.v[3], a.v[4], a.v[5]);
-					bmn = mk3(b.v[0], b.v[1], b.v[2]);
-					bmx = mk3(b.v[3], b.v[4], b.v[5]);
-				}
-				else
-				{
-					load_box6_cg(boxes + c.x, amn, amx);
-					load_box6_cg(boxes + c.y, bmn, bmx);
-				}
-				mn = vmin(amn, bmn);
-				mx = vmax(amx, bmx);
+				load_box6_cg(boxes + c.x, amn, amx);
+				load_box6_cg(boxes + c.y, bmn, bmx);
+				const f3 mn = vmin(amn, bmn), mx = vmax(amx, bmx);
 				__stcg(&boxes[node].mn, make_float4(mn.x, mn.y, mn.z, 0.0f));
 				__stcg(&boxes[node].mx, make_float4(mx.x, mx.y, mx.z, 1.0f));
-				if (local)
-					s_inner[node - base] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
-				node = here ? s_parent[node - base] : __ldg(parent + node);
+				node = __ldg(parent + node);
 			}
 		}
 
