@@ -149,6 +149,8 @@ class Workload:
         self.batch = name.startswith("batch")
         self.repair = False
         self.params = dict(max_contours=ALL_CONTOURS, batch_size=ALL_CONTOURS)
+        # single-mesh workloads: the contours the CPU legs evaluate (None: every 8th)
+        self.oracle_contours = None
         if name == "batch64":
             self.full = synthetic.batch_scenes(64, seed=2)
             self.timed_ids = list(range(0, 64, TIMED_STRIDE))
@@ -189,6 +191,9 @@ class Workload:
             self.timed_ids = None
             self.params = dict(max_contours=256, batch_size=32)
             self.repair = True
+            # the oracle needs 3-30 s for most contours of this mesh and minutes for the largest
+            # regions (contour 0): the CPU legs evaluate contours 1 and 3
+            self.oracle_contours = (1, 3)
             self.config = {"workload": "layered_sheets_5x512x512", "seed": 4, "layers": 5, "triangles": int(self.full.num_faces),
                            "spacing_mm": 1, "displacement_mm": "U[2, 20] multi-octave", "directions": "reference seeds (<=10)",
                            "opt_iterations": 0, "contours": "first 256 of each pass", "update": "response step, scale 1"}
@@ -246,6 +251,11 @@ def reference_arm(args, wl):
         warm = lambda: oracle_pass(scenes[smallest], wl.params)
         sample = (f"the {len(scenes)} timed scenes ({wl.config['timed_scenes']}), each a full pass (EF detection, every "
                   f"contour, response), split over the {args.steps} steps: one pass over the timed workload")
+    elif wl.oracle_contours:
+        cs = wl.oracle_contours
+        step = lambda i: [oracle_pass(wl.full, wl.params, stride=1 << 20, offset=cs[i % len(cs)])[1:]]
+        warm = lambda: None
+        sample = f"EF detection and one of the contours {list(cs)} each step (step i: contour {list(cs)}[i % {len(cs)}])"
     else:
         stride = max(args.steps, 1)
         step = lambda i: [oracle_pass(wl.full, wl.params, stride=stride, offset=i)[1:]]
@@ -287,6 +297,14 @@ def cpu_baseline_and_parity(wl, res, tmesh):
             ncont += c
             nhits += h
         sample = f"the {len(ids)} timed scenes, one full pass each (every contour, response)"
+    elif wl.oracle_contours:
+        for c in wl.oracle_contours:
+            run, t, s = oracle_pass(wl.full, wl.params, stride=1 << 20, offset=c)
+            tests += t
+            sec += s
+            nhits += compare_contours(res, run, [c])
+            ncont += 1
+        sample = f"EF detection and one contour, for each of the contours {list(wl.oracle_contours)} of the timed pass"
     else:
         stride = 8
         run, t, s = oracle_pass(wl.full, wl.params, stride=stride)
@@ -379,6 +397,28 @@ def _traffic(kernel, workload):
         return json.load(f).get(kernel, {}).get(workload)
 
 
+def profile_pass(args, wl):
+    """The pass an ncu capture measures: the bench's warm-up passes (the autotuner runs in the
+    first unless --raycast-config fixes the configuration), then one pass of the timed workload
+    between cudaProfilerStart and cudaProfilerStop."""
+    import torch
+    from untangling26_b200 import Context
+    ctx = Context(0)
+    runner = PassRunner(ctx, wl.timed_mesh(), wl.params)
+    for _ in range(max(args.warmup, 1)):
+        runner.run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    res = runner.run()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_pass": args.workload, "leaf_tests": res.tested, "requests": res.requests, "contours": len(res.contours),
+                      "raycast_config": {k: res.raycast_config[k] for k in ("parts", "blocks_per_sm", "queue")},
+                      "gpu_ms": {k: round(v, 3) for k, v in res.gpu_ms.items()}}))
+    runner.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -388,11 +428,25 @@ def main():
     ap.add_argument("--workload", default="batch64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-full-batch", action="store_true", help="skip the whole-batch chosen / plain timing")
+    ap.add_argument("--raycast-config", default=None,
+                    help="a fixed traversal configuration ('4x7', '8x7q', ...) instead of the autotuner's choice")
+    ap.add_argument("--profile-pass", action="store_true",
+                    help="for ncu (--profile-from-start off): warm-up passes, then one pass of the timed workload "
+                         "inside cudaProfilerStart / Stop; prints one line and exits")
     args = ap.parse_args()
     ws, rank, local = _dist_env()
     wl = Workload(args.workload)
+    if args.raycast_config:
+        from untangling26_b200.prp import RAYCAST_CONFIGS, config_name
+        names = [config_name(c) for c in RAYCAST_CONFIGS]
+        if args.raycast_config not in names:
+            raise SystemExit(f"--raycast-config must be one of {names}")
+        wl.params = dict(wl.params, autotune=0, raycast_config=names.index(args.raycast_config) + 1)
+        wl.config["raycast_config"] = f"fixed {args.raycast_config}"
     if args.impl == "reference":
         return reference_arm(args, wl)
+    if args.profile_pass:
+        return profile_pass(args, wl)
 
     import torch
     import torch.distributed as dist
@@ -493,6 +547,11 @@ def main():
                          "unit": "warp inst/s", "frac": tr["warp_inst"] / (rc_ms / 1e3) / issue_peak,
                          "peak_basis": f"148 SMs x 4 schedulers x {mhz:.0f} MHz (sampled median)"}
         roof["traffic_source"] = tr.get("source")
+        # the capture's traversal configuration against this run's (the DRAM bytes and
+        # instructions of a pass depend a little on it)
+        from untangling26_b200.prp import config_name
+        mine = config_name((r0.raycast_config["parts"], r0.raycast_config["blocks_per_sm"], r0.raycast_config["queue"]))
+        roof["traffic_config"] = {"captured": tr.get("raycast_config"), "this_run": mine, "same": tr.get("raycast_config") == mine}
     roof["packet_record_bytes_per_pass"] = 32 * r0.node_fetches + 48 * r0.tri_fetches + 32 * r0.edge_fetches + 24 * r0.requests
 
     # ---- LBVH refit alone (fused leaf update + bottom-up refit of a face tree), L2 flushed

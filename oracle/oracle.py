@@ -428,6 +428,50 @@ def canonical_ef(pairs, indices):
     return pairs[order], indices[order]
 
 
+def response_step(pairs, x, scale=1.0):
+    """The repair loop's position update: a fixed step along the assembled response pairs,
+    restating u26_response_step (a library-defined update that stands in for the solver step
+    of the reference's IP loop). Each pair with k2 > 0 asks its sides apart by
+    Delta = -k1 / k2 along its normal: the first primitive (VF vertex, first EE edge) takes
+    +Delta / 2 n, the second -Delta / 2 n, per vertex weighted by the template's barycentric
+    weights (weights <= 0 are skipped). Sums are 2^-40 m / 2^-32 fixed point (round half to
+    even), each moved vertex takes scale x sum(w d) / sum(w) in FP64, rounded to FP32.
+    Returns (new positions [V, 3] float32, vertices moved)."""
+    tb = np.uint32(0x80000000)
+    p = np.ascontiguousarray(pairs)
+    x = np.asarray(x, np.float32).reshape(-1, 3)
+    nv = len(x)
+    k1, k2 = p["vec2"][:, 0], p["vec2"][:, 1]
+    p = p[(k2 > 0) & np.isfinite(k1)]
+    idx = p["indices"]
+    delta = (-p["vec2"][:, 0]) / p["vec2"][:, 1]
+    half = p["vec1"][:, :3] * (np.float32(0.5) * delta)[:, None]
+    one = np.float32(1.0)
+    vf = (idx[:, 2] & tb) != 0
+    ee = ~vf & ((idx[:, 3] & tb) != 0)
+    b0, b1 = p["vec2"][:, 2], p["vec2"][:, 3]
+    terms = []  # (vertex ids, +-half, weights) per template slot
+    terms += [(idx[vf, 0], half[vf], np.ones(int(vf.sum()), np.float32)), (idx[vf, 1], -half[vf], b0[vf]),
+              (idx[vf, 2] & ~tb, -half[vf], b1[vf]), (idx[vf, 3], -half[vf], (one - b0[vf]) - b1[vf])]
+    terms += [(idx[ee, 0], half[ee], b0[ee]), (idx[ee, 1], half[ee], one - b0[ee]), (idx[ee, 2], -half[ee], b1[ee]),
+              (idx[ee, 3] & ~tb, -half[ee], one - b1[ee])]
+    acc = np.zeros((nv, 4), np.int64)
+    for v, d, w in terms:
+        keep = (v < nv) & (w > 0)
+        v, d, w = v[keep].astype(np.int64), d[keep], w[keep]
+        fx = np.rint((d * w[:, None]).astype(np.float64) * 2.0 ** 40).astype(np.int64)
+        fw = np.rint(w.astype(np.float64) * 2.0 ** 32).astype(np.int64)
+        for c in range(3):
+            np.add.at(acc[:, c], v, fx[:, c])
+        np.add.at(acc[:, 3], v, fw)
+    moved = acc[:, 3] > 0
+    out = x.copy()
+    inv = 2.0 ** 32 / acc[moved, 3].astype(np.float64) / 2.0 ** 40
+    s = np.float64(np.float32(scale))
+    out[moved] = (x[moved].astype(np.float64) + s * (acc[moved, :3].astype(np.float64) * inv[:, None])).astype(np.float32)
+    return out, int(moved.sum())
+
+
 def filter_broad_phase(vf, ee, num_ef, invalid, regions, faces, edges):
     """IntersectionResolver::filter_broad_phase_pairs; returns flagged copies of the lists."""
     L = lib()

@@ -96,3 +96,45 @@ def test_response_rules_two_sheets(oracle):
     frows = _check_rows_sorted(ref.face_regions, m.num_faces)
     for f, r in enumerate(frows):
         assert set(r.tolist()) == set().union(*(vr[int(v)] for v in m.faces[f]))
+
+
+def _pair(idx, n, k1, k2, a, b):
+    p = np.zeros(1, oracle_dtype())
+    p["indices"][0] = idx
+    p["vec1"][0, :3] = n
+    p["vec2"][0] = (k1, k2, a, b)
+    return p
+
+
+def oracle_dtype():
+    from oracle.oracle import COLLISION_PAIR_DTYPE
+    return COLLISION_PAIR_DTYPE
+
+
+def test_response_step_rules(oracle):
+    """The repair loop's step: a VF pair moves its vertex by +Delta/2 n and its face's vertices by
+    -Delta/2 n (Delta = -k1 / k2); vertices shared by several pairs take the weighted mean;
+    pairs with k2 <= 0 or weights <= 0 move nothing."""
+    tb = 0x80000000
+    x = np.zeros((6, 3), np.float32)
+    vf = _pair([0, 1, 2 | tb, 3], [0, 0, 1], -4e-3, 1.0, 0.5, 0.25)  # Delta = 4e-3
+    out, moved = oracle.response_step(vf, x)
+    assert moved == 4
+    assert np.allclose(out[0], [0, 0, 2e-3]) and np.allclose(out[1:4], [[0, 0, -2e-3]] * 3)
+    assert not out[4:].any()
+    # an EE pair with edge parameter 1 on its first edge: its second vertex has weight 0
+    ee = _pair([4, 5, 1, 3 | tb], [1, 0, 0], -2e-3, 1.0, 1.0, 0.5)
+    out, moved = oracle.response_step(np.concatenate([vf, ee]), x)
+    assert moved == 5  # vertex 5 has weight 0
+    assert np.allclose(out[4], [1e-3, 0, 0])
+    # vertex 1: -2e-3 z (VF, weight 0.5) and -1e-3 x (EE, weight 0.5): the mean of the two
+    assert np.allclose(out[1], [-0.5e-3, 0, -1e-3])
+    dead = _pair([0, 1, 2 | tb, 3], [0, 0, 1], -4e-3, 0.0, 0.5, 0.25)
+    out, moved = oracle.response_step(dead, x)
+    assert moved == 0 and not out.any()
+    # scale multiplies the step; the fixed-point sums do not depend on the pairs' order
+    both = np.concatenate([vf, ee])
+    a, _ = oracle.response_step(both, x + 0.1, 0.5)
+    b, _ = oracle.response_step(both[::-1].copy(), x + 0.1, 0.5)
+    assert a.tobytes() == b.tobytes()
+    assert np.allclose(a[4], [0.1 + 0.5e-3, 0.1, 0.1])
