@@ -317,7 +317,12 @@ def cpu_baseline_and_parity(wl, res, tmesh):
            "pass_seconds": sec if wl.batch else None}
     parity = {"ok": True, "contours_compared": ncont, "hits_compared": nhits,
               "fields": "every per-contour result field, candidate directions, support hits (bytes)",
-              "against": "oracle (CPU restatement of the reference)"}
+              "against": "oracle (CPU restatement of the reference)",
+              # executed leaf tests of the same work: the oracle's CachedBVH (8 primitives per leaf,
+              # rays from the object root) and this pass's per-object LBVHs
+              "oracle_leaf_tests": int(tests)}
+    if not wl.batch and wl.oracle_contours is None:
+        parity["oracle_leaf_tests_note"] = "EF detection and the sampled contours only"
     return cpu, parity
 
 

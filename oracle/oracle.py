@@ -263,10 +263,13 @@ assert RESULT_DTYPE.itemsize == 144 and HIT_DTYPE.itemsize == 48
 class PrpRun:
     """All outputs of one oracle PRP pass."""
 
-    def __init__(self, mesh, ef_pairs, ef_indices, params=None, x=None, response=None):
+    def __init__(self, mesh, ef_pairs, ef_indices, params=None, x=None, response=None, order_spread=0):
         """response: (depth_threshold, stiffness) to also assemble the response pairs and the
         vertex / edge / face region CSRs (attributes response_pairs, response_info,
-        vert_regions, edge_regions, face_regions)."""
+        vert_regions, edge_regions, face_regions). order_spread = k > 0: per contour, the largest
+        relative difference of the selected support's FP32 area, volume, cost and J between the
+        canonical summation order and the reference's block reduce over the hits in key order
+        and k seeded shuffles (attribute order_spread)."""
         L = lib()
         L.oracle_prp_run.restype = ctypes.c_void_p
         for n in ("oracle_prp_num_pairs", "oracle_prp_num_orig_pairs", "oracle_prp_num_contours", "oracle_prp_contour",
@@ -327,6 +330,12 @@ class PrpRun:
                 d32 = self.results["depth"].astype(np.float64)
                 jerr = np.abs(j32 - f64[:nc, 0]) / f64[:nc, 0]
                 derr = np.abs(d32 - f64[:nc, 1]) / f64[:nc, 1]
+            self.order_spread = None
+            if order_spread:
+                self.order_spread = np.zeros(max(nc, 1), np.float64)
+                L.oracle_prp_order_spread(h, ctypes.c_uint32(order_spread), ctypes.c_uint32(1),
+                                          self.order_spread.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+                self.order_spread = self.order_spread[:nc]
             self.fp64 = {"rechecks": int(rc[0]), "flips": int(rc[1]), "dc_tie_rechecks": int(f64[:nc, 3].sum()),
                          "dc_tie_flips": int(f64[:nc, 4].sum()),
                          "delta_rel_err": float(f64[:nc, 2].max()) if nc else 0.0,

@@ -26,8 +26,9 @@
 //  * Sums over a hit list (J, volume, area, displacement cost) run over the hits in
 //    canonical order (type, source id, target id) with a fixed 32-lane strided partial
 //    sum and xor-butterfly combine, the reduction order of the CUDA metrics kernel.
-//    The reference reduces in its own (BVH-dependent) hit order; its sets are what
-//    parity pins, its float sums agree to rounding.
+//    The reference reduces in its own (BVH-dependent) hit order with its block reduce
+//    (reference_block_sum below); its sets are what parity pins, and oracle_prp_order_spread
+//    measures how far the two orders' FP32 sums lie apart on a given support.
 //  * Solid-interior hit links (intersection_resolver2.cpp:3298-3464) apply only to rigid
 //    or tetrahedral meshes; the scenes here are cloth, so they never fire and are not
 //    restated.
@@ -35,6 +36,7 @@
 #include <memory>
 #include <mutex>
 #include <queue>
+#include <random>
 #include <set>
 #include <string>
 
@@ -1764,6 +1766,35 @@ namespace
 			{ return cs[i]; });
 	}
 
+	// The reference's deterministic parallel reduce (CpuParallel::parallel_for_and_reduce,
+	// Solver/Utils/cpu_parallel.h:505-538, fiber backend) as a sum: blocks of 256 terms in index
+	// order, each summed sequentially from zero, then the block sums combined by std::reduce,
+	// restated with the GNU C++ library's order for random-access ranges (two pair sums folded
+	// into the running value four blocks at a time, the remaining blocks one by one).
+	template <typename F>
+	float reference_block_sum(uint n, F&& val)
+	{
+		const uint nb = (n + 255u) / 256u;
+		std::vector<float> b(nb, 0.0f);
+		for (uint k = 0; k < nb; k++)
+		{
+			float v = 0.0f;
+			for (uint i = 256u * k; i < std::min(n, 256u * k + 256u); i++)
+				v = v + val(i);
+			b[k] = v;
+		}
+		float acc = 0.0f;
+		uint i = 0;
+		for (; i + 4 <= nb; i += 4)
+		{
+			const float v1 = b[i] + b[i + 1], v2 = b[i + 2] + b[i + 3];
+			acc = acc + (v1 + v2);
+		}
+		for (; i < nb; i++)
+			acc = acc + b[i];
+		return acc;
+	}
+
 	struct PenMetrics
 	{
 		float depth = 0, volume = 0, area = 0, objective = 0, cost = 0;
@@ -1773,7 +1804,9 @@ namespace
 	// A = rest area of the source primitive, alpha = |n_src . r|, delta = dist; depth = max
 	// delta, volume = sum A alpha delta, J = (sum A) depth^2, displacement cost = sum
 	// (delta + 3e-3)^2 / kappa_h. Sums in the canonical 32-lane strided order.
-	PenMetrics penetration_metrics(const MeshIn& m, const V3* vn, const V3* en, const V3* fn, V3 dir, const std::vector<Hit>& hits)
+	// reference_order: the sums in the reference's block-reduce order over the hits as given
+	PenMetrics penetration_metrics(const MeshIn& m, const V3* vn, const V3* en, const V3* fn, V3 dir, const std::vector<Hit>& hits,
+		bool reference_order = false)
 	{
 		struct HitsRef
 		{
@@ -1820,11 +1853,13 @@ namespace
 		float depth = 0.0f;
 		for (const Hit& h : c.hits)
 			depth = std::fmax(depth, h.dist);
-		const float area = chunked_sum(n, [&](uint i)
+		auto sum = [&](auto&& term)
+		{ return reference_order ? reference_block_sum(n, term) : chunked_sum(n, term); };
+		const float area = sum([&](uint i)
 			{ float a, al; area_alpha(c.hits[i], a, al); return a; });
-		const float volume = chunked_sum(n, [&](uint i)
+		const float volume = sum([&](uint i)
 			{ float a, al; area_alpha(c.hits[i], a, al); return (a * al) * c.hits[i].dist; });
-		const float kappa = chunked_sum(n, [&](uint i)
+		const float kappa = sum([&](uint i)
 			{
 				const float sd = c.hits[i].dist + 3e-3f;
 				const float e = eff_inv(c.hits[i]);
@@ -3062,6 +3097,39 @@ extern "C"
 			o[2] = derr;
 			o[3] = tie ? 1.0 : 0.0;
 			o[4] = (tie && arg64 != arg32) ? 1.0 : 0.0;
+		}
+	}
+	// Summation-order sensitivity of the selected supports' FP32 metrics: per contour with a
+	// response, out[c] = the largest relative difference of area, volume, displacement cost and
+	// J between the canonical order (the kernels' and this oracle's) and the reference's block
+	// reduce over the hits in key order and in `nperm` seeded shuffles (the reference's hit order
+	// at that point follows its ray-casting output); 0 elsewhere.
+	void oracle_prp_order_spread(void* h, uint nperm, uint seed, double* out)
+	{
+		Scene* S = static_cast<Scene*>(h);
+		auto rel = [](float a, float b)
+		{ return a == b ? 0.0 : std::fabs(double(a) - double(b)) / std::fmax(std::fabs(double(a)), 1e-30); };
+		for (uint c = 0; c < uint(S->selected.size()); c++)
+		{
+			out[c] = 0.0;
+			const ComboInfo& ci = S->selected[c];
+			if (!ci.present || ci.hits.empty())
+				continue;
+			std::vector<Hit> hs = ci.hits;
+			std::sort(hs.begin(), hs.end(), [](const Hit& a, const Hit& b)
+				{ return a.key() < b.key(); });
+			const PenMetrics base = penetration_metrics(S->m, S->vn.data(), S->en.data(), S->fn.data(), ci.dir, hs);
+			std::mt19937 rng(seed + c);
+			double worst = 0.0;
+			for (uint k = 0; k <= nperm; k++)
+			{
+				if (k > 0)
+					std::shuffle(hs.begin(), hs.end(), rng);
+				const PenMetrics r = penetration_metrics(S->m, S->vn.data(), S->en.data(), S->fn.data(), ci.dir, hs, true);
+				worst = std::fmax(worst, std::fmax(std::fmax(rel(base.area, r.area), rel(base.volume, r.volume)),
+											 std::fmax(rel(base.cost, r.cost), rel(base.objective, r.objective))));
+			}
+			out[c] = worst;
 		}
 	}
 	// response pairs and region CSRs of a finished run; returns the pair count. Any output
