@@ -541,6 +541,7 @@ def main():
     rc_ms = r0.gpu_ms["raycast"]
     tr = _traffic("raycast_kernel", args.workload)
     roof = {"bound": "hbm", "kernel": "raycast_kernel", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+            "limiter": "instruction issue (see issue.frac): the tree and mesh are served from L1 / L2",
             "kernel_ms_per_pass": rc_ms, "traffic": None, "achieved": None, "frac": None}
     if tr:
         roof["traffic"] = tr["dram_bytes"]
