@@ -189,14 +189,18 @@ class Workload:
             # along its assembled response (the repair loop), so the K steps are K passes of it
             self.full = synthetic.layered_sheets(512, layers=5, seed=4)
             self.timed_ids = None
-            self.params = dict(max_contours=256, batch_size=32)
+            # one batch of 32 contours per pass: the 199 contours of the first pass grow to whole
+            # sheets (4.9 G requests, 75 s per pass); the traversal configuration is the batch
+            # workload's tuned one (tuning here would run 18 full ray-casting passes)
+            self.params = dict(max_contours=32, batch_size=32, autotune=0, raycast_config=2)
             self.repair = True
             # the oracle needs 3-30 s for most contours of this mesh and minutes for the largest
             # regions (contour 0): the CPU legs evaluate contours 1 and 3
             self.oracle_contours = (1, 3)
             self.config = {"workload": "layered_sheets_5x512x512", "seed": 4, "layers": 5, "triangles": int(self.full.num_faces),
                            "spacing_mm": 1, "displacement_mm": "U[2, 20] multi-octave", "directions": "reference seeds (<=10)",
-                           "opt_iterations": 0, "contours": "first 256 of each pass", "update": "response step, scale 1"}
+                           "opt_iterations": 0, "contours": "first 32 of each pass (one batch)", "update": "response step, scale 1",
+                           "raycast_config": "fixed 4x7"}
         else:
             raise SystemExit(f"unknown workload {name}")
         self.config["l2"] = "flushed between steps (256 MB write)"
@@ -424,6 +428,28 @@ def profile_pass(args, wl):
     ctx.close()
 
 
+def profile_refit(args, wl):
+    """The refit an ncu capture measures: --warmup refits of the workload's timed mesh's face
+    tree, then one between cudaProfilerStart and cudaProfilerStop."""
+    import torch
+    from untangling26_b200 import Context
+    from untangling26_b200.intersection_resolver import CollisionScene
+    ctx = Context(0)
+    mesh = wl.timed_mesh()
+    sc = CollisionScene(ctx, mesh, d_hat=1e-3, thickness=0.0, max_broad_pairs=1, max_ef_pairs=1)
+    sc.construct_lbvh()
+    for _ in range(max(args.warmup, 1)):
+        sc.refit_face_tree()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    sc.refit_face_tree()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_refit": args.workload, "triangles": int(mesh.num_faces)}))
+    sc.close()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -438,6 +464,9 @@ def main():
     ap.add_argument("--profile-pass", action="store_true",
                     help="for ncu (--profile-from-start off): warm-up passes, then one pass of the timed workload "
                          "inside cudaProfilerStart / Stop; prints one line and exits")
+    ap.add_argument("--profile-refit", action="store_true",
+                    help="for ncu (--profile-from-start off): the face-tree refit (fused leaf update) of the timed mesh, "
+                         "--warmup refits, then one inside cudaProfilerStart / Stop; prints one line and exits")
     args = ap.parse_args()
     ws, rank, local = _dist_env()
     wl = Workload(args.workload)
@@ -452,6 +481,8 @@ def main():
         return reference_arm(args, wl)
     if args.profile_pass:
         return profile_pass(args, wl)
+    if args.profile_refit:
+        return profile_refit(args, wl)
 
     import torch
     import torch.distributed as dist
