@@ -1,9 +1,10 @@
 """The scale form at full size: five stacked 512 x 512 sheets (2.6 M triangles, nested
 contours through several neighbours), two passes of the repair loop.
 
-* pass 1: the GPU's EF list and every contour equal the oracle's; contours 1 and 3 (the
-  oracle needs 3-30 s per contour of this mesh, up to minutes for the largest regions) are
-  compared field by field, direction by direction and hit by hit;
+* pass 1 (all 199 contours, up to 10^9 ray requests in one level): the GPU's EF list and
+  every contour equal the oracle's; contours 1, 3 and 5 (the oracle needs 3-30 s per contour
+  of this mesh, up to minutes for the largest regions) are compared field by field, direction
+  by direction and hit by hit;
 * the fixed step along the GPU's assembled response (u26_response_step) gives the positions
   the oracle's restatement of the step gives, bit for bit;
 * pass 2 on the stepped positions: the GPU's EF list equals the oracle's again (the
@@ -34,13 +35,16 @@ def test_layered_repair_two_passes(oracle, u26ctx):
         assert res.device_error_flags == 0
         ef, idx = oracle.detect_ef(m)
         assert len(ef) > 10000
-        for off in (1, 3):
+        nh = 0
+        for off in (1, 3, 5):
             ref = oracle.PrpRun(m, ef, idx, oracle.prp_params(contour_stride=256, contour_offset=off, **PARAMS))
             if off == 1:
                 assert res.pairs.tobytes() == ref.pairs.tobytes()
                 assert len(res.contours) == len(ref.contours) > 100
                 assert all(np.array_equal(a, b) for a, b in zip(res.contours, ref.contours))
-            assert compare_contours(res, ref, [off]) > 0
+            # a contour suppressed in the whole pass is compared on its pre-suppression fields
+            nh += compare_contours(res, ref, [off])
+        assert nh > 0
         # the step along the GPU's response, restated on the CPU
         want, moved = oracle.response_step(res.response.host_pairs(), m.x, 1.0)
         assert sc.response_step(res.response, 1.0) == moved > 0

@@ -892,7 +892,8 @@ namespace u26
 			// QUEUE (persistent form): every warp takes work items from a device counter until none is
 			// left, so no warp idles while the other warps of its block finish; otherwise the grid
 			// has one warp per item
-			uint32_t wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+			// warp index from the block index (a level's grid can exceed 2^32 threads: requests x parts)
+			uint32_t wi = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 			for (;;)
 			{
 			if constexpr (QUEUE)
@@ -4283,6 +4284,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	{
 		auto tl = std::chrono::steady_clock::now();
 		uint32_t total_req = 0;
+		uint64_t total_req64 = 0;
 		for (Task& t : tasks)
 		{
 			const uint32_t v0 = counts[3 * t.slot0], e0 = counts[3 * t.slot0 + 1], f0 = counts[3 * t.slot0 + 2];
@@ -4291,7 +4293,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			t.n_ee = e1 ? e0 : 0;
 			t.n_fv = f0 ? v1 : 0;
 			t.req_begin = total_req;
-			total_req += t.n_vf + t.n_ee + t.n_fv;
+			total_req64 += uint64_t(t.n_vf) + t.n_ee + t.n_fv;
+			// request ids are 32-bit (and a launch's work items stay below 2^31)
+			if (total_req64 >= (uint64_t(1) << 31))
+				return set_error(ctx, U26_ERR_CAPACITY, "PRP level needs %llu ray requests (limit 2^31): lower max_contours",
+					(unsigned long long)total_req64);
+			total_req = uint32_t(total_req64);
 			if (!hits_out)
 				alg_tests += uint64_t(t.n_vf) * f1 + uint64_t(t.n_ee) * e1 + uint64_t(t.n_fv) * f0;
 		}
