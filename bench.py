@@ -379,9 +379,10 @@ def _timed_passes(runner, steps, flush, stream, repair=False):
 
 def refit_rate(sc, mesh, flush, stream, peak, n=10):
     """Median time of the fused leaf update + refit of the scene's face tree over n launches
-    (L2 flushed before each). Algorithmic bytes, each once: V x (12 B position + 4 B
-    thickness) + F x (12 B face + 4 B leaf order + 32 B leaf box written) + (F - 1) x
-    (8 B children + 4 B parent + 4 B range + 64 B child boxes read + 32 B box written)."""
+    (L2 flushed before each). Algorithmic bytes, each once (the refit's byte count with
+    positions read once, x_start = x_end): V x (12 B position + 4 B thickness) + F x (12 B face
+    + 4 B leaf order + 32 B leaf box written) + (F - 1) x (8 B children + 4 B parent + 64 B
+    child boxes read + 32 B box written)."""
     import torch
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n + 2)]
     for i, (a, b) in enumerate(ev):
@@ -391,8 +392,8 @@ def refit_rate(sc, mesh, flush, stream, peak, n=10):
         b.record(stream)
     torch.cuda.synchronize()
     ms = statistics.median(a.elapsed_time(b) for a, b in ev[2:])
-    byts = 16 * mesh.num_verts + 48 * mesh.num_faces + 112 * max(mesh.num_faces - 1, 0)
-    out = {"kernel": "refit_block_kernel", "triangles": int(mesh.num_faces), "ms": ms, "algorithmic_bytes": byts,
+    byts = 16 * mesh.num_verts + 48 * mesh.num_faces + 108 * max(mesh.num_faces - 1, 0)
+    out = {"kernel": "refit_chunk_kernel + refit_top_kernel", "triangles": int(mesh.num_faces), "ms": ms, "algorithmic_bytes": byts,
            "achieved": byts / (ms / 1e3) / 1e9, "unit": "GB/s", "peak": peak}
     out["frac"] = out["achieved"] / peak
     return out

@@ -97,7 +97,13 @@ U26_API u26_status u26_lbvh_update_leaves(u26_lbvh* tree, const float* thickness
 	const float* x_end, const uint32_t* prims);
 /* LBVH::refit (lbvh.cpp:1087-1092): bottom-up union of the leaf AABBs. */
 U26_API u26_status u26_lbvh_refit(u26_lbvh* tree);
-/* Fused leaf update + refit in one launch (same result as the two calls above). */
+/* Fused leaf update + refit (same result as the two calls above): a launch over chunks of at
+ * most 1024 leaves (whole subtrees; leaf boxes and the chunk's inner nodes united height by
+ * height in shared memory) and a one-block launch for the nodes above them (construct_tree
+ * prepares both, once per topology). When prims is the table the tree was
+ * constructed from (the pointer given to the last reduce_aabb before construct_tree), the
+ * leaf boxes read the tree's copy of it in leaf order; the topology is assumed unchanged
+ * since that construction. Another table is read through the leaf order. */
 U26_API u26_status u26_lbvh_update_and_refit(u26_lbvh* tree, const float* thickness, const float* x_start,
 	const float* x_end, const uint32_t* prims);
 /* LBVH::broad_phase_query_from_{verts,edges,edges_unculled} (lbvh.cpp:1193-1262).

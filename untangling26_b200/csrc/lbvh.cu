@@ -274,28 +274,57 @@ namespace u26
 			const uint32_t* __restrict__ prims, uint32_t pid, f3& mn, f3& mx)
 		{
 			uint32_t first;
+			// x_start == x_end (a refit at one state): min(v, v) = v, so one set of loads gives the
+			// same box bit for bit
+			const bool same = x0 == x1;
 			if constexpr (TYPE == U26_TREE_FACE)
 			{
 				const uint32_t a = __ldg(prims + 3 * pid), b = __ldg(prims + 3 * pid + 1), c = __ldg(prims + 3 * pid + 2);
 				const f3 s0 = ld3(x0, a), s1 = ld3(x0, b), s2 = ld3(x0, c);
-				const f3 e0 = ld3(x1, a), e1 = ld3(x1, b), e2 = ld3(x1, c);
-				mn = vmin(vmin(s0, vmin(s1, s2)), vmin(e0, vmin(e1, e2)));
-				mx = vmax(vmax(s0, vmax(s1, s2)), vmax(e0, vmax(e1, e2)));
+				if (same)
+				{
+					mn = vmin(s0, vmin(s1, s2));
+					mx = vmax(s0, vmax(s1, s2));
+				}
+				else
+				{
+					const f3 e0 = ld3(x1, a), e1 = ld3(x1, b), e2 = ld3(x1, c);
+					mn = vmin(vmin(s0, vmin(s1, s2)), vmin(e0, vmin(e1, e2)));
+					mx = vmax(vmax(s0, vmax(s1, s2)), vmax(e0, vmax(e1, e2)));
+				}
 				first = a;
 			}
 			else if constexpr (TYPE == U26_TREE_EDGE)
 			{
 				const uint32_t a = __ldg(prims + 2 * pid), b = __ldg(prims + 2 * pid + 1);
-				const f3 s0 = ld3(x0, a), s1 = ld3(x0, b), e0 = ld3(x1, a), e1 = ld3(x1, b);
-				mn = vmin(vmin(s0, s1), vmin(e0, e1));
-				mx = vmax(vmax(s0, s1), vmax(e0, e1));
+				const f3 s0 = ld3(x0, a), s1 = ld3(x0, b);
+				if (same)
+				{
+					mn = vmin(s0, s1);
+					mx = vmax(s0, s1);
+				}
+				else
+				{
+					const f3 e0 = ld3(x1, a), e1 = ld3(x1, b);
+					mn = vmin(vmin(s0, s1), vmin(e0, e1));
+					mx = vmax(vmax(s0, s1), vmax(e0, e1));
+				}
 				first = a;
 			}
 			else
 			{
-				const f3 s0 = ld3(x0, pid), e0 = ld3(x1, pid);
-				mn = vmin(s0, e0);
-				mx = vmax(s0, e0);
+				const f3 s0 = ld3(x0, pid);
+				if (same)
+				{
+					mn = s0;
+					mx = s0;
+				}
+				else
+				{
+					const f3 e0 = ld3(x1, pid);
+					mn = vmin(s0, e0);
+					mx = vmax(s0, e0);
+				}
 				first = pid;
 			}
 			const float t = __ldg(thickness + first);
@@ -320,152 +349,421 @@ namespace u26
 			boxes[n - 1 + lid] = b;
 		}
 
-		// Bottom-up union (fn_refit_tree_aabb, lbvh.cpp:694-758) without spin-waits. One thread
-		// per leaf climbs; at each inner node the first arrival stops and the second owns the
-		// union. The climb stays inside its block while it can: block b owns the leaves
-		// [b * kRefitBlock, (b + 1) * kRefitBlock), and an inner node's leaves form a contiguous
-		// range with the node's own index at one end (Karras 2012), so a node whose range lies
-		// inside the block is reached by the block's threads only. Its arrival counter and its
-		// box live in shared memory (the box is written out as well). A node whose range
-		// crosses a block boundary, and every ancestor of it, joins through a device counter
-		// that gains 2 per refit: an even value before the increment marks the first arrival,
-		// so the counters need no reset between refits. The leaf update runs in the same
-		// thread when FUSED. Every climb is bounded by kMaxClimb steps.
-		constexpr uint32_t kRefitBlock = 512;
+		// Bottom-up union (fn_refit_tree_aabb, lbvh.cpp:694-758) without atomics or waits, level
+		// by level. construct_tree prepares, once per topology:
+		//  * the height of every inner node (1 + the larger child height, leaves 0); a Karras
+		//    tree over unique 64-bit keys is at most 64 deep, so a height fits a byte;
+		//  * treelets: the maximal subtrees of at most kTreelet leaves (each a contiguous leaf
+		//    range, Karras 2012), packed in leaf order into chunks of at most kTreelet leaves;
+		//  * the top nodes (more than kTreelet leaves) sorted by height, their children as
+		//    compact ids (top node j, or 0x80000000 | treelet b).
+		// refit_chunk_kernel: one block per chunk. Leaf boxes, the chunk's inner nodes (child
+		// links and heights) and their boxes live in shared memory; the nodes of height h are
+		// united in step h, after a barrier, so every union reads finished children without
+		// atomics or fences. Boxes go out coalesced.
+		// refit_top_kernel: one block for the top tree. The treelet roots' boxes are read once,
+		// then the top nodes height by height, in shared memory when the tree fits, else
+		// through L2.
+		// Unions keep the (first child, second child) operand order of the reference.
+		constexpr uint32_t kTreelet = 1024;
+		constexpr uint32_t kTopRoot = 0x80000000u;
+		constexpr uint32_t kMaxHeight = 64;
+		constexpr size_t kTopSharedBytes = 226u * 1024u; // the top tree in shared memory up to this size (227 KB per block, less static)
+		constexpr size_t kChunkSmem = 2 * 24 * kTreelet + sizeof(uint32_t) * kTreelet;
 		struct Box6
 		{
 			float v[6];
 		};
-		__device__ __forceinline__ void load_box6_cg(const NodeBox* p, f3& mn, f3& mx)
+		__device__ __forceinline__ Box6 unite(const Box6& a, const Box6& b)
+		{
+			return Box6{ { fminf(a.v[0], b.v[0]), fminf(a.v[1], b.v[1]), fminf(a.v[2], b.v[2]), fmaxf(a.v[3], b.v[3]), fmaxf(a.v[4], b.v[4]),
+				fmaxf(a.v[5], b.v[5]) } };
+		}
+		__device__ __forceinline__ void store_box6(NodeBox* p, const Box6& b, float w_mx)
+		{
+			__stcg(&p->mn, make_float4(b.v[0], b.v[1], b.v[2], 0.0f));
+			__stcg(&p->mx, make_float4(b.v[3], b.v[4], b.v[5], w_mx));
+		}
+		__device__ __forceinline__ Box6 load_box6(const NodeBox* p)
 		{
 			const float4 a = __ldcg(&p->mn), b = __ldcg(&p->mx);
-			mn = mk3(a.x, a.y, a.z);
-			mx = mk3(b.x, b.y, b.z);
+			return Box6{ { a.x, a.y, a.z, b.x, b.y, b.z } };
 		}
-		template <int TYPE, bool FUSED>
-		__global__ void __launch_bounds__(kRefitBlock) refit_block_kernel(const uint32_t* __restrict__ sorted_get_original,
-			NodeBox* __restrict__ boxes, const float* __restrict__ x0, const float* __restrict__ x1, const float* __restrict__ thickness,
-			const uint32_t* __restrict__ prims, const uint32_t* __restrict__ parent, const uint2* __restrict__ children,
-			const uint32_t* __restrict__ node_range, uint32_t* __restrict__ flags, uint32_t n, uint32_t* __restrict__ health)
+		// leaf order -> primitive table, permuted once per construction
+		template <int K>
+		__global__ void __launch_bounds__(256) permute_prims_kernel(const uint32_t* __restrict__ sorted_get_original,
+			const uint32_t* __restrict__ prims, uint32_t n, uint32_t* __restrict__ out)
 		{
-			__shared__ uint32_t s_cnt[kRefitBlock];
-			__shared__ Box6 s_leaf[kRefitBlock];
-			__shared__ Box6 s_inner[kRefitBlock];
-			// topology of the inner nodes [base, base + cnt), read once with coalesced loads, so
-			// that the climb's dependent lookups inside the block hit shared memory
-			__shared__ uint2 s_child[kRefitBlock];
-			__shared__ uint32_t s_parent[kRefitBlock], s_range[kRefitBlock];
-			const uint32_t base = blockIdx.x * kRefitBlock;
-			const uint32_t cnt = min(kRefitBlock, n - base);
-			const uint32_t ni = n - 1;
-			const uint32_t t = threadIdx.x;
-			s_cnt[t] = 0u;
-			bool inner_local = false; // inner node base + t lies inside the block (its box is written below)
-			if (base + t < ni)
-			{
-				s_child[t] = __ldg(children + base + t);
-				s_parent[t] = __ldg(parent + base + t);
-				const uint32_t r = __ldg(node_range + base + t);
-				s_range[t] = r;
-				inner_local = min(base + t, r) >= base && max(base + t, r) < base + cnt;
-			}
-			// phase 1: leaf boxes (into shared memory; written out in phase 3)
-			const uint32_t lid = base + t;
-			if (t < cnt)
-			{
-				f3 mn, mx;
-				if constexpr (FUSED)
-					leaf_box<TYPE>(x0, x1, thickness, prims, __ldg(sorted_get_original + lid), mn, mx);
-				else
-					load_box6_cg(boxes + ni + lid, mn, mx);
-				s_leaf[t] = Box6{ { mn.x, mn.y, mn.z, mx.x, mx.y, mx.z } };
-			}
-			__syncthreads();
-			// phase 2: the climb through the nodes inside the block, in shared memory only (no device
-			// stores in flight, so the block-scope fences stay cheap). A thread that reaches a node
-			// crossing the block boundary keeps it as `pending` for phase 4.
-			constexpr uint32_t kMaxClimb = 100000u;
-			uint32_t pending = kInvalid;
-			if (t < cnt)
-			{
-				uint32_t node = __ldg(parent + ni + lid);
-				uint32_t steps = 0;
-				while (node != kInvalid)
-				{
-					if (++steps > kMaxClimb || node >= ni)
-					{
-						atomicExch(health, 0u);
-						node = kInvalid;
-						break;
-					}
-					const uint32_t k = node - base;
-					if (!(k < cnt && min(node, s_range[k]) >= base && max(node, s_range[k]) < base + cnt))
-					{
-						pending = node; // crosses the block boundary
-						break;
-					}
-					__threadfence_block(); // this thread's shared boxes before its arrival
-					if (atomicAdd(&s_cnt[k], 1u) == 0u)
-						break;
-					__threadfence_block();
-					const uint2 c = s_child[k];
-					// children of a node inside the block are inside it too (checked, not assumed)
-					const uint32_t ia = c.x >= ni ? c.x - ni - base : c.x - base, ib = c.y >= ni ? c.y - ni - base : c.y - base;
-					if (ia >= cnt || ib >= cnt)
-					{
-						atomicExch(health, 0u);
-						break;
-					}
-					const Box6 ba = c.x >= ni ? s_leaf[ia] : s_inner[ia];
-					const Box6 bb = c.y >= ni ? s_leaf[ib] : s_inner[ib];
-					s_inner[k] = Box6{ { fminf(ba.v[0], bb.v[0]), fminf(ba.v[1], bb.v[1]), fminf(ba.v[2], bb.v[2]), fmaxf(ba.v[3], bb.v[3]),
-						fmaxf(ba.v[4], bb.v[4]), fmaxf(ba.v[5], bb.v[5]) } };
-					node = s_parent[k];
-				}
-			}
-			__syncthreads();
-			// phase 3: the block's leaf boxes and local inner boxes, written out coalesced
-			if (t < cnt)
-			{
-				const Box6 l = s_leaf[t];
-				__stcg(&boxes[ni + lid].mn, make_float4(l.v[0], l.v[1], l.v[2], 0.0f));
-				__stcg(&boxes[ni + lid].mx, make_float4(l.v[3], l.v[4], l.v[5], 1.0f));
-			}
-			if (inner_local)
-			{
-				const Box6 b = s_inner[t];
-				__stcg(&boxes[base + t].mn, make_float4(b.v[0], b.v[1], b.v[2], 0.0f));
-				__stcg(&boxes[base + t].mx, make_float4(b.v[3], b.v[4], b.v[5], 1.0f));
-			}
-			__syncthreads();
-			if (pending == kInvalid)
+			const uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x;
+			if (lid >= n)
 				return;
-			// phase 4: nodes crossing block boundaries, through device counters that gain 2 per refit
-			// (an even value before the increment marks the first arrival). The acq_rel arrival
-			// releases the block's boxes written above (ordered before it by the barrier) and the
-			// second arrival acquires the sibling's.
-			__threadfence(); // the block's phase 3 stores, ordered by the barrier, before the release below
-			uint32_t node = pending;
+			const uint32_t p = sorted_get_original[lid];
+#pragma unroll
+			for (int k = 0; k < K; k++)
+				out[size_t(K) * lid + k] = prims[size_t(K) * p + k];
+		}
+
+		// ---- construction: heights, treelets, top nodes
+		// heights: a thread per leaf climbs; at each inner node the first arrival stops and the
+		// second (acquiring the first's height) stores 1 + the larger child height. counters are
+		// zero on entry. Bounded by the tree depth (<= 64 levels, capped at kMaxClimb).
+		__global__ void __launch_bounds__(256) height_kernel(const uint32_t* __restrict__ parent, const uint2* __restrict__ children, uint32_t n,
+			uint32_t* __restrict__ counters, uint8_t* __restrict__ height, uint32_t* __restrict__ health)
+		{
+			const uint32_t lid = blockIdx.x * blockDim.x + threadIdx.x;
+			if (lid >= n)
+				return;
+			const uint32_t ni = n - 1;
+			uint32_t node = parent[ni + lid];
 			uint32_t steps = 0;
 			while (node != kInvalid)
 			{
-				if (++steps > kMaxClimb || node >= ni)
+				if (++steps > 100000u || node >= ni)
 				{
 					atomicExch(health, 0u);
 					return;
 				}
-				const uint32_t arrived = cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(flags[node]).fetch_add(1u,
-					cuda::memory_order_acq_rel);
-				if ((arrived & 1u) == 0u)
+				if (cuda::atomic_ref<uint32_t, cuda::thread_scope_device>(counters[node]).fetch_add(1u, cuda::memory_order_acq_rel) == 0u)
 					return;
-				const uint2 c = __ldg(children + node);
-				f3 amn, amx, bmn, bmx;
-				load_box6_cg(boxes + c.x, amn, amx);
-				load_box6_cg(boxes + c.y, bmn, bmx);
-				const f3 mn = vmin(amn, bmn), mx = vmax(amx, bmx);
-				__stcg(&boxes[node].mn, make_float4(mn.x, mn.y, mn.z, 0.0f));
-				__stcg(&boxes[node].mx, make_float4(mx.x, mx.y, mx.z, 1.0f));
-				node = __ldg(parent + node);
+				const uint2 c = children[node];
+				// the sibling's height, ordered after its store by the arrival's acquire
+				const uint32_t ha = c.x >= ni ? 0u : height[c.x];
+				const uint32_t hb = c.y >= ni ? 0u : height[c.y];
+				const uint32_t h = 1u + max(ha, hb);
+				if (h > kMaxHeight)
+				{
+					atomicExch(health, 0u);
+					return;
+				}
+				height[node] = uint8_t(h);
+				node = parent[node];
+			}
+		}
+		__device__ __forceinline__ uint32_t node_size(uint32_t x, uint32_t ni, const uint32_t* __restrict__ range)
+		{
+			if (x >= ni)
+				return 1u;
+			const uint32_t r = range[x];
+			return (x > r ? x - r : r - x) + 1u;
+		}
+		// treelet roots (key: first leaf) and top nodes (key: height, node) appended to two lists
+		__global__ void __launch_bounds__(256) treelet_mark_kernel(const uint32_t* __restrict__ parent, const uint32_t* __restrict__ range,
+			const uint8_t* __restrict__ height, uint32_t n, uint32_t* __restrict__ counts, uint64_t* __restrict__ top_keys,
+			uint32_t* __restrict__ top_vals, uint64_t* __restrict__ root_keys, uint32_t* __restrict__ root_vals)
+		{
+			const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+			const uint32_t ni = n - 1;
+			if (x >= 2 * n - 1)
+				return;
+			const uint32_t sz = node_size(x, ni, range);
+			if (sz > kTreelet)
+			{
+				const uint32_t j = atomicAdd(counts + 0, 1u);
+				top_keys[j] = (uint64_t(height[x]) << 32) | x;
+				top_vals[j] = x;
+				return;
+			}
+			const uint32_t p = parent[x];
+			if (p == kInvalid || node_size(p, ni, range) > kTreelet)
+			{
+				const uint32_t lo = x >= ni ? x - ni : min(x, range[x]);
+				const uint32_t b = atomicAdd(counts + 1, 1u);
+				root_keys[b] = lo;
+				root_vals[b] = x;
+			}
+		}
+		// compact ids of the sorted lists, then each top node's children as compact ids, the end
+		// of each height's run, and the treelets' leaf ranges
+		__global__ void __launch_bounds__(256) treelet_map_kernel(const uint32_t* __restrict__ top_nodes, uint32_t m,
+			const uint32_t* __restrict__ roots, uint32_t nt, uint32_t* __restrict__ cmap)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i < m)
+				cmap[top_nodes[i]] = i;
+			else if (i < m + nt)
+				cmap[roots[i - m]] = kTopRoot | (i - m);
+		}
+		__global__ void __launch_bounds__(256) treelet_links_kernel(const uint32_t* __restrict__ top_nodes, uint32_t m,
+			const uint2* __restrict__ children, const uint32_t* __restrict__ cmap, const uint8_t* __restrict__ height,
+			uint2* __restrict__ top_links, uint32_t* __restrict__ height_end, const uint32_t* __restrict__ roots, uint32_t nt,
+			const uint32_t* __restrict__ range, uint32_t n, uint32_t* __restrict__ root_size, uint8_t* __restrict__ top_height)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i < m)
+			{
+				const uint32_t x = top_nodes[i];
+				const uint2 c = children[x];
+				top_links[i] = make_uint2(cmap[c.x], cmap[c.y]);
+				const uint32_t h = height[x];
+				top_height[i] = uint8_t(h);
+				if (i + 1 == m || height[top_nodes[i + 1]] != h)
+					height_end[h] = i + 1;
+			}
+			if (i < nt)
+				root_size[i] = node_size(roots[i], n - 1, range);
+		}
+		// treelets (in leaf order) packed greedily into chunks of at most kTreelet leaves; one
+		// thread (a few thousand treelets)
+		// (chunk_tb: each chunk's first treelet, then nt)
+		__global__ void treelet_chunks_kernel(const uint32_t* __restrict__ root_size, uint32_t nt, uint32_t* __restrict__ chunk_lo,
+			uint32_t* __restrict__ chunk_tb, uint32_t* __restrict__ nchunks)
+		{
+			if (threadIdx.x != 0 || blockIdx.x != 0)
+				return;
+			uint32_t k = 0, lo = 0, fill = 0, tb = 0;
+			for (uint32_t b = 0; b < nt; b++)
+			{
+				const uint32_t sz = root_size[b];
+				if (fill > 0 && fill + sz > kTreelet)
+				{
+					chunk_tb[k] = tb;
+					chunk_lo[k++] = lo;
+					lo += fill;
+					fill = 0;
+					tb = b;
+				}
+				fill += sz;
+			}
+			chunk_tb[k] = tb;
+			chunk_lo[k++] = lo;
+			chunk_lo[k] = lo + fill;
+			chunk_tb[k] = nt;
+			*nchunks = k;
+		}
+
+		// ---- refit
+		// a box in shared memory: six floats on an 8-byte boundary (three 8-byte accesses)
+		struct __align__(8) SBox
+		{
+			float2 v[3]; // (mn.x, mn.y), (mn.z, mx.x), (mx.y, mx.z)
+		};
+		__device__ __forceinline__ SBox sbox(f3 mn, f3 mx)
+		{
+			return SBox{ { make_float2(mn.x, mn.y), make_float2(mn.z, mx.x), make_float2(mx.y, mx.z) } };
+		}
+		__device__ __forceinline__ SBox unite_s(const SBox& a, const SBox& b)
+		{
+			return SBox{ { make_float2(fminf(a.v[0].x, b.v[0].x), fminf(a.v[0].y, b.v[0].y)),
+				make_float2(fminf(a.v[1].x, b.v[1].x), fmaxf(a.v[1].y, b.v[1].y)),
+				make_float2(fmaxf(a.v[2].x, b.v[2].x), fmaxf(a.v[2].y, b.v[2].y)) } };
+		}
+		__device__ __forceinline__ void store_sbox(NodeBox* p, const SBox& b)
+		{
+			__stcg(&p->mn, make_float4(b.v[0].x, b.v[0].y, b.v[1].x, 0.0f));
+			__stcg(&p->mx, make_float4(b.v[1].y, b.v[2].x, b.v[2].y, 1.0f));
+		}
+		// One 512-thread block per chunk of at most 1024 leaves, two leaves and two inner-node
+		// slots per thread, so that four chunks share an SM and one chunk's loads overlap another's
+		// height steps.
+		constexpr uint32_t kChunkThreads = 512;
+		template <int TYPE, bool FUSED>
+		__global__ void __launch_bounds__(kChunkThreads, 4) refit_chunk_kernel(const uint32_t* __restrict__ sorted_get_original,
+			NodeBox* __restrict__ boxes, const float* __restrict__ x0, const float* __restrict__ x1, const float* __restrict__ thickness,
+			const uint32_t* __restrict__ prims, bool prims_in_leaf_order, const uint2* __restrict__ children,
+			const uint32_t* __restrict__ node_range, const uint8_t* __restrict__ height, const uint32_t* __restrict__ chunk_lo, uint32_t n,
+			const uint32_t* __restrict__ chunk_tb, const uint32_t* __restrict__ roots, SBox* __restrict__ root_box, uint32_t* __restrict__ health)
+		{
+			// dynamic shared memory (kChunkSmem bytes, four blocks per SM): leaf boxes, inner boxes,
+			// child links as two 16-bit chunk-local slots (bit 15: leaf)
+			extern __shared__ __align__(16) unsigned char s_raw[];
+			SBox* s_leaf = reinterpret_cast<SBox*>(s_raw);
+			SBox* s_inner = s_leaf + kTreelet;
+			uint32_t* s_child = reinterpret_cast<uint32_t*>(s_inner + kTreelet);
+			__shared__ uint32_t s_hmax;
+			const uint32_t base = chunk_lo[blockIdx.x];
+			const uint32_t cnt = chunk_lo[blockIdx.x + 1] - base;
+			const uint32_t ni = n - 1;
+			const uint32_t t = threadIdx.x;
+			if (cnt > kTreelet || base + cnt > n)
+			{
+				// a plan that does not match the tree: nothing is read or written
+				if (t == 0)
+					atomicExch(health, 0u);
+				return;
+			}
+			if (t == 0)
+				s_hmax = 0u;
+			// inner nodes base + t and base + t + 512: links and heights when their leaf ranges lie
+			// inside the chunk
+			uint32_t h[2] = { 0u, 0u };
+#pragma unroll
+			for (int q = 0; q < 2; q++)
+			{
+				const uint32_t tq = t + q * kChunkThreads, x = base + tq;
+				if (tq < cnt && x < ni)
+				{
+					const uint32_t r = __ldg(node_range + x);
+					if (min(x, r) >= base && max(x, r) < base + cnt)
+					{
+						// children of a node inside the chunk are inside it too (checked, not assumed)
+						const uint2 c = __ldg(children + x);
+						const uint32_t ia = c.x >= ni ? c.x - ni - base : c.x - base, ib = c.y >= ni ? c.y - ni - base : c.y - base;
+						if (ia < cnt && ib < cnt)
+						{
+							s_child[tq] = (ia | (c.x >= ni ? 0x8000u : 0u)) | ((ib | (c.y >= ni ? 0x8000u : 0u)) << 16);
+							h[q] = __ldg(height + x);
+						}
+						else
+							atomicExch(health, 0u);
+					}
+				}
+			}
+#pragma unroll
+			for (int q = 0; q < 2; q++)
+			{
+				const uint32_t tq = t + q * kChunkThreads, lid = base + tq;
+				if (tq < cnt)
+				{
+					f3 mn, mx;
+					if constexpr (FUSED)
+					{
+						if (prims_in_leaf_order)
+							leaf_box<TYPE>(x0, x1, thickness, prims, lid, mn, mx);
+						else
+							leaf_box<TYPE>(x0, x1, thickness, prims, __ldg(sorted_get_original + lid), mn, mx);
+					}
+					else
+					{
+						const float4 a = __ldcg(&boxes[ni + lid].mn), b = __ldcg(&boxes[ni + lid].mx);
+						mn = mk3(a.x, a.y, a.z);
+						mx = mk3(b.x, b.y, b.z);
+					}
+					s_leaf[tq] = sbox(mn, mx);
+				}
+			}
+			const uint32_t wmax = __reduce_max_sync(0xFFFFFFFFu, max(h[0], h[1]));
+			if ((t & 31) == 0 && wmax)
+				atomicMax(&s_hmax, wmax);
+			__syncthreads();
+			const uint32_t hmax = s_hmax;
+			for (uint32_t lv = 1; lv <= hmax; lv++)
+			{
+#pragma unroll
+				for (int q = 0; q < 2; q++)
+				{
+					if (h[q] != lv)
+						continue;
+					const uint32_t tq = t + q * kChunkThreads;
+					const uint32_t c = s_child[tq], ca = c & 0xFFFFu, cb = c >> 16;
+					s_inner[tq] = unite_s((ca & 0x8000u) ? s_leaf[ca & 0x3FFu] : s_inner[ca & 0x3FFu],
+						(cb & 0x8000u) ? s_leaf[cb & 0x3FFu] : s_inner[cb & 0x3FFu]);
+				}
+				__syncthreads();
+			}
+#pragma unroll
+			for (int q = 0; q < 2; q++)
+			{
+				const uint32_t tq = t + q * kChunkThreads;
+				if (tq < cnt)
+				{
+					store_sbox(boxes + ni + base + tq, s_leaf[tq]);
+					if (h[q])
+						store_sbox(boxes + base + tq, s_inner[tq]);
+				}
+			}
+			// the chunk's treelet roots' boxes, also in a compact array for the top-tree launch
+			if (root_box)
+			{
+				const uint32_t tb0 = chunk_tb[blockIdx.x], tb1 = chunk_tb[blockIdx.x + 1];
+				for (uint32_t b = tb0 + t; b < tb1; b += kChunkThreads)
+				{
+					const uint32_t x = roots[b];
+					const uint32_t k = x >= ni ? x - ni - base : x - base;
+					if (k < cnt)
+						root_box[b] = x >= ni ? s_leaf[k] : s_inner[k];
+					else
+						atomicExch(health, 0u);
+				}
+			}
+		}
+
+		// The top tree in one block: the treelet roots' boxes are read once, then the top nodes are
+		// united height by height. SHARED (every box fits in shared memory, at most kTopSlots x 1024
+		// top nodes): each thread holds its nodes' links, ids and heights in registers, so a height
+		// step touches shared memory only (its box stores go out behind it). Otherwise the
+		// children are read back through L2 (the block's barrier orders its own stores before the
+		// next height's loads).
+		constexpr uint32_t kTopSlots = 8;
+		template <bool SHARED>
+		__global__ void __launch_bounds__(1024) refit_top_kernel(NodeBox* __restrict__ boxes, const uint32_t* __restrict__ top_nodes,
+			const uint2* __restrict__ top_links, const uint32_t* __restrict__ height_end, uint32_t m, const uint32_t* __restrict__ roots,
+			uint32_t nt, const uint8_t* __restrict__ top_height, const SBox* __restrict__ root_box, uint32_t* __restrict__ health)
+		{
+			extern __shared__ SBox s_box[]; // [nt] treelet roots, then [m] top nodes
+			const uint32_t t = threadIdx.x;
+			auto valid = [&](uint32_t id, uint32_t j) { return (id & kTopRoot) ? (id & ~kTopRoot) < nt : id < j; };
+			if constexpr (SHARED)
+			{
+				uint2 l[kTopSlots];
+				uint32_t node[kTopSlots], hh[kTopSlots];
+				uint32_t hmax = 0;
+#pragma unroll
+				for (uint32_t k = 0; k < kTopSlots; k++)
+				{
+					const uint32_t j = t + k * blockDim.x;
+					hh[k] = 0;
+					if (j < m)
+					{
+						l[k] = top_links[j];
+						node[k] = top_nodes[j];
+						hh[k] = top_height[j];
+						hmax = max(hmax, hh[k]);
+					}
+				}
+				// the treelet roots' boxes: one coalesced read of the compact copy
+				for (uint32_t b = t; b < nt; b += blockDim.x)
+					s_box[b] = root_box[b];
+				hmax = __reduce_max_sync(0xFFFFFFFFu, hmax);
+				__shared__ uint32_t s_hmax;
+				if (t == 0)
+					s_hmax = 0;
+				__syncthreads();
+				if ((t & 31) == 0)
+					atomicMax(&s_hmax, hmax);
+				__syncthreads();
+				hmax = s_hmax;
+				for (uint32_t lv = 1; lv <= hmax; lv++)
+				{
+#pragma unroll
+					for (uint32_t k = 0; k < kTopSlots; k++)
+					{
+						if (hh[k] != lv)
+							continue;
+						const uint32_t j = t + k * blockDim.x;
+						if (!valid(l[k].x, j) || !valid(l[k].y, j))
+						{
+							atomicExch(health, 0u);
+							continue;
+						}
+						const SBox a = (l[k].x & kTopRoot) ? s_box[l[k].x & ~kTopRoot] : s_box[nt + l[k].x];
+						const SBox c = (l[k].y & kTopRoot) ? s_box[l[k].y & ~kTopRoot] : s_box[nt + l[k].y];
+						const SBox u = unite_s(a, c);
+						s_box[nt + j] = u;
+						store_sbox(boxes + node[k], u);
+					}
+					__syncthreads();
+				}
+			}
+			else
+			{
+				uint32_t begin = 0;
+				for (uint32_t h = 1; h <= kMaxHeight && begin < m; h++)
+				{
+					const uint32_t end = max(begin, height_end[h]);
+					for (uint32_t j = begin + t; j < end && j < m; j += blockDim.x)
+					{
+						const uint2 l = top_links[j];
+						if (!valid(l.x, j) || !valid(l.y, j))
+						{
+							atomicExch(health, 0u);
+							continue;
+						}
+						auto child = [&](uint32_t id) { return load_box6(boxes + ((id & kTopRoot) ? roots[id & ~kTopRoot] : top_nodes[id])); };
+						store_box6(boxes + top_nodes[j], unite(child(l.x), child(l.y)), 1.0f);
+					}
+					begin = end;
+					__syncthreads();
+				}
 			}
 		}
 
@@ -574,8 +872,11 @@ namespace u26
 		U26_CUDA(ctx, t->block_aabb.reserve(sizeof(float) * 6 * div_up(n, 256)));
 		U26_CUDA(ctx, t->global_aabb.reserve(sizeof(float) * 6));
 		U26_CUDA(ctx, t->refit_flags.reserve(sizeof(uint32_t) * std::max<uint32_t>(n - 1, 1)));
-		U26_CUDA(ctx, cudaMemsetAsync(t->refit_flags.ptr, 0, sizeof(uint32_t) * std::max<uint32_t>(n - 1, 1), ctx->stream));
 		U26_CUDA(ctx, t->node_range.reserve(sizeof(uint32_t) * std::max<uint32_t>(n - 1, 1)));
+		U26_CUDA(ctx, t->height.reserve(std::max<uint32_t>(n - 1, 1)));
+		U26_CUDA(ctx, t->height_end.reserve(sizeof(uint32_t) * (kMaxHeight + 1)));
+		if (t->type != U26_TREE_VERT)
+			U26_CUDA(ctx, t->leaf_prims.reserve(sizeof(uint32_t) * (t->type == U26_TREE_FACE ? 3u : 2u) * size_t(n)));
 		U26_CUDA(ctx, t->health.reserve(sizeof(uint32_t)));
 		U26_CUDA(ctx, cudaMemsetAsync(t->health.ptr, 0, sizeof(uint32_t), ctx->stream));
 		U26_CUDA(ctx, cudaMemsetAsync(t->node_aabb.ptr, 0, sizeof(NodeBox) * nn, ctx->stream));
@@ -635,6 +936,17 @@ U26_API void u26_lbvh_destroy(u26_lbvh* t)
 	t->global_aabb.release();
 	t->refit_flags.release();
 	t->node_range.release();
+	t->height.release();
+	t->chunk_lo.release();
+	t->top_nodes.release();
+	t->top_links.release();
+	t->height_end.release();
+	t->roots.release();
+	t->chunk_tb.release();
+	t->top_height.release();
+	t->root_box.release();
+	t->plan_scratch.release();
+	t->leaf_prims.release();
 	t->health.release();
 	t->sorter.release();
 	delete t;
@@ -657,6 +969,84 @@ U26_API u26_status u26_lbvh_reduce_aabb(u26_lbvh* t, const float* x, uint32_t nu
 	t->last_x = x;
 	t->last_prims = prims;
 	t->last_num_verts = num_verts;
+	return U26_OK;
+}
+
+// The refit plan of a constructed tree (heights, treelets, chunks, top nodes by height).
+static u26_status refit_plan(u26_lbvh* t)
+{
+	u26_ctx* ctx = t->ctx;
+	cudaStream_t st = ctx->stream;
+	const uint32_t n = t->n, ni = n - 1, nn = 2 * n - 1;
+	uint32_t* health = t->health.as<uint32_t>();
+	// heights
+	U26_CUDA(ctx, cudaMemsetAsync(t->refit_flags.ptr, 0, sizeof(uint32_t) * ni, st));
+	U26_CUDA(ctx, cudaMemsetAsync(t->height.ptr, 0, ni, st));
+	height_kernel<<<div_up(n, 256), 256, 0, st>>>(t->parent.as<uint32_t>(), t->children.as<uint2>(), n, t->refit_flags.as<uint32_t>(),
+		t->height.as<uint8_t>(), health);
+	U26_TRY(after_launch(ctx, "height_kernel"));
+	// scratch: counts[2], top keys / vals [ni], root keys / vals [n], compact map [nn], root sizes [n]
+	// every region starts on a 256-byte boundary
+	auto up = [](size_t v) { return (v + 255) & ~size_t(255); };
+	const size_t off_tk = 256, off_tv = up(off_tk + 8 * size_t(ni)), off_rk = up(off_tv + 4 * size_t(ni)), off_rv = up(off_rk + 8 * size_t(n)),
+				 off_map = up(off_rv + 4 * size_t(n)), off_sz = up(off_map + 4 * size_t(nn)), total = up(off_sz + 4 * size_t(n));
+	U26_CUDA(ctx, t->plan_scratch.reserve(total));
+	unsigned char* sc = static_cast<unsigned char*>(t->plan_scratch.ptr);
+	uint32_t* counts = reinterpret_cast<uint32_t*>(sc);
+	uint64_t* top_keys = reinterpret_cast<uint64_t*>(sc + off_tk);
+	uint32_t* top_vals = reinterpret_cast<uint32_t*>(sc + off_tv);
+	uint64_t* root_keys = reinterpret_cast<uint64_t*>(sc + off_rk);
+	uint32_t* root_vals = reinterpret_cast<uint32_t*>(sc + off_rv);
+	uint32_t* cmap = reinterpret_cast<uint32_t*>(sc + off_map);
+	uint32_t* root_size = reinterpret_cast<uint32_t*>(sc + off_sz);
+	U26_CUDA(ctx, cudaMemsetAsync(counts, 0, 2 * sizeof(uint32_t), st));
+	treelet_mark_kernel<<<div_up(nn, 256), 256, 0, st>>>(t->parent.as<uint32_t>(), t->node_range.as<uint32_t>(), t->height.as<uint8_t>(), n,
+		counts, top_keys, top_vals, root_keys, root_vals);
+	U26_TRY(after_launch(ctx, "treelet_mark_kernel"));
+	uint32_t mt[2] = { 0, 0 };
+	U26_CUDA(ctx, cudaMemcpyAsync(mt, counts, sizeof(mt), cudaMemcpyDeviceToHost, st));
+	U26_CUDA(ctx, cudaStreamSynchronize(st));
+	const uint32_t m = mt[0], nt = mt[1];
+	if (nt == 0 || nt > n || m > ni)
+		return set_error(ctx, U26_ERR_INVALID_INPUT, "refit plan: %u treelets, %u top nodes for %u leaves", nt, m, n);
+	if (m > 1)
+		U26_TRY(t->sorter.sort(ctx, top_keys, top_vals, m, 0, 40));
+	if (nt > 1)
+		U26_TRY(t->sorter.sort(ctx, root_keys, root_vals, nt, 0, 32));
+	U26_CUDA(ctx, t->top_nodes.reserve(sizeof(uint32_t) * std::max(m, 1u)));
+	U26_CUDA(ctx, t->top_links.reserve(sizeof(uint2) * std::max(m, 1u)));
+	U26_CUDA(ctx, t->roots.reserve(sizeof(uint32_t) * nt));
+	U26_CUDA(ctx, t->chunk_lo.reserve(sizeof(uint32_t) * (nt + 2)));
+	U26_CUDA(ctx, t->chunk_tb.reserve(sizeof(uint32_t) * (nt + 2)));
+	U26_CUDA(ctx, t->top_height.reserve(std::max(m, 1u)));
+	U26_CUDA(ctx, t->root_box.reserve(sizeof(SBox) * nt));
+	if (m)
+		U26_CUDA(ctx, cudaMemcpyAsync(t->top_nodes.ptr, top_vals, sizeof(uint32_t) * m, cudaMemcpyDeviceToDevice, st));
+	U26_CUDA(ctx, cudaMemcpyAsync(t->roots.ptr, root_vals, sizeof(uint32_t) * nt, cudaMemcpyDeviceToDevice, st));
+	treelet_map_kernel<<<div_up(m + nt, 256), 256, 0, st>>>(t->top_nodes.as<uint32_t>(), m, t->roots.as<uint32_t>(), nt, cmap);
+	U26_TRY(after_launch(ctx, "treelet_map_kernel"));
+	U26_CUDA(ctx, cudaMemsetAsync(t->height_end.ptr, 0, sizeof(uint32_t) * (kMaxHeight + 1), st));
+	treelet_links_kernel<<<div_up(std::max(m, nt), 256), 256, 0, st>>>(t->top_nodes.as<uint32_t>(), m, t->children.as<uint2>(), cmap,
+		t->height.as<uint8_t>(), t->top_links.as<uint2>(), t->height_end.as<uint32_t>(), t->roots.as<uint32_t>(), nt,
+		t->node_range.as<uint32_t>(), n, root_size, t->top_height.as<uint8_t>());
+	U26_TRY(after_launch(ctx, "treelet_links_kernel"));
+	treelet_chunks_kernel<<<1, 32, 0, st>>>(root_size, nt, t->chunk_lo.as<uint32_t>(), t->chunk_tb.as<uint32_t>(), counts);
+	U26_TRY(after_launch(ctx, "treelet_chunks_kernel"));
+	U26_CUDA(ctx, cudaMemcpyAsync(mt, counts, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+	U26_CUDA(ctx, cudaStreamSynchronize(st));
+	t->nchunks = mt[0];
+	t->ntop = m;
+	t->ntreelets = nt;
+	const size_t top_bytes = sizeof(SBox) * (size_t(m) + nt);
+	t->top_in_shared = top_bytes <= kTopSharedBytes && m <= kTopSlots * 1024u;
+	if (t->top_in_shared && m)
+		U26_CUDA(ctx, cudaFuncSetAttribute(refit_top_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTopSharedBytes)));
+	// the chunk kernels' dynamic shared memory (above the 48 KB default)
+	const void* chunk_kernels[] = { (const void*)refit_chunk_kernel<U26_TREE_VERT, false>, (const void*)refit_chunk_kernel<U26_TREE_VERT, true>,
+		(const void*)refit_chunk_kernel<U26_TREE_EDGE, false>, (const void*)refit_chunk_kernel<U26_TREE_EDGE, true>,
+		(const void*)refit_chunk_kernel<U26_TREE_FACE, false>, (const void*)refit_chunk_kernel<U26_TREE_FACE, true> };
+	for (const void* k : chunk_kernels)
+		U26_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChunkSmem)));
 	return U26_OK;
 }
 
@@ -688,6 +1078,23 @@ U26_API u26_status u26_lbvh_construct_tree(u26_lbvh* t)
 			t->health.as<uint32_t>());
 		U26_TRY(after_launch(ctx, "check_kernel"));
 	}
+	// the primitive table in leaf order, for the refits' coalesced leaf reads (the mesh
+	// topology is fixed between constructions; a refit given another table gathers)
+	t->leaf_prims_src = nullptr;
+	if (t->type == U26_TREE_FACE)
+	{
+		permute_prims_kernel<3><<<div_up(n, 256), 256, 0, ctx->stream>>>(vals, t->last_prims, n, t->leaf_prims.as<uint32_t>());
+		U26_TRY(after_launch(ctx, "permute_prims_kernel"));
+		t->leaf_prims_src = t->last_prims;
+	}
+	else if (t->type == U26_TREE_EDGE)
+	{
+		permute_prims_kernel<2><<<div_up(n, 256), 256, 0, ctx->stream>>>(vals, t->last_prims, n, t->leaf_prims.as<uint32_t>());
+		U26_TRY(after_launch(ctx, "permute_prims_kernel"));
+		t->leaf_prims_src = t->last_prims;
+	}
+	if (n > 1)
+		U26_TRY(refit_plan(t));
 	t->built = true;
 	return U26_OK;
 }
@@ -715,11 +1122,13 @@ static u26_status refit_impl(u26_lbvh* t, bool fused, const float* thickness, co
 	}
 	if (!t->built)
 		return set_error(ctx, U26_ERR_INVALID_INPUT, "refit: call u26_lbvh_construct_tree first");
-	const uint32_t grid = div_up(t->n, kRefitBlock);
+	const bool sorted = fused && prims && prims == t->leaf_prims_src;
+	SBox* root_box = (t->ntop && t->top_in_shared) ? t->root_box.as<SBox>() : nullptr;
+	const uint32_t* lp = sorted ? t->leaf_prims.as<uint32_t>() : prims;
 #define U26_REFIT(T, F)                                                                                                          \
-	refit_block_kernel<T, F><<<grid, kRefitBlock, 0, ctx->stream>>>(t->sorted_get_original.as<uint32_t>(), t->node_aabb.as<NodeBox>(), \
-		x0, x1, thickness, prims, t->parent.as<uint32_t>(), t->children.as<uint2>(), t->node_range.as<uint32_t>(),                   \
-		t->refit_flags.as<uint32_t>(), t->n, t->health.as<uint32_t>())
+	refit_chunk_kernel<T, F><<<t->nchunks, kChunkThreads, kChunkSmem, ctx->stream>>>(t->sorted_get_original.as<uint32_t>(), t->node_aabb.as<NodeBox>(), \
+		x0, x1, thickness, lp, sorted, t->children.as<uint2>(), t->node_range.as<uint32_t>(), t->height.as<uint8_t>(),                  \
+		t->chunk_lo.as<uint32_t>(), t->n, t->chunk_tb.as<uint32_t>(), t->roots.as<uint32_t>(), root_box, t->health.as<uint32_t>())
 	if (t->type == U26_TREE_FACE)
 	{
 		if (fused)
@@ -739,7 +1148,18 @@ static u26_status refit_impl(u26_lbvh* t, bool fused, const float* thickness, co
 	else
 		U26_REFIT(U26_TREE_VERT, false);
 #undef U26_REFIT
-	return after_launch(ctx, "refit_block_kernel");
+	U26_TRY(after_launch(ctx, "refit_chunk_kernel"));
+	if (t->ntop == 0)
+		return U26_OK;
+	if (t->top_in_shared)
+		refit_top_kernel<true><<<1, 1024, sizeof(SBox) * (size_t(t->ntop) + t->ntreelets), ctx->stream>>>(t->node_aabb.as<NodeBox>(),
+			t->top_nodes.as<uint32_t>(), t->top_links.as<uint2>(), t->height_end.as<uint32_t>(), t->ntop, t->roots.as<uint32_t>(), t->ntreelets,
+			t->top_height.as<uint8_t>(), t->root_box.as<SBox>(), t->health.as<uint32_t>());
+	else
+		refit_top_kernel<false><<<1, 1024, 0, ctx->stream>>>(t->node_aabb.as<NodeBox>(), t->top_nodes.as<uint32_t>(), t->top_links.as<uint2>(),
+			t->height_end.as<uint32_t>(), t->ntop, t->roots.as<uint32_t>(), t->ntreelets, t->top_height.as<uint8_t>(), nullptr,
+			t->health.as<uint32_t>());
+	return after_launch(ctx, "refit_top_kernel");
 }
 
 U26_API u26_status u26_lbvh_refit(u26_lbvh* t)

@@ -16,8 +16,23 @@ struct u26_lbvh
 	u26::DevBuf node_aabb;			 // NodeBox[2n-1]
 	u26::DevBuf block_aabb;			 // float[ceil(n/256)][6]
 	u26::DevBuf global_aabb;		 // float[6]
-	u26::DevBuf refit_flags;		 // uint32[max(n-1,1)]: arrival counters, even between refits
+	u26::DevBuf refit_flags;		 // uint32[max(n-1,1)]: arrival counters of the height pass (construction)
 	u26::DevBuf node_range;			 // uint32[max(n-1,1)]: inner node i covers leaves [min(i, r), max(i, r)], r = node_range[i]
+	// refit plan, prepared by construct_tree (one per topology)
+	u26::DevBuf height;			 // uint8[max(n-1,1)]: inner node height (leaves 0)
+	u26::DevBuf chunk_lo;		 // uint32[nchunks + 1]: first leaf of each refit chunk, then n
+	u26::DevBuf top_nodes;		 // uint32[m]: nodes of more than 1024 leaves, by height
+	u26::DevBuf top_links;		 // uint2[m]: their children as compact ids (top j, or 0x80000000 | treelet b)
+	u26::DevBuf height_end;		 // uint32[65]: end of each height's run in top_nodes (0: none)
+	u26::DevBuf roots;			 // uint32[nt]: treelet roots (maximal subtrees of <= 1024 leaves) in leaf order
+	u26::DevBuf chunk_tb;		 // uint32[nchunks + 1]: first treelet of each chunk, then nt
+	u26::DevBuf top_height;		 // uint8[m]: heights of top_nodes
+	u26::DevBuf root_box;		 // float[nt][6]: the treelet roots' boxes of the last refit, compact
+	u26::DevBuf plan_scratch;	 // construction scratch: list keys, counts, compact map
+	uint32_t nchunks = 0, ntop = 0, ntreelets = 0;
+	bool top_in_shared = false;
+	u26::DevBuf leaf_prims;			 // uint32[n][K]: the primitive table in leaf order (edge / face trees)
+	const uint32_t* leaf_prims_src = nullptr; // the table leaf_prims was permuted from
 	u26::DevBuf health;				 // uint32[1]: 1 healthy
 	u26::RadixSorter sorter;
 	// inputs of the last reduce_aabb (construct_tree reads them, as the reference
