@@ -696,7 +696,7 @@ namespace u26
 			{
 				uint2 l[kTopSlots];
 				uint32_t node[kTopSlots], hh[kTopSlots];
-				uint32_t hmax = 0;
+				uint32_t hmax = 0, hmin = kMaxHeight + 1;
 #pragma unroll
 				for (uint32_t k = 0; k < kTopSlots; k++)
 				{
@@ -708,21 +708,30 @@ namespace u26
 						node[k] = top_nodes[j];
 						hh[k] = top_height[j];
 						hmax = max(hmax, hh[k]);
+						hmin = min(hmin, hh[k]);
 					}
 				}
 				// the treelet roots' boxes: one coalesced read of the compact copy
 				for (uint32_t b = t; b < nt; b += blockDim.x)
 					s_box[b] = root_box[b];
+				// the heights present: the loop runs from the lowest top node's height to the root's
 				hmax = __reduce_max_sync(0xFFFFFFFFu, hmax);
-				__shared__ uint32_t s_hmax;
+				hmin = __reduce_min_sync(0xFFFFFFFFu, hmin);
+				__shared__ uint32_t s_hmax, s_hmin;
 				if (t == 0)
+				{
 					s_hmax = 0;
+					s_hmin = kMaxHeight + 1;
+				}
 				__syncthreads();
 				if ((t & 31) == 0)
+				{
 					atomicMax(&s_hmax, hmax);
+					atomicMin(&s_hmin, hmin);
+				}
 				__syncthreads();
 				hmax = s_hmax;
-				for (uint32_t lv = 1; lv <= hmax; lv++)
+				for (uint32_t lv = s_hmin; lv <= hmax; lv++)
 				{
 #pragma unroll
 					for (uint32_t k = 0; k < kTopSlots; k++)
