@@ -195,8 +195,8 @@ class Workload:
             self.params = dict(max_contours=32, batch_size=32, autotune=0, raycast_config=2)
             self.repair = True
             # the oracle needs 3-30 s for most contours of this mesh and minutes for the largest
-            # regions (contour 0): the CPU legs evaluate contours 1 and 3
-            self.oracle_contours = (1, 3)
+            # regions (contour 0): the CPU legs evaluate contours 1, 3 and 5
+            self.oracle_contours = (1, 3, 5)
             self.config = {"workload": "layered_sheets_5x512x512", "seed": 4, "layers": 5, "triangles": int(self.full.num_faces),
                            "spacing_mm": 1, "displacement_mm": "U[2, 20] multi-octave", "directions": "reference seeds (<=10)",
                            "opt_iterations": 0, "contours": "first 32 of each pass (one batch)", "update": "response step, scale 1",

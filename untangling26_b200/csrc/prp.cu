@@ -31,6 +31,7 @@
 //                             displacement cost (1806-1954) with a canonical reduction order
 //   gather_kernel             selected supports S(r) compacted for the host
 #include <algorithm>
+#include <functional>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -2129,14 +2130,25 @@ namespace u26
 		{
 			uint32_t b, e;
 		};
-		__device__ __forceinline__ EntryRun entry_run(const uint64_t* __restrict__ ek, uint32_t n, uint64_t prefix, int rb)
+		// the run of keys with the given (task, side, vertex) prefix inside [lo, hi): two binary searches
+		__device__ __forceinline__ EntryRun entry_run(const uint64_t* __restrict__ ek, uint32_t lo, uint32_t hi, uint64_t prefix, int rb)
 		{
-			const uint32_t b = lower_bound64(ek, n, prefix);
-			uint32_t e = b;
-			const uint64_t hi = prefix + (uint64_t(1) << rb);
-			while (e < n && ek[e] < hi)
-				e++;
+			const uint32_t b = lo + lower_bound64(ek + lo, hi - lo, prefix);
+			const uint32_t e = b + lower_bound64(ek + b, hi - b, prefix + (uint64_t(1) << rb));
 			return EntryRun{ b, e };
+		}
+		// each task's range of the sorted support entries (tasks without entries keep [0, 0))
+		__global__ void entry_ranges_kernel(const uint64_t* __restrict__ ek, uint32_t n, int shift, uint32_t* __restrict__ tbeg,
+			uint32_t* __restrict__ tend)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			const uint64_t t = ek[i] >> shift;
+			if (i == 0 || (ek[i - 1] >> shift) != t)
+				tbeg[t] = i;
+			if (i + 1 == n || (ek[i + 1] >> shift) != t)
+				tend[t] = i + 1;
 		}
 		__device__ __forceinline__ bool run_has(const uint64_t* __restrict__ ek, EntryRun r, uint64_t key)
 		{
@@ -2158,7 +2170,8 @@ namespace u26
 		// on side m^1 gains one covered anchor (cov[] is indexed by the component's root).
 		__global__ void coverage_count_kernel(const Task* __restrict__ tasks, uint32_t ntasks, const uint32_t* __restrict__ task_anchor_begin,
 			const uint32_t* __restrict__ anchor_off, const uint32_t* __restrict__ anchors, const uint64_t* __restrict__ ekeys, uint32_t nentries,
-			int vb, int rb, const uint32_t* __restrict__ seg, uint32_t* __restrict__ cov)
+			const uint32_t* __restrict__ tbeg, const uint32_t* __restrict__ tend, int vb, int rb, const uint32_t* __restrict__ seg,
+			uint32_t* __restrict__ cov)
 		{
 			const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
 			if (g >= task_anchor_begin[ntasks])
@@ -2179,12 +2192,13 @@ namespace u26
 			const uint64_t tb = uint64_t(t) << (1 + vb + rb);
 			auto prefix = [&](uint32_t side, uint32_t v)
 			{ return tb | (uint64_t(side) << (vb + rb)) | (uint64_t(v) << rb); };
-			const EntryRun E0 = entry_run(ekeys, nentries, prefix(m, A[1]), rb);
-			const EntryRun E1 = entry_run(ekeys, nentries, prefix(m, A[2]), rb);
+			const uint32_t lo_t = min(tbeg[t], nentries), hi_t = min(max(tend[t], lo_t), nentries);
+			const EntryRun E0 = entry_run(ekeys, lo_t, hi_t, prefix(m, A[1]), rb);
+			const EntryRun E1 = entry_run(ekeys, lo_t, hi_t, prefix(m, A[2]), rb);
 			if (E0.b == E0.e && E1.b == E1.e)
 				return;
-			const EntryRun F[3] = { entry_run(ekeys, nentries, prefix(m ^ 1u, A[3]), rb), entry_run(ekeys, nentries, prefix(m ^ 1u, A[4]), rb),
-				entry_run(ekeys, nentries, prefix(m ^ 1u, A[5]), rb) };
+			const EntryRun F[3] = { entry_run(ekeys, lo_t, hi_t, prefix(m ^ 1u, A[3]), rb), entry_run(ekeys, lo_t, hi_t, prefix(m ^ 1u, A[4]), rb),
+				entry_run(ekeys, lo_t, hi_t, prefix(m ^ 1u, A[5]), rb) };
 			if (F[0].b == F[0].e && F[1].b == F[1].e && F[2].b == F[2].e)
 				return;
 			const uint64_t rmask = (uint64_t(1) << rb) - 1u;
@@ -2963,27 +2977,48 @@ namespace u26
 				return double(h.dist); // FP64 misses the hit (an FP32 / FP64 flip): keep its FP32 depth
 			return t64 * 1.0;
 		}
+		// The FP64 depth of every selected support hit, a thread per hit (the contours' supports are
+		// consecutive ranges of the hit list).
+		__global__ void fp64_depths_kernel(uint32_t nc, const Fp64In* __restrict__ in, uint32_t nh, const u26_prp_hit* __restrict__ hits,
+			const float* __restrict__ x, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, double* __restrict__ d64)
+		{
+			const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+			if (h >= nh)
+				return;
+			uint32_t lo = 0, hi = nc;
+			while (hi - lo > 1)
+			{
+				const uint32_t mid = (lo + hi) >> 1;
+				if (in[mid].hit_begin <= h)
+					lo = mid;
+				else
+					hi = mid;
+			}
+			const Fp64In ci = in[lo];
+			if (h < ci.hit_begin || h >= ci.hit_end)
+				return;
+			d64[h] = hit_delta_f64(hits[h], mk3(ci.dir[0], ci.dir[1], ci.dir[2]), x, edges, faces);
+		}
 		// Warp per contour. Each lane takes the hits h = begin + lane, begin + lane + 32, ...: their
 		// FP64 depths, its partial source-area sum (in that order), the maxima; the partial sums
 		// then combine by the xor butterfly (lane l adds lane l ^ 16, ^ 8, ^ 4, ^ 2, ^ 1), a fixed
 		// order the oracle restates. Ties of a maximum keep the smallest hit index.
 		__global__ void fp64_metrics_kernel(uint32_t nc, const Fp64In* __restrict__ in, const u26_prp_hit* __restrict__ hits,
-			const float* __restrict__ x, const uint2* __restrict__ edges, const uint32_t* __restrict__ faces, const float* __restrict__ varea,
-			const float* __restrict__ earea, const float* __restrict__ farea, Fp64Out* __restrict__ out)
+			const double* __restrict__ d64s, const float* __restrict__ varea, const float* __restrict__ earea, const float* __restrict__ farea,
+			Fp64Out* __restrict__ out)
 		{
 			const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 			const uint32_t lane = threadIdx.x & 31u;
 			if (c >= nc)
 				return;
 			const Fp64In ci = in[c];
-			const f3 dir = mk3(ci.dir[0], ci.dir[1], ci.dir[2]);
 			double area = 0.0, dc64 = -1.0, derr = 0.0;
 			float m32 = -1.0f, s32 = -1.0f;
 			uint32_t arg32 = kInvalid, arg64 = kInvalid;
 			for (uint32_t h = ci.hit_begin + lane; h < ci.hit_end; h += 32u)
 			{
 				const u26_prp_hit hh = hits[h];
-				const double d64 = hit_delta_f64(hh, dir, x, edges, faces);
+				const double d64 = d64s[h];
 				area += double(hh.type == 0u ? varea[hh.src_id] : hh.type == 1u ? earea[hh.src_id] : farea[hh.src_id]);
 				if (d64 > dc64)
 				{
@@ -3210,12 +3245,13 @@ struct u26_scene
 	DevBuf d_f64in, d_f64hits, d_f64delta, d_f64out; // FP64 evaluation of the selected supports
 	DevBuf d_queue;									  // work-item counter of the persistent ray casts
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
+	DevBuf d_trange; // per task: first and past-the-end index of its support entries
 	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals, d_zero_th;
 	RadixSorter sorter, esorter, csorter, fvsorter;
 	std::vector<uint8_t> vsolid; // per vertex: its object is rigid / tetrahedral
 	bool any_solid = false;
 	std::vector<u26_lbvh*> otree_f, otree_e; // per-object ray-casting trees (built at the first pass)
-	bool otrees_built = false;
+	bool otrees_built = false, fronts_built = false;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
 	int tuned_cfg = -1;				  // autotuned ray-casting configuration (-1: not tuned yet)
@@ -3421,7 +3457,7 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
 		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp, &s->d_vsolid,
 		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals,
-		&s->d_zero_th };
+		&s->d_zero_th, &s->d_trange };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
@@ -3504,7 +3540,8 @@ namespace
 	}
 
 	// returns the EF pair count after the degenerate filter (before loop-vertex pairs)
-	uint32_t build_graph(const u26_scene& S, const std::vector<float>& x, HostGraph& G, bool ignore_near_zero)
+	uint32_t build_graph(const u26_scene& S, const std::vector<float>& x, HostGraph& G, bool ignore_near_zero,
+		const std::function<void(const char*)>& mark)
 	{
 		uint32_t n = uint32_t(G.ef.size());
 		// the canonical EF list is sorted by edge: each edge's pairs form one run
@@ -3550,6 +3587,7 @@ namespace
 		});
 		};
 		build_adj();
+		mark("  EF adjacency");
 		// degenerate filter (intersection_resolver.cpp:841-896): with near-zero-distance pairs in
 		// play, a pair with a barycentric coordinate below 1e-4 stays only when one of its
 		// adjacent pairs is not degenerate; if that would remove every pair, all stay
@@ -3595,6 +3633,7 @@ namespace
 			}
 		}
 		const uint32_t n_kept = n;
+		mark("  degenerate filter");
 		// loop-vertex pairs
 		struct Loop
 		{
@@ -3655,6 +3694,7 @@ namespace
 				for (uint32_t q : G.adj[p])
 					s += hlen(G.pos3[q] - G.pos3[p]);
 				G.len[p] = 0.5f * s; });
+		mark("  loop pairs, lengths");
 		// flood fill with mesh-side parity
 		G.mesh_index.assign(na, kInfH);
 		std::vector<uint8_t> seen(na, 0);
@@ -3718,6 +3758,7 @@ namespace
 				t = nb == 1 ? 4u : nb == 2 ? 5u : 0u;
 			G.type[c] = t;
 		}
+		mark("  contours, types");
 		// vertex boundary flags 2c + side (CSR, sorted unique per vertex): bucketed by vertex
 		// (counting sort), then each short row sorted and deduplicated
 		std::vector<uint32_t> row(S.nv + 1, 0u);
@@ -3919,8 +3960,13 @@ static u26_status fp64_metrics(u26_scene* S, const float* d_x, u26_prp_output* o
 	U26_TRY(upload(ctx, d_hits, out->hits));
 	U26_CUDA(ctx, d_out.reserve(sizeof(Fp64Out) * in.size()));
 	const uint32_t nc = uint32_t(in.size());
-	fp64_metrics_kernel<<<div_up(nc * 32u, 128u), 128, 0, st>>>(nc, d_in.as<Fp64In>(), d_hits.as<u26_prp_hit>(), d_x, S->d_edges.as<uint2>(),
-		S->d_faces.as<uint32_t>(), S->d_varea.as<float>(), S->d_earea.as<float>(), S->d_farea.as<float>(), d_out.as<Fp64Out>());
+	const uint32_t nh = uint32_t(out->hits.size());
+	U26_CUDA(ctx, S->d_f64delta.reserve(sizeof(double) * nh));
+	fp64_depths_kernel<<<div_up(nh, 128u), 128, 0, st>>>(nc, d_in.as<Fp64In>(), nh, d_hits.as<u26_prp_hit>(), d_x, S->d_edges.as<uint2>(),
+		S->d_faces.as<uint32_t>(), S->d_f64delta.as<double>());
+	U26_TRY(after_launch(ctx, "fp64_depths_kernel"));
+	fp64_metrics_kernel<<<div_up(nc * 32u, 128u), 128, 0, st>>>(nc, d_in.as<Fp64In>(), d_hits.as<u26_prp_hit>(), S->d_f64delta.as<double>(),
+		S->d_varea.as<float>(), S->d_earea.as<float>(), S->d_farea.as<float>(), d_out.as<Fp64Out>());
 	U26_TRY(after_launch(ctx, "fp64_metrics_kernel"));
 	std::vector<Fp64Out> res;
 	U26_TRY(download(ctx, res, d_out.ptr, in.size()));
@@ -3946,10 +3992,19 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	cudaStream_t st = ctx->stream;
 	const auto t_total = std::chrono::steady_clock::now();
 	auto t0 = t_total;
+	// with U26_PRP_TRACE set: the host-side time line of the pass, printed at its end
+	const bool trace_marks = std::getenv("U26_PRP_TRACE") != nullptr;
+	std::vector<std::pair<const char*, double>> marks;
+	auto mark = [&](const char* what)
+	{
+		if (trace_marks)
+			marks.emplace_back(what, ms_since(t_total));
+	};
 	// ---- 1. host copies of positions and the canonical EF list
 	std::vector<float> x;
 	HostGraph G;
 	U26_TRY(download(ctx, x, d_x, 3 * size_t(S->nv)));
+	mark("positions downloaded");
 	U26_TRY(download(ctx, G.ef, d_pairs, num_pairs));
 	std::vector<uint32_t> idx;
 	U26_TRY(download(ctx, idx, d_idx, 2 * size_t(num_pairs)));
@@ -3974,7 +4029,9 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		G.ee[i] = idx[2 * i];
 		G.ff[i] = idx[2 * i + 1];
 	}
-	out->num_orig_pairs = build_graph(*S, x, G, P->ignore_near_zero_dist_pairs != 0);
+	mark("EF list downloaded, normals");
+	out->num_orig_pairs = build_graph(*S, x, G, P->ignore_near_zero_dist_pairs != 0, mark);
+	mark("EF graph, contours");
 	out->stage_ms[0] = ms_since(t0);
 	const uint32_t na = uint32_t(G.ef.size());
 	const uint32_t nc = uint32_t(G.contours.size());
@@ -4058,6 +4115,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		r.present.assign(nd, 0);
 		r.active.assign(nd, 1);
 	}
+	mark("runtimes, anchors, directions");
 	const uint32_t nslots = 2 * nact;
 	const uint32_t vs = std::max(1u, S->vmax_obj), es_ = std::max(1u, S->emax_obj), fs = std::max(1u, S->fmax_obj);
 	if (nact > 0)
@@ -4156,8 +4214,13 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		}
 		U26_CUDA(ctx, S->d_fgrow.reserve(sizeof(NodeBox) * std::max(foff[nobj], 1u)));
 		U26_CUDA(ctx, S->d_egrow.reserve(sizeof(NodeBox) * std::max(eoff[nobj], 1u)));
-		U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride));
-		U26_CUDA(ctx, cudaMemsetAsync(S->d_front.ptr, 0xFF, sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride, st));
+		// the split traversals' subtree roots depend on the trees' topology only: found once
+		const bool fronts = !S->fronts_built;
+		if (fronts)
+		{
+			U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride));
+			U26_CUDA(ctx, cudaMemsetAsync(S->d_front.ptr, 0xFF, sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride, st));
+		}
 		for (uint32_t o = 0; o < nobj; o++)
 			for (int kind = 0; kind < 2; kind++)
 			{
@@ -4173,10 +4236,14 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				grow_boxes_kernel<<<div_up(nn, 256), 256, 0, st>>>(tv.boxes, tv.children, tv.object_idx, nn, kind, node_off, prim_off,
 					(kind == 0 ? S->d_fgrow : S->d_egrow).as<NodeBox>());
 				U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
-				frontier_kernel<<<1, 32, 0, st>>>(tv.children, tv.object_idx, nn, node_off,
-					S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kFrontStride);
-				U26_TRY(after_launch(ctx, "frontier_kernel"));
+				if (fronts)
+				{
+					frontier_kernel<<<1, 32, 0, st>>>(tv.children, tv.object_idx, nn, node_off,
+						S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kFrontStride);
+					U26_TRY(after_launch(ctx, "frontier_kernel"));
+				}
 			}
+		S->fronts_built = true;
 	}
 	const uint32_t bnd_words = vs / 32 + 1;
 	if (nslots)
@@ -4548,8 +4615,13 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			U26_CUDA(ctx, cudaMemsetAsync(S->d_cov.ptr, 0, sizeof(uint32_t) * std::max(nh, 1u), st));
 			if (tab[nt] && ne_entries)
 			{
+				U26_CUDA(ctx, S->d_trange.reserve(sizeof(uint32_t) * 2 * size_t(nt)));
+				U26_CUDA(ctx, cudaMemsetAsync(S->d_trange.ptr, 0, sizeof(uint32_t) * 2 * size_t(nt), st));
+				uint32_t* tbeg = S->d_trange.as<uint32_t>();
+				entry_ranges_kernel<<<div_up(ne_entries, 256), 256, 0, st>>>(S->d_ekeys.as<uint64_t>(), ne_entries, 1 + vb + rb, tbeg, tbeg + nt);
+				U26_TRY(after_launch(ctx, "entry_ranges_kernel"));
 				coverage_count_kernel<<<div_up(tab[nt], 256), 256, 0, st>>>(S->d_tasks.as<Task>(), nt, S->d_tab.as<uint32_t>(),
-					S->d_anchor_off.as<uint32_t>(), S->d_anchors.as<uint32_t>(), S->d_ekeys.as<uint64_t>(), ne_entries, vb, rb,
+					S->d_anchor_off.as<uint32_t>(), S->d_anchors.as<uint32_t>(), S->d_ekeys.as<uint64_t>(), ne_entries, tbeg, tbeg + nt, vb, rb,
 					S->d_seg.as<uint32_t>(), S->d_cov.as<uint32_t>());
 				U26_TRY(after_launch(ctx, "coverage_count_kernel"));
 			}
@@ -4839,7 +4911,9 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	{
 		std::vector<uint32_t> all(nact);
 		std::iota(all.begin(), all.end(), 0u);
+		mark("distances, uploads, trees");
 		U26_TRY(run_levels(all));
+		mark("k-ring levels");
 	}
 	// ---- materialize: re-evaluate the listed (contour, direction) results once more with
 	// the supports gathered (the evaluation is deterministic, so these are the hits the
@@ -4898,6 +4972,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_TRY(materialize(cc));
 	}
 
+	mark("materialize");
 	// ---- S^2 direction refinement (prp_optimize_runtime_directions,
 	// intersection_resolver2.cpp:1371-1486): per iteration, the steps of all open contours
 	// in one launch, then every trial direction evaluated from the initial k-ring level in
@@ -5025,6 +5100,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		U26_TRY(materialize(cc));
 	}
 
+	mark("refinement");
 	// ---- 4. selection, merge capture, suppression, output
 	t0 = std::chrono::steady_clock::now();
 	std::vector<ComboState> chosen(nc);
@@ -5109,6 +5185,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		{
 			if (pre_area[a] != pre_area[bb]) return pre_area[a] > pre_area[bb];
 			return a < bb; });
+	mark("selection, merge adjacency");
 	std::vector<uint8_t> supp(nc, 0);
 	for (uint32_t o : conflicting)
 	{
@@ -5197,6 +5274,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->hit_offsets[c + 1] = out->hit_offsets[c] + rr.hit_count;
 		out->hits.insert(out->hits.end(), cs.hits.begin(), cs.hits.end());
 	}
+	mark("suppression, outputs");
 	std::vector<unsigned long long> stats;
 	U26_TRY(download(ctx, stats, S->d_stats.ptr, 16));
 	U26_CUDA(ctx, cudaMemcpyAsync(ctx->host_word, ctx->dev_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
@@ -5220,6 +5298,16 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		S->tuned_cfg = int(std::min_element(out->tune_ms, out->tune_ms + kNumRaycastConfigs) - out->tune_ms);
 	out->raycast_cfg = P->form != 0 ? -1 : forced ? cfg_now : S->tuned_cfg >= 0 ? S->tuned_cfg : kDefaultRaycastConfig;
 	out->tuned = tuning ? 1u : 0u;
+	mark("stats, FP64 metrics");
+	if (trace_marks)
+	{
+		double prev = 0.0;
+		for (const auto& [what, at] : marks)
+		{
+			fprintf(stderr, "[u26 prp] host %-32s %8.2f ms (+%.2f)\n", what, at, at - prev);
+			prev = at;
+		}
+	}
 	out->stage_ms[6] = ms_since(t0);
 	out->stage_ms[7] = ms_since(t_total);
 	if (out->dev_err & (U26_DEVERR_STACK_OVERFLOW | U26_DEVERR_ITERATION_CAP))
