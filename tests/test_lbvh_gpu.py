@@ -153,11 +153,11 @@ def test_capacity_truncation_reports_count(oracle, u26ctx):
     assert (pairs.cpu().numpy() != -7).all()
 
 
-@pytest.mark.parametrize("n_leaves", [511, 512, 513, 1025, 70000])
+@pytest.mark.parametrize("n_leaves", [511, 512, 513, 1023, 1024, 1025, 2049, 70000])
 def test_repeated_refits(oracle, u26ctx, n_leaves):
-    """Refit after refit at moving positions, fused and leaf-only: the block-local climb's
-    device arrival counters carry over between refits (2 per refit, never reset), every
-    refit's boxes equal the oracle's."""
+    """Refit after refit at moving positions, fused and leaf-only, around the 1024-leaf treelet
+    bound (one chunk, a top tree of one node, several chunks): the refit plan made at
+    construction serves every later refit, and every refit's boxes equal the oracle's."""
     rng = np.random.default_rng(n_leaves)
     x = rng.uniform(-1, 1, (n_leaves * 3, 3)).astype(np.float32)
     f = np.arange(n_leaves * 3, dtype=np.uint32).reshape(-1, 3)
@@ -173,5 +173,22 @@ def test_repeated_refits(oracle, u26ctx, n_leaves):
             t.refit()
         else:
             t.update_and_refit(dth, dxk, dxk, dprims)
+        assert t.check_health()
+        _assert_tree_equal(ot, t.arrays())
+
+
+@pytest.mark.parametrize("clusters", [1, 7])
+def test_refit_deep_tree(oracle, u26ctx, clusters):
+    """Triangles crowded into a few points share Morton codes, so the Karras tree splits on the
+    leaf index below them: long chains, treelets of every size, single-leaf treelets hanging off
+    top nodes. The refit (fused and leaf-only) still equals the oracle bit for bit."""
+    rng = np.random.default_rng(clusters)
+    n = 6000
+    centers = rng.uniform(-1, 1, (clusters, 3)).astype(np.float32)
+    which = rng.integers(0, clusters, n * 3)
+    x = (centers[which] + rng.normal(0, 1e-7, (n * 3, 3))).astype(np.float32)
+    m = Mesh(x, np.arange(n * 3, dtype=np.uint32).reshape(-1, 3))
+    for fused in (True, False):
+        ot, t, _ = _build_both(oracle, u26ctx, TREE_FACE, m, fused=fused)
         assert t.check_health()
         _assert_tree_equal(ot, t.arrays())
