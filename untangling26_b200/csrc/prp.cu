@@ -33,6 +33,8 @@
 #include <algorithm>
 #include <functional>
 #include <chrono>
+#include <condition_variable>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
@@ -43,6 +45,7 @@
 #include <set>
 #include <atomic>
 #include <thread>
+#include <unistd.h>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -3492,12 +3495,92 @@ namespace
 		std::vector<uint32_t> vflag_off, vflags;
 	};
 
-	// fn(i) for i in [0, n) over the host cores in static chunks; fn(i) writes only what i owns
+	// Host worker threads, started once per process and reused by every parallel loop of a
+	// pass (starting threads for each loop cost more than most loops do). One loop at a time:
+	// a caller holds run_mtx while its items are handed out; the calling thread works too.
+	class HostPool
+	{
+	public:
+		// never destroyed: the workers stay parked on their condition variable until the
+		// process ends (no join at exit, none in a forked child)
+		static HostPool& get()
+		{
+			static HostPool* pool = new HostPool();
+			return *pool;
+		}
+		uint32_t size() const { return uint32_t(workers_.size()) + 1u; }
+		// job(i) for every i in [0, n), items handed out one at a time
+		void run(uint32_t n, const std::function<void(uint32_t)>& job)
+		{
+			// a forked child has none of the workers: it runs the loop itself
+			if (workers_.empty() || n <= 1 || getpid() != pid_)
+			{
+				for (uint32_t i = 0; i < n; i++)
+					job(i);
+				return;
+			}
+			std::lock_guard<std::mutex> one(run_mtx_);
+			{
+				std::lock_guard<std::mutex> lk(mtx_);
+				job_ = &job;
+				n_ = n;
+				next_.store(0u);
+				busy_ = uint32_t(workers_.size());
+				gen_++;
+			}
+			cv_.notify_all();
+			work();
+			std::unique_lock<std::mutex> lk(mtx_);
+			done_cv_.wait(lk, [&] { return busy_ == 0; });
+			job_ = nullptr;
+		}
+
+	private:
+		HostPool() : pid_(getpid())
+		{
+			const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+			for (uint32_t t = 1; t < hw; t++)
+				workers_.emplace_back([this] { loop(); });
+		}
+		void work()
+		{
+			for (uint32_t i = next_.fetch_add(1u); i < n_; i = next_.fetch_add(1u))
+				(*job_)(i);
+		}
+		void loop()
+		{
+			uint64_t seen = 0;
+			for (;;)
+			{
+				{
+					std::unique_lock<std::mutex> lk(mtx_);
+					cv_.wait(lk, [&] { return gen_ != seen; });
+					seen = gen_;
+				}
+				work();
+				{
+					std::lock_guard<std::mutex> lk(mtx_);
+					busy_--;
+				}
+				done_cv_.notify_one();
+			}
+		}
+		pid_t pid_;
+		std::vector<std::thread> workers_;
+		std::mutex run_mtx_, mtx_;
+		std::condition_variable cv_, done_cv_;
+		const std::function<void(uint32_t)>* job_ = nullptr;
+		uint32_t n_ = 0, busy_ = 0;
+		uint64_t gen_ = 0;
+		std::atomic<uint32_t> next_{ 0u };
+	};
+
+	// fn(i) for i in [0, n) over the host cores in contiguous chunks; fn(i) writes only what i owns
 	template <typename F>
 	void host_parallel_for(uint32_t n, F&& fn)
 	{
-		const uint32_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-		const uint32_t nt = n < 8192 ? 1u : hw;
+		HostPool& pool = HostPool::get();
+		const uint32_t nt = n < 8192 ? 1u : pool.size();
 		if (nt == 1)
 		{
 			for (uint32_t i = 0; i < n; i++)
@@ -3505,15 +3588,11 @@ namespace
 			return;
 		}
 		const uint32_t chunk = (n + nt - 1) / nt;
-		std::vector<std::thread> th;
-		for (uint32_t t = 0; t < nt; t++)
-			th.emplace_back([&, t]()
-				{
-					const uint32_t e = std::min(n, (t + 1) * chunk);
-					for (uint32_t i = t * chunk; i < e; i++)
-						fn(i); });
-		for (auto& h : th)
-			h.join();
+		pool.run(nt, [&](uint32_t t)
+			{
+				const uint32_t e = std::min(n, (t + 1) * chunk);
+				for (uint32_t i = t * chunk; i < e; i++)
+					fn(i); });
 	}
 
 	// fn(i) for i in [0, n) over the host cores, items handed out one at a time (for few,
@@ -3521,22 +3600,7 @@ namespace
 	template <typename F>
 	void host_parallel_dynamic(uint32_t n, F&& fn)
 	{
-		const uint32_t nt = std::min(n, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-		if (nt <= 1)
-		{
-			for (uint32_t i = 0; i < n; i++)
-				fn(i);
-			return;
-		}
-		std::atomic<uint32_t> next{ 0u };
-		std::vector<std::thread> th;
-		for (uint32_t t = 0; t < nt; t++)
-			th.emplace_back([&]()
-				{
-					for (uint32_t i = next.fetch_add(1u); i < n; i = next.fetch_add(1u))
-						fn(i); });
-		for (auto& h : th)
-			h.join();
+		HostPool::get().run(n, [&](uint32_t i) { fn(i); });
 	}
 
 	// returns the EF pair count after the degenerate filter (before loop-vertex pairs)
@@ -3544,20 +3608,16 @@ namespace
 		const std::function<void(const char*)>& mark)
 	{
 		uint32_t n = uint32_t(G.ef.size());
-		// the canonical EF list is sorted by edge: each edge's pairs form one run
-		std::vector<uint32_t> run(S.ne + 1, 0u);
+		// the canonical EF list is sorted by edge: each edge's pairs form one run, found by
+		// binary search (no table over all of the mesh's edges)
 		auto edge_run = [&](uint32_t e, uint32_t& b, uint32_t& t)
 		{
-			b = run[e];
-			t = run[e + 1];
+			const auto r = std::equal_range(G.ee.begin(), G.ee.begin() + n, e);
+			b = uint32_t(r.first - G.ee.begin());
+			t = uint32_t(r.second - G.ee.begin());
 		};
 		auto build_adj = [&]()
 		{
-		std::fill(run.begin(), run.end(), 0u);
-		for (uint32_t p = 0; p < n; p++)
-			run[G.ee[p] + 1]++;
-		for (uint32_t e = 0; e < S.ne; e++)
-			run[e + 1] += run[e];
 		G.adj.assign(n, {});
 		host_parallel_for(n, [&](uint32_t p)
 		{
@@ -4045,12 +4105,26 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	const uint32_t nscene = S->oscene.empty() ? 1u : *std::max_element(S->oscene.begin(), S->oscene.end()) + 1u;
 	std::vector<V3h> gcs(nscene, mkv(0, 0, 0));
 	std::vector<float> tms(nscene, 0.0f);
-	for (uint32_t v = 0; v < S->nv; v++)
 	{
-		const uint32_t sc = S->oscene[S->vobj[v]];
-		const float w = std::fmax(S->varea[v], 1e-8f);
-		gcs[sc] = gcs[sc] + mkv(x[3 * v], x[3 * v + 1], x[3 * v + 2]) * w;
-		tms[sc] += w;
+		// each scene's sums run over its vertices in vertex order (its objects' contiguous
+		// ranges, in object order); the scenes in parallel
+		std::vector<std::vector<uint32_t>> objs(nscene);
+		for (uint32_t o = 0; o < S->nobj; o++)
+			objs[S->oscene.empty() ? 0u : S->oscene[o]].push_back(o);
+		host_parallel_dynamic(nscene, [&](uint32_t sc)
+		{
+			V3h g = mkv(0, 0, 0);
+			float tm = 0.0f;
+			for (uint32_t o : objs[sc])
+				for (uint32_t v = S->pv[o]; v < S->pv[o + 1]; v++)
+				{
+					const float w = std::fmax(S->varea[v], 1e-8f);
+					g = g + mkv(x[3 * v], x[3 * v + 1], x[3 * v + 2]) * w;
+					tm += w;
+				}
+			gcs[sc] = g;
+			tms[sc] = tm;
+		});
 	}
 	for (uint32_t sc = 0; sc < nscene; sc++)
 		if (tms[sc] > 1e-8f)
@@ -5106,8 +5180,6 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	std::vector<ComboState> chosen(nc);
 	std::vector<std::vector<uint32_t>> merge(nc);
 	std::vector<float> pre_area(nc, 0.0f);
-	auto flags_of = [&](uint32_t v)
-	{ return std::vector<uint32_t>(G.vflags.begin() + G.vflag_off[v], G.vflags.begin() + G.vflag_off[v + 1]); };
 	// per contour (independent: each writes its own chosen / pre_area / merge entry)
 	host_parallel_dynamic(nact, [&](uint32_t c)
 	{
@@ -5119,6 +5191,25 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		std::set<uint32_t> adjc;
 		auto flagged = [&](uint32_t v)
 		{ return v == kInfH || G.vflag_off[v + 1] > G.vflag_off[v]; };
+		// the boundary flags common to every listed vertex (sorted unique flag lists, intersected
+		// in place of copies), without this contour's own two
+		auto common = [&](const uint32_t* vs, int nvs, std::vector<uint32_t>& out)
+		{
+			out.clear();
+			const uint32_t* b0 = G.vflags.data() + G.vflag_off[vs[0]];
+			const uint32_t* e0 = G.vflags.data() + G.vflag_off[vs[0] + 1];
+			for (const uint32_t* f = b0; f < e0; f++)
+			{
+				if (*f == 2 * c || *f == 2 * c + 1)
+					continue;
+				bool all = true;
+				for (int j = 1; j < nvs && all; j++)
+					all = std::binary_search(G.vflags.data() + G.vflag_off[vs[j]], G.vflags.data() + G.vflag_off[vs[j] + 1], *f);
+				if (all)
+					out.push_back(*f);
+			}
+		};
+		std::vector<uint32_t> sf, df;
 		for (const u26_prp_hit& h : chosen[c].hits)
 		{
 			// a hit links contours only through vertices that all carry boundary flags
@@ -5127,30 +5218,17 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				any_empty = any_empty || !flagged(h.src_verts[k]) || !flagged(h.dst_verts[k]);
 			if (any_empty)
 				continue;
-			std::vector<uint32_t> sv, dv;
+			uint32_t sv[3], dv[3];
+			int ns = 0, nd = 0;
 			for (int k = 0; k < 3; k++)
 			{
 				if (h.src_verts[k] != kInfH)
-					sv.push_back(h.src_verts[k]);
+					sv[ns++] = h.src_verts[k];
 				if (h.dst_verts[k] != kInfH)
-					dv.push_back(h.dst_verts[k]);
+					dv[nd++] = h.dst_verts[k];
 			}
-			auto common = [&](const std::vector<uint32_t>& vs_)
-			{
-				std::vector<uint32_t> acc = flags_of(vs_.front());
-				for (uint32_t v : vs_)
-				{
-					const auto fl = flags_of(v);
-					std::vector<uint32_t> tt;
-					std::set_intersection(fl.begin(), fl.end(), acc.begin(), acc.end(), std::back_inserter(tt));
-					acc.swap(tt);
-				}
-				std::vector<uint32_t> tt;
-				const uint32_t rm[2] = { 2 * c, 2 * c + 1 };
-				std::set_difference(acc.begin(), acc.end(), rm, rm + 2, std::back_inserter(tt));
-				return tt;
-			};
-			const auto sf = common(sv), df = common(dv);
+			common(sv, ns, sf);
+			common(dv, nd, df);
 			for (uint32_t a : sf)
 				for (uint32_t bb : df)
 					if (a == (bb ^ 1u))
