@@ -148,6 +148,7 @@ class Workload:
         self.name = name
         self.batch = name.startswith("batch")
         self.repair = False
+        self.repair_scale = 1.0
         self.params = dict(max_contours=ALL_CONTOURS, batch_size=ALL_CONTOURS)
         # single-mesh workloads: the contours the CPU legs evaluate (None: every 8th)
         self.oracle_contours = None
@@ -194,12 +195,16 @@ class Workload:
             # workload's tuned one (tuning here would run 18 full ray-casting passes)
             self.params = dict(max_contours=32, batch_size=32, autotune=0, raycast_config=2)
             self.repair = True
+            # the fixed step: a quarter of the assembled response, so that no vertex moves more
+            # than 0.375 mm (a pair asks for up to the 3 mm response depth, half per side) between
+            # sheets 1 mm apart
+            self.repair_scale = 0.25
             # the oracle needs 3-30 s for most contours of this mesh and minutes for the largest
             # regions (contour 0): the CPU legs evaluate contours 1, 3 and 5
             self.oracle_contours = (1, 3, 5)
             self.config = {"workload": "layered_sheets_5x512x512", "seed": 4, "layers": 5, "triangles": int(self.full.num_faces),
                            "spacing_mm": 1, "displacement_mm": "U[2, 20] multi-octave", "directions": "reference seeds (<=10)",
-                           "opt_iterations": 0, "contours": "first 32 of each pass (one batch)", "update": "response step, scale 1",
+                           "opt_iterations": 0, "contours": "first 32 of each pass (one batch)", "update": "response step, scale 0.25",
                            "raycast_config": "fixed 4x7"}
         else:
             raise SystemExit(f"unknown workload {name}")
@@ -359,7 +364,7 @@ class PassRunner:
         self.sc.close()
 
 
-def _timed_passes(runner, steps, flush, stream, repair=False):
+def _timed_passes(runner, steps, flush, stream, repair=False, scale=1.0):
     """K timed passes; with repair, each pass is followed (inside its timed step) by the fixed
     step along its assembled response, so the passes form the repair sequence."""
     import torch
@@ -370,7 +375,7 @@ def _timed_passes(runner, steps, flush, stream, repair=False):
         ev[i][0].record(stream)
         res = runner.run()
         if repair:
-            runner.sc.response_step(res.response, 1.0)
+            runner.sc.response_step(res.response, scale)
         out.append(res)
         ev[i][1].record(stream)
     torch.cuda.synchronize()
@@ -517,7 +522,7 @@ def main():
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    step_ms, results = _timed_passes(runner, args.steps, flush, stream, repair=wl.repair)
+    step_ms, results = _timed_passes(runner, args.steps, flush, stream, repair=wl.repair, scale=wl.repair_scale)
     if ws > 1:
         dist.barrier()
     clk = clocks.stop()
