@@ -3512,14 +3512,16 @@ namespace
 		// job(i) for every i in [0, n), items handed out one at a time
 		void run(uint32_t n, const std::function<void(uint32_t)>& job)
 		{
-			// a forked child has none of the workers: it runs the loop itself
-			if (workers_.empty() || n <= 1 || getpid() != pid_)
+			// a forked child has none of the workers, and a loop started inside a pool job would
+			// wait for itself: both run the loop in the calling thread
+			if (workers_.empty() || n <= 1 || getpid() != pid_ || in_job())
 			{
 				for (uint32_t i = 0; i < n; i++)
 					job(i);
 				return;
 			}
 			std::lock_guard<std::mutex> one(run_mtx_);
+			InJob mark;
 			{
 				std::lock_guard<std::mutex> lk(mtx_);
 				job_ = &job;
@@ -3547,8 +3549,19 @@ namespace
 			for (uint32_t i = next_.fetch_add(1u); i < n_; i = next_.fetch_add(1u))
 				(*job_)(i);
 		}
+		static bool& in_job()
+		{
+			thread_local bool flag = false;
+			return flag;
+		}
+		struct InJob
+		{
+			InJob() { in_job() = true; }
+			~InJob() { in_job() = false; }
+		};
 		void loop()
 		{
+			in_job() = true;
 			uint64_t seen = 0;
 			for (;;)
 			{
@@ -4129,6 +4142,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	for (uint32_t sc = 0; sc < nscene; sc++)
 		if (tms[sc] > 1e-8f)
 			gcs[sc] = gcs[sc] / tms[sc];
+	mark("  scene centroids");
 	std::vector<uint32_t> anchor_off(nact + 1, 0u), anchors, bnd;
 	std::vector<Slot> slots(2 * size_t(nact));
 	for (uint32_t c = 0; c < nact; c++)
@@ -4180,16 +4194,25 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			sl.pad[1] = o; // the side's object: its ray-casting trees
 			bnd.insert(bnd.end(), b[sd].begin(), b[sd].end());
 		}
-		const uint32_t rsc = S->oscene[r.obj[0]];
-		r.dirs = directions(*S, x, G, r, P->direction_mode, gcs[rsc], tms[rsc] > 1e-8f);
-		const size_t nd = r.dirs.size();
-		r.res.assign(nd, ComboState{});
-		r.conv.assign(nd, 0);
-		r.pruned.assign(nd, 0);
-		r.present.assign(nd, 0);
-		r.active.assign(nd, 1);
 	}
-	mark("runtimes, anchors, directions");
+	// candidate directions of each contour (host, in parallel), while the GPU computes the
+	// slots' distances below
+	auto contour_directions = [&]()
+	{
+		host_parallel_dynamic(nact, [&](uint32_t c)
+		{
+			ContourRT& r = R[c];
+			const uint32_t rsc = S->oscene[r.obj[0]];
+			r.dirs = directions(*S, x, G, r, P->direction_mode, gcs[rsc], tms[rsc] > 1e-8f);
+			const size_t nd = r.dirs.size();
+			r.res.assign(nd, ComboState{});
+			r.conv.assign(nd, 0);
+			r.pruned.assign(nd, 0);
+			r.present.assign(nd, 0);
+			r.active.assign(nd, 1);
+		});
+	};
+	mark("runtimes, anchors");
 	const uint32_t nslots = 2 * nact;
 	const uint32_t vs = std::max(1u, S->vmax_obj), es_ = std::max(1u, S->emax_obj), fs = std::max(1u, S->fmax_obj);
 	if (nact > 0)
@@ -4222,6 +4245,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			S->d_geo.as<float>(), S->d_order.as<uint32_t>(), S->d_level_end.as<uint32_t>(), S->d_work.as<uint32_t>(),
 			S->d_mark.as<uint32_t>(), ctx->dev_err);
 		U26_TRY(after_launch(ctx, "distances_kernel"));
+		contour_directions();
+		mark("directions (beside the distances)");
 		U26_TRY(download(ctx, slots, S->d_slots.ptr, nslots));
 		U26_CUDA(ctx, cudaStreamSynchronize(st));
 	}
