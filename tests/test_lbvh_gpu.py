@@ -153,7 +153,7 @@ def test_capacity_truncation_reports_count(oracle, u26ctx):
     assert (pairs.cpu().numpy() != -7).all()
 
 
-@pytest.mark.parametrize("n_leaves", [511, 512, 513, 1023, 1024, 1025, 2049, 70000])
+@pytest.mark.parametrize("n_leaves", [2, 3, 33, 511, 512, 513, 1023, 1024, 1025, 2049, 70000])
 def test_repeated_refits(oracle, u26ctx, n_leaves):
     """Refit after refit at moving positions, fused and leaf-only, around the 1024-leaf treelet
     bound (one chunk, a top tree of one node, several chunks): the refit plan made at
