@@ -194,27 +194,35 @@ namespace u26
 		}
 		if (band.fail)
 			return; // certainly separated: the remaining conditions cannot change the outcome
+		// the remaining conditions in turn, each numerator computed when it is needed and an
+		// early return once one certainly fails (the common case: a miss): a failed condition
+		// decides the band whatever the others give, so the result is the full band's
 		const f3 e2v = q1 - q0;
 		const f3 rr = q0 - p0;
 		const f3 n = cross(e1, e2v);
 		const float det = -dot(dir, n);
-		const float n_sv = -dot(rr, n);
-		const float n_t1 = -dot(dir, cross(rr, e2v));
-		const float n_t2 = dot(dir, cross(e1, rr));
-		const float s1 = norm1(e1), s2 = norm1(e2v), sr = norm1(rr), sd = norm_inf(dir);
+		const float s1 = norm1(e1), s2 = norm1(e2v), sd = norm_inf(dir);
 		const float e_det = kBandGamma * ((sd * s1) * s2);
-		const float e_sv = kBandGamma * ((norm_inf(rr) * s1) * s2);
-		const float e_t1 = kBandGamma * ((sd * sr) * s2);
-		const float e_t2 = kBandGamma * ((sd * s1) * sr);
 		const float s = det >= 0.0f ? 1.0f : -1.0f;
 		const float ad = fabsf(det);
-		band.add(ad - 1e-10f, e_det);									 // |det| >= 1e-10
-		band.add(n_sv * s, e_sv);										 // s >= 0
-		band.add(ray_max * ad - n_sv * s, e_sv + ray_max * e_det);		 // s <= ray_max
-		band.add(n_t1 * s, e_t1);										 // t1 >= 0
-		band.add(ad - n_t1 * s, e_t1 + e_det);							 // t1 <= 1
-		band.add(n_t2 * s, e_t2);										 // t2 >= 0
-		band.add(ad - n_t2 * s, e_t2 + e_det);							 // t2 <= 1
+		band.add(ad - 1e-10f, e_det); // |det| >= 1e-10
+		const float n_sv = -dot(rr, n);
+		const float e_sv = kBandGamma * ((norm_inf(rr) * s1) * s2);
+		band.add(n_sv * s, e_sv);								// s >= 0
+		band.add(ray_max * ad - n_sv * s, e_sv + ray_max * e_det); // s <= ray_max
+		if (band.fail)
+			return;
+		const float sr = norm1(rr);
+		const float n_t1 = -dot(dir, cross(rr, e2v));
+		const float e_t1 = kBandGamma * ((sd * sr) * s2);
+		band.add(n_t1 * s, e_t1);			 // t1 >= 0
+		band.add(ad - n_t1 * s, e_t1 + e_det); // t1 <= 1
+		if (band.fail)
+			return;
+		const float n_t2 = dot(dir, cross(e1, rr));
+		const float e_t2 = kBandGamma * ((sd * s1) * sr);
+		band.add(n_t2 * s, e_t2);			 // t2 >= 0
+		band.add(ad - n_t2 * s, e_t2 + e_det); // t2 <= 1
 	}
 
 	// The swept edge - edge test in FP64 (same steps as the FP32 test).

@@ -1207,22 +1207,27 @@ namespace u26
 										const float det = -dot(dir, n);
 										if (!(fabsf(det) < 1e-10f))
 										{
-											const float d_r_e1_e2 = dot(rr, cross(e1, e2v));
-											const float d_dir_r_e2 = dot(dir, cross(rr, e2v));
-											const float d_dir_e1_r = dot(dir, cross(e1, rr));
-											const float n_sv = -d_r_e1_e2, n_t1 = -d_dir_r_e2, n_t2 = d_dir_e1_r; // x = n_x / det
-											// misses decided before the division, only where the test below rejects too:
-											// a numerator (|n| >= 1e-20, so n / det stays nonzero) of the other sign than
-											// det, or t1, t2 beyond 1 / sv beyond ray_max by a 1e-5 relative margin
+											// x = n_x / det. Misses decided before the division, only where the test
+											// below rejects too: a numerator (|n| >= 1e-20, so n / det stays nonzero) of
+											// the other sign than det, or t1, t2 beyond 1 / sv beyond ray_max by a 1e-5
+											// relative margin; each numerator is computed once the earlier ones pass
+											const float n_sv = -dot(rr, cross(e1, e2v));
 											const float adet = fabsf(det);
-											bool maybe = true;
-											if (adet <= 1e20f)
+											const bool screen = adet <= 1e20f;
+											auto neg = [&](float v)
+											{ return fabsf(v) >= 1e-20f && ((v > 0.0f) != (det > 0.0f)); };
+											const float lim = adet * (1.0f + 1e-5f);
+											bool maybe = !(screen && (neg(n_sv) || (ray_max >= 1e-20f && fabsf(n_sv) > lim * ray_max)));
+											float n_t1 = 0.0f, n_t2 = 0.0f;
+											if (maybe)
 											{
-												auto neg = [&](float v)
-												{ return fabsf(v) >= 1e-20f && ((v > 0.0f) != (det > 0.0f)); };
-												const float lim = adet * (1.0f + 1e-5f);
-												maybe = !(neg(n_sv) || neg(n_t1) || neg(n_t2) || fabsf(n_t1) > lim || fabsf(n_t2) > lim ||
-													(ray_max >= 1e-20f && fabsf(n_sv) > lim * ray_max));
+												n_t1 = -dot(dir, cross(rr, e2v));
+												maybe = !(screen && (neg(n_t1) || fabsf(n_t1) > lim));
+											}
+											if (maybe)
+											{
+												n_t2 = dot(dir, cross(e1, rr));
+												maybe = !(screen && (neg(n_t2) || fabsf(n_t2) > lim));
 											}
 											if (maybe)
 											{
