@@ -34,6 +34,10 @@ roofline = raycast_kernel (the dominant kernel, profiles/launch_list_*): the DRA
          time) against 4 warp instructions per SM cycle at the sampled clock.
 cpu_baseline = the CPU oracle of the same 16 scenes on the host cores (all threads).
 
+--profile-pass / --profile-refit run one pass / one face-tree refit of the workload between
+cudaProfilerStart and cudaProfilerStop for `ncu --profile-from-start off` (profiles/ names the
+commands); --raycast-config fixes the traversal configuration instead of the autotuner's choice.
+
 --impl reference times the reference's algorithm on the host cores: the reference cannot
 be built here (its LuisaCompute runtime is not in the checkout), so the CPU restatement
 (the oracle) runs with all host threads over the same scenes.
@@ -669,6 +673,7 @@ def main():
                      "contours": len(r0.contours), "levels": r0.levels, "requests": r0.requests, "leaf_tests": r0.tested,
                      "candidate_leaf_tests": r0.candidate_tests, "ray_node_visits": r0.ray_visits,
                      "request_candidate_pairs": r0.pairs_tested, "response_pairs": r0.response.num_pairs,
+                     "response_ms": round(r0.response.ms, 2),
                      "gpu_ms": {k: round(v, 2) for k, v in r0.gpu_ms.items()},
                      "stage_ms": {k: round(v, 2) for k, v in r0.stage_ms.items()}},
             "parity": parity,

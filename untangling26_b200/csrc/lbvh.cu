@@ -1056,6 +1056,9 @@ static u26_status refit_plan(u26_lbvh* t)
 		(const void*)refit_chunk_kernel<U26_TREE_FACE, false>, (const void*)refit_chunk_kernel<U26_TREE_FACE, true> };
 	for (const void* k : chunk_kernels)
 		U26_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChunkSmem)));
+	// the lists and the compact map (about 40 B per leaf) are needed at construction only; the
+	// stream is idle here (synchronised above)
+	t->plan_scratch.release();
 	return U26_OK;
 }
 

@@ -28,7 +28,7 @@ struct u26_lbvh
 	u26::DevBuf chunk_tb;		 // uint32[nchunks + 1]: first treelet of each chunk, then nt
 	u26::DevBuf top_height;		 // uint8[m]: heights of top_nodes
 	u26::DevBuf root_box;		 // float[nt][6]: the treelet roots' boxes of the last refit, compact
-	u26::DevBuf plan_scratch;	 // construction scratch: list keys, counts, compact map
+	u26::DevBuf plan_scratch;	 // construction scratch (list keys, counts, compact map), freed when the plan is made
 	uint32_t nchunks = 0, ntop = 0, ntreelets = 0;
 	bool top_in_shared = false;
 	u26::DevBuf leaf_prims;			 // uint32[n][K]: the primitive table in leaf order (edge / face trees)
