@@ -3259,6 +3259,13 @@ struct u26_scene
 	std::vector<uint8_t> vsolid; // per vertex: its object is rigid / tetrahedral
 	bool any_solid = false;
 	std::vector<u26_lbvh*> otree_f, otree_e; // per-object ray-casting trees (built at the first pass)
+	// the per-pass refit + grow of those trees as one CUDA graph, captured at the second pass
+	// for the positions pointer forest_x and replayed while it stays the same
+	cudaStream_t forest_stream = nullptr;
+	cudaGraphExec_t forest_exec = nullptr;
+	const float* forest_x = nullptr;
+	uint64_t forest_launches = 0;
+	bool forest_graph_failed = false;
 	bool otrees_built = false, fronts_built = false;
 	uint32_t vmax_obj = 0, emax_obj = 0, fmax_obj = 0;
 	uint32_t hit_cap = 0, e_cap = 0; // capacities that survive between passes
@@ -3473,6 +3480,10 @@ U26_API void u26_scene_destroy(u26_scene* s)
 	s->csorter.release();
 	s->fvsorter.release();
 	s->resp.release();
+	if (s->forest_exec)
+		cudaGraphExecDestroy(s->forest_exec);
+	if (s->forest_stream)
+		cudaStreamDestroy(s->forest_stream);
 	if (s->cap_host)
 		cudaFreeHost(s->cap_host);
 	for (u26_lbvh* t : s->otree_f)
@@ -4325,28 +4336,88 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			U26_CUDA(ctx, S->d_front.reserve(sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride));
 			U26_CUDA(ctx, cudaMemsetAsync(S->d_front.ptr, 0xFF, sizeof(uint32_t) * 2 * size_t(nobj) * kFrontStride, st));
 		}
-		for (uint32_t o = 0; o < nobj; o++)
-			for (int kind = 0; kind < 2; kind++)
-			{
-				u26_lbvh* t = (kind == 0 ? S->otree_f : S->otree_e)[o];
-				if (!t)
-					continue;
-				const uint32_t* prims = kind == 0 ? S->d_faces.as<uint32_t>() + 3 * size_t(S->pf[o]) : S->d_edges.as<uint32_t>() + 2 * size_t(S->pe[o]);
-				U26_TRY(u26_lbvh_update_and_refit(t, S->d_zero_th.as<float>(), d_x, d_x, prims));
-				const TreeView tv = tree_view(t);
-				const uint32_t nn = t->num_nodes();
-				const uint32_t node_off = kind == 0 ? foff[o] : eoff[o];
-				const uint32_t prim_off = kind == 0 ? S->pf[o] : S->pe[o];
-				grow_boxes_kernel<<<div_up(nn, 256), 256, 0, st>>>(tv.boxes, tv.children, tv.object_idx, nn, kind, node_off, prim_off,
-					(kind == 0 ? S->d_fgrow : S->d_egrow).as<NodeBox>());
-				U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
-				if (fronts)
+		// refit + grow of every object tree on stream `on` (and the frontiers when asked)
+		auto forest_pass = [&](cudaStream_t on, bool with_fronts) -> u26_status
+		{
+			for (uint32_t o = 0; o < nobj; o++)
+				for (int kind = 0; kind < 2; kind++)
 				{
-					frontier_kernel<<<1, 32, 0, st>>>(tv.children, tv.object_idx, nn, node_off,
-						S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kFrontStride);
-					U26_TRY(after_launch(ctx, "frontier_kernel"));
+					u26_lbvh* t = (kind == 0 ? S->otree_f : S->otree_e)[o];
+					if (!t)
+						continue;
+					const uint32_t* prims = kind == 0 ? S->d_faces.as<uint32_t>() + 3 * size_t(S->pf[o]) : S->d_edges.as<uint32_t>() + 2 * size_t(S->pe[o]);
+					U26_TRY(u26_lbvh_update_and_refit(t, S->d_zero_th.as<float>(), d_x, d_x, prims));
+					const TreeView tv = tree_view(t);
+					const uint32_t nn = t->num_nodes();
+					const uint32_t node_off = kind == 0 ? foff[o] : eoff[o];
+					const uint32_t prim_off = kind == 0 ? S->pf[o] : S->pe[o];
+					grow_boxes_kernel<<<div_up(nn, 256), 256, 0, on>>>(tv.boxes, tv.children, tv.object_idx, nn, kind, node_off, prim_off,
+						(kind == 0 ? S->d_fgrow : S->d_egrow).as<NodeBox>());
+					U26_TRY(after_launch(ctx, "grow_boxes_kernel"));
+					if (with_fronts)
+					{
+						frontier_kernel<<<1, 32, 0, on>>>(tv.children, tv.object_idx, nn, node_off,
+							S->d_front.as<uint32_t>() + (size_t(kind) * nobj + o) * kFrontStride);
+						U26_TRY(after_launch(ctx, "frontier_kernel"));
+					}
 				}
+			return U26_OK;
+		};
+		if (fronts)
+			U26_TRY(forest_pass(st, true)); // first pass: trees just built, frontiers found
+		else
+		{
+			if (S->forest_exec && S->forest_x != d_x)
+			{
+				cudaGraphExecDestroy(S->forest_exec);
+				S->forest_exec = nullptr;
 			}
+			if (!S->forest_exec && !S->forest_graph_failed)
+			{
+				// capture the launches on a private stream (the context's may be the legacy
+				// default stream, which cannot be captured); the library's launches follow the
+				// context's stream, so it points at the capture stream meanwhile
+				if (!S->forest_stream)
+					U26_CUDA(ctx, cudaStreamCreateWithFlags(&S->forest_stream, cudaStreamNonBlocking));
+				const uint64_t l0 = ctx->launches;
+				cudaStream_t orig = ctx->stream;
+				cudaGraph_t graph = nullptr;
+				cudaError_t ce = cudaStreamBeginCapture(S->forest_stream, cudaStreamCaptureModeThreadLocal);
+				u26_status fs = U26_ERR_CUDA;
+				if (ce == cudaSuccess)
+				{
+					ctx->stream = S->forest_stream;
+					fs = forest_pass(S->forest_stream, false);
+					ctx->stream = orig;
+					ce = cudaStreamEndCapture(S->forest_stream, &graph);
+				}
+				if (fs == U26_OK && ce == cudaSuccess && graph)
+					ce = cudaGraphInstantiate(&S->forest_exec, graph, 0);
+				if (graph)
+					cudaGraphDestroy(graph);
+				if (fs != U26_OK || ce != cudaSuccess || !S->forest_exec)
+				{
+					// not capturable here: direct launches from now on
+					cudaGetLastError();
+					S->forest_exec = nullptr;
+					S->forest_graph_failed = true;
+					ctx->last_error.clear();
+				}
+				else
+				{
+					S->forest_launches = ctx->launches - l0;
+					S->forest_x = d_x;
+				}
+				ctx->launches = l0;
+			}
+			if (S->forest_exec)
+			{
+				U26_CUDA(ctx, cudaGraphLaunch(S->forest_exec, st));
+				ctx->launches += S->forest_launches; // the graph's kernels, as launches of this pass
+			}
+			else
+				U26_TRY(forest_pass(st, false));
+		}
 		S->fronts_built = true;
 	}
 	const uint32_t bnd_words = vs / 32 + 1;
