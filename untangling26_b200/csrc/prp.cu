@@ -4161,7 +4161,11 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	mark("  scene centroids");
 	std::vector<uint32_t> anchor_off(nact + 1, 0u), anchors, bnd;
 	std::vector<Slot> slots(2 * size_t(nact));
-	for (uint32_t c = 0; c < nact; c++)
+	// per contour (in parallel): objects, the restriction switch, the two sides' boundary vertices
+	// (sorted unique) and the EF anchors; then the slots and the flat lists in contour order
+	std::vector<uint8_t> ccr(nact, 0);
+	std::vector<std::vector<uint32_t>> anch(nact);
+	host_parallel_dynamic(nact, [&](uint32_t c)
 	{
 		ContourRT& r = R[c];
 		r.contour = c;
@@ -4178,7 +4182,10 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			ccr_on = r.obj[0] != kInfH && r.obj[1] != kInfH;
 		else if (ccr_on)
 			ccr_on = r.obj[0] == r.obj[1] && comp[0] != kInfH && comp[0] == comp[1];
+		ccr[c] = ccr_on ? 1 : 0;
 		std::vector<uint32_t> b[2];
+		std::vector<uint32_t>& an = anch[c];
+		an.reserve(6 * G.contours[c].size());
 		for (uint32_t p : G.contours[c])
 		{
 			const uint32_t mi = G.mesh_index[p];
@@ -4186,14 +4193,22 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			b[mi].push_back(G.ef[p].idx[1]);
 			for (int k = 2; k < 5; k++)
 				b[mi ^ 1].push_back(G.ef[p].idx[k]);
-			anchors.insert(anchors.end(), { mi, G.ef[p].idx[0], G.ef[p].idx[1], G.ef[p].idx[2], G.ef[p].idx[3], G.ef[p].idx[4] });
+			an.insert(an.end(), { mi, G.ef[p].idx[0], G.ef[p].idx[1], G.ef[p].idx[2], G.ef[p].idx[3], G.ef[p].idx[4] });
 		}
-		anchor_off[c + 1] = uint32_t(anchors.size() / 6);
 		for (int sd = 0; sd < 2; sd++)
 		{
 			std::sort(b[sd].begin(), b[sd].end());
 			b[sd].erase(std::unique(b[sd].begin(), b[sd].end()), b[sd].end());
-			r.bnd[sd] = b[sd];
+			r.bnd[sd] = std::move(b[sd]);
+		}
+	});
+	for (uint32_t c = 0; c < nact; c++)
+	{
+		const ContourRT& r = R[c];
+		anchors.insert(anchors.end(), anch[c].begin(), anch[c].end());
+		anchor_off[c + 1] = uint32_t(anchors.size() / 6);
+		for (int sd = 0; sd < 2; sd++)
+		{
 			Slot& sl = slots[2 * c + sd];
 			const uint32_t o = r.obj[sd];
 			sl.v_lo = S->pv[o];
@@ -4203,12 +4218,12 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			sl.f_lo = S->pf[o];
 			sl.f_cnt = S->pf[o + 1] - S->pf[o];
 			sl.bnd_off = uint32_t(bnd.size());
-			sl.bnd_cnt = uint32_t(b[sd].size());
+			sl.bnd_cnt = uint32_t(r.bnd[sd].size());
 			sl.k = 0;
 			sl.diam = 0;
-			sl.pad[0] = ccr_on ? 1u : 0u;
+			sl.pad[0] = ccr[c];
 			sl.pad[1] = o; // the side's object: its ray-casting trees
-			bnd.insert(bnd.end(), b[sd].begin(), b[sd].end());
+			bnd.insert(bnd.end(), r.bnd[sd].begin(), r.bnd[sd].end());
 		}
 	}
 	// candidate directions of each contour (host, in parallel), while the GPU computes the
@@ -5402,7 +5417,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		rr.num_pairs = uint32_t(G.contours[c].size());
 		rr.combo_idx = kInfH;
 		const bool processed = c < nact;
-		const ComboState& cs = processed && !supp[c] ? chosen[c] : ComboState{};
+		static const ComboState kNoResponse{};
+		const ComboState& cs = processed && !supp[c] ? chosen[c] : kNoResponse; // a reference, not a copy
 		if (processed)
 		{
 			const ContourRT& r = R[c];
@@ -5451,8 +5467,14 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		rr.opt_attempted = cs.opt_attempted;
 		rr.opt_accepted = cs.opt_accepted;
 		out->hit_offsets[c + 1] = out->hit_offsets[c] + rr.hit_count;
-		out->hits.insert(out->hits.end(), cs.hits.begin(), cs.hits.end());
 	}
+	// the supports, copied into place over the host threads
+	out->hits.resize(out->hit_offsets[nc]);
+	host_parallel_dynamic(nc, [&](uint32_t c)
+	{
+		if (out->hit_offsets[c + 1] > out->hit_offsets[c])
+			std::copy(chosen[c].hits.begin(), chosen[c].hits.end(), out->hits.begin() + out->hit_offsets[c]);
+	});
 	mark("suppression, outputs");
 	std::vector<unsigned long long> stats;
 	U26_TRY(download(ctx, stats, S->d_stats.ptr, 16));
