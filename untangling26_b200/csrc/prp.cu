@@ -2952,6 +2952,18 @@ namespace u26
 		// direction), D_C = max delta, J = (sum of the source rest areas) D_C^2, all in double
 		// and in the hits' canonical order; and the D_C tie check: when the largest and second
 		// largest FP32 depths lie within the depth's error band, the argmax is re-decided in FP64.
+		// copies of captured supports out of the pass's support store: block q copies
+		// [off[q], off[q] + cnt[q]) to [pos[q], ...)
+		__global__ void __launch_bounds__(256) support_gather_kernel(const u26_prp_hit* __restrict__ store, const uint64_t* __restrict__ off,
+			const uint32_t* __restrict__ cnt, const uint32_t* __restrict__ pos, u26_prp_hit* __restrict__ out)
+		{
+			const uint32_t q = blockIdx.x;
+			const u26_prp_hit* src = store + off[q];
+			u26_prp_hit* dst = out + pos[q];
+			for (uint32_t i = threadIdx.x; i < cnt[q]; i += blockDim.x)
+				dst[i] = src[i];
+		}
+
 		struct Fp64In
 		{
 			uint32_t hit_begin, hit_end;
@@ -3173,6 +3185,10 @@ namespace
 		float depth = 0, volume = 0, area = 0, cost = 0, objective = 0, coverage = 0;
 		uint32_t opt_attempted = 0, opt_accepted = 0; // direction_optimization_{iteration,accepted}_count
 		std::vector<u26_prp_hit> hits;
+		// the support, when captured on the device: [store_off, store_off + hit_count) of the
+		// pass's support store (hits stays empty until the support is fetched)
+		uint64_t store_off = ~0ull;
+		bool in_store() const { return store_off != ~0ull; }
 	};
 
 	inline bool usable(const ComboState& c)
@@ -3254,6 +3270,9 @@ struct u26_scene
 	DevBuf d_queue;									  // work-item counter of the persistent ray casts
 	DevBuf d_fgrow, d_egrow, d_front, d_cur_own, d_cur_opp, d_tab, d_cov;
 	DevBuf d_trange; // per task: first and past-the-end index of its support entries
+	DevBuf d_store;	 // the pass's captured supports (u26_prp_hit), grown with its contents kept
+	uint64_t store_used = 0;
+	DevBuf d_fetch_off, d_fetch_cnt, d_fetch_pos;
 	DevBuf d_vrank, d_erank, d_cand_off, d_ckeys, d_cvals, d_cap_list, d_cap_off, d_capture, d_chunk_off, d_csum, scan_tmp, d_vsolid, d_fvk, d_fvv, d_rflag, d_heads, d_hkeys, d_hvals, d_zero_th;
 	RadixSorter sorter, esorter, csorter, fvsorter;
 	std::vector<uint8_t> vsolid; // per vertex: its object is rigid / tetrahedral
@@ -3472,7 +3491,7 @@ U26_API void u26_scene_destroy(u26_scene* s)
 		&s->d_cur_opp, &s->d_tab, &s->d_cov, &s->d_vrank, &s->d_erank, &s->d_cand_off, &s->d_ckeys, &s->d_cvals,
 		&s->d_cap_list, &s->d_cap_off, &s->d_capture, &s->d_chunk_off, &s->d_csum, &s->scan_tmp, &s->d_vsolid,
 		&s->d_fvk, &s->d_fvv, &s->d_rflag, &s->d_heads, &s->d_hkeys, &s->d_hvals,
-		&s->d_zero_th, &s->d_trange };
+		&s->d_zero_th, &s->d_trange, &s->d_store, &s->d_fetch_off, &s->d_fetch_cnt, &s->d_fetch_pos };
 	for (DevBuf* b : bufs)
 		b->release();
 	s->sorter.release();
@@ -4081,6 +4100,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 	cudaStream_t st = ctx->stream;
 	const auto t_total = std::chrono::steady_clock::now();
 	auto t0 = t_total;
+	S->store_used = 0; // the support store holds this pass's captures only
 	// with U26_PRP_TRACE set: the host-side time line of the pass, printed at its end
 	const bool trace_marks = std::getenv("U26_PRP_TRACE") != nullptr;
 	std::vector<std::pair<const char*, double>> marks;
@@ -4921,6 +4941,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				}
 		}
 		uint32_t level = 0;
+		uint64_t captured = 0; // support hits gathered at this level (trace)
 		for (; !remaining.empty() && level < 65; level++)
 		{
 			auto tl = std::chrono::steady_clock::now();
@@ -4933,6 +4954,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				}
 			std::vector<uint32_t> counts;
 			U26_TRY(build_candidates(sids, counts));
+			if (trace)
+				fprintf(stderr, "[u26 prp]   level candidates %.2f ms (%zu slots)\n", ms_since(tl), sids.size());
 			out->stage_ms[2] += ms_since(tl);
 			std::vector<Task> tasks;
 			for (uint32_t c : remaining)
@@ -4998,6 +5021,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			// winner needs no re-evaluation (materialize covers whatever is not captured)
 			{
 				constexpr uint64_t kCaptureCap = uint64_t(1) << 24;
+				captured = 0;
 				std::vector<int> task_of(size_t(nact) * 26, -1);
 				for (size_t t = 0; t < tasks.size(); t++)
 					if (tasks[t].combo < 26)
@@ -5011,7 +5035,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 						continue;
 					const int t = task_of[size_t(c) * 26 + sel];
 					const ComboState& cs = R[c].res[sel];
-					if (t < 0 || cs.hits.size() == cs.hit_count || total + cs.hit_count > kCaptureCap)
+					if (t < 0 || cs.hits.size() == cs.hit_count || cs.in_store() || total + cs.hit_count > kCaptureCap)
 						continue;
 					list.push_back(uint32_t(t));
 					total += cs.hit_count;
@@ -5019,33 +5043,29 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				}
 				if (!list.empty() && total > 0)
 				{
+					// gathered into the pass's support store on the device; the winners' supports
+					// are fetched once, after the levels (fetch_supports)
 					U26_TRY(upload(ctx, S->d_cap_list, list));
 					U26_TRY(upload(ctx, S->d_cap_off, off));
-					U26_CUDA(ctx, S->d_capture.reserve(sizeof(u26_prp_hit) * total));
+					const size_t need = sizeof(u26_prp_hit) * (S->store_used + total);
+					if (need > S->d_store.bytes)
+					{
+						DevBuf grown;
+						U26_CUDA(ctx, grown.reserve(need + need / 2));
+						if (S->store_used)
+							U26_CUDA(ctx, cudaMemcpyAsync(grown.ptr, S->d_store.ptr, sizeof(u26_prp_hit) * S->store_used, cudaMemcpyDeviceToDevice, st));
+						std::swap(grown.ptr, S->d_store.ptr);
+						std::swap(grown.bytes, S->d_store.bytes);
+						grown.release(); // after the copy: cudaFree waits for the device
+					}
 					capture_kernel<<<uint32_t(list.size()), 256, 0, st>>>(S->d_cap_list.as<uint32_t>(), S->d_cap_off.as<uint32_t>(),
 						S->d_keys.as<uint64_t>(), S->d_root.as<uint32_t>(), S->d_best.as<uint32_t>(), S->d_seg.as<uint32_t>(), S->d_pay.as<float>(),
-						HitKeyCodec{ b }, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_capture.as<u26_prp_hit>());
+						HitKeyCodec{ b }, S->d_edges.as<uint2>(), S->d_faces.as<uint32_t>(), S->d_store.as<u26_prp_hit>() + S->store_used);
 					U26_TRY(after_launch(ctx, "capture_kernel"));
-					// through pinned staging: the captured supports can be tens of MB per level
-					const size_t bytes = sizeof(u26_prp_hit) * total;
-					if (S->cap_host_bytes < bytes)
-					{
-						if (S->cap_host)
-							cudaFreeHost(S->cap_host);
-						S->cap_host = nullptr;
-						S->cap_host_bytes = 0;
-						U26_CUDA(ctx, cudaMallocHost(&S->cap_host, bytes + bytes / 2));
-						g_alloc_count.fetch_add(1, std::memory_order_relaxed);
-						S->cap_host_bytes = bytes + bytes / 2;
-					}
-					U26_CUDA(ctx, cudaMemcpyAsync(S->cap_host, S->d_capture.ptr, bytes, cudaMemcpyDeviceToHost, st));
-					U26_CUDA(ctx, cudaStreamSynchronize(st));
-					const u26_prp_hit* got = static_cast<const u26_prp_hit*>(S->cap_host);
-					host_parallel_dynamic(uint32_t(list.size()), [&](uint32_t q)
-						{
-							ComboState& cs = R[tasks[list[q]].contour_local].res[tasks[list[q]].combo];
-							cs.hits.assign(got + off[q], got + off[q + 1]);
-						});
+					for (size_t q = 0; q < list.size(); q++)
+						R[tasks[list[q]].contour_local].res[tasks[list[q]].combo].store_off = S->store_used + off[q];
+					S->store_used += total;
+					captured = total;
 				}
 			}
 			std::vector<uint32_t> next;
@@ -5093,6 +5113,8 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				next.push_back(c);
 			}
 			remaining.swap(next);
+			if (trace)
+				fprintf(stderr, "[u26 prp]   level control %.2f ms (captured %llu support hits)\n", ms_since(tl), (unsigned long long)captured);
 			out->stage_ms[5] += ms_since(tl);
 		}
 		out->levels = std::max(out->levels, level);
@@ -5150,6 +5172,66 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 		out->stage_ms[6] += ms_since(tl);
 		return U26_OK;
 	};
+	// the supports of the listed results that the levels captured on the device, fetched into
+	// their hit lists with one gather and one copy back; the rest are left to materialize
+	auto fetch_supports = [&](const std::vector<std::pair<uint32_t, uint32_t>>& cc) -> u26_status
+	{
+		std::vector<uint64_t> offs;
+		std::vector<uint32_t> cnts, poss;
+		std::vector<ComboState*> dst;
+		uint64_t total = 0;
+		for (const auto& [c, d] : cc)
+		{
+			ComboState& cs = R[c].res[d];
+			if (!cs.in_store() || cs.hit_count == 0 || cs.hits.size() == cs.hit_count)
+				continue;
+			offs.push_back(cs.store_off);
+			cnts.push_back(cs.hit_count);
+			poss.push_back(uint32_t(total));
+			total += cs.hit_count;
+			dst.push_back(&cs);
+		}
+		if (dst.empty())
+			return U26_OK;
+		if (total > 0xFFFFFFFFull)
+			return set_error(ctx, U26_ERR_CAPACITY, "PRP support fetch of %llu hits", (unsigned long long)total);
+		U26_TRY(upload(ctx, S->d_fetch_off, offs));
+		U26_TRY(upload(ctx, S->d_fetch_cnt, cnts));
+		U26_TRY(upload(ctx, S->d_fetch_pos, poss));
+		const size_t bytes = sizeof(u26_prp_hit) * total;
+		U26_CUDA(ctx, S->d_capture.reserve(bytes));
+		support_gather_kernel<<<uint32_t(dst.size()), 256, 0, st>>>(S->d_store.as<u26_prp_hit>(), S->d_fetch_off.as<uint64_t>(),
+			S->d_fetch_cnt.as<uint32_t>(), S->d_fetch_pos.as<uint32_t>(), S->d_capture.as<u26_prp_hit>());
+		U26_TRY(after_launch(ctx, "support_gather_kernel"));
+		if (S->cap_host_bytes < bytes)
+		{
+			if (S->cap_host)
+				cudaFreeHost(S->cap_host);
+			S->cap_host = nullptr;
+			S->cap_host_bytes = 0;
+			U26_CUDA(ctx, cudaMallocHost(&S->cap_host, bytes + bytes / 2));
+			g_alloc_count.fetch_add(1, std::memory_order_relaxed);
+			S->cap_host_bytes = bytes + bytes / 2;
+		}
+		U26_CUDA(ctx, cudaMemcpyAsync(S->cap_host, S->d_capture.ptr, bytes, cudaMemcpyDeviceToHost, st));
+		U26_CUDA(ctx, cudaStreamSynchronize(st));
+		const u26_prp_hit* got = static_cast<const u26_prp_hit*>(S->cap_host);
+		host_parallel_dynamic(uint32_t(dst.size()), [&](uint32_t q)
+			{ dst[q]->hits.assign(got + poss[q], got + poss[q] + cnts[q]); });
+		return U26_OK;
+	};
+	auto fetch_then_materialize = [&](const std::vector<std::pair<uint32_t, uint32_t>>& cc) -> u26_status
+	{
+		U26_TRY(fetch_supports(cc));
+		std::vector<std::pair<uint32_t, uint32_t>> rest;
+		for (const auto& e : cc)
+		{
+			const ComboState& cs = R[e.first].res[e.second];
+			if (cs.hits.size() != cs.hit_count)
+				rest.push_back(e);
+		}
+		return materialize(rest);
+	};
 	std::vector<int> chosen_idx(nc, -1);
 	{
 		std::vector<std::pair<uint32_t, uint32_t>> cc;
@@ -5159,7 +5241,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			if (chosen_idx[c] >= 0 && R[c].res[chosen_idx[c]].hits.size() != R[c].res[chosen_idx[c]].hit_count)
 				cc.emplace_back(c, uint32_t(chosen_idx[c]));
 		}
-		U26_TRY(materialize(cc));
+		U26_TRY(fetch_then_materialize(cc));
 	}
 
 	mark("materialize");
@@ -5278,7 +5360,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 				acc[c] = ComboState{};
 			}
 			// the accepted trials' supports feed the next step and the output
-			U26_TRY(materialize(taken));
+			U26_TRY(fetch_then_materialize(taken));
 		}
 		std::vector<std::pair<uint32_t, uint32_t>> cc;
 		for (uint32_t c = 0; c < nact; c++)
@@ -5287,7 +5369,7 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			if (chosen_idx[c] >= 0 && R[c].res[chosen_idx[c]].hits.size() != R[c].res[chosen_idx[c]].hit_count)
 				cc.emplace_back(c, uint32_t(chosen_idx[c]));
 		}
-		U26_TRY(materialize(cc));
+		U26_TRY(fetch_then_materialize(cc));
 	}
 
 	mark("refinement");
