@@ -572,9 +572,28 @@ namespace u26
 		// Candidate vertices / edges of each slot ordered by the Morton code of their rest
 		// position (edge midpoint), so that the 32 requests of a warp packet start from a
 		// compact patch. Only the request order changes: hits are keyed by primitive ids.
+		// Dense request-order ranks, made once per scene: the position of each vertex (edge) in
+		// the order of (Morton code, id). Candidates keyed by (slot, rank) sort into the
+		// (slot, code, id) order over the slot and id bits alone.
+		__global__ void rank_keys_kernel(const uint32_t* __restrict__ code, uint32_t n, int id_bits, uint64_t* __restrict__ keys,
+			uint32_t* __restrict__ vals)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			keys[i] = (uint64_t(code[i]) << id_bits) | i;
+			vals[i] = i;
+		}
+		__global__ void rank_scatter_kernel(const uint32_t* __restrict__ sorted_ids, uint32_t n, uint32_t* __restrict__ rank)
+		{
+			const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+			if (i >= n)
+				return;
+			rank[sorted_ids[i]] = i;
+		}
 		__global__ void cand_keys_kernel(const uint32_t* __restrict__ slot_ids, const uint32_t* __restrict__ off, uint32_t nsid,
-			const uint32_t* __restrict__ cand, uint32_t stride, const uint32_t* __restrict__ rank, int code_bits, int id_bits,
-			uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
+			const uint32_t* __restrict__ cand, uint32_t stride, const uint32_t* __restrict__ rank, int id_bits, uint64_t* __restrict__ keys,
+			uint32_t* __restrict__ vals)
 		{
 			const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
 			if (g >= off[nsid])
@@ -589,9 +608,9 @@ namespace u26
 					hi = mid;
 			}
 			const uint32_t id = cand[size_t(slot_ids[lo]) * stride + (g - off[lo])];
-			// (slot, Morton code, id): unique keys, so the request order (and the packets) do not
-			// depend on the order the candidates were found in
-			keys[g] = (uint64_t(lo) << (code_bits + id_bits)) | (uint64_t(rank[id] >> (30 - code_bits)) << id_bits) | id;
+			// (slot, dense rank of (Morton code, id)): unique keys, so the request order (and the
+			// packets) do not depend on the order the candidates were found in
+			keys[g] = (uint64_t(lo) << id_bits) | rank[id];
 			vals[g] = id;
 		}
 		__global__ void cand_scatter_kernel(const uint32_t* __restrict__ slot_ids, const uint32_t* __restrict__ off, uint32_t nsid,
@@ -3466,6 +3485,28 @@ U26_API u26_status u26_scene_create(u26_ctx* ctx, const u26_mesh_desc* m, u26_sc
 		}
 		U26_TRY(upload(ctx, s->d_vrank, vr));
 		U26_TRY(upload(ctx, s->d_erank, er));
+		// the codes become dense ranks of (code, id), in place
+		auto dense = [&](DevBuf& rank, uint32_t n) -> u26_status
+		{
+			if (n < 2)
+			{
+				U26_CUDA(ctx, cudaMemsetAsync(rank.ptr, 0, sizeof(uint32_t), ctx->stream));
+				return U26_OK;
+			}
+			int id_bits = 1;
+			while (id_bits < 32 && (uint64_t(1) << id_bits) < n)
+				id_bits++;
+			U26_CUDA(ctx, s->d_ckeys.reserve(sizeof(uint64_t) * n));
+			U26_CUDA(ctx, s->d_cvals.reserve(sizeof(uint32_t) * n));
+			rank_keys_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(rank.as<uint32_t>(), n, id_bits, s->d_ckeys.as<uint64_t>(),
+				s->d_cvals.as<uint32_t>());
+			U26_TRY(after_launch(ctx, "rank_keys_kernel"));
+			U26_TRY(s->csorter.sort(ctx, s->d_ckeys.as<uint64_t>(), s->d_cvals.as<uint32_t>(), n, 0, 30 + id_bits));
+			rank_scatter_kernel<<<div_up(n, 256), 256, 0, ctx->stream>>>(s->d_cvals.as<uint32_t>(), n, rank.as<uint32_t>());
+			return after_launch(ctx, "rank_scatter_kernel");
+		};
+		U26_TRY(dense(s->d_vrank, s->nv));
+		U26_TRY(dense(s->d_erank, s->ne));
 	}
 	U26_CUDA(ctx, s->d_fn.reserve(sizeof(float) * 3 * std::max(1u, s->nf)));
 	U26_CUDA(ctx, s->d_en.reserve(sizeof(float) * 3 * std::max(1u, s->ne)));
@@ -4540,13 +4581,10 @@ static u26_status prp_run(u26_scene* S, u26_lbvh* face_tree, u26_lbvh* edge_tree
 			uint32_t* cand = kind == 0 ? S->d_cand_v.as<uint32_t>() : S->d_cand_e.as<uint32_t>();
 			const uint32_t stride = kind == 0 ? vs : es_;
 			const int id_bits = bits_for(kind == 0 ? S->nv : S->ne);
-			const int code_bits = std::max(0, std::min(30, 64 - sid_bits - id_bits));
 			cand_keys_kernel<<<div_up(total, 256), 256, 0, st>>>(S->d_slot_ids.as<uint32_t>(), S->d_cand_off.as<uint32_t>(), nsid, cand, stride,
-				kind == 0 ? S->d_vrank.as<uint32_t>() : S->d_erank.as<uint32_t>(), code_bits, id_bits, S->d_ckeys.as<uint64_t>(),
-				S->d_cvals.as<uint32_t>());
+				kind == 0 ? S->d_vrank.as<uint32_t>() : S->d_erank.as<uint32_t>(), id_bits, S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>());
 			U26_TRY(after_launch(ctx, "cand_keys_kernel"));
-			U26_TRY(S->csorter.sort(ctx, S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>(), total, 0,
-				std::min(64, sid_bits + code_bits + id_bits)));
+			U26_TRY(S->csorter.sort(ctx, S->d_ckeys.as<uint64_t>(), S->d_cvals.as<uint32_t>(), total, 0, sid_bits + id_bits));
 			cand_scatter_kernel<<<div_up(total, 256), 256, 0, st>>>(S->d_slot_ids.as<uint32_t>(), S->d_cand_off.as<uint32_t>(), nsid,
 				S->d_cvals.as<uint32_t>(), cand, stride);
 			U26_TRY(after_launch(ctx, "cand_scatter_kernel"));
