@@ -588,6 +588,52 @@ def classify_contour(is_loop, is_boundary, adj_degree, mesh_index):
     return f(len(il), il.ctypes.data_as(ctypes.c_void_p), ib.ctypes.data_as(ctypes.c_void_p), _p(dg, _u32p), _p(mi, _u32p))
 
 
+def _csr_call(name, row_ptr, col, flip):
+    rp = np.ascontiguousarray(row_ptr, np.uint32)
+    cl = np.ascontiguousarray(col, np.uint32)
+    fl = np.ascontiguousarray(flip, np.uint32)
+    n = len(rp) - 1
+    root = np.zeros(max(n, 1), np.uint32)
+    parity = np.zeros(max(n, 1), np.uint32)
+    f = _sig(name, _U, [_U, _u32p, _u32p, _u32p, _u32p, _u32p])
+    bad = f(n, _p(rp, _u32p), _p(cl, _u32p), _p(fl, _u32p), _p(root, _u32p), _p(parity, _u32p))
+    return root[:n], parity[:n], bool(bad)
+
+
+def flood_components(row_ptr, col, flip):
+    """The contour flood fill with mesh parity (flood_components in oracle_prp.cpp, the one the
+    PRP restatement runs) over a CSR graph: (root = smallest node of each node's component,
+    parity, inconsistent)."""
+    return _csr_call("oracle_flood_components", row_ptr, col, flip)
+
+
+def contour_test_bfs(row_ptr, col, flip):
+    """cpu_reference of test_parallel_contour_construction.cpp: breadth-first flood, same outputs."""
+    return _csr_call("oracle_cc_bfs", row_ptr, col, flip)
+
+
+CONTOUR_TEST_GRAPHS = ("small_fixed", "10K_chains_x10", "1K_chains_x100", "grid_100x100", "grid_200x250",
+                       "random_50K_d4_c100", "random_100K_d6_c500", "singletons+pairs_100K")
+
+
+def contour_test_graph(which):
+    """Case `which` of test_parallel_contour_construction.cpp's main, as CSR (row_ptr, col, flip)."""
+    mk = _sig("oracle_cc_graph_make", ctypes.c_void_p, [_I])
+    h = mk(which)
+    if not h:
+        raise ValueError(f"no contour test graph {which}")
+    try:
+        n, m = _U(), _U()
+        _sig("oracle_cc_graph_size", None, [ctypes.c_void_p, ctypes.POINTER(_U), ctypes.POINTER(_U)])(h, ctypes.byref(n), ctypes.byref(m))
+        rp = np.zeros(n.value + 1, np.uint32)
+        cl = np.zeros(max(m.value, 1), np.uint32)
+        fl = np.zeros(max(m.value, 1), np.uint32)
+        _sig("oracle_cc_graph_copy", None, [ctypes.c_void_p, _u32p, _u32p, _u32p])(h, _p(rp, _u32p), _p(cl, _u32p), _p(fl, _u32p))
+        return rp, cl[:m.value], fl[:m.value]
+    finally:
+        _sig("oracle_cc_graph_free", None, [ctypes.c_void_p])(h)
+
+
 def suppress(adjacency, pre_area, active):
     """prp_select_pre_finalize_contours_to_suppress: sorted suppressed contour ids."""
     nc = len(adjacency)

@@ -1106,20 +1106,18 @@ namespace
 		return t;
 	}
 
-	void contours(Scene& S)
+	// Connected components of an undirected graph with a 0/1 flip weight per adjacency entry,
+	// and a parity per node (the contour flood fill and mesh parity of
+	// intersection_contour_construction_from_ext_adjacent): seeds in increasing node order, each
+	// component filled depth first from its seed (parity 0); a node's parity is the sum of the
+	// weights along its discovery path, mod 2. Components list their nodes in discovery order.
+	// Returns whether some edge joins two nodes of a component whose parities differ by other
+	// than its weight (an odd cycle of flips: that component's parities depend on the walk).
+	bool flood_components(uint n, const std::vector<std::vector<uint>>& adj, const std::vector<std::vector<uint>>& w,
+		std::vector<uint>& parity, std::vector<std::vector<uint>>& comps)
 	{
-		const uint n = uint(S.ef.size());
-		std::vector<std::vector<uint>> w(n);
-		for (uint p = 0; p < n; p++)
-		{
-			for (uint q : S.adj[p])
-			{
-				const bool same = S.ef[p].idx[2] == S.ef[q].idx[2] && S.ef[p].idx[3] == S.ef[q].idx[3] && S.ef[p].idx[4] == S.ef[q].idx[4];
-				w[p].push_back(same ? 0u : 1u);
-			}
-		}
 		std::vector<uint8_t> visited(n, 0);
-		S.mesh_index.assign(n, kInf);
+		parity.assign(n, kInf);
 		for (uint seed = 0; seed < n; seed++)
 		{
 			if (visited[seed])
@@ -1130,9 +1128,9 @@ namespace
 			{
 				const auto [pi, ps] = todo.back();
 				todo.pop_back();
-				for (size_t j = 0; j < S.adj[pi].size(); j++)
+				for (size_t j = 0; j < adj[pi].size(); j++)
 				{
-					const uint q = S.adj[pi][j];
+					const uint q = adj[pi][j];
 					if (!visited[q])
 					{
 						visited[q] = 1;
@@ -1145,10 +1143,34 @@ namespace
 			for (auto& [pi, ps] : group)
 			{
 				c.push_back(pi);
-				S.mesh_index[pi] = ps % 2;
+				parity[pi] = ps % 2;
 			}
-			S.contours.push_back(c);
+			comps.push_back(c);
 		}
+		bool inconsistent = false;
+		for (uint p = 0; p < n && !inconsistent; p++)
+			for (size_t j = 0; j < adj[p].size(); j++)
+				if ((parity[p] ^ parity[adj[p][j]]) != (w[p][j] & 1u))
+				{
+					inconsistent = true;
+					break;
+				}
+		return inconsistent;
+	}
+
+	void contours(Scene& S)
+	{
+		const uint n = uint(S.ef.size());
+		std::vector<std::vector<uint>> w(n);
+		for (uint p = 0; p < n; p++)
+		{
+			for (uint q : S.adj[p])
+			{
+				const bool same = S.ef[p].idx[2] == S.ef[q].idx[2] && S.ef[p].idx[3] == S.ef[q].idx[3] && S.ef[p].idx[4] == S.ef[q].idx[4];
+				w[p].push_back(same ? 0u : 1u);
+			}
+		}
+		flood_components(n, S.adj, w, S.mesh_index, S.contours);
 		S.contour_index.assign(n, kInf);
 		for (uint c = 0; c < S.contours.size(); c++)
 			for (uint p : S.contours[c])
@@ -3237,6 +3259,27 @@ extern "C"
 	}
 	float oracle_response_objective(float objective, float coverage) { return objective_div_cov2(objective, coverage); }
 
+	// flood_components over a CSR graph (row_ptr[n + 1], col[m], flip[m]): root[i] = the seed
+	// (smallest node) of i's component, parity[i]; returns 1 when some component is inconsistent
+	uint oracle_flood_components(uint n, const uint* row_ptr, const uint* col, const uint* flip, uint* root, uint* parity)
+	{
+		std::vector<std::vector<uint>> adj(n), w(n);
+		for (uint u = 0; u < n; u++)
+			for (uint e = row_ptr[u]; e < row_ptr[u + 1]; e++)
+			{
+				adj[u].push_back(col[e]);
+				w[u].push_back(flip[e] & 1u);
+			}
+		std::vector<uint> par;
+		std::vector<std::vector<uint>> comps;
+		const bool bad = flood_components(n, adj, w, par, comps);
+		for (const auto& c : comps)
+			for (uint p : c)
+				root[p] = c.front();
+		for (uint i = 0; i < n; i++)
+			parity[i] = par[i];
+		return bad ? 1u : 0u;
+	}
 	uint oracle_classify_contour(uint n, const uint8_t* is_loop, const uint8_t* is_bnd, const uint* deg, const uint* mesh_index)
 	{
 		return classify_contour(n, is_loop, is_bnd, deg, mesh_index);
